@@ -1,0 +1,160 @@
+"""ctypes binding of ``libfirestep.so`` (the C ABI in ``include/firestep.h``).
+
+The library is built in-tree by ``firewebapp_b200/csrc/Makefile``.  There is
+no fallback: if the shared object is missing or a symbol is absent, importing
+anything that needs it raises ``RuntimeError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("FIRESTEP_LIB", _HERE / "libfirestep.so"))
+
+P = C.c_void_p
+D = C.c_double
+I = C.c_int
+I64 = C.c_int64
+PP = C.POINTER(C.c_void_p)
+
+
+class FsGrid(C.Structure):
+    _fields_ = [("nx", I), ("ny", I), ("nz", I), ("dx", D), ("dy", D),
+                ("dz", P), ("d_above", P), ("d_below", P)]
+
+
+class FsBedParticles(C.Structure):
+    _fields_ = [(n, P) for n in ("x", "y", "z", "alive", "m_solid", "m_water", "m_char",
+                                 "T_s", "m_water_0", "sav", "m_char_max")]
+
+
+class FsBedSegments(C.Structure):
+    _fields_ = [("nseg", I), ("seg_start", P), ("seg_cell", P), ("perm", P)]
+
+
+class FsBedSources(C.Structure):
+    _fields_ = [(n, P) for n in ("S_pyro", "S_drying", "Q_pyro", "Q_drying", "Y_F_source",
+                                 "Q_char", "Q_smold", "Q_g_conv")]
+
+
+class FsBedParams(C.Structure):
+    _fields_ = [("dt", D), ("h_conv", D), ("rho_true", D), ("cp_solid", D), ("eps_solid", D),
+                ("T_amb", D), ("view", D), ("h_bed", D), ("kappa_bed", D), ("char_cap", D),
+                ("ash_exp", D), ("do_dry", I), ("do_pyro", I), ("do_char", I),
+                ("do_smold", I), ("mode", I), ("geometric", I), ("n_split", I),
+                ("Qsx", P), ("q_rad", P), ("drip_on", I), ("n_z_bed", I), ("i_src0", I),
+                ("i_src1", I)]
+
+
+_G = C.POINTER(FsGrid)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "fs_last_error": (C.c_char_p, []),
+    "fs_version": (I, []),
+    "fs_species_transport": (I, [_G, I, PP, PP, PP, C.POINTER(D), P, P, P, P, D, D, P]),
+    "fs_species_sources": (I, [I64, P, P, P, P, P, P, P, P, P]),
+    "fs_advect_scalar_muscl": (I, [_G, P, P, P, P, P, D, P]),
+    "fs_gas_energy_adv": (I, [_G, P, P, P, P, P, D, D, D, P]),
+    "fs_turb_diffusion_nsub": (I, [_G, P, D, D, C.POINTER(I), C.POINTER(D), P]),
+    "fs_turb_diffusion_substep": (I, [_G, I, PP, PP, P, D, D, I, C.POINTER(D),
+                                      C.POINTER(D), P]),
+    "fs_drag_force": (I, [I64, P, P, P, P, P, D, D, P, P, P, P]),
+    "fs_tentative_velocity": (I, [_G, P, P, P, P, P, P, P, P, P, D, D, P, P, P, P, P, P,
+                                  D, D, P]),
+    "fs_outflow_sponge": (I, [_G, P, P, P, P, D, D, P]),
+    "fs_k_epsilon": (I, [_G, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, D, D, D, D, D, P]),
+    "fs_edc_scratch_bytes": (I64, [I64]),
+    "fs_edc": (I, [I64, P, P, P, P, P, P, P, P, D, D, D, I, D, D, I, P, P]),
+    "fs_gas_energy_update": (I, [_G, P, P, P, P, P, P, P, P, P, D, D, D, I, I, I, I, P]),
+    "fs_eos": (I, [_G, P, P, P, P, D, P]),
+    "fs_clip": (I, [I64, P, D, D, P]),
+    "fs_solid_conduction": (I, [_G, P, P, P, D, D, D, D, P]),
+    "fs_soil_step": (I, [I, I, I, P, P, D, P, P, P, D, D, D, D, D, P]),
+    "fs_proj_create": (I, [_G, PP]),
+    "fs_proj_destroy": (None, [P]),
+    "fs_proj_rebuild": (I, [P, P, P]),
+    "fs_proj_project": (I, [P, P, P, P, P, P, D, D, I, C.POINTER(I), P]),
+    "fs_proj_pressure": (P, [P]),
+    "fs_proj_apply": (I, [P, P, P, P]),
+    "fs_divergence_max": (I, [_G, P, P, P, P, P, P, C.POINTER(D), P]),
+    "fs_dom_create": (I, [_G, I, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(D), D,
+                          PP]),
+    "fs_dom_destroy": (None, [P]),
+    "fs_dom_solve": (I, [P, P, P, P, P, D, D, P, P, P, P, P, P, P, P]),
+    "fs_dom_intensity": (P, [P]),
+    "fs_dom_iterations": (I, [P]),
+    "fs_bed_step": (I, [_G, C.POINTER(FsBedParticles), C.POINTER(FsBedSegments),
+                        C.POINTER(FsBedSources), C.POINTER(FsBedParams), P, P, P]),
+    "fs_bed_aggregate": (I, [C.POINTER(FsBedParticles), C.POINTER(FsBedSegments), P, I, P]),
+    "fs_bed_hcond": (I, [_G, P, P, P, I, D, D, D, D, C.POINTER(FsBedParticles),
+                         C.POINTER(FsBedSegments), P, P]),
+    "fs_levelset": (I, [_G, P, P, P, D, I, P]),
+    "fs_active_count": (I, [I64, P, P, P, P, P, P]),
+    "fs_field_max": (I, [_G, P, I, C.POINTER(D), P]),
+}
+
+STATUS = {0: "ok", 1: "bad argument", 2: "non-finite value", 3: "solver did not converge",
+          4: "device wait timed out", 5: "CUDA error"}
+
+
+class FireStepError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"firestep status {status} ({STATUS.get(status, '?')}): {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Load the shared library (once) and bind every declared entry point."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"libfirestep.so not found at {LIB_PATH}; build it with "
+            f"`make -C firewebapp_b200/csrc` (no CPU fallback exists)")
+    L = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)  # AttributeError -> missing symbol: fail loudly
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status: int, where: str = ""):
+    if status != 0:
+        msg = lib().fs_last_error().decode(errors="replace")
+        raise FireStepError(status, f"{where}: {msg}" if where else msg)
+
+
+def ptr(t) -> int:
+    """Device pointer of a torch tensor (None -> NULL)."""
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def ptr_array(ts):
+    arr = (C.c_void_p * len(ts))()
+    for k, t in enumerate(ts):
+        arr[k] = ptr(t)
+    return arr
+
+
+def dbl_array(xs):
+    arr = (C.c_double * len(xs))()
+    for k, x in enumerate(xs):
+        arr[k] = float(x)
+    return arr
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

@@ -1,0 +1,376 @@
+// extern "C" entry points of libfirestep.so (declared in include/firestep.h).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include "common.cuh"
+#include "kernels.h"
+
+static thread_local char g_err[512] = "";
+
+void fs_set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+static int check(int st, const char* where) {
+  if (st == FS_OK) return st;
+  cudaError_t e = cudaGetLastError();
+  if (st == FS_ECUDA)
+    fs_set_error("%s: CUDA error: %s", where, cudaGetErrorString(e));
+  else if (st == FS_EARG)
+    fs_set_error("%s: bad argument", where);
+  else if (st == FS_ENONFINITE)
+    fs_set_error("%s: non-finite value", where);
+  else if (st == FS_ENOCONV)
+    fs_set_error("%s: solver did not converge", where);
+  else
+    fs_set_error("%s: status %d", where, st);
+  return st;
+}
+
+static bool to_grid(const FsGrid* g, GridDev& d, const char* where) {
+  if (!g || g->nx < 1 || g->ny < 1 || g->nz < 1 || !g->dz || !g->d_above || !g->d_below ||
+      !(g->dx > 0.0) || !(g->dy > 0.0)) {
+    fs_set_error("%s: invalid grid", where);
+    return false;
+  }
+  d.nx = g->nx; d.ny = g->ny; d.nz = g->nz; d.dx = g->dx; d.dy = g->dy;
+  d.dz = g->dz; d.da = g->d_above; d.db = g->d_below;
+  return true;
+}
+
+#define ST(s) ((cudaStream_t)(s))
+#define GRID(name)                           \
+  GridDev gd;                                \
+  if (!to_grid(g, gd, name)) return FS_EARG;
+
+extern "C" {
+
+const char* fs_last_error(void) { return g_err; }
+int fs_version(void) { return 1; }
+
+int fs_species_transport(const FsGrid* g, int nspec, const double* const* Y, double* const* Y_out,
+                         const double* const* S, const double* Y_inlet, const double* rho,
+                         const double* u, const double* v, const double* w, double dt, double D,
+                         void* stream) {
+  GRID("fs_species_transport");
+  if (!Y || !Y_out || !S || !Y_inlet || nspec < 1 || nspec > 3) {
+    fs_set_error("fs_species_transport: bad species arguments");
+    return FS_EARG;
+  }
+  return check(launch_species(gd, nspec, Y, Y_out, S, Y_inlet, rho, u, v, w, dt, D, ST(stream)),
+               "fs_species_transport");
+}
+
+int fs_species_sources(int64_t n, const double* S_pyro, const double* S_drying, const double* Y_F,
+                       const double* Y_O2, const double* Y_H2O, double* S_F, double* S_O2,
+                       double* S_H2O, void* stream) {
+  if (n < 0) return FS_EARG;
+  return check(launch_species_sources(n, S_pyro, S_drying, Y_F, Y_O2, Y_H2O, S_F, S_O2, S_H2O,
+                                      ST(stream)),
+               "fs_species_sources");
+}
+
+int fs_advect_scalar_muscl(const FsGrid* g, const double* phi, const double* u, const double* v,
+                           const double* w, double* rhs, double phi_inlet, void* stream) {
+  GRID("fs_advect_scalar_muscl");
+  return check(launch_advect_scalar(gd, phi, u, v, w, rhs, phi_inlet, ST(stream)),
+               "fs_advect_scalar_muscl");
+}
+
+int fs_gas_energy_adv(const FsGrid* g, const double* T_g, const double* u, const double* v,
+                      const double* w, double* T_out, double dt, double alpha_th, double T_amb,
+                      void* stream) {
+  GRID("fs_gas_energy_adv");
+  return check(launch_gas_energy_adv(gd, T_g, u, v, w, T_out, dt, alpha_th, T_amb, ST(stream)),
+               "fs_gas_energy_adv");
+}
+
+int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, void* stream) {
+  GRID("fs_field_max");
+  unsigned long long* key = nullptr;
+  double* dres = nullptr;
+  if (cudaMallocAsync(&key, sizeof(unsigned long long), ST(stream)) != cudaSuccess ||
+      cudaMallocAsync(&dres, sizeof(double), ST(stream)) != cudaSuccess) {
+    fs_set_error("fs_field_max: allocation failed");
+    return FS_ECUDA;
+  }
+  launch_init_keys(key, 1, mode == 2 ? 1 : 0, ST(stream));
+  launch_max(gd, f, mode, key, ST(stream));
+  launch_keys_to_double(key, dres, 1, ST(stream));
+  cudaMemcpyAsync(result, dres, sizeof(double), cudaMemcpyDeviceToHost, ST(stream));
+  cudaFreeAsync(key, ST(stream));
+  cudaFreeAsync(dres, ST(stream));
+  if (cudaStreamSynchronize(ST(stream)) != cudaSuccess) return check(FS_ECUDA, "fs_field_max");
+  return FS_OK;
+}
+
+int fs_turb_diffusion_nsub(const FsGrid* g, const double* nu_t, double sc_t, double dt,
+                           int* n_sub, double* dt_sub, void* stream) {
+  GRID("fs_turb_diffusion_nsub");
+  // turbulence_3d.py:880-915
+  double dz_min = 0.0;
+  {
+    double* h = new double[gd.nz];
+    cudaMemcpy(h, gd.dz, sizeof(double) * gd.nz, cudaMemcpyDeviceToHost);
+    dz_min = h[0];
+    for (int k = 1; k < gd.nz; ++k)
+      if (h[k] < dz_min) dz_min = h[k];
+    delete[] h;
+  }
+  double dx2 = gd.dx * gd.dx, dy2 = gd.dy * gd.dy, dz2 = dz_min * dz_min;
+  double h_min2 = dx2 < (dy2 < dz2 ? dy2 : dz2) ? dx2 : (dy2 < dz2 ? dy2 : dz2);
+  double nu_max = 0.0;
+  int st = fs_field_max(g, nu_t, 2, &nu_max, stream);
+  if (st) return st;
+  *n_sub = 0;
+  *dt_sub = 0.0;
+  double D_max = nu_max / sc_t;
+  if (D_max <= 1.0e-12) return FS_OK;
+  if (!(D_max - D_max == 0.0)) return FS_OK;  // non-finite: skipped
+  double dt_sub_max = 0.4 * h_min2 / D_max;
+  if (dt_sub_max <= 0.0) return FS_OK;
+  double target = dt / dt_sub_max;
+  if (target > 1000.0) return FS_OK;
+  int n = (int)ceil(target);
+  if (n < 1) n = 1;
+  *n_sub = n;
+  *dt_sub = dt / n;
+  return FS_OK;
+}
+
+int fs_turb_diffusion_substep(const FsGrid* g, int nfield, const double* const* f,
+                              double* const* f_out, const double* nu_t, double sc_t, double dt_sub,
+                              int clip, const double* lo, const double* hi, void* stream) {
+  GRID("fs_turb_diffusion_substep");
+  return check(launch_turb_diff(gd, nfield, f, f_out, nu_t, sc_t, dt_sub, clip, lo, hi,
+                                ST(stream)),
+               "fs_turb_diffusion_substep");
+}
+
+int fs_drag_force(int64_t n, const double* u, const double* v, const double* w, const double* rho,
+                  const double* alpha_s, double sigma_sav, double C_D, double* Fx, double* Fy,
+                  double* Fz, void* stream) {
+  return check(launch_drag(n, u, v, w, rho, alpha_s, sigma_sav, C_D, Fx, Fy, Fz, ST(stream)),
+               "fs_drag_force");
+}
+
+int fs_tentative_velocity(const FsGrid* g, const double* u, const double* v, const double* w,
+                          const double* rho, const double* T_g, const double* Fx, const double* Fy,
+                          const double* Fz, const double* alpha_s, double sigma_sav, double C_D,
+                          const double* u_inlet, const double* v_inlet, const double* w_inlet,
+                          double* u_out, double* v_out, double* w_out, double dt, double T_amb,
+                          void* stream) {
+  GRID("fs_tentative_velocity");
+  return check(launch_momentum(gd, u, v, w, rho, T_g, Fx, Fy, Fz, alpha_s, sigma_sav, C_D, u_inlet,
+                               v_inlet, w_inlet, u_out, v_out, w_out, dt, T_amb, ST(stream)),
+               "fs_tentative_velocity");
+}
+
+int fs_outflow_sponge(const FsGrid* g, double* u, const double* u_target, const double* sigma_x,
+                      const double* Y_F, double Y_F_skip, double dt, void* stream) {
+  GRID("fs_outflow_sponge");
+  return check(launch_sponge(gd, u, u_target, sigma_x, Y_F, Y_F_skip, dt, ST(stream)),
+               "fs_outflow_sponge");
+}
+
+int fs_k_epsilon(const FsGrid* g, const double* k, const double* eps, const double* u,
+                 const double* v, const double* w, const double* T_g, const double* alpha_s,
+                 const double* u_inlet, const double* k_wall, const double* eps_wall, double* k_out,
+                 double* eps_out, double* nu_t_out, double* S2_out, double* O2_out,
+                 double sigma_sav, double dt, double T_amb, double beta_p, double beta_d,
+                 void* stream) {
+  GRID("fs_k_epsilon");
+  return check(launch_keps(gd, k, eps, u, v, w, T_g, alpha_s, u_inlet, k_wall, eps_wall, k_out,
+                           eps_out, nu_t_out, S2_out, O2_out, sigma_sav, dt, T_amb, beta_p, beta_d,
+                           ST(stream)),
+               "fs_k_epsilon");
+}
+
+int64_t fs_edc_scratch_bytes(int64_t n) { return (int64_t)edc_scratch_bytes(n); }
+
+int fs_edc(int64_t n, const double* rho, double* T_g, double* Y_F, double* Y_O2, const double* k,
+           const double* eps, const double* Y_H2O, double* omega, double chi_rad, double cp_g,
+           double dt, int n_substeps, double s_stoich, double hoc_J, int extinction, void* scratch,
+           void* stream) {
+  if (n < 0 || !scratch) {
+    fs_set_error("fs_edc: bad argument");
+    return FS_EARG;
+  }
+  return check(launch_edc(n, rho, T_g, Y_F, Y_O2, k, eps, Y_H2O, omega, chi_rad, cp_g, dt,
+                          n_substeps, s_stoich, hoc_J, extinction, scratch, ST(stream)),
+               "fs_edc");
+}
+
+int fs_gas_energy_update(const FsGrid* g, double* T_g, const double* rho, const double* Y_H2O,
+                         const double* T_s, const double* S_pyro, const double* S_drying,
+                         const double* Q_g_conv, const double* q_rad_gas, double* Q_comb_out,
+                         double dt_sub, double T_amb, double h_bed, int drip_on, int n_z_bed,
+                         int i_src0, int i_src1, void* stream) {
+  GRID("fs_gas_energy_update");
+  return check(launch_gas_update(gd, T_g, rho, Y_H2O, T_s, S_pyro, S_drying, Q_g_conv, q_rad_gas,
+                                 Q_comb_out, nullptr, dt_sub, T_amb, h_bed, drip_on, n_z_bed,
+                                 i_src0, i_src1, ST(stream)),
+               "fs_gas_energy_update");
+}
+
+int fs_eos(const FsGrid* g, double* rho, double* rho_prev, const double* T_g, double* Y_O2,
+           double T_amb, void* stream) {
+  GRID("fs_eos");
+  const double R_air = 8.314 / 0.029;
+  return check(launch_eos(gd, rho, rho_prev, T_g, Y_O2, 101325.0, R_air, T_amb, ST(stream)),
+               "fs_eos");
+}
+
+int fs_clip(int64_t n, double* f, double lo, double hi, void* stream) {
+  return check(launch_clip(n, f, lo, hi, ST(stream)), "fs_clip");
+}
+
+int fs_solid_conduction(const FsGrid* g, const double* T_s, const double* alpha_s, double* T_out,
+                        double k_solid, double rho_solid, double cp_solid, double dt,
+                        void* stream) {
+  GRID("fs_solid_conduction");
+  return check(launch_solid_cond(gd, T_s, alpha_s, T_out, k_solid, rho_solid, cp_solid, dt, gd.nz,
+                                 ST(stream)),
+               "fs_solid_conduction");
+}
+
+int fs_soil_step(int nsoil, int ny, int nx, double* T_soil, const double* q_in, double dt,
+                 const double* soil_dz, const double* d_above, const double* d_below, double k_s,
+                 double rho_s, double cp_s, double eps_s, double T_amb, void* stream) {
+  if (nsoil < 1 || ny < 1 || nx < 1) return FS_EARG;
+  return check(launch_soil(nsoil, ny, nx, T_soil, q_in, dt, soil_dz, d_above, d_below, k_s, rho_s,
+                           cp_s, eps_s, T_amb, ST(stream)),
+               "fs_soil_step");
+}
+
+int fs_proj_create(const FsGrid* g, void** handle) {
+  GRID("fs_proj_create");
+  *handle = proj_create(gd);
+  if (!*handle) {
+    fs_set_error("fs_proj_create: allocation failed");
+    return FS_ECUDA;
+  }
+  return FS_OK;
+}
+
+void fs_proj_destroy(void* handle) { proj_destroy(handle); }
+
+int fs_proj_rebuild(void* handle, const double* rho, void* stream) {
+  if (!handle) return FS_EARG;
+  return check(proj_rebuild(handle, rho, ST(stream)), "fs_proj_rebuild");
+}
+
+int fs_proj_project(void* handle, double* u, double* v, double* w, const double* u_inlet,
+                    const double* div_target, double dt, double rtol, int maxiter, int* iters,
+                    void* stream) {
+  if (!handle || !iters || !(dt > 0.0)) return FS_EARG;
+  return check(proj_project(handle, u, v, w, u_inlet, div_target, dt, rtol, maxiter, iters,
+                            ST(stream)),
+               "fs_proj_project");
+}
+
+double* fs_proj_pressure(void* handle) { return handle ? proj_pressure(handle) : nullptr; }
+
+int fs_proj_apply(void* handle, const double* x, double* y, void* stream) {
+  if (!handle) return FS_EARG;
+  return check(proj_apply(handle, x, y, ST(stream)), "fs_proj_apply");
+}
+
+int fs_divergence_max(const FsGrid* g, const double* u, const double* v, const double* w,
+                      const double* u_inlet, const double* div_target, double* div_out,
+                      double* result, void* stream) {
+  GRID("fs_divergence_max");
+  unsigned long long* key = nullptr;
+  if (cudaMallocAsync(&key, sizeof(unsigned long long), ST(stream)) != cudaSuccess)
+    return check(FS_ECUDA, "fs_divergence_max");
+  int st = launch_div_resid_max(gd, u, v, w, u_inlet, div_target, div_out, key, ST(stream));
+  unsigned long long hk = 0;
+  cudaMemcpyAsync(&hk, key, sizeof(hk), cudaMemcpyDeviceToHost, ST(stream));
+  cudaFreeAsync(key, ST(stream));
+  if (cudaStreamSynchronize(ST(stream)) != cudaSuccess) return check(FS_ECUDA, "fs_divergence_max");
+  memcpy(result, &hk, sizeof(double));
+  return check(st, "fs_divergence_max");
+}
+
+int fs_dom_create(const FsGrid* g, int M, const double* ox, const double* oy, const double* oz,
+                  const double* w, double kappa_gas_max, void** handle) {
+  GRID("fs_dom_create");
+  if (M < 1 || !ox || !oy || !oz || !w) return FS_EARG;
+  *handle = dom_create(gd, M, ox, oy, oz, w, kappa_gas_max);
+  if (!*handle) {
+    fs_set_error("fs_dom_create: allocation failed");
+    return FS_ECUDA;
+  }
+  return FS_OK;
+}
+
+void fs_dom_destroy(void* handle) { dom_destroy(handle); }
+
+int fs_dom_solve(void* handle, const double* T_s, const double* T_g, const double* alpha_s,
+                 const double* omega, double sigma_sav, double T_amb, const double* T_soil0,
+                 const double* Y_H2O, const double* rho, const double* M_local, double* q_rad_solid,
+                 double* q_rad_gas, double* q_in_soil, void* stream) {
+  if (!handle) return FS_EARG;
+  return check(dom_solve(handle, T_s, T_g, alpha_s, omega, sigma_sav, T_amb, T_soil0, Y_H2O, rho,
+                         M_local, q_rad_solid, q_rad_gas, q_in_soil, ST(stream)),
+               "fs_dom_solve");
+}
+
+double* fs_dom_intensity(void* handle) { return handle ? dom_intensity(handle) : nullptr; }
+int fs_dom_iterations(void* handle) { return handle ? dom_last_iters(handle) : -1; }
+
+int fs_bed_step(const FsGrid* g, const FsBedParticles* p, const FsBedSegments* s,
+                const FsBedSources* o, const FsBedParams* prm, const double* T_g,
+                const double* Y_O2, void* stream) {
+  GRID("fs_bed_step");
+  if (!p || !s || !o || !prm || !(prm->dt > 0.0)) {
+    fs_set_error("fs_bed_step: bad argument");
+    return FS_EARG;
+  }
+  BedOutH oh{o->S_pyro, o->S_drying, o->Q_pyro, o->Q_drying, o->Y_F_source, o->Q_char,
+             o->Q_smold, o->Q_g_conv};
+  BedParamsH b{};
+  b.dt = prm->dt; b.h_conv = prm->h_conv; b.rho_true = prm->rho_true; b.cp_solid = prm->cp_solid;
+  b.eps_solid = prm->eps_solid; b.T_amb = prm->T_amb; b.view = prm->view; b.h_bed = prm->h_bed;
+  b.kappa_bed = prm->kappa_bed; b.char_cap = prm->char_cap; b.ash_exp = prm->ash_exp;
+  b.do_dry = prm->do_dry; b.do_pyro = prm->do_pyro; b.do_char = prm->do_char;
+  b.do_smold = prm->do_smold; b.mode = prm->mode; b.geometric = prm->geometric;
+  b.n_split = prm->n_split; b.Qsx = prm->Qsx; b.q_rad = prm->q_rad; b.drip_on = prm->drip_on;
+  b.n_z_bed = prm->n_z_bed; b.i_src0 = prm->i_src0; b.i_src1 = prm->i_src1;
+  return check(launch_bed_step(gd, *p, *s, oh, b, T_g, Y_O2, ST(stream)), "fs_bed_step");
+}
+
+int fs_bed_aggregate(const FsBedParticles* p, const FsBedSegments* s, double* out, int mode,
+                     void* stream) {
+  if (!p || !s || (mode != 0 && mode != 1)) return FS_EARG;
+  return check(launch_bed_aggregate(*p, *s, out, mode, ST(stream)), "fs_bed_aggregate");
+}
+
+int fs_bed_hcond(const FsGrid* g, double* T_s_grid, double* scratch, const double* alpha_s,
+                 int n_z_bed, double k_solid, double rho_true, double cp_solid, double dt,
+                 const FsBedParticles* p, const FsBedSegments* s, const int* seg_of_cell,
+                 void* stream) {
+  GRID("fs_bed_hcond");
+  if (!p || !s || !scratch || !seg_of_cell) return FS_EARG;
+  return check(launch_bed_hcond(gd, T_s_grid, scratch, alpha_s, n_z_bed, k_solid, rho_true,
+                                cp_solid, dt, *p, *s, seg_of_cell, ST(stream)),
+               "fs_bed_hcond");
+}
+
+int fs_levelset(const FsGrid* g, const double* phi, const double* aux, double* out, double coef,
+                int mode, void* stream) {
+  GRID("fs_levelset");
+  if (mode < 0 || mode > 2 || (mode > 0 && !aux)) return FS_EARG;
+  return check(launch_levelset(gd, phi, aux, out, coef, mode, ST(stream)), "fs_levelset");
+}
+
+int fs_active_count(int64_t n, const double* omega, const double* T_g, const double* Y_F,
+                    unsigned long long* count, unsigned char* mask, void* stream) {
+  return check(launch_active_count(n, omega, T_g, Y_F, count, mask, ST(stream)),
+               "fs_active_count");
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// Shared device helpers for the Tier-3 step kernels (sm_100a, FP64).
+//
+// Layout: every 3D field is a C-contiguous float64 array (Nz, Ny, Nx),
+// cell (k, j, i) at flat index (k*Ny + j)*Nx + i, exactly the numpy layout
+// the reference kernels mutate in place (spread_3d.py:88-155).
+//
+// Arithmetic is transcribed operation by operation from the reference
+// expressions and the library is compiled with --fmad=false, so each cell
+// rounds the way the numba (no fast-math) build does; remaining differences
+// come only from libm transcendental functions (exp/pow/tanh), which are
+// within a few ulp of glibc.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#include "../../include/firestep.h"
+
+// Grid geometry as the kernels see it.  dz/da/db are device arrays of length nz
+// (dz_arr, d_face_above, d_face_below of Grid3D, spread_3d.py:180-188).
+struct GridDev {
+  int nx, ny, nz;
+  double dx, dy;
+  const double* dz;
+  const double* da;
+  const double* db;
+};
+
+__host__ __device__ inline int64_t cidx(const GridDev& g, int k, int j, int i) {
+  return ((int64_t)k * g.ny + j) * (int64_t)g.nx + i;
+}
+
+__device__ __forceinline__ int wrapj(int j, int ny) {
+  int r = j % ny;
+  return r < 0 ? r + ny : r;
+}
+
+// minmod limiter (muscl_3d.py:37-44)
+__device__ __forceinline__ double minmod(double a, double b) {
+  if (a * b <= 0.0) return 0.0;
+  if (a > 0.0) return a < b ? a : b;
+  return a > b ? a : b;
+}
+
+// upwind-biased MUSCL face value at i+1/2 from cells i-1..i+2 (muscl_3d.py:47-64)
+__device__ __forceinline__ double muscl_face(double pim1, double pi, double pip1,
+                                             double pip2, double uf) {
+  if (uf >= 0.0) {
+    double s = minmod(pi - pim1, pip1 - pi);
+    return pi + 0.5 * s;
+  } else {
+    double s = minmod(pip1 - pi, pip2 - pip1);
+    return pip1 - 0.5 * s;
+  }
+}
+
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
+// Launch geometry helpers: one thread per cell, x fastest.
+struct Launch3 {
+  dim3 grid, block;
+};
+inline Launch3 launch_cells(const GridDev& g) {
+  Launch3 L;
+  int bx = g.nx >= 128 ? 128 : (g.nx >= 64 ? 64 : 32);
+  int by = 256 / bx;
+  L.block = dim3(bx, by, 1);
+  L.grid = dim3((g.nx + bx - 1) / bx, (g.ny + by - 1) / by, g.nz);
+  return L;
+}
+
+__host__ __device__ inline int64_t ncells(const GridDev& g) { return (int64_t)g.nx * g.ny * g.nz; }
+__device__ __forceinline__ int64_t ncells_dev(const GridDev& g) { return (int64_t)g.nx * g.ny * g.nz; }
+
+inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// last CUDA error -> status
+inline int cuda_status() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? FS_OK : FS_ECUDA;
+}
+
+// Per-thread error text for fs_last_error().
+void fs_set_error(const char* fmt, ...);

@@ -1,0 +1,118 @@
+// Internal launcher declarations shared by the .cu files and the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/firestep.h"
+
+typedef FsBedParticles BedPartH;
+typedef FsBedSegments BedSegH;
+typedef FsBedSources BedOutHPub;
+
+struct BedOutH {
+  double *S_pyro, *S_dry, *Q_pyro, *Q_dry, *YF_src, *Q_char, *Q_smold, *Q_gconv;
+};
+
+struct BedParamsH {
+  double dt, h_conv, rho_true, cp_solid, eps_solid, T_amb, view, h_bed, kappa_bed;
+  double char_cap, ash_exp;
+  int do_dry, do_pyro, do_char, do_smold, mode, geometric, n_split;
+  const double* Qsx;
+  const double* q_rad;
+  int drip_on, n_z_bed, i_src0, i_src1;
+};
+
+struct GridDev;
+
+int launch_species(const GridDev& g, int nspec, const double* const* Y, double* const* Yo,
+                   const double* const* S, const double* Y_inlet, const double* rho,
+                   const double* u, const double* v, const double* w, double dt, double D,
+                   cudaStream_t st);
+int launch_species_sources(int64_t n, const double* Sp, const double* Sd, const double* YF,
+                           const double* YO, const double* YH, double* SF, double* SO,
+                           double* SH, cudaStream_t st);
+int launch_advect_scalar(const GridDev& g, const double* phi, const double* u, const double* v,
+                         const double* w, double* rhs, double phi_inlet, cudaStream_t st);
+int launch_gas_energy_adv(const GridDev& g, const double* T, const double* u, const double* v,
+                          const double* w, double* To, double dt, double alpha, double T_amb,
+                          cudaStream_t st);
+int launch_turb_diff(const GridDev& g, int nfield, const double* const* f, double* const* fo,
+                     const double* nu_t, double sc_t, double dt_sub, int clip, const double* lo,
+                     const double* hi, cudaStream_t st);
+int launch_drag(int64_t n, const double* u, const double* v, const double* w, const double* rho,
+                const double* as, double sigma, double C_D, double* Fx, double* Fy, double* Fz,
+                cudaStream_t st);
+int launch_momentum(const GridDev& g, const double* u, const double* v, const double* w,
+                    const double* rho, const double* T, const double* Fx, const double* Fy,
+                    const double* Fz, const double* alpha_s, double sigma, double C_D,
+                    const double* u_in, const double* v_in, const double* w_in, double* uo,
+                    double* vo, double* wo, double dt, double T_amb, cudaStream_t st);
+int launch_sponge(const GridDev& g, double* u, const double* u_t, const double* sig_x,
+                  const double* YF, double skip, double dt, cudaStream_t st);
+int launch_keps(const GridDev& g, const double* k, const double* e, const double* u,
+                const double* v, const double* w, const double* T, const double* alpha_s,
+                const double* u_in, const double* kwall, const double* ewall, double* ko,
+                double* eo, double* nuo, double* S2o, double* O2o, double sigma, double dt,
+                double T_amb, double beta_p, double beta_d, cudaStream_t st);
+int launch_solid_cond(const GridDev& g, const double* Ts, const double* as, double* To,
+                      double k_solid, double rho_s, double cp_s, double dt, int nz_active,
+                      cudaStream_t st);
+int launch_soil(int nsoil, int ny, int nx, double* T, const double* qin, double dt,
+                const double* sdz, const double* sda, const double* sdb, double k_s,
+                double rho_s, double cp_s, double eps_s, double T_amb, cudaStream_t st);
+
+int edc_scratch_bytes(int64_t n);
+int launch_edc(int64_t n, const double* rho, double* Tg, double* Yf, double* YO, const double* kt,
+               const double* et, const double* YH, double* omega, double chi_rad, double cp_g,
+               double dt, int n_substeps, double s_stoich, double hoc_J, int extinction,
+               void* scratch, cudaStream_t st);
+int launch_gas_update(const GridDev& g, double* Tg, const double* rho, const double* YH,
+                      const double* Ts, const double* Sp, const double* Sd, const double* Qgc,
+                      const double* qrg, double* Qcomb_out, unsigned long long* qc_max,
+                      double dt_sub, double T_amb, double h_bed, int drip_on, int n_z_bed,
+                      int i_src0, int i_src1, cudaStream_t st);
+int launch_eos(const GridDev& g, double* rho, double* rho_prev, const double* Tg, double* YO,
+               double P0, double R_air, double T_amb, cudaStream_t st);
+int launch_clip(int64_t n, double* f, double lo, double hi, cudaStream_t st);
+int launch_max(const GridDev& g, const double* f, int mode, unsigned long long* out_key,
+               cudaStream_t st);
+int launch_init_keys(unsigned long long* out, int n, int mode2_mask, cudaStream_t st);
+int launch_keys_to_double(const unsigned long long* in, double* out, int n, cudaStream_t st);
+
+void* proj_create(const GridDev& g);
+void proj_destroy(void* h);
+double* proj_pressure(void* h);
+const double* proj_inv_rho(void* h);
+int proj_nlevels(void* h);
+int proj_rebuild(void* h, const double* rho, cudaStream_t st);
+int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
+                 const double* target, double dt, double rtol, int maxiter, int* iters,
+                 cudaStream_t st);
+int proj_apply(void* h, const double* x, double* y, cudaStream_t st);
+int launch_div_resid_max(const GridDev& g, const double* u, const double* v, const double* w,
+                         const double* u_in, const double* target, double* div_out,
+                         unsigned long long* out_key, cudaStream_t st);
+
+void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, const double* oz,
+                 const double* w, double kgmax);
+void dom_destroy(void* h);
+double* dom_intensity(void* h);
+double* dom_G(void* h);
+int dom_last_iters(void* h);
+int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, const double* om,
+              double sigma, double T_amb, const double* Tsoil0, const double* YH, const double* rho,
+              const double* Mloc, double* q_solid, double* q_gas, double* q_in_soil,
+              cudaStream_t st);
+
+int launch_bed_step(const GridDev& g, const BedPartH& ph, const BedSegH& sh, const BedOutH& oh,
+                    const BedParamsH& bp, const double* Tg, const double* YO2, cudaStream_t st);
+int launch_bed_aggregate(const BedPartH& ph, const BedSegH& sh, double* out, int mode,
+                         cudaStream_t st);
+int launch_bed_hcond(const GridDev& g, double* T_grid, double* scratch, const double* as,
+                     int n_z_bed, double k_solid, double rho_true, double cp_solid, double dt,
+                     const BedPartH& ph, const BedSegH& sh, const int* seg_of_cell,
+                     cudaStream_t st);
+
+int launch_levelset(const GridDev& g, const double* phi, const double* aux, double* out,
+                    double coef, int mode, cudaStream_t st);
+int launch_active_count(int64_t n, const double* om, const double* Tg, const double* YF,
+                        unsigned long long* count, unsigned char* mask, cudaStream_t st);

@@ -1,0 +1,368 @@
+// Pointwise kernels of the Tier-3 step: EDC chemistry, the Lagrangian-branch
+// gas-energy update, EoS, caps and the step's max reductions.
+#include "common.cuh"
+#include "kernels.h"
+
+// ---------------------------------------------------------------------------
+// EDC (chemistry_closures/edc.py:134-335 step_chemistry_ode_edc, n_substeps=1)
+//
+// The reference assigns the H2O-quench flag `_h2o_quench_substantial` only in
+// the branch taken when Y_F > 1e-9 and Y_O2 > 1e-9 (edc.py:223).  Cells that
+// skip that branch reuse the value left by the previously visited cell, which
+// with one thread is the previous cell in flat k-j-i order (initially False).
+// The flag gates the wet-bulb relaxation of T_g.  To reproduce that order on
+// the GPU the flag is resolved by a flat-order "last assigned value" scan:
+//   pass 1: per 1024-cell block, the last assigned flag (or none);
+//   pass 2: one thread carries the flag across blocks;
+//   pass 3: in-block inclusive scan + carry, then the EDC update itself.
+// ---------------------------------------------------------------------------
+#define EDC_BLK 1024
+
+__device__ __forceinline__ int edc_flag_code(double Yf, double YO2, double YH, int t) {
+  // -1: flag not assigned in this cell; else (t << 1) | flag
+  if (Yf <= 1e-9 || YO2 <= 1e-9) return -1;
+  int f = 0;
+  if (YH > 0.0) {
+    double fac = 1.0 - YH / 0.18;
+    if (fac < 0.0) fac = 0.0;
+    if (fac < 0.5) f = 1;
+  }
+  return (t << 1) | f;
+}
+
+__device__ __forceinline__ int block_max_int(int v, int* sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? sh[threadIdx.x] : -1;
+  if (wid == 0) {
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  }
+  return v;  // valid in thread 0
+}
+
+__global__ void k_edc_agg(int64_t n, const double* __restrict__ Yf, const double* __restrict__ YO,
+                          const double* __restrict__ YH, signed char* agg) {
+  __shared__ int sh[32];
+  int64_t c = (int64_t)blockIdx.x * EDC_BLK + threadIdx.x;
+  int v = -1;
+  if (c < n) v = edc_flag_code(Yf[c], YO[c], YH[c], threadIdx.x);
+  v = block_max_int(v, sh);
+  if (threadIdx.x == 0) agg[blockIdx.x] = (signed char)(v < 0 ? -1 : (v & 1));
+}
+
+__global__ void k_edc_carry(int nb, const signed char* agg, signed char* carry,
+                            const signed char* carry_in) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  signed char cur = carry_in ? carry_in[0] : 0;
+  for (int b = 0; b < nb; ++b) {
+    carry[b] = cur;
+    if (agg[b] >= 0) cur = agg[b];
+  }
+}
+
+struct EdcArgs {
+  const double* rho;
+  double *Tg, *Yf, *YO;
+  const double *kt, *et, *YH;
+  double* omega;
+  const signed char* carry;
+  double chi_rad, cp_g, dt, s_stoich, HoC_eff, relax;
+  int extinction, nsub;
+};
+
+__global__ void k_edc_main(int64_t n, EdcArgs a) {
+  __shared__ int sh[32];
+  const int t = threadIdx.x;
+  const int64_t c = (int64_t)blockIdx.x * EDC_BLK + t;
+  const bool live = c < n;
+  double Yf = 0, YO2 = 0, YH = 0;
+  if (live) { Yf = a.Yf[c]; YO2 = a.YO[c]; YH = a.YH[c]; }
+  int v = live ? edc_flag_code(Yf, YO2, YH, t) : -1;
+  // inclusive max-scan over the block (flat order == thread order)
+  const int lane = t & 31, wid = t >> 5;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v = max(v, y);
+  }
+  if (lane == 31) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    int w = (lane < (blockDim.x >> 5)) ? sh[lane] : -1;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w = max(w, y);
+    }
+    sh[lane] = w;
+  }
+  __syncthreads();
+  if (wid > 0) v = max(v, sh[wid - 1]);
+  if (!live) return;
+  bool flag = (v >= 0) ? (v & 1) : (a.carry[blockIdx.x] > 0);
+
+  double Tg = a.Tg[c];
+  const double rho_i = a.rho[c];
+  double k_t = a.kt[c];
+  if (k_t < 1.0e-4) k_t = 1.0e-4;
+  double e_t = a.et[c];
+  if (e_t < 1.0e-6) e_t = 1.0e-6;
+  double ratio = 1.5e-5 * e_t / (k_t * k_t);
+  if (ratio < 1e-30) ratio = 1e-30;
+  double gx = 2.1377 * pow(ratio, 0.25);
+  double gamma_star = gx * (gx * gx);
+  if (gamma_star > 1.0) gamma_star = 1.0;
+  double tau_star = 0.4083 * sqrt(1.5e-5 / e_t);
+  const double h = a.dt / (double)a.nsub;
+  double acc = 0.0;
+  for (int sub = 0; sub < a.nsub; ++sub) {
+    double omega;
+    if (Yf <= 1e-9 || YO2 <= 1e-9) {
+      omega = 0.0;
+    } else {
+      double lim = YO2 / a.s_stoich;
+      double Y_lim = Yf < lim ? Yf : lim;
+      double omega_fine = rho_i * Y_lim / tau_star;
+      omega = gamma_star * omega_fine;
+      if (YH > 0.0) {
+        double fac = 1.0 - YH / 0.18;
+        if (fac < 0.0) fac = 0.0;
+        omega = omega * fac;
+      }
+    }
+    bool fired = false;
+    if (a.extinction && omega > 0.0) {
+      double Yib = 1.0 - Yf - YO2;
+      if (Yib > 0.88) {
+        double rs = (1.0 - Yib) / (1.0 - 0.88);
+        if (rs < 0.0) rs = 0.0;
+        omega = omega * rs;
+        if (rs < 0.5) fired = true;
+      }
+      if (omega > 0.0 && Tg < 1200.0) { omega = 0.0; fired = true; }
+      if (omega > 0.0) {
+        double Q_rate = omega * a.HoC_eff;
+        if (Q_rate < 75000.0) { omega = 0.0; fired = true; }
+      }
+    }
+    if ((fired || flag) && Tg > 373.15) {
+      if (YH > 0.0) {
+        double wb = YH / 0.10;
+        if (wb > 1.0) wb = 1.0;
+        double dT_wb = (Tg - 373.15) * a.relax * wb;
+        Tg = Tg - dT_wb;
+      }
+    }
+    double dY = -omega * h / rho_i;
+    Yf = Yf + dY;
+    if (Yf < 0.0) Yf = 0.0;
+    YO2 = YO2 + a.s_stoich * dY;
+    if (YO2 < 0.0) YO2 = 0.0;
+    double cp_mix = (1.0 - YH) * a.cp_g + YH * 2000.0;
+    Tg = Tg + omega * a.HoC_eff * h / (rho_i * cp_mix);
+    if (Tg > 2400.0) Tg = 2400.0;
+    acc += omega * h;
+  }
+  a.Yf[c] = Yf;
+  a.YO[c] = YO2;
+  a.Tg[c] = Tg;
+  a.omega[c] = a.dt > 0.0 ? acc / a.dt : 0.0;
+}
+
+int edc_scratch_bytes(int64_t n) {
+  int64_t nb = (n + EDC_BLK - 1) / EDC_BLK;
+  return (int)(2 * nb + 16);
+}
+
+int launch_edc(int64_t n, const double* rho, double* Tg, double* Yf, double* YO, const double* kt,
+               const double* et, const double* YH, double* omega, double chi_rad, double cp_g,
+               double dt, int n_substeps, double s_stoich, double hoc_J, int extinction,
+               void* scratch, cudaStream_t st) {
+  int64_t nb = (n + EDC_BLK - 1) / EDC_BLK;
+  signed char* agg = (signed char*)scratch;
+  signed char* carry = agg + nb;
+  k_edc_agg<<<(unsigned)nb, EDC_BLK, 0, st>>>(n, Yf, YO, YH, agg);
+  k_edc_carry<<<1, 32, 0, st>>>((int)nb, agg, carry, nullptr);
+  EdcArgs a{};
+  a.rho = rho; a.Tg = Tg; a.Yf = Yf; a.YO = YO; a.kt = kt; a.et = et; a.YH = YH;
+  a.omega = omega; a.carry = carry;
+  a.chi_rad = chi_rad; a.cp_g = cp_g; a.dt = dt; a.s_stoich = s_stoich;
+  a.HoC_eff = hoc_J * (1.0 - chi_rad);
+  a.nsub = n_substeps > 1 ? n_substeps : 1;
+  a.relax = 1.0 - exp(-(dt / (double)a.nsub) / 0.5);
+  a.extinction = extinction;
+  k_edc_main<<<(unsigned)nb, EDC_BLK, 0, st>>>(n, a);
+  return cuda_status();
+}
+
+// ---------------------------------------------------------------------------
+// Lagrangian-branch gas-energy update (spread_3d.py:3088-3146):
+//   Q_comb = drip (20 % of 30 kW/m^2 / h_bed in source bed cells during the
+//   ignition window, spread_3d.py:2916-2957) + q_rad_gas / dz
+//   T_g += (Q_comb - Q_g_conv - vapour debit) dt_sub / (max(rho,1e-3) cp_mix)
+//   T_g = max(T_g, T_amb)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long dkey(double x) {
+  long long b = __double_as_longlong(x);
+  return b >= 0 ? ((unsigned long long)b ^ 0x8000000000000000ull) : ~(unsigned long long)b;
+}
+__device__ __forceinline__ double dkey_inv(unsigned long long k) {
+  long long b = (k & 0x8000000000000000ull) ? (long long)(k ^ 0x8000000000000000ull)
+                                            : (long long)(~k);
+  return __longlong_as_double(b);
+}
+
+struct GasArgs {
+  double* Tg;
+  const double *rho, *YH, *Ts, *Sp, *Sd, *Qgc, *qrg;
+  double* Qcomb_out;           // optional
+  unsigned long long* qc_max;  // optional
+  double dt_sub, T_amb, q_drip_gas;
+  int drip_on, n_z_bed, i_src0, i_src1;
+};
+
+__global__ void k_gas_update(GridDev g, GasArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  int64_t c = cidx(g, k, j, i);
+  double qc = 0.0;
+  if (a.drip_on && k < a.n_z_bed && i >= a.i_src0 && i < a.i_src1) qc = qc + a.q_drip_gas;
+  qc = qc + a.qrg[c] / g.dz[k];
+  double T = a.Tg[c];
+  double YH = a.YH[c];
+  double cp = (1.0 - YH) * 1100.0 + YH * 2000.0;
+  double d1 = T - a.Ts[c];
+  if (!(d1 >= 0.0)) d1 = (d1 != d1) ? d1 : 0.0;
+  double d2 = T - 373.15;
+  if (!(d2 >= 0.0)) d2 = (d2 != d2) ? d2 : 0.0;
+  double debit = (a.Sp[c] * d1 + a.Sd[c] * d2) * 2000.0;
+  double r = a.rho[c];
+  double rm = (r >= 1.0e-3 || r != r) ? r : 1.0e-3;
+  double ginv = a.dt_sub / (rm * cp);
+  double Tn = T + (qc - a.Qgc[c] - debit) * ginv;
+  if (Tn < a.T_amb) Tn = a.T_amb;
+  a.Tg[c] = Tn;
+  if (a.Qcomb_out) a.Qcomb_out[c] = qc;
+  if (a.qc_max) atomicMax(a.qc_max, dkey(qc));
+}
+
+int launch_gas_update(const GridDev& g, double* Tg, const double* rho, const double* YH,
+                      const double* Ts, const double* Sp, const double* Sd, const double* Qgc,
+                      const double* qrg, double* Qcomb_out, unsigned long long* qc_max,
+                      double dt_sub, double T_amb, double h_bed, int drip_on, int n_z_bed,
+                      int i_src0, int i_src1, cudaStream_t st) {
+  GasArgs a{};
+  a.Tg = Tg; a.rho = rho; a.YH = YH; a.Ts = Ts; a.Sp = Sp; a.Sd = Sd; a.Qgc = Qgc; a.qrg = qrg;
+  a.Qcomb_out = Qcomb_out; a.qc_max = qc_max;
+  a.dt_sub = dt_sub; a.T_amb = T_amb;
+  double q_drip = 30000.0 / (h_bed > 1e-3 ? h_bed : 1e-3);
+  a.q_drip_gas = (1.0 - 0.80) * q_drip;
+  a.drip_on = drip_on; a.n_z_bed = n_z_bed; a.i_src0 = i_src0; a.i_src1 = i_src1;
+  Launch3 L = launch_cells(g);
+  k_gas_update<<<L.grid, L.block, 0, st>>>(g, a);
+  return cuda_status();
+}
+
+// ---------------------------------------------------------------------------
+// Start-of-step bookkeeping (spread_3d.py:1984-2050):
+//   rho_prev = rho; rho = P0 / (R_air max(T_g, T_amb)); Y_O2[:, :, 0] = 0.232
+// and the closing EoS (spread_3d.py:3440) with prev == null.
+// ---------------------------------------------------------------------------
+__global__ void k_eos(GridDev g, double* rho, double* rho_prev, const double* __restrict__ Tg,
+                      double* YO, double P0, double R_air, double T_amb) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  int64_t c = cidx(g, k, j, i);
+  if (rho_prev) rho_prev[c] = rho[c];
+  double T = Tg[c];
+  double Tm = (T >= T_amb || T != T) ? T : T_amb;
+  rho[c] = P0 / (R_air * Tm);
+  if (YO && i == 0) YO[c] = 0.232;
+}
+
+int launch_eos(const GridDev& g, double* rho, double* rho_prev, const double* Tg, double* YO,
+               double P0, double R_air, double T_amb, cudaStream_t st) {
+  Launch3 L = launch_cells(g);
+  k_eos<<<L.grid, L.block, 0, st>>>(g, rho, rho_prev, Tg, YO, P0, R_air, T_amb);
+  return cuda_status();
+}
+
+// clip a field to [lo, hi] (numpy minimum/maximum semantics: NaN stays NaN)
+__global__ void k_clip(int64_t n, double* f, double lo, double hi) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  double x = f[c];
+  if (x > hi) x = hi;
+  if (x < lo) x = lo;
+  f[c] = x;
+}
+
+int launch_clip(int64_t n, double* f, double lo, double hi, cudaStream_t st) {
+  k_clip<<<blocks_for(n, 256), 256, 0, st>>>(n, f, lo, hi);
+  return cuda_status();
+}
+
+// ---------------------------------------------------------------------------
+// Max reductions.  Slots written as order-preserving uint64 keys.
+//   mode 0: max |f| (NaN propagates)      mode 1: max f (NaN propagates)
+//   mode 2: max f over k in [1,Nz-2], i in [1,Nx-2], starting at 0, NaN ignored
+//           (turbulence_3d.py:894-900)
+// ---------------------------------------------------------------------------
+__global__ void k_max(GridDev g, const double* __restrict__ f, int mode,
+                      unsigned long long* out) {
+  int64_t n = ncells_dev(g);
+  unsigned long long best = dkey(mode == 2 ? 0.0 : -INFINITY);
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    double x = f[c];
+    if (mode == 0) x = fabs(x);
+    if (mode == 2) {
+      int i = (int)(c % g.nx);
+      int k = (int)(c / ((int64_t)g.nx * g.ny));
+      if (k < 1 || k > g.nz - 2 || i < 1 || i > g.nx - 2) continue;
+      if (x != x) continue;
+    }
+    if (x != x) x = __longlong_as_double(0x7ff8000000000000ll);
+    unsigned long long kk = dkey(x);
+    if (kk > best) best = kk;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long y = __shfl_xor_sync(0xffffffffu, best, o);
+    if (y > best) best = y;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, best);
+}
+
+__global__ void k_init_keys(unsigned long long* out, int n, int mode2_mask) {
+  int t = threadIdx.x;
+  if (t < n) out[t] = ((mode2_mask >> t) & 1) ? dkey(0.0) : dkey(-INFINITY);
+}
+
+int launch_max(const GridDev& g, const double* f, int mode, unsigned long long* out_key,
+               cudaStream_t st) {
+  int64_t n = ncells(g);
+  unsigned nb = blocks_for(n, 256);
+  if (nb > 148 * 8) nb = 148 * 8;
+  k_max<<<nb, 256, 0, st>>>(g, f, mode, out_key);
+  return cuda_status();
+}
+
+int launch_init_keys(unsigned long long* out, int n, int mode2_mask, cudaStream_t st) {
+  k_init_keys<<<1, 64, 0, st>>>(out, n, mode2_mask);
+  return cuda_status();
+}
+
+__global__ void k_keys_to_double(const unsigned long long* in, double* out, int n) {
+  int t = threadIdx.x;
+  if (t < n) out[t] = dkey_inv(in[t]);
+}
+
+int launch_keys_to_double(const unsigned long long* in, double* out, int n, cudaStream_t st) {
+  k_keys_to_double<<<1, 64, 0, st>>>(in, out, n);
+  return cuda_status();
+}

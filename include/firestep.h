@@ -1,0 +1,232 @@
+/*
+ * firestep.h -- C ABI of libfirestep.so, the sm_100a implementation of the
+ * Tier-3 step of the FireWebApp 3D grass-fire solver
+ * (src/model_outdoor/spread_3d.py driving src/model_outdoor/physics_3d/).
+ *
+ * Conventions (the same contract the reference kernels follow):
+ *  - every 3D field is a C-contiguous float64 array (Nz, Ny, Nx) in device
+ *    memory, cell (k,j,i) at (k*Ny + j)*Nx + i (spread_3d.py:88-155);
+ *  - the caller owns every field; solver objects own their workspaces;
+ *  - entry points take a cudaStream_t passed as void* and never synchronise
+ *    the host, except where the name says so or the reference loop is
+ *    data-dependent (documented per function);
+ *  - every function returns an int status:
+ *      0 ok, 1 bad argument, 2 non-finite value, 3 solver did not converge,
+ *      4 device wait timed out, 5 CUDA error; fs_last_error() has the text.
+ *
+ * Each declaration names the reference function it replaces (file:line).
+ */
+#ifndef FIRESTEP_H
+#define FIRESTEP_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FS_OK 0
+#define FS_EARG 1
+#define FS_ENONFINITE 2
+#define FS_ENOCONV 3
+#define FS_ETIMEOUT 4
+#define FS_ECUDA 5
+
+/* Grid3D geometry (spread_3d.py:158-188): dz, d_above, d_below are device
+ * arrays of length nz (dz_arr, d_face_above, d_face_below). */
+typedef struct FsGrid {
+  int nx, ny, nz;
+  double dx, dy;
+  const double* dz;
+  const double* d_above;
+  const double* d_below;
+} FsGrid;
+
+/* Lagrangian bed particle buffers (lagrangian_bed_3d.py:193-218). */
+typedef struct FsBedParticles {
+  double *x, *y, *z;
+  signed char* alive;
+  double *m_solid, *m_water, *m_char, *T_s, *m_water_0, *sav, *m_char_max;
+} FsBedParticles;
+
+/* Occupied cells and their particle slots in slot order (built on the host
+ * from the fixed particle positions: particles do not move). */
+typedef struct FsBedSegments {
+  int nseg;
+  const int* seg_start; /* [nseg+1] offsets into perm */
+  const int* seg_cell;  /* [nseg] flat cell index */
+  const int* perm;      /* slots grouped by cell */
+} FsBedSegments;
+
+/* Per-cell source grids written by fs_bed_step (lagrangian_bed_3d.py:610-619). */
+typedef struct FsBedSources {
+  double *S_pyro, *S_drying, *Q_pyro, *Q_drying, *Y_F_source, *Q_char, *Q_smold, *Q_g_conv;
+} FsBedSources;
+
+typedef struct FsBedParams {
+  double dt, h_conv, rho_true, cp_solid, eps_solid, T_amb, view, h_bed, kappa_bed;
+  double char_cap, ash_exp;
+  int do_dry, do_pyro, do_char, do_smold, mode, geometric, n_split;
+  /* Q_solid_ext: either a per-cell grid (Qsx) or assembled in-kernel from
+   * the previous q_rad and the ignition drip (spread_3d.py:2078-2103). */
+  const double* Qsx;
+  const double* q_rad;
+  int drip_on, n_z_bed, i_src0, i_src1;
+} FsBedParams;
+
+const char* fs_last_error(void);
+int fs_version(void);
+
+/* species_3d.py:41 step_species_transport, up to 3 species in one pass,
+ * out-of-place (Y -> Y_out, clipped to [0,1]). */
+int fs_species_transport(const FsGrid* g, int nspec, const double* const* Y, double* const* Y_out,
+                         const double* const* S, const double* Y_inlet, const double* rho,
+                         const double* u, const double* v, const double* w, double dt, double D,
+                         void* stream);
+
+/* spread_3d.py:2996-3004 dilution-form species sources (Lagrangian bed). */
+int fs_species_sources(int64_t n, const double* S_pyro, const double* S_drying,
+                       const double* Y_F, const double* Y_O2, const double* Y_H2O, double* S_F,
+                       double* S_O2, double* S_H2O, void* stream);
+
+/* muscl_3d.py:68 advect_3d_scalar_muscl: rhs -= u . grad(phi). */
+int fs_advect_scalar_muscl(const FsGrid* g, const double* phi, const double* u, const double* v,
+                           const double* w, double* rhs, double phi_inlet, void* stream);
+
+/* spread_3d.py:3827 _adv_gas_energy, out-of-place. */
+int fs_gas_energy_adv(const FsGrid* g, const double* T_g, const double* u, const double* v,
+                      const double* w, double* T_out, double dt, double alpha_th, double T_amb,
+                      void* stream);
+
+/* turbulence_3d.py:862 apply_turbulent_diffusion: the sub-step count
+ * (host result, synchronises the stream) ... */
+int fs_turb_diffusion_nsub(const FsGrid* g, const double* nu_t, double sc_t, double dt,
+                           int* n_sub, double* dt_sub, void* stream);
+/* ... and one sub-step for up to 4 fields, out-of-place, optional clip. */
+int fs_turb_diffusion_substep(const FsGrid* g, int nfield, const double* const* f,
+                              double* const* f_out, const double* nu_t, double sc_t, double dt_sub,
+                              int clip, const double* lo, const double* hi, void* stream);
+
+/* drag_3d.py:100 step_drag_force. */
+int fs_drag_force(int64_t n, const double* u, const double* v, const double* w, const double* rho,
+                  const double* alpha_s, double sigma_sav, double C_D, double* Fx, double* Fy,
+                  double* Fz, void* stream);
+
+/* momentum_3d.py:42 step_tentative_velocity, out-of-place.  With Fx == NULL
+ * the drag force is evaluated in-kernel from alpha_s (drag_3d.py:100). */
+int fs_tentative_velocity(const FsGrid* g, const double* u, const double* v, const double* w,
+                          const double* rho, const double* T_g, const double* Fx, const double* Fy,
+                          const double* Fz, const double* alpha_s, double sigma_sav, double C_D,
+                          const double* u_inlet, const double* v_inlet, const double* w_inlet,
+                          double* u_out, double* v_out, double* w_out, double dt, double T_amb,
+                          void* stream);
+
+/* momentum_3d.py:293 apply_outflow_sponge, in place. */
+int fs_outflow_sponge(const FsGrid* g, double* u, const double* u_target, const double* sigma_x,
+                      const double* Y_F, double Y_F_skip, double dt, void* stream);
+
+/* turbulence_3d.py:482 step_k_epsilon (with :392 _strain_and_vorticity_squared
+ * evaluated in-kernel; S2/O2 outputs optional), out-of-place.  Only the
+ * production options: bvg_factor = L_min = durbin_alpha = 0. */
+int fs_k_epsilon(const FsGrid* g, const double* k, const double* eps, const double* u,
+                 const double* v, const double* w, const double* T_g, const double* alpha_s,
+                 const double* u_inlet, const double* k_wall, const double* eps_wall, double* k_out,
+                 double* eps_out, double* nu_t_out, double* S2_out, double* O2_out,
+                 double sigma_sav, double dt, double T_amb, double beta_p, double beta_d,
+                 void* stream);
+
+/* chemistry_closures/edc.py:134 step_chemistry_ode_edc, in place; scratch of
+ * fs_edc_scratch_bytes(n) bytes.  The H2O-quench flag of cells that skip the
+ * reacting branch is the one left by the previous cell in flat k-j-i order
+ * (the reference's one-thread behaviour, edc.py:223). */
+int64_t fs_edc_scratch_bytes(int64_t n);
+int fs_edc(int64_t n, const double* rho, double* T_g, double* Y_F, double* Y_O2, const double* k,
+           const double* eps, const double* Y_H2O, double* omega, double chi_rad, double cp_g,
+           double dt, int n_substeps, double s_stoich, double hoc_J, int extinction, void* scratch,
+           void* stream);
+
+/* spread_3d.py:2916-2957 + 3104-3146: drip + q_rad_gas into Q_comb and the
+ * Lagrangian-branch gas-energy update, in place. */
+int fs_gas_energy_update(const FsGrid* g, double* T_g, const double* rho, const double* Y_H2O,
+                         const double* T_s, const double* S_pyro, const double* S_drying,
+                         const double* Q_g_conv, const double* q_rad_gas, double* Q_comb_out,
+                         double dt_sub, double T_amb, double h_bed, int drip_on, int n_z_bed,
+                         int i_src0, int i_src1, void* stream);
+
+/* spread_3d.py:2042 / :3440 EoS; with rho_prev != NULL also copies the old
+ * rho (:1984) and with Y_O2 != NULL sets the inlet column to 0.232 (:2050). */
+int fs_eos(const FsGrid* g, double* rho, double* rho_prev, const double* T_g, double* Y_O2,
+           double T_amb, void* stream);
+
+/* numpy clip (minimum then maximum), in place. */
+int fs_clip(int64_t n, double* f, double lo, double hi, void* stream);
+
+/* solid_conduction_3d.py:56 step_solid_conduction_vertical, out-of-place. */
+int fs_solid_conduction(const FsGrid* g, const double* T_s, const double* alpha_s, double* T_out,
+                        double k_solid, double rho_solid, double cp_solid, double dt,
+                        void* stream);
+
+/* soil_3d.py:106 step_soil_conduction, in place. */
+int fs_soil_step(int nsoil, int ny, int nx, double* T_soil, const double* q_in, double dt,
+                 const double* soil_dz, const double* d_above, const double* d_below, double k_s,
+                 double rho_s, double cp_s, double eps_s, double T_amb, void* stream);
+
+/* projection_3d.py:178 ProjectionSolver3D (fft_pcg path): create/destroy,
+ * :317 rebuild_for_rho, :677 project (synchronises once per CG iteration;
+ * warm start from the previous solution) and :847 divergence. */
+int fs_proj_create(const FsGrid* g, void** handle);
+void fs_proj_destroy(void* handle);
+int fs_proj_rebuild(void* handle, const double* rho, void* stream);
+int fs_proj_project(void* handle, double* u, double* v, double* w, const double* u_inlet,
+                    const double* div_target, double dt, double rtol, int maxiter, int* iters,
+                    void* stream);
+double* fs_proj_pressure(void* handle);
+int fs_proj_apply(void* handle, const double* x, double* y, void* stream);
+/* max |div(u) - target| to *result (synchronises); div_out optional. */
+int fs_divergence_max(const FsGrid* g, const double* u, const double* v, const double* w,
+                      const double* u_inlet, const double* div_target, double* div_out,
+                      double* result, void* stream);
+
+/* dom_3d.py:230 DOMRadiationSolver: create (ordinates/weights host arrays),
+ * :286 solve (synchronises once per source iteration). */
+int fs_dom_create(const FsGrid* g, int M, const double* ox, const double* oy, const double* oz,
+                  const double* w, double kappa_gas_max, void** handle);
+void fs_dom_destroy(void* handle);
+int fs_dom_solve(void* handle, const double* T_s, const double* T_g, const double* alpha_s,
+                 const double* omega, double sigma_sav, double T_amb, const double* T_soil0,
+                 const double* Y_H2O, const double* rho, const double* M_local, double* q_rad_solid,
+                 double* q_rad_gas, double* q_in_soil, void* stream);
+double* fs_dom_intensity(void* handle);
+int fs_dom_iterations(void* handle);
+
+/* lagrangian_bed_3d.py:594 step_bed_particles (sources overwritten only in
+ * occupied cells; zero the grids once), :501 aggregate_particles_to_T_s_grid
+ * (mode 0) and :550 aggregate_particles_to_M_local_grid (mode 1), :428
+ * step_horizontal_solid_conduction_scatter (T_s in place; scratch of
+ * n_z_bed*Ny*Nx doubles). */
+int fs_bed_step(const FsGrid* g, const FsBedParticles* p, const FsBedSegments* s,
+                const FsBedSources* o, const FsBedParams* prm, const double* T_g,
+                const double* Y_O2, void* stream);
+int fs_bed_aggregate(const FsBedParticles* p, const FsBedSegments* s, double* out, int mode,
+                     void* stream);
+int fs_bed_hcond(const FsGrid* g, double* T_s_grid, double* scratch, const double* alpha_s,
+                 int n_z_bed, double k_solid, double rho_true, double cp_solid, double dt,
+                 const FsBedParticles* p, const FsBedSegments* s, const int* seg_of_cell,
+                 void* stream);
+
+/* flame_front_3d.py:114 godunov_grad_norm (mode 0), :332 evolve (mode 1,
+ * aux = v_n, coef = dt), one :339 reinitialize sub-step (mode 2,
+ * aux = phi_0, coef = dtau); out-of-place. */
+int fs_levelset(const FsGrid* g, const double* phi, const double* aux, double* out, double coef,
+                int mode, void* stream);
+/* flame_front_3d.py:756-813 active-flame mask and its cell count (device
+ * counter, accumulated). */
+int fs_active_count(int64_t n, const double* omega, const double* T_g, const double* Y_F,
+                    unsigned long long* count, unsigned char* mask, void* stream);
+
+/* max reductions: mode 0 max|f|, 1 max f (NaN propagates), 2 interior max
+ * ignoring NaN from 0 (turbulence_3d.py:894-900); results to host. */
+int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

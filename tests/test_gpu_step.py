@@ -1,0 +1,93 @@
+"""Whole-step parity of the GPU Tier-3 step against the reference solver.
+
+The reference states come from running the reference's own ``run_3d_spread``
+on the 32 x 8 x 12 TINY case (tests/golden/make_fixtures.py, one numba
+thread, projection rtol 1e-12, seeded particle jitter).  The GPU path must
+match every field to relative L2 <= 1e-9 after each captured step, from the
+same initial state and also one step from a captured mid-run state.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-9
+FIELDS = ("rho", "u", "v", "w", "T_g", "Y_fuel", "Y_O2", "Y_H2O", "T_s", "k_turb",
+          "eps_turb", "nu_t", "omega", "q_rad", "T_soil", "phi",
+          "p_T_s", "p_m_solid", "p_m_water", "p_m_char", "S_pyro_b", "S_dry_b", "Q_gconv_b")
+
+
+def _solver(case):
+    from firewebapp_b200.solver import Tier3Solver
+    return Tier3Solver(case, projection_cg_rtol=1e-13, proj_maxiter=400)
+
+
+def _compare(got, want, tag, tol=TOL):
+    bad = {}
+    for k in FIELDS:
+        if k not in want:
+            continue
+        e = rel_l2(got[k], want[k])
+        if not e <= tol:
+            bad[k] = e
+    if "p_alive" in want:
+        assert np.array_equal(got["p_alive"].astype(np.int64), want["p_alive"].astype(np.int64)), tag
+    e_p = rel_l2(got["p_prev"], want["p_prev"])
+    if not e_p <= 1e-7:
+        bad["p_prev"] = e_p
+    assert not bad, f"{tag}: fields above tolerance: {bad}"
+
+
+def test_initial_state_matches_reference(ref_tiny):
+    from firewebapp_b200.cases import TINY
+    s = _solver(TINY)
+    try:
+        got = s.state()
+        init = ref_tiny["init"]
+        for k in ("rho", "u", "T_g", "Y_O2", "alpha_s", "T_s"):
+            assert np.array_equal(got[k], init[k]), k
+        for k in ("x", "y", "z", "m_solid", "m_water", "T_s"):
+            assert np.array_equal(got["p_" + k], init["p_" + k]), k
+    finally:
+        s.close()
+
+
+def test_ten_steps_match_reference(ref_tiny):
+    from firewebapp_b200.cases import TINY
+    s = _solver(TINY)
+    try:
+        dts = []
+        for n in range(1, 11):
+            assert s.step()
+            dts.append(s.diag.dt)
+            if f"s{n}" in ref_tiny:
+                _compare(s.state(), ref_tiny[f"s{n}"], f"step {n}")
+        assert np.allclose(dts, ref_tiny["trace"]["dt"], rtol=1e-12, atol=0.0)
+    finally:
+        s.close()
+
+
+def test_single_step_from_reference_state(ref_tiny):
+    from firewebapp_b200.cases import TINY
+    s = _solver(TINY)
+    try:
+        dts = ref_tiny["trace"]["dt"]
+        s.load_state(ref_tiny["s9"], t=float(np.sum(dts[:9])), dt_prev=float(dts[8]), step=9)
+        assert s.step()
+        _compare(s.state(), ref_tiny["s10"], "s9 -> s10")
+    finally:
+        s.close()
+
+
+def test_smoke_case_matches_reference(ref_smoke):
+    from firewebapp_b200.cases import SMOKE
+    s = _solver(SMOKE)
+    try:
+        for n in range(1, 4):
+            assert s.step()
+            if f"s{n}" in ref_smoke:
+                _compare(s.state(), ref_smoke[f"s{n}"], f"smoke step {n}")
+    finally:
+        s.close()
