@@ -245,6 +245,30 @@ class Tier3Solver:
             pass
 
     # --------------------------------------------------------------- helpers
+    def enable_phase_timers(self, on=True):
+        """Accumulate CUDA-event time per phase of the step (diagnostics)."""
+        self._timers = {} if on else None
+        self._mark = None
+
+    def _phase(self, label):
+        tm = getattr(self, "_timers", None)
+        if tm is None:
+            return
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        if self._mark is not None:
+            lab0, ev0 = self._mark
+            tm.setdefault(lab0, []).append((ev0, ev))
+        self._mark = (label, ev) if label else None
+
+    def phase_times(self):
+        """{phase: total milliseconds} of the phases recorded so far."""
+        torch.cuda.synchronize()
+        out = {}
+        for k, pairs in (getattr(self, "_timers", None) or {}).items():
+            out[k] = sum(a.elapsed_time(b) for a, b in pairs)
+        return out
+
     def _s(self):
         return torch.cuda.current_stream(self.dev).cuda_stream
 
@@ -268,6 +292,7 @@ class Tier3Solver:
         self.step_count += 1
         d = StepDiag()
         # --- 0. adaptive dt (spread_3d.py:1906-1941)
+        self._phase("dt")
         u_now = max(self._max(f["u"], 0), self._max(f["v"], 0), self._max(f["w"], 0),
                     p["U_mf"], math.sqrt(G_ACC * p["h_bed"] * 0.5), 0.1)
         nu_now = max(self._max(f["nu_t"], 1), 1.0e-3)
@@ -284,9 +309,11 @@ class Tier3Solver:
         t = self.t
         ign = t < p["ignition_duration_s"]
         # --- 1. rho_prev, EoS, inlet O2 (spread_3d.py:1984-2050)
+        self._phase("eos")
         check(L.fs_eos(gp, ptr(f["rho"]), ptr(w["rho_prev"]), ptr(f["T_g"]), ptr(f["Y_O2"]),
                        p["T_amb"], s), "eos")
         # --- 2. Lagrangian bed (spread_3d.py:2064-2181)
+        self._phase("bed")
         bp = FsBedParams(dt, p["h_conv"], p["rho_solid_true"], p["cp_solid"], p["eps_solid"],
                          p["T_amb"], p["view_factor"], p["h_bed"], p["kappa_bed_eff"],
                          p["char_ox_flux_cap"], p["char_ox_ash_exp"], 1, 1, 1, 1,
@@ -304,6 +331,7 @@ class Tier3Solver:
                              ptr(self.seg_of_cell), s), "bed_hcond")
         Sp, Sd = self.bed_out["S_pyro"], self.bed_out["S_drying"]
         # --- 3/4. drag + tentative momentum (spread_3d.py:2223-2276)
+        self._phase("momentum")
         check(L.fs_tentative_velocity(gp, ptr(f["u"]), ptr(f["v"]), ptr(f["w"]), ptr(f["rho"]),
                                       ptr(f["T_g"]), None, None, None, ptr(f["alpha_s"]),
                                       p["sav"], p["canopy_C_d"], ptr(self.u_inlet),
@@ -314,6 +342,7 @@ class Tier3Solver:
         self._swap("v", "tmp2")
         self._swap("w", "tmp3")
         # --- 5. projection (spread_3d.py:2300-2360)
+        self._phase("projection")
         self._div_target(dt)
         check(L.fs_proj_rebuild(self.proj, ptr(f["rho"]), s), "proj_rebuild")
         n_it = 0
@@ -335,9 +364,11 @@ class Tier3Solver:
         d.proj_iters = n_it
         d.proj_div_max = div_max
         # --- 6. outflow sponge (spread_3d.py:2369)
+        self._phase("sponge")
         check(L.fs_outflow_sponge(gp, ptr(f["u"]), ptr(self.u_inlet), ptr(self.sigma_x),
                                   ptr(f["Y_fuel"]), 1.0e-3, dt, s), "sponge")
         # --- 7. k-epsilon (spread_3d.py:2409)
+        self._phase("k_eps")
         check(L.fs_k_epsilon(gp, ptr(f["k_turb"]), ptr(f["eps_turb"]), ptr(f["u"]), ptr(f["v"]),
                              ptr(f["w"]), ptr(f["T_g"]), ptr(f["alpha_s"]), ptr(self.u_inlet),
                              ptr(self.k_wall), ptr(self.eps_wall), ptr(w["tmp1"]),
@@ -347,6 +378,7 @@ class Tier3Solver:
         self._swap("eps_turb", "tmp2")
         self._swap("nu_t", "tmp3")
         # --- 8. DOM (every dom_subcycle_every steps) + soil (spread_3d.py:2472-2514)
+        self._phase("dom")
         if self.step_count % max(p["dom_subcycle_every"], 1) == 0:
             check(L.fs_bed_aggregate(_ctypes_ref(self.fs_parts), _ctypes_ref(self.fs_segs),
                                      ptr(w["M_local"]), 1, s), "bed_aggregate_M")
@@ -360,6 +392,7 @@ class Tier3Solver:
                              ptr(self.soil_dz), ptr(self.soil_da), ptr(self.soil_db), 0.48,
                              1500.0, 800.0, 0.85, p["T_amb"], s), "soil")
         # --- 9. ignition pulse on the top bed layer of the source strip (:2528-2532)
+        self._phase("misc")
         if ign and g.n_z_bed > 0:
             sl = w["q_rad"][g.n_z_bed - 1, :, p["i_src_start"]:p["i_src_end"]]
             sl += 240_000.0 * p["ignition_q_mult"]
@@ -368,21 +401,25 @@ class Tier3Solver:
         check(L.fs_active_count(self.n, ptr(w["omega"]), ptr(f["T_g"]), ptr(f["Y_fuel"]),
                                 ptr(self.active_count), None, s), "active_count")
         # --- 11. gas-temperature advection (:2648)
+        self._phase("gas_adv")
         check(L.fs_gas_energy_adv(gp, ptr(f["T_g"]), ptr(f["u"]), ptr(f["v"]), ptr(f["w"]),
                                   ptr(w["tmp1"]), dt, 2.0e-5, p["T_amb"], s), "gas_adv")
         self._swap("T_g", "tmp1")
         # --- 12. ten chemistry/transport sub-steps (:2678-3196)
+        self._phase("substeps")
         dt_sub = dt / N_SUB
         n_sc, dts_sc = self._nsub(SC_T, dt_sub)
         n_pr, dts_pr = self._nsub(PR_T, dt_sub)
         d.n_sub_sc, d.n_sub_pr = n_sc, n_pr
         drip = int(ign)
         for _sub in range(N_SUB):
+            self._phase("edc")
             check(L.fs_edc(self.n, ptr(f["rho"]), ptr(f["T_g"]), ptr(f["Y_fuel"]),
                            ptr(f["Y_O2"]), ptr(f["k_turb"]), ptr(f["eps_turb"]),
                            ptr(f["Y_H2O"]), ptr(w["omega"]), p["chi_rad"], 1100.0, dt_sub,
                            1, 1.3, 17_000_000.0, int(p["edc_extinction_enable"]),
                            ptr(self.edc_scratch), s), "edc")
+            self._phase("species")
             check(L.fs_species_sources(self.n, ptr(Sp), ptr(Sd), ptr(f["Y_fuel"]),
                                        ptr(f["Y_O2"]), ptr(f["Y_H2O"]), ptr(w["S_F"]),
                                        ptr(w["S_O2"]), ptr(w["S_H2O"]), s), "sources")
@@ -396,6 +433,7 @@ class Tier3Solver:
             self._swap("Y_fuel", "tmp1")
             self._swap("Y_O2", "tmp2")
             self._swap("Y_H2O", "tmp3")
+            self._phase("turb_diff_Y")
             check(L.fs_clip(self.n, ptr(f["Y_O2"]), 0.0, 0.232, s), "clip_O2")
             if n_sc > 0:
                 for q in range(n_sc):
@@ -409,15 +447,18 @@ class Tier3Solver:
                     self._swap("Y_fuel", "tmp1")
                     self._swap("Y_O2", "tmp2")
                     self._swap("Y_H2O", "tmp3")
+            self._phase("gas_update")
             check(L.fs_gas_energy_update(gp, ptr(f["T_g"]), ptr(f["rho"]), ptr(f["Y_H2O"]),
                                          ptr(f["T_s"]), ptr(Sp), ptr(Sd),
                                          ptr(self.bed_out["Q_g_conv"]), ptr(w["q_rad_gas"]),
                                          ptr(w["Q_comb"]), dt_sub, p["T_amb"], p["h_bed"],
                                          drip, g.n_z_bed, p["i_src_start"], p["i_src_end"], s),
                   "gas_update")
+            self._phase("solid_cond")
             check(L.fs_solid_conduction(gp, ptr(f["T_s"]), ptr(f["alpha_s"]), ptr(w["tmp4"]),
                                         0.20, 500.0, 1300.0, dt_sub, s), "solid_cond")
             self._swap("T_s", "tmp4")
+            self._phase("turb_diff_T")
             if n_pr > 0:
                 for q in range(n_pr):
                     last = q == n_pr - 1
@@ -430,6 +471,7 @@ class Tier3Solver:
                 check(L.fs_clip(self.n, ptr(f["T_g"]), p["T_amb"], T_CAP, s), "cap_Tg")
             check(L.fs_clip(self.n, ptr(f["T_s"]), p["T_amb"], T_CAP, s), "cap_Ts")
         # --- 13. level set (passive: v_n = 0, so evolve leaves phi; reinit every 10)
+        self._phase("levelset")
         self.lset_step += 1
         if self.lset_step % 10 == 0:
             self._reinit_levelset()
@@ -453,6 +495,7 @@ class Tier3Solver:
         if math.isfinite(fx) and fx > self.front_x[-1]:
             self.front_t.append(t)
             self.front_x.append(fx)
+        self._phase(None)
         self.t = t + dt
         d.t, d.dt = self.t, dt
         self.diag = d

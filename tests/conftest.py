@@ -14,6 +14,10 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
 
 
+INT_KEYS = ("nz", "ny", "nx", "n_z_bed", "n_per_cell", "n_max", "n_alloc", "n_sub",
+            "n_substeps", "drying_mode", "n_soil", "lambda_x", "n_iters")
+
+
 class Vectors:
     """Access to the reference's golden kernel vectors (tests/golden/kernel_vectors.npz)."""
 
@@ -33,6 +37,9 @@ class Vectors:
             if k.startswith(pre):
                 v = self.d[k]
                 out[k[len(pre):]] = v.item() if v.ndim == 0 else v
+        for k in INT_KEYS:
+            if k in out:
+                out[k] = int(out[k])
         return out
 
 
@@ -61,8 +68,8 @@ def ref_smoke():
 
 
 def rel_l2(a, b):
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
     den = np.linalg.norm(b.ravel())
     num = np.linalg.norm((a - b).ravel())
     if den == 0.0:
