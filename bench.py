@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark of the Tier-3 step: 3D solver cell-steps/s on B200.
+
+Workload: the 400 x 120 x 60 cell case (2.88M cells, dx = dy = 0.1 m,
+dz = 0.0625 m, DOM S8 with 80 ordinates, U10 = 6 m/s, moisture 0.06,
+rho_b = 0.35 kg/m^3, 16 bed particles per surface cell, seeded jitter), plain
+FP64 path, projection tolerance 1e-6 (the reference's production default).
+Synthetic initial state built from the case deck (no dataset exists for this
+solver).  Inputs exceed L2 (state ~0.7 GB + DOM intensities 1.84 GB), so no
+L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one process per GPU) every rank advances its own
+independent replica of the case ("replicas only": the single-case step does
+not shard); value = cell-steps/s summed over ranks, time = max over ranks.
+``--impl reference`` times the CPU restatement of the reference algorithm
+(oracle/) on the host on a bounded slice of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "3D solver cell-steps/s on 1 B200 (plain FP64 Tier-3 step)"
+UNIT = "cell-steps/s"
+WORKLOAD = "tier3_step_400x120x60_S8_fp64"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def start(self):
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(
+                        ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                         "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                        timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._th = threading.Thread(target=run, daemon=True)
+        self._th.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._th:
+            self._th.join(timeout=6)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _oracle_slice(case_nx, seed=0):
+    """Oracle state for the workload restricted to its first ``case_nx`` x-cells."""
+    from firewebapp_b200.cases import CFG2, scaled
+    from firewebapp_b200.grid import build_setup
+    from firewebapp_b200.quadrature import level_symmetric
+    from oracle.step import OracleState, geometry_from_setup
+    case = dict(scaled(CFG2, nx=case_nx), jitter_seed=seed)
+    su = build_setup(case)
+    snap = dict(su.fields)
+    snap["T_soil"] = su.soil["T"]
+    for k, v in su.particles.items():
+        snap["p_" + k] = v
+    om, wq = level_symmetric(8)
+    S = OracleState(snap, geometry_from_setup(su), su.params, om, wq)
+    S.proj_solver = "bicgstab"
+    S.proj_rtol = 1.0e-6
+    return S, su.grid.n_cells
+
+
+def cpu_sample(nx_slice=50, steps=1):
+    """Time the oracle port on a bounded slice (one or more outer steps)."""
+    from oracle.step import step
+    S, cells = _oracle_slice(nx_slice)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step(S)
+    el = time.perf_counter() - t0
+    return cells * steps / el, cells, el
+
+
+def _ref_worker(nx_slice, warmup, steps, seed, q):
+    """One host process: the oracle on its own slice replica (spawned)."""
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from oracle.step import step
+    S, cells = _oracle_slice(nx_slice, seed)
+    for _ in range(warmup):
+        step(S)
+    q.put(("ready", seed))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step(S)
+    q.put(("done", cells * steps, time.perf_counter() - t0))
+
+
+def run_reference_arm(args):
+    """The CPU restatement on the host cores: one spawned process per core
+    (capped), each stepping its own replica of an x-slice of the workload."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    nx_slice = int(os.environ.get("FIRE_REF_SLICE_NX", "25"))
+    try:
+        ncpu = len(os.sched_getaffinity(0))
+    except AttributeError:
+        ncpu = os.cpu_count() or 1
+    nproc = max(1, min(ncpu, int(os.environ.get("FIRE_REF_MAX_PROCS", "16"))))
+    for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[v] = "1"
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_ref_worker, args=(nx_slice, args.warmup, args.steps, r, q))
+             for r in range(nproc)]
+    for pr in procs:
+        pr.start()
+    work, times = 0, []
+    for _ in range(2 * nproc):
+        msg = q.get(timeout=3600)
+        if msg[0] == "done":
+            work += msg[1]
+            times.append(msg[2])
+    for pr in procs:
+        pr.join()
+    el = max(times)
+    value = work / el
+    cells = work // (nproc * args.steps)
+    sample = (f"{nproc} processes x {args.steps} outer steps, each on its own replica of the "
+              f"first {nx_slice} x-cells of the {WORKLOAD} case ({cells} cells), numpy "
+              f"oracle port, projection BiCGSTAB rtol 1e-6, value = all work / slowest process")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"x-slice of {nx_slice} cells",
+                   "parallelism": f"host x{nproc}"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--nx", type=int, default=None,
+                    help="run the workload cut to its first NX x-cells (profiling)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    from firewebapp_b200 import _lib
+    from firewebapp_b200.cases import CFG2
+    from firewebapp_b200.solver import Tier3Solver
+
+    case = dict(CFG2, jitter_seed=rank)
+    if args.nx:
+        from firewebapp_b200.cases import scaled
+        case = dict(scaled(CFG2, nx=args.nx), jitter_seed=rank)
+    solver = Tier3Solver(case, projection_cg_rtol=1.0e-6)
+    cells = solver.n
+    for _ in range(args.warmup):
+        solver.step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    # ---- timed region: device-resident state, CUDA events on the stream
+    solver.enable_kernel_timers(True)
+    lib = _lib.lib()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    n0 = lib.fs_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        solver.step()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = int(lib.fs_launch_count() - n0)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    kt = solver.kernel_times()
+    solver.enable_kernel_timers(False)
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ws * cells / (ms * 1e-3)
+
+    # ---- roofline of the dominant bracketed kernel
+    peak, peak_src = _peaks()
+    N = cells
+    M = solver.Omega.shape[0]
+    alg = {  # algorithmic bytes per launch (distinct fields read + written, 8 B each)
+        "dom_sweep": N * (8.0 * M + 16.0),
+        "species_transport": N * 8.0 * 12,
+        "edc": N * 8.0 * 11,
+        "turb_diffusion_Y": N * 8.0 * 7,
+        "momentum_drag": N * 8.0 * 10,
+        "k_epsilon": N * 8.0 * 14,
+        "gas_energy_adv": N * 8.0 * 5,
+    }
+    dom_k = max((k for k in kt if k in alg), key=lambda k: kt[k][0])
+    tot_ms, nl = kt[dom_k]
+    avg_ms = tot_ms / max(nl, 1)
+    achieved = alg[dom_k] / (avg_ms * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(dom_k)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": dom_k,
+                "peak_source": peak_src, "launches": nl, "avg_launch_ms": avg_ms,
+                "algorithmic_bytes_per_launch": alg[dom_k],
+                "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()}}
+
+    # ---- end to end through the public API: host state in, result out
+    e2e = None
+    if not args.no_e2e:
+        e2e = measure_e2e(case, args.steps, ws)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, c, el = cpu_sample(nx_slice=50, steps=1)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"1 outer step of the {WORKLOAD} case on its first 50 x-cells "
+                         f"({c} cells, {el:.1f} s), numpy oracle port, projection "
+                         f"BiCGSTAB rtol 1e-6"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD if not args.nx else
+                       f"tier3_step_{args.nx}x120x60_S8_fp64", "cells": cells, "ordinates": M,
+                       "parallelism": f"replicas{ws}", "l2": "inputs larger than L2",
+                       "projection_rtol": 1e-6},
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def measure_e2e(case, steps, ws):
+    """Cell-steps/s through the public host-buffer API: every step uploads the
+    caller's state (fields, particles, soil) from pinned host memory, advances
+    one outer step and downloads the state again; max time over ranks."""
+    import torch
+    from firewebapp_b200.api import run_3d_spread_gpu_e2e
+    res = run_3d_spread_gpu_e2e(case, steps)
+    sec = res["seconds"]
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([sec], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+    return {"value": ws * res["cells"] * steps / sec, "unit": UNIT,
+            "h2d_bytes_per_step": res["h2d_bytes"] / steps,
+            "d2h_bytes_per_step": res["d2h_bytes"] / steps}
+
+
+if __name__ == "__main__":
+    main()

@@ -54,6 +54,7 @@ _G = C.POINTER(FsGrid)
 SIGNATURES = {
     "fs_last_error": (C.c_char_p, []),
     "fs_version": (I, []),
+    "fs_launch_count": (C.c_ulonglong, []),
     "fs_species_transport": (I, [_G, I, PP, PP, PP, C.POINTER(D), P, P, P, P, D, D, P]),
     "fs_species_sources": (I, [I64, P, P, P, P, P, P, P, P, P]),
     "fs_advect_scalar_muscl": (I, [_G, P, P, P, P, P, D, P]),
@@ -86,6 +87,7 @@ SIGNATURES = {
     "fs_dom_solve": (I, [P, P, P, P, P, D, D, P, P, P, P, P, P, P, P]),
     "fs_dom_intensity": (P, [P]),
     "fs_dom_iterations": (I, [P]),
+    "fs_dom_sweep_timing": (I, [P, I, C.POINTER(D), C.POINTER(C.c_longlong)]),
     "fs_bed_step": (I, [_G, C.POINTER(FsBedParticles), C.POINTER(FsBedSegments),
                         C.POINTER(FsBedSources), C.POINTER(FsBedParams), P, P, P]),
     "fs_bed_aggregate": (I, [C.POINTER(FsBedParticles), C.POINTER(FsBedSegments), P, I, P]),
@@ -94,6 +96,7 @@ SIGNATURES = {
     "fs_levelset": (I, [_G, P, P, P, D, I, P]),
     "fs_active_count": (I, [I64, P, P, P, P, P, P]),
     "fs_field_max": (I, [_G, P, I, C.POINTER(D), P]),
+    "fs_field_max_multi": (I, [_G, I, PP, C.POINTER(I), C.POINTER(D), P, P]),
 }
 
 STATUS = {0: "ok", 1: "bad argument", 2: "non-finite value", 3: "solver did not converge",

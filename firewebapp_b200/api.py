@@ -1,0 +1,274 @@
+"""Public entry points of the Tier-3 drop-in.
+
+``run_3d_spread_gpu`` is the production mode of the boundary: it takes a case
+(the deck keys ``cases.py`` names, plus the wind speed), runs the
+``run_3d_spread`` loop (``spread_3d.py:1897-3683``) device-resident, records
+the per-step diagnostics the reference appends (``spread_3d.py:3503-3512``)
+and returns a :class:`Spread3DResultGPU` whose ``save`` writes the same
+``.npz`` keys as ``Spread3DResult.save`` (``spread_3d.py:460-511``).
+
+``HostStepper`` is the kernel-level mode: the caller owns the state in host
+memory (as the reference's caller owns its numpy arrays,
+``spread_3d.py:1529-1580``) and each ``step`` uploads it, advances one outer
+step and downloads it again.  The persistent solver objects (projection
+warm-start pressure, DOM intensities) stay on the device, as the reference's
+``ProjectionSolver3D`` and ``DOMRadiationSolver`` keep them
+(``projection_3d.py:755,791``, ``dom_3d.py:286-300``).
+"""
+from __future__ import annotations
+
+import json
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from ._lib import check, ptr, ptr_array
+from .solver import Tier3Solver, _ctypes_double
+
+HOC_J = 1.7e7            # heat of combustion, _constants.py:36
+T_IGN_ROS = 600.0        # _cheney_phase16_worker.py:208-231 ignition threshold
+
+
+@dataclass
+class Spread3DResultGPU:
+    """Fields of ``Spread3DResult`` (``spread_3d.py:425-451``) for a GPU run."""
+    ros_m_s: float
+    n_cells_ignited: int
+    front_t: list
+    front_x: list
+    grid: object
+    state_final: dict
+    diag_t: list = field(default_factory=list)
+    diag_Tg_max: list = field(default_factory=list)
+    diag_Ts_max: list = field(default_factory=list)
+    diag_Sp_max: list = field(default_factory=list)
+    diag_Qc_max: list = field(default_factory=list)
+    diag_omega_max: list = field(default_factory=list)
+    diag_Y_max: list = field(default_factory=list)
+    diag_n_ign: list = field(default_factory=list)
+    diag_proj_div_max: list = field(default_factory=list)
+    diag_proj_n_iter: list = field(default_factory=list)
+    k_turb_final: np.ndarray | None = None
+    eps_turb_final: np.ndarray | None = None
+    nu_t_final: np.ndarray | None = None
+    ros_Ts: float | None = None
+    hrrpua_peak: float | None = None
+
+    def save(self, path, metadata=None):
+        """Write the ``Spread3DResult.save`` key set (``spread_3d.py:460-511``).
+
+        State arrays the Lagrangian production path does not carry (p_dyn,
+        Y_CO and the Eulerian component masses) are written as zeros, which
+        is what they hold in the reference for this path."""
+        path = Path(path)
+        if not str(path).endswith(".npz"):
+            path = path.with_suffix(".npz")
+        path.parent.mkdir(parents=True, exist_ok=True)
+        g, s = self.grid, self.state_final
+        z = np.zeros(g.shape)
+        np.savez_compressed(
+            path,
+            _meta_json=np.array(json.dumps({
+                "ros_m_s": float(self.ros_m_s), "n_cells_ignited": int(self.n_cells_ignited),
+                "Nx": int(g.Nx), "Ny": int(g.Ny), "Nz": int(g.Nz), "dx": float(g.dx),
+                "dy": float(g.dy), "dz": float(g.dz), "Lx": float(g.Lx), "Ly": float(g.Ly),
+                "Lz": float(g.Lz), "n_z_bed": int(g.n_z_bed), "user": metadata or {}})),
+            x_mid=g.x_mid, y_mid=g.y_mid, z_mid=g.z_mid, dz_arr=g.dz_arr,
+            inv_dz_arr=1.0 / g.dz_arr, z_face=g.z_face, d_face_above=g.d_face_above,
+            d_face_below=g.d_face_below,
+            rho=s["rho"], u=s["u"], v=s["v"], w=s["w"], p_dyn=s.get("p_prev", z),
+            T_g=s["T_g"], Y_fuel=s["Y_fuel"], Y_O2=s["Y_O2"], Y_H2O=s["Y_H2O"], Y_CO=z,
+            alpha_s=s["alpha_s"], T_s=s["T_s"], m_hemi=z, m_cell=z, m_lign=z, m_char=z,
+            front_t=np.array(self.front_t), front_x=np.array(self.front_x),
+            diag_t=np.array(self.diag_t), diag_Tg_max=np.array(self.diag_Tg_max),
+            diag_Ts_max=np.array(self.diag_Ts_max), diag_Sp_max=np.array(self.diag_Sp_max),
+            diag_Qc_max=np.array(self.diag_Qc_max),
+            diag_omega_max=np.array(self.diag_omega_max),
+            diag_Y_max=np.array(self.diag_Y_max), diag_n_ign=np.array(self.diag_n_ign))
+        return path
+
+
+def compute_steady_ros(front_t, front_x, t_end, source_x, domain_m):
+    """``_compute_steady_ros`` (``spread_3d.py:3792-3824``)."""
+    if len(front_t) < 2:
+        return 0.0
+    if front_x[-1] - source_x < 0.1:
+        return 0.0
+    if t_end - front_t[-1] > 30.0 and not front_x[-1] > domain_m * 0.7:
+        return 0.0
+    t0 = float(front_t[0])
+    if t_end > t0:
+        return float((front_x[-1] - front_x[0]) / (t_end - t0))
+    return 0.0
+
+
+def ros_from_snapshots(times, x_lead):
+    """ROS_Ts: least-squares slope of the leading x with T_s >= 600 K over
+    the snapshots with t >= 1 s (``_cheney_phase16_worker.py:208-231``)."""
+    t = np.asarray(times, dtype=np.float64)
+    x = np.asarray(x_lead, dtype=np.float64)
+    ok = (t >= 1.0) & np.isfinite(x)
+    if ok.sum() < 2:
+        return float("nan")
+    return float(np.polyfit(t[ok], x[ok], 1)[0])
+
+
+class _Diag:
+    """Per-step maxima of ``spread_3d.py:3503-3512`` on the device."""
+
+    def __init__(self, solver: Tier3Solver):
+        self.s = solver
+        self.sp = torch.empty_like(solver.f["rho"])
+        self.col = torch.empty(solver.shape, dtype=torch.float64, device=solver.dev)
+
+    def record(self, res: Spread3DResultGPU):
+        s = self.s
+        torch.add(s.bed_out["S_pyro"], s.bed_out["S_drying"], out=self.sp)
+        m = s._maxes([s.f["T_g"], s.f["T_s"], self.sp, s.w["Q_comb"], s.w["omega"],
+                      s.f["Y_fuel"]], [1, 1, 1, 1, 1, 1])
+        n_ign = int((s.f["T_s"] >= s.p["T_ign"]).sum().item())
+        res.diag_t.append(s.t)
+        res.diag_Tg_max.append(m[0])
+        res.diag_Ts_max.append(m[1])
+        res.diag_Sp_max.append(m[2])
+        res.diag_Qc_max.append(m[3])
+        res.diag_omega_max.append(m[4])
+        res.diag_Y_max.append(m[5])
+        res.diag_n_ign.append(n_ign)
+        res.diag_proj_div_max.append(s.diag.proj_div_max)
+        res.diag_proj_n_iter.append(len(s.diag.proj_iters))
+
+    def lead_x_Ts(self):
+        """Largest cell-centre x with any T_s >= 600 K, or NaN."""
+        s = self.s
+        hot = (s.f["T_s"] >= T_IGN_ROS).any(dim=0).any(dim=0)
+        idx = torch.nonzero(hot)
+        if idx.numel() == 0:
+            return float("nan")
+        return (float(idx.max().item()) + 0.5) * s.grid.dx
+
+    def hrrpua_x(self):
+        """HRRPUA(x) = (1/Ly) sum_{j,k} omega * HOC_J * dz_k * dy  [W/m^2]."""
+        s = self.s
+        w = s.w["omega"] * s.dz_t.view(-1, 1, 1)
+        return (w.sum(dim=(0, 1)) * HOC_J * s.grid.dy / s.grid.Ly)
+
+
+def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | None = None,
+                      snapshot_every_s: float = 1.0, device="cuda",
+                      projection_cg_rtol: float = 1.0e-6) -> Spread3DResultGPU:
+    """Device-resident ``run_3d_spread`` for a case; stops at ``n_steps``
+    outer steps, at ``t_end`` simulated seconds or at the reference's own
+    exit tests, whichever comes first."""
+    if n_steps is None and t_end is None:
+        raise ValueError("run_3d_spread_gpu needs n_steps or t_end")
+    s = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol)
+    try:
+        g = s.grid
+        res = Spread3DResultGPU(ros_m_s=0.0, n_cells_ignited=0, front_t=s.front_t,
+                                front_x=s.front_x, grid=g, state_final={})
+        dg = _Diag(s)
+        snap_t, snap_x = [], []
+        next_snap = snapshot_every_s
+        hrr_peak = 0.0
+        k = 0
+        while True:
+            if n_steps is not None and k >= n_steps:
+                break
+            if t_end is not None and s.t >= t_end:
+                break
+            if not s.step():
+                break
+            k += 1
+            dg.record(res)
+            hrr_peak = max(hrr_peak, float(dg.hrrpua_x().max().item()))
+            if s.t >= next_snap:
+                snap_t.append(s.t)
+                snap_x.append(dg.lead_x_Ts())
+                next_snap += snapshot_every_s
+        st = s.state()
+        res.state_final = st
+        res.k_turb_final = st["k_turb"]
+        res.eps_turb_final = st["eps_turb"]
+        res.nu_t_final = st["nu_t"]
+        res.n_cells_ignited = int(np.sum(st["T_s"] >= s.p["T_ign"]))
+        res.ros_m_s = compute_steady_ros(s.front_t, s.front_x, s.t,
+                                         source_x=s.p["i_src_end"] * g.dx, domain_m=g.Lx)
+        res.ros_Ts = ros_from_snapshots(snap_t, snap_x)
+        res.hrrpua_peak = hrr_peak
+        return res
+    finally:
+        s.close()
+
+
+class HostStepper:
+    """Outer steps on state owned by the caller in (pinned) host memory."""
+
+    FIELDS = Tier3Solver.FIELDS
+    WORK = ("omega", "q_rad", "q_rad_gas")
+    PARTS = ("x", "y", "z", "alive", "m_solid", "m_water", "m_char", "T_s", "m_water_0",
+             "sav", "m_char_max")
+
+    def __init__(self, case: dict, device="cuda", projection_cg_rtol: float = 1.0e-6):
+        self.solver = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol)
+        s = self.solver
+        self.host = {}
+        for k in self.FIELDS:
+            self.host[k] = s.f[k].cpu().pin_memory()
+        for k in self.WORK:
+            self.host[k] = s.w[k].cpu().pin_memory()
+        self.host["T_soil"] = s.T_soil.cpu().pin_memory()
+        for k in self.PARTS:
+            self.host["p_" + k] = s.part[k].cpu().pin_memory()
+
+    def _dev(self, k):
+        s = self.solver
+        if k in self.FIELDS:
+            return s.f[k]
+        if k in self.WORK:
+            return s.w[k]
+        if k == "T_soil":
+            return s.T_soil
+        return s.part[k[2:]]
+
+    def bytes_per_transfer(self):
+        return sum(t.numel() * t.element_size() for t in self.host.values())
+
+    def step(self):
+        """Upload the host state, advance one outer step, download it."""
+        for k, h in self.host.items():
+            self._dev(k).copy_(h, non_blocking=True)
+        alive = self.solver.step()
+        for k, h in self.host.items():
+            h.copy_(self._dev(k), non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return alive
+
+    def close(self):
+        self.solver.close()
+
+
+def run_3d_spread_gpu_e2e(case: dict, steps: int, warmup: int = 1,
+                          projection_cg_rtol: float = 1.0e-6):
+    """Time ``steps`` host-buffer outer steps (uploads and downloads inside
+    the timed region), after ``warmup`` untimed ones."""
+    hs = HostStepper(case, projection_cg_rtol=projection_cg_rtol)
+    try:
+        for _ in range(warmup):
+            hs.step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            hs.step()
+        e1.record()
+        torch.cuda.synchronize()
+        nb = hs.bytes_per_transfer()
+        return {"cells": hs.solver.n, "seconds": e0.elapsed_time(e1) * 1e-3,
+                "h2d_bytes": nb * steps, "d2h_bytes": nb * steps}
+    finally:
+        hs.close()

@@ -268,8 +268,8 @@ int launch_bed_step(const GridDev& g, const BedPartH& ph, const BedSegH& sh, con
   B.n_z_bed = bp.n_z_bed; B.i_src0 = bp.i_src0; B.i_src1 = bp.i_src1; B.drip_on = bp.drip_on;
   B.q_rad = bp.q_rad; B.Qsx = bp.Qsx;
   if (!B.q_rad && !B.Qsx) return FS_EARG;
-  if (S.nseg > 0)
-    k_bed_step<<<blocks_for(S.nseg, 128), 128, 0, st>>>(g, P, S, O, B, Tg, YO2);
+  if (S.nseg > 0) {
+    k_bed_step<<<blocks_for(S.nseg, 128), 128, 0, st>>>(g, P, S, O, B, Tg, YO2); fs_count_launch(); }
   return cuda_status();
 }
 
@@ -305,7 +305,8 @@ int launch_bed_aggregate(const BedPartH& ph, const BedSegH& sh, double* out, int
   BedPart P{ph.x, ph.y, ph.z, ph.alive, ph.m_solid, ph.m_water, ph.m_char, ph.T_s, ph.m_water_0,
             ph.sav, ph.m_char_max};
   BedSeg S{sh.nseg, sh.seg_start, sh.seg_cell, sh.perm};
-  if (S.nseg > 0) k_bed_aggregate<<<blocks_for(S.nseg, 128), 128, 0, st>>>(P, S, out, mode);
+  if (S.nseg > 0) {
+    k_bed_aggregate<<<blocks_for(S.nseg, 128), 128, 0, st>>>(P, S, out, mode); fs_count_launch(); }
   return cuda_status();
 }
 
@@ -361,6 +362,6 @@ int launch_bed_hcond(const GridDev& g, double* T_grid, double* scratch, const do
   double diff = k_solid / (rho_true * cp_solid);
   k_bed_hcond<<<L.grid, L.block, 0, st>>>(g, scratch, T_grid, as, nzb, diff,
                                           1.0 / (g.dx * g.dx), 1.0 / (g.dy * g.dy), dt, P, S,
-                                          seg_of_cell);
+                                          seg_of_cell); fs_count_launch();
   return cuda_status();
 }

@@ -5,7 +5,12 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <atomic>
+
 static thread_local char g_err[512] = "";
+static std::atomic<unsigned long long> g_launches{0};
+
+void fs_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void fs_set_error(const char* fmt, ...) {
   va_list ap;
@@ -50,6 +55,7 @@ extern "C" {
 
 const char* fs_last_error(void) { return g_err; }
 int fs_version(void) { return 1; }
+unsigned long long fs_launch_count(void) { return g_launches.load(); }
 
 int fs_species_transport(const FsGrid* g, int nspec, const double* const* Y, double* const* Y_out,
                          const double* const* S, const double* Y_inlet, const double* rho,
@@ -105,6 +111,24 @@ int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, voi
   cudaFreeAsync(dres, ST(stream));
   if (cudaStreamSynchronize(ST(stream)) != cudaSuccess) return check(FS_ECUDA, "fs_field_max");
   return FS_OK;
+}
+
+int fs_field_max_multi(const FsGrid* g, int nf, const double* const* f, const int* modes,
+                       double* results, void* scratch, void* stream) {
+  GRID("fs_field_max_multi");
+  if (nf < 1 || nf > 16 || !scratch) return FS_EARG;
+  unsigned long long* key = (unsigned long long*)scratch;
+  double* dres = (double*)(key + 16);
+  int mask2 = 0;
+  for (int q = 0; q < nf; ++q)
+    if (modes[q] == 2) mask2 |= 1 << q;
+  launch_init_keys(key, nf, mask2, ST(stream));
+  for (int q = 0; q < nf; ++q) launch_max(gd, f[q], modes[q], key + q, ST(stream));
+  launch_keys_to_double(key, dres, nf, ST(stream));
+  cudaMemcpyAsync(results, dres, sizeof(double) * nf, cudaMemcpyDeviceToHost, ST(stream));
+  if (cudaStreamSynchronize(ST(stream)) != cudaSuccess)
+    return check(FS_ECUDA, "fs_field_max_multi");
+  return check(cuda_status(), "fs_field_max_multi");
 }
 
 int fs_turb_diffusion_nsub(const FsGrid* g, const double* nu_t, double sc_t, double dt,
@@ -320,6 +344,13 @@ int fs_dom_solve(void* handle, const double* T_s, const double* T_g, const doubl
 }
 
 double* fs_dom_intensity(void* handle) { return handle ? dom_intensity(handle) : nullptr; }
+
+int fs_dom_sweep_timing(void* handle, int enable, double* total_ms, long long* sweeps) {
+  if (!handle) return FS_EARG;
+  if (enable >= 0) dom_set_timing(handle, enable);
+  if (total_ms && sweeps) dom_sweep_stats(handle, total_ms, sweeps);
+  return FS_OK;
+}
 int fs_dom_iterations(void* handle) { return handle ? dom_last_iters(handle) : -1; }
 
 int fs_bed_step(const FsGrid* g, const FsBedParticles* p, const FsBedSegments* s,

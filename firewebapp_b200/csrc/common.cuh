@@ -83,3 +83,6 @@ inline int cuda_status() {
 
 // Per-thread error text for fs_last_error().
 void fs_set_error(const char* fmt, ...);
+
+// Count of kernel launches issued by this library (fs_launch_count()).
+void fs_count_launch();

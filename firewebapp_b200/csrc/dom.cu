@@ -32,6 +32,11 @@ struct DomCtx {
   double eps_w, tol, relax, kgmax;
   int max_iter;
   int last_iters;
+  // optional per-sweep timing (CUDA events on the launching stream)
+  int timing;
+  cudaEvent_t ev0[32], ev1[32];
+  double sweep_ms;
+  long long sweep_count;
 };
 
 __device__ __forceinline__ double clip01(double x) {
@@ -131,6 +136,66 @@ __global__ void k_dom_plane(GridDev g, SweepArgs a) {
   I[c] = num / den;
 }
 
+// One thread block sweeps one ordinate over the whole grid in hyperplane order.
+// In sweep coordinates (i',j',k') every upwind neighbour of a cell on plane d
+// lies on plane d-1 in the same (k',j') pencil (x), the (k',j'-1) pencil (y)
+// or the (k'-1,j') pencil (z), so the block keeps, for every pencil, its value
+// on the previous plane in shared memory (double buffered: plane d writes the
+// buffer plane d-2 used).  Only the y-periodic inflow of the first row reads
+// global memory: the previous sweep's value at the far end of the row, which
+// this sweep overwrites only on a later plane.
+__global__ void __launch_bounds__(1024) k_dom_sweep_block(GridDev g, SweepArgs a) {
+  extern __shared__ double sh[];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int npen = ny * nz;
+  double* bufA = sh;
+  double* bufB = sh + npen;
+  const int n = blockIdx.x;
+  const double xi = a.ox[n], eta = a.oy[n], mu = a.oz[n];
+  const bool fx = xi >= 0.0, fy = eta >= 0.0, fz = mu >= 0.0;
+  const double ix = fabs(xi) * a.inv_dx;
+  const double iy = fabs(eta) * a.inv_dy;
+  const double amu = fabs(mu);
+  const int64_t N = ncells_dev(g);
+  double* I = a.I + (int64_t)n * N;
+  const int64_t sy = nx;
+  const int nplanes = nx + ny + nz - 2;
+  for (int d = 0; d < nplanes; ++d) {
+    double* cur = (d & 1) ? bufB : bufA;
+    const double* prev = (d & 1) ? bufA : bufB;
+    // pencils on this plane: k' in [kp0, kp1], j' such that 0 <= d-j'-k' < nx
+    const int kp0 = max(0, d - (nx - 1) - (ny - 1));
+    const int kp1 = min(nz - 1, d);
+    for (int q = kp0 * ny + threadIdx.x; q <= kp1 * ny + ny - 1; q += blockDim.x) {
+      const int kp = q / ny;
+      const int jp = q - kp * ny;
+      const int ip = d - jp - kp;
+      if (ip < 0 || ip >= nx) continue;
+      const int i = fx ? ip : nx - 1 - ip;
+      const int j = fy ? jp : ny - 1 - jp;
+      const int k = fz ? kp : nz - 1 - kp;
+      const int64_t c = cidx(g, k, j, i);
+      const double Ix = ip > 0 ? prev[q] : a.I_amb;
+      double Iy;
+      if (jp > 0) Iy = prev[q - 1];
+      else Iy = a.periodic ? I[c + (fy ? (int64_t)(ny - 1) * sy : -(int64_t)(ny - 1) * sy)]
+                           : a.I_amb;
+      double Iz;
+      if (kp > 0) Iz = prev[q - ny];
+      else if (fz) Iz = mu > 0.0 ? a.Ig[(int64_t)j * nx + i] : 0.0;
+      else Iz = a.I_amb;
+      const double iz = amu / g.dz[k];
+      const double kap = a.ksafe[c];
+      const double num = kap * a.B[c] + ix * Ix + iy * Iy + iz * Iz;
+      const double den = kap + ix + iy + iz;
+      const double v = num / den;
+      cur[q] = v;
+      I[c] = v;
+    }
+    __syncthreads();
+  }
+}
+
 // G = sum_n w_n I_n (ordinate order); also max G and max |G - G_prev|
 __global__ void k_dom_G(int64_t N, int M, const double* __restrict__ w,
                         const double* __restrict__ I, double* G, const double* __restrict__ Gp,
@@ -226,6 +291,11 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   cudaMallocHost(&D->h_keys, sizeof(unsigned long long) * 4);
   D->eps_w = 0.85; D->tol = 1.0e-3; D->relax = 0.7; D->kgmax = kgmax; D->max_iter = 30;
   D->last_iters = 0;
+  D->timing = 0; D->sweep_ms = 0.0; D->sweep_count = 0;
+  for (int q = 0; q < 32; ++q) {
+    cudaEventCreate(&D->ev0[q]);
+    cudaEventCreate(&D->ev1[q]);
+  }
   if (cudaGetLastError() != cudaSuccess) {
     dom_destroy(D);
     return nullptr;
@@ -240,7 +310,24 @@ void dom_destroy(void* h) {
   cudaFree(D->G); cudaFree(D->Gp); cudaFree(D->ks); cudaFree(D->kg); cudaFree(D->ksafe);
   cudaFree(D->B); cudaFree(D->Ig_out); cudaFree(D->Isoil); cudaFree(D->qin); cudaFree(D->keys);
   cudaFreeHost(D->h_keys);
+  for (int q = 0; q < 32; ++q) {
+    cudaEventDestroy(D->ev0[q]);
+    cudaEventDestroy(D->ev1[q]);
+  }
   delete D;
+}
+
+void dom_set_timing(void* h, int on) {
+  DomCtx* D = (DomCtx*)h;
+  D->timing = on;
+  D->sweep_ms = 0.0;
+  D->sweep_count = 0;
+}
+
+void dom_sweep_stats(void* h, double* ms, long long* count) {
+  DomCtx* D = (DomCtx*)h;
+  *ms = D->sweep_ms;
+  *count = D->sweep_count;
 }
 
 double* dom_intensity(void* h) { return ((DomCtx*)h)->I; }
@@ -263,10 +350,10 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   const int M = D->M;
   const double Tamb4 = pow(T_amb, 4.0);
   k_dom_setup<<<blocks_for(N, 256), 256, 0, st>>>(g, Ts, Tg, as, om, YH, rho, Mloc, sigma, Tamb4,
-                                                  D->kgmax, D->ks, D->kg, D->ksafe, D->B);
+                                                  D->kgmax, D->ks, D->kg, D->ksafe, D->B); fs_count_launch();
   const double I_amb = SIGMA_SB_D * Tamb4 / PI_D;
   k_dom_ground_init<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, Tsoil0, D->eps_w, I_amb, D->Isoil,
-                                                        D->Ig_out);
+                                                        D->Ig_out); fs_count_launch();
   SweepArgs a{};
   a.ox = D->ox; a.oy = D->oy; a.oz = D->oz; a.I = D->I; a.ksafe = D->ksafe; a.B = D->B;
   a.Ig = D->Ig_out; a.I_amb = I_amb; a.inv_dx = 1.0 / g.dx; a.inv_dy = 1.0 / g.dy; a.M = M;
@@ -275,18 +362,32 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   const int64_t nthr = (int64_t)g.ny * g.nz * M;
   const double refl = (1.0 - D->eps_w) / PI_D;
   int it;
+  const size_t smem = sizeof(double) * 2 * (size_t)g.ny * g.nz;
+  int max_smem = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const bool block_sweep = smem <= (size_t)max_smem;
+  if (block_sweep)
+    cudaFuncSetAttribute(k_dom_sweep_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
   for (it = 0; it < D->max_iter; ++it) {
     std::swap(D->G, D->Gp);
-    for (int d = 0; d < nplanes; ++d) {
-      a.plane = d;
-      k_dom_plane<<<blocks_for(nthr, 256), 256, 0, st>>>(g, a);
+    if (block_sweep) {
+      if (D->timing) cudaEventRecord(D->ev0[it], st);
+      k_dom_sweep_block<<<M, 1024, smem, st>>>(g, a); fs_count_launch();
+      if (D->timing) cudaEventRecord(D->ev1[it], st);
+    } else {
+      for (int d = 0; d < nplanes; ++d) {
+        a.plane = d;
+        k_dom_plane<<<blocks_for(nthr, 256), 256, 0, st>>>(g, a); fs_count_launch();
+      }
     }
     cudaMemsetAsync(D->keys, 0, sizeof(unsigned long long) * 2, st);
     unsigned nb = blocks_for(N, 256);
     if (nb > 1184) nb = 1184;
-    k_dom_G<<<nb, 256, 0, st>>>(N, M, D->w, D->I, D->G, D->Gp, D->keys);
+    k_dom_G<<<nb, 256, 0, st>>>(N, M, D->w, D->I, D->G, D->Gp, D->keys); fs_count_launch();
     k_dom_ground<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, M, D->oz, D->w, D->I, N, D->Isoil,
-                                                      refl, D->relax, D->Ig_out, D->qin);
+                                                      refl, D->relax, D->Ig_out, D->qin); fs_count_launch();
     if (it > 0) {
       cudaMemcpyAsync(D->h_keys, D->keys, sizeof(unsigned long long) * 2, cudaMemcpyDeviceToHost,
                       st);
@@ -299,9 +400,18 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
     }
   }
   D->last_iters = it;
+  if (D->timing && block_sweep) {
+    cudaEventSynchronize(D->ev1[it - 1]);
+    for (int q = 0; q < it; ++q) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, D->ev0[q], D->ev1[q]);
+      D->sweep_ms += ms;
+      D->sweep_count += 1;
+    }
+  }
   k_dom_finish<<<blocks_for(N, 256), 256, 0, st>>>(g, D->ks, D->kg, D->ksafe, D->B, D->G, q_solid,
-                                                   q_gas);
-  if (q_in_soil)
-    k_scale2<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, D->qin, D->eps_w, q_in_soil);
+                                                   q_gas); fs_count_launch();
+  if (q_in_soil) {
+    k_scale2<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, D->qin, D->eps_w, q_in_soil); fs_count_launch(); }
   return cuda_status();
 }

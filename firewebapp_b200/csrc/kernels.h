@@ -98,6 +98,8 @@ void dom_destroy(void* h);
 double* dom_intensity(void* h);
 double* dom_G(void* h);
 int dom_last_iters(void* h);
+void dom_set_timing(void* h, int on);
+void dom_sweep_stats(void* h, double* ms, long long* count);
 int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, const double* om,
               double sigma, double T_amb, const double* Tsoil0, const double* YH, const double* rho,
               const double* Mloc, double* q_solid, double* q_gas, double* q_in_soil,

@@ -74,7 +74,7 @@ __global__ void k_levelset(GridDev g, const double* __restrict__ phi, const doub
 int launch_levelset(const GridDev& g, const double* phi, const double* aux, double* out,
                     double coef, int mode, cudaStream_t st) {
   Launch3 L = launch_cells(g);
-  k_levelset<<<L.grid, L.block, 0, st>>>(g, phi, aux, out, coef, mode, 1.0 / g.dx, 1.0 / g.dy);
+  k_levelset<<<L.grid, L.block, 0, st>>>(g, phi, aux, out, coef, mode, 1.0 / g.dx, 1.0 / g.dy); fs_count_launch();
   return cuda_status();
 }
 
@@ -95,6 +95,6 @@ __global__ void k_active_count(int64_t n, const double* __restrict__ om,
 
 int launch_active_count(int64_t n, const double* om, const double* Tg, const double* YF,
                         unsigned long long* count, unsigned char* mask, cudaStream_t st) {
-  k_active_count<<<blocks_for(n, 256), 256, 0, st>>>(n, om, Tg, YF, count, mask);
+  k_active_count<<<blocks_for(n, 256), 256, 0, st>>>(n, om, Tg, YF, count, mask); fs_count_launch();
   return cuda_status();
 }

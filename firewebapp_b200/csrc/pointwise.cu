@@ -182,8 +182,8 @@ int launch_edc(int64_t n, const double* rho, double* Tg, double* Yf, double* YO,
   int64_t nb = (n + EDC_BLK - 1) / EDC_BLK;
   signed char* agg = (signed char*)scratch;
   signed char* carry = agg + nb;
-  k_edc_agg<<<(unsigned)nb, EDC_BLK, 0, st>>>(n, Yf, YO, YH, agg);
-  k_edc_carry<<<1, 32, 0, st>>>((int)nb, agg, carry, nullptr);
+  k_edc_agg<<<(unsigned)nb, EDC_BLK, 0, st>>>(n, Yf, YO, YH, agg); fs_count_launch();
+  k_edc_carry<<<1, 32, 0, st>>>((int)nb, agg, carry, nullptr); fs_count_launch();
   EdcArgs a{};
   a.rho = rho; a.Tg = Tg; a.Yf = Yf; a.YO = YO; a.kt = kt; a.et = et; a.YH = YH;
   a.omega = omega; a.carry = carry;
@@ -192,7 +192,7 @@ int launch_edc(int64_t n, const double* rho, double* Tg, double* Yf, double* YO,
   a.nsub = n_substeps > 1 ? n_substeps : 1;
   a.relax = 1.0 - exp(-(dt / (double)a.nsub) / 0.5);
   a.extinction = extinction;
-  k_edc_main<<<(unsigned)nb, EDC_BLK, 0, st>>>(n, a);
+  k_edc_main<<<(unsigned)nb, EDC_BLK, 0, st>>>(n, a); fs_count_launch();
   return cuda_status();
 }
 
@@ -262,7 +262,7 @@ int launch_gas_update(const GridDev& g, double* Tg, const double* rho, const dou
   a.q_drip_gas = (1.0 - 0.80) * q_drip;
   a.drip_on = drip_on; a.n_z_bed = n_z_bed; a.i_src0 = i_src0; a.i_src1 = i_src1;
   Launch3 L = launch_cells(g);
-  k_gas_update<<<L.grid, L.block, 0, st>>>(g, a);
+  k_gas_update<<<L.grid, L.block, 0, st>>>(g, a); fs_count_launch();
   return cuda_status();
 }
 
@@ -288,7 +288,7 @@ __global__ void k_eos(GridDev g, double* rho, double* rho_prev, const double* __
 int launch_eos(const GridDev& g, double* rho, double* rho_prev, const double* Tg, double* YO,
                double P0, double R_air, double T_amb, cudaStream_t st) {
   Launch3 L = launch_cells(g);
-  k_eos<<<L.grid, L.block, 0, st>>>(g, rho, rho_prev, Tg, YO, P0, R_air, T_amb);
+  k_eos<<<L.grid, L.block, 0, st>>>(g, rho, rho_prev, Tg, YO, P0, R_air, T_amb); fs_count_launch();
   return cuda_status();
 }
 
@@ -303,7 +303,7 @@ __global__ void k_clip(int64_t n, double* f, double lo, double hi) {
 }
 
 int launch_clip(int64_t n, double* f, double lo, double hi, cudaStream_t st) {
-  k_clip<<<blocks_for(n, 256), 256, 0, st>>>(n, f, lo, hi);
+  k_clip<<<blocks_for(n, 256), 256, 0, st>>>(n, f, lo, hi); fs_count_launch();
   return cuda_status();
 }
 
@@ -348,12 +348,12 @@ int launch_max(const GridDev& g, const double* f, int mode, unsigned long long* 
   int64_t n = ncells(g);
   unsigned nb = blocks_for(n, 256);
   if (nb > 148 * 8) nb = 148 * 8;
-  k_max<<<nb, 256, 0, st>>>(g, f, mode, out_key);
+  k_max<<<nb, 256, 0, st>>>(g, f, mode, out_key); fs_count_launch();
   return cuda_status();
 }
 
 int launch_init_keys(unsigned long long* out, int n, int mode2_mask, cudaStream_t st) {
-  k_init_keys<<<1, 64, 0, st>>>(out, n, mode2_mask);
+  k_init_keys<<<1, 64, 0, st>>>(out, n, mode2_mask); fs_count_launch();
   return cuda_status();
 }
 
@@ -363,6 +363,6 @@ __global__ void k_keys_to_double(const unsigned long long* in, double* out, int 
 }
 
 int launch_keys_to_double(const unsigned long long* in, double* out, int n, cudaStream_t st) {
-  k_keys_to_double<<<1, 64, 0, st>>>(in, out, n);
+  k_keys_to_double<<<1, 64, 0, st>>>(in, out, n); fs_count_launch();
   return cuda_status();
 }

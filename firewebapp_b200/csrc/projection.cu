@@ -580,21 +580,21 @@ int proj_rebuild(void* h, const double* rho, cudaStream_t st) {
   MGLevel& l0 = P->lev[0];
   Launch3 L = launch_cells(g);
   k_proj_level0<<<L.grid, L.block, 0, st>>>(g, rho, P->ir, l0.gx, l0.gy, l0.gz, l0.e,
-                                            g.dx * g.dx, g.dy * g.dy);
+                                            g.dx * g.dx, g.dy * g.dy); fs_count_launch();
   for (int l = 0; l < P->nlev; ++l) {
     MGLevel& f = P->lev[l];
     if (l > 0) {
       MGLevel& pf = P->lev[l - 1];
       k_mg_coarsen<<<blocks_for(f.n, 128), 128, 0, st>>>(pf.nx, pf.ny, pf.nz, pf.gx, pf.gy, pf.gz,
                                                         pf.e, f.nx, f.ny, f.nz, f.gx, f.gy, f.gz,
-                                                        f.e, 0.5);
+                                                        f.e, 0.5); fs_count_launch();
     }
     k_mg_diag<<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e,
-                                                    f.dinv);
+                                                    f.dinv); fs_count_launch();
   }
   MGLevel& c = P->lev[P->nlev - 1];
-  if (c.n <= MG_COARSE_MAX)
-    k_mg_coarse_inverse<<<1, 64, 0, st>>>(c.nx, c.ny, c.nz, c.gx, c.gy, c.gz, c.e, P->Ainv);
+  if (c.n <= MG_COARSE_MAX) {
+    k_mg_coarse_inverse<<<1, 64, 0, st>>>(c.nx, c.ny, c.nz, c.gx, c.gy, c.gz, c.e, P->Ainv); fs_count_launch(); }
   return cuda_status();
 }
 
@@ -603,14 +603,14 @@ static void vcycle(ProjCtx* P, int l, const double* b, double* x, cudaStream_t s
   MGLevel& f = P->lev[l];
   if (l == P->nlev - 1) {
     if (f.n <= MG_COARSE_MAX) {
-      k_mg_coarse_solve<<<1, 64, 0, st>>>((int)f.n, P->Ainv, b, x);
+      k_mg_coarse_solve<<<1, 64, 0, st>>>((int)f.n, P->Ainv, b, x); fs_count_launch();
     } else {
       // not coarsenable and too large for the dense solve: smoothing only
       k_mg_jacobi<<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e,
-                                                       f.dinv, b, nullptr, x, MG_OMEGA);
+                                                       f.dinv, b, nullptr, x, MG_OMEGA); fs_count_launch();
       for (int s = 0; s < 8; ++s) {
         k_mg_jacobi<<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz,
-                                                         f.e, f.dinv, b, x, f.t, MG_OMEGA);
+                                                         f.e, f.dinv, b, x, f.t, MG_OMEGA); fs_count_launch();
         cudaMemcpyAsync(x, f.t, sizeof(double) * f.n, cudaMemcpyDeviceToDevice, st);
       }
     }
@@ -620,18 +620,18 @@ static void vcycle(ProjCtx* P, int l, const double* b, double* x, cudaStream_t s
   unsigned nb = blocks_for(f.n, 256);
   // pre-smoothing: x = w b/d ; t = x + w (b - S x)/d
   k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, nullptr, x,
-                                  MG_OMEGA);
+                                  MG_OMEGA); fs_count_launch();
   k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, x, f.t,
-                                  MG_OMEGA);
+                                  MG_OMEGA); fs_count_launch();
   k_mg_restrict_residual<<<blocks_for(cl.n, 128), 128, 0, st>>>(
-      f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, b, f.t, cl.nx, cl.ny, cl.nz, cl.b);
+      f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, b, f.t, cl.nx, cl.ny, cl.nz, cl.b); fs_count_launch();
   vcycle(P, l + 1, cl.b, cl.x, st);
-  k_mg_prolong<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.t, cl.nx, cl.ny, cl.x);
+  k_mg_prolong<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.t, cl.nx, cl.ny, cl.x); fs_count_launch();
   // post-smoothing: x = t + w(b - S t)/d ; out = x + w(b - S x)/d
   k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, f.t, x,
-                                  MG_OMEGA);
+                                  MG_OMEGA); fs_count_launch();
   k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, x, f.t,
-                                  MG_OMEGA);
+                                  MG_OMEGA); fs_count_launch();
   cudaMemcpyAsync(x, f.t, sizeof(double) * f.n, cudaMemcpyDeviceToDevice, st);
 }
 
@@ -651,12 +651,12 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
   const int64_t n = l0.n;
   *iters = 0;
   k_proj_rhs<<<RED_BLOCKS, RED_THREADS, 0, st>>>(g, u, v, w, u_in, target, dt, P->rhs,
-                                                 P->partial);
-  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 4);  // ||b_A||^2
+                                                 P->partial); fs_count_launch();
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 4); fs_count_launch();  // ||b_A||^2
   double* x = P->p_prev;
   k_pcg_residual<<<RED_BLOCKS, RED_THREADS, 0, st>>>(g, l0.gx, l0.gy, l0.gz, l0.e, P->rhs, x,
-                                                     P->pc_r, P->partial);
-  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5);  // ||r_A||^2
+                                                     P->pc_r, P->partial); fs_count_launch();
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5); fs_count_launch();  // ||r_A||^2
   int stt = fetch(P, 6, st);
   if (stt) return stt;
   double bn = sqrt(P->h_scal[4]);
@@ -671,16 +671,16 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
     while (!done) {
       if (it >= maxiter) return FS_ENOCONV;
       vcycle(P, 0, P->pc_r, P->pc_z, st);
-      k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, P->pc_r, P->pc_z, P->partial);
-      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 2);  // rz_new
-      k_pcg_dir<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, P->pc_z, P->pc_p, it == 0);
-      k_set_scal<<<1, 1, 0, st>>>(P->scal, 0, 2);  // rz = rz_new
+      k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, P->pc_r, P->pc_z, P->partial); fs_count_launch();
+      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 2); fs_count_launch();  // rz_new
+      k_pcg_dir<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, P->pc_z, P->pc_p, it == 0); fs_count_launch();
+      k_set_scal<<<1, 1, 0, st>>>(P->scal, 0, 2); fs_count_launch();  // rz = rz_new
       k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.nx, l0.ny, l0.nz, l0.gx, l0.gy, l0.gz,
-                                                       l0.e, P->pc_p, P->pc_q, P->partial);
-      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 1);  // pq
+                                                       l0.e, P->pc_p, P->pc_q, P->partial); fs_count_launch();
+      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 1); fs_count_launch();  // pq
       k_pcg_update<<<RED_BLOCKS, RED_THREADS, 0, st>>>(g, P->scal, x, P->pc_r, P->pc_p, P->pc_q,
-                                                       P->partial);
-      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5);
+                                                       P->partial); fs_count_launch();
+      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5); fs_count_launch();
       ++it;
       stt = fetch(P, 6, st);
       if (stt) return stt;
@@ -692,7 +692,7 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
   }
   P->have_prev = 1;
   Launch3 L = launch_cells(g);
-  k_proj_correct<<<L.grid, L.block, 0, st>>>(g, u, v, w, x, P->ir, dt);
+  k_proj_correct<<<L.grid, L.block, 0, st>>>(g, u, v, w, x, P->ir, dt); fs_count_launch();
   return cuda_status();
 }
 
@@ -703,7 +703,7 @@ int launch_div_resid_max(const GridDev& g, const double* u, const double* v, con
   int64_t n = ncells(g);
   unsigned nb = blocks_for(n, 256);
   if (nb > 1184) nb = 1184;
-  k_div_resid_max<<<nb, 256, 0, st>>>(g, u, v, w, u_in, target, div_out, out_key);
+  k_div_resid_max<<<nb, 256, 0, st>>>(g, u, v, w, u_in, target, div_out, out_key); fs_count_launch();
   return cuda_status();
 }
 
@@ -712,6 +712,6 @@ int proj_apply(void* h, const double* x, double* y, cudaStream_t st) {
   ProjCtx* P = (ProjCtx*)h;
   MGLevel& l0 = P->lev[0];
   k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.nx, l0.ny, l0.nz, l0.gx, l0.gy, l0.gz, l0.e,
-                                                   x, y, P->partial);
+                                                   x, y, P->partial); fs_count_launch();
   return cuda_status();
 }

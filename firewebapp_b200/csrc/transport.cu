@@ -95,7 +95,7 @@ int launch_species(const GridDev& g, int nspec, const double* const* Y, double* 
   double inv_dx = 1.0 / g.dx, inv_dy = 1.0 / g.dy;
   Launch3 L = launch_cells(g);
   k_species<<<L.grid, L.block, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
-                                        inv_dx * inv_dx, inv_dy * inv_dy);
+                                        inv_dx * inv_dx, inv_dy * inv_dy); fs_count_launch();
   return cuda_status();
 }
 
@@ -119,7 +119,7 @@ __global__ void k_species_sources(int64_t n, const double* __restrict__ Sp,
 int launch_species_sources(int64_t n, const double* Sp, const double* Sd, const double* YF,
                            const double* YO, const double* YH, double* SF, double* SO,
                            double* SH, cudaStream_t st) {
-  k_species_sources<<<blocks_for(n, 256), 256, 0, st>>>(n, Sp, Sd, YF, YO, YH, SF, SO, SH);
+  k_species_sources<<<blocks_for(n, 256), 256, 0, st>>>(n, Sp, Sd, YF, YO, YH, SF, SO, SH); fs_count_launch();
   return cuda_status();
 }
 
@@ -175,7 +175,7 @@ __global__ void k_advect_scalar(GridDev g, const double* __restrict__ phi,
 int launch_advect_scalar(const GridDev& g, const double* phi, const double* u, const double* v,
                          const double* w, double* rhs, double phi_inlet, cudaStream_t st) {
   Launch3 L = launch_cells(g);
-  k_advect_scalar<<<L.grid, L.block, 0, st>>>(g, phi, u, v, w, rhs, phi_inlet);
+  k_advect_scalar<<<L.grid, L.block, 0, st>>>(g, phi, u, v, w, rhs, phi_inlet); fs_count_launch();
   return cuda_status();
 }
 
@@ -233,7 +233,7 @@ int launch_gas_energy_adv(const GridDev& g, const double* T, const double* u, co
   if (g.nx < 3 || g.nz < 3) return FS_EARG;
   Launch3 L = launch_cells(g);
   k_gas_energy_adv<<<L.grid, L.block, 0, st>>>(g, T, u, v, w, To, dt, alpha, T_amb,
-                                               1.0 / (g.dx * g.dx), g.dy * g.dy);
+                                               1.0 / (g.dx * g.dx), g.dy * g.dy); fs_count_launch();
   return cuda_status();
 }
 
@@ -299,7 +299,7 @@ int launch_turb_diff(const GridDev& g, int nfield, const double* const* f, doubl
   }
   Launch3 L = launch_cells(g);
   k_turb_diff<<<L.grid, L.block, 0, st>>>(g, a, nu_t, sc_t, dt_sub, 1.0 / (g.dx * g.dx),
-                                          1.0 / (g.dy * g.dy));
+                                          1.0 / (g.dy * g.dy)); fs_count_launch();
   return cuda_status();
 }
 
@@ -335,7 +335,7 @@ int launch_drag(int64_t n, const double* u, const double* v, const double* w, co
                 const double* as, double sigma, double C_D, double* Fx, double* Fy, double* Fz,
                 cudaStream_t st) {
   k_drag<<<blocks_for(n, 256), 256, 0, st>>>(n, u, v, w, rho, as, sigma, sigma * sigma, C_D, Fx,
-                                             Fy, Fz);
+                                             Fy, Fz); fs_count_launch();
   return cuda_status();
 }
 
@@ -487,7 +487,7 @@ int launch_momentum(const GridDev& g, const double* u, const double* v, const do
   a.inv_dx = 1.0 / g.dx; a.inv_dy = 1.0 / g.dy;
   a.inv_dx2 = a.inv_dx * a.inv_dx; a.inv_dy2 = a.inv_dy * a.inv_dy;
   Launch3 L = launch_cells(g);
-  k_momentum<<<L.grid, L.block, 0, st>>>(g, a);
+  k_momentum<<<L.grid, L.block, 0, st>>>(g, a); fs_count_launch();
   return cuda_status();
 }
 
@@ -512,7 +512,7 @@ __global__ void k_sponge(GridDev g, double* u, const double* __restrict__ u_t,
 int launch_sponge(const GridDev& g, double* u, const double* u_t, const double* sig_x,
                   const double* YF, double skip, double dt, cudaStream_t st) {
   Launch3 L = launch_cells(g);
-  k_sponge<<<L.grid, L.block, 0, st>>>(g, u, u_t, sig_x, YF, skip, dt);
+  k_sponge<<<L.grid, L.block, 0, st>>>(g, u, u_t, sig_x, YF, skip, dt); fs_count_launch();
   return cuda_status();
 }
 
@@ -725,7 +725,7 @@ int launch_keps(const GridDev& g, const double* k, const double* e, const double
   a.inv_dx2 = 1.0 / (g.dx * g.dx); a.inv_dy2 = 1.0 / (g.dy * g.dy);
   if (g.nz < 2) return FS_EARG;
   Launch3 L = launch_cells(g);
-  k_keps<<<L.grid, L.block, 0, st>>>(g, a);
+  k_keps<<<L.grid, L.block, 0, st>>>(g, a); fs_count_launch();
   return cuda_status();
 }
 
@@ -770,7 +770,7 @@ int launch_solid_cond(const GridDev& g, const double* Ts, const double* as, doub
   GridDev gg = g;
   Launch3 L = launch_cells(g);
   (void)nz_active;
-  k_solid_cond<<<L.grid, L.block, 0, st>>>(gg, Ts, as, To, k_solid, 1.0 / (rho_s * cp_s), dt);
+  k_solid_cond<<<L.grid, L.block, 0, st>>>(gg, Ts, as, To, k_solid, 1.0 / (rho_s * cp_s), dt); fs_count_launch();
   return cuda_status();
 }
 
@@ -805,6 +805,6 @@ int launch_soil(int nsoil, int ny, int nx, double* T, const double* qin, double 
                 double rho_s, double cp_s, double eps_s, double T_amb, cudaStream_t st) {
   int64_t n2 = (int64_t)ny * nx;
   k_soil<<<blocks_for(n2, 128), 128, 0, st>>>(nsoil, ny, nx, T, qin, dt, sdz, sda, sdb, k_s,
-                                             1.0 / (rho_s * cp_s), eps_s, T_amb);
+                                             1.0 / (rho_s * cp_s), eps_s, T_amb); fs_count_launch();
   return cuda_status();
 }

@@ -135,6 +135,7 @@ class Tier3Solver:
         self.edc_scratch = torch.zeros(int(self.lib.fs_edc_scratch_bytes(self.n)) + 64,
                                        dtype=torch.uint8, device=dev)
         self.active_count = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.max_scratch = torch.zeros(64, dtype=torch.float64, device=dev)
         # soil
         so = su.soil
         self.soil_dz = torch.tensor(so["dz"], **f64)
@@ -261,6 +262,31 @@ class Tier3Solver:
             tm.setdefault(lab0, []).append((ev0, ev))
         self._mark = (label, ev) if label else None
 
+    def enable_kernel_timers(self, on=True):
+        """Bracket individual kernel launches with CUDA events (same stream)."""
+        self._kt_on = bool(on)
+        self._kt = {}
+        if getattr(self, "dom", None):
+            self.lib.fs_dom_sweep_timing(self.dom, 1 if on else 0, None, None)
+
+    def _ktime(self, label):
+        if not getattr(self, "_kt_on", False):
+            return _NullCtx()
+        return _KernelTimer(self._kt, label)
+
+    def kernel_times(self):
+        """{kernel: (total ms, launches)} of the bracketed kernels."""
+        torch.cuda.synchronize()
+        out = {k: (sum(a.elapsed_time(b) for a, b in v), len(v))
+               for k, v in getattr(self, "_kt", {}).items()}
+        if getattr(self, "dom", None):
+            ms = _C.c_double()
+            cnt = _C.c_longlong()
+            self.lib.fs_dom_sweep_timing(self.dom, -1, _C.byref(ms), _C.byref(cnt))
+            if cnt.value:
+                out["dom_sweep"] = (ms.value, cnt.value)
+        return out
+
     def phase_times(self):
         """{phase: total milliseconds} of the phases recorded so far."""
         torch.cuda.synchronize()
@@ -293,9 +319,10 @@ class Tier3Solver:
         d = StepDiag()
         # --- 0. adaptive dt (spread_3d.py:1906-1941)
         self._phase("dt")
-        u_now = max(self._max(f["u"], 0), self._max(f["v"], 0), self._max(f["w"], 0),
-                    p["U_mf"], math.sqrt(G_ACC * p["h_bed"] * 0.5), 0.1)
-        nu_now = max(self._max(f["nu_t"], 1), 1.0e-3)
+        mu_, mv_, mw_, mnu_, mT_ = self._maxes([f["u"], f["v"], f["w"], f["nu_t"], f["T_g"]],
+                                               [0, 0, 0, 1, 1])
+        u_now = max(mu_, mv_, mw_, p["U_mf"], math.sqrt(G_ACC * p["h_bed"] * 0.5), 0.1)
+        nu_now = max(mnu_, 1.0e-3)
         dz_min = p["dz_min"]
         dt_adv = p["cfl"] * min(g.dx, g.dy, dz_min) / u_now
         dt_diff = 0.25 * dz_min * dz_min / nu_now
@@ -303,7 +330,7 @@ class Tier3Solver:
         dt_new = min(dt_new, self.dt * 1.5)
         if dt_new < p["min_dt_s"]:
             dt_new = p["min_dt_s"]
-        if not math.isfinite(self._max(f["T_g"], 1)):
+        if not math.isfinite(mT_):
             raise RuntimeError(f"State NaN/Inf at t={self.t:.3f}s -- simulation exploded.")
         self.dt = dt = dt_new
         t = self.t
@@ -332,12 +359,13 @@ class Tier3Solver:
         Sp, Sd = self.bed_out["S_pyro"], self.bed_out["S_drying"]
         # --- 3/4. drag + tentative momentum (spread_3d.py:2223-2276)
         self._phase("momentum")
-        check(L.fs_tentative_velocity(gp, ptr(f["u"]), ptr(f["v"]), ptr(f["w"]), ptr(f["rho"]),
-                                      ptr(f["T_g"]), None, None, None, ptr(f["alpha_s"]),
-                                      p["sav"], p["canopy_C_d"], ptr(self.u_inlet),
-                                      ptr(self.zero2), ptr(self.zero2), ptr(w["tmp1"]),
-                                      ptr(w["tmp2"]), ptr(w["tmp3"]), dt, p["T_amb"], s),
-              "momentum")
+        with self._ktime("momentum_drag"):
+            check(L.fs_tentative_velocity(gp, ptr(f["u"]), ptr(f["v"]), ptr(f["w"]),
+                                          ptr(f["rho"]), ptr(f["T_g"]), None, None, None,
+                                          ptr(f["alpha_s"]), p["sav"], p["canopy_C_d"],
+                                          ptr(self.u_inlet), ptr(self.zero2), ptr(self.zero2),
+                                          ptr(w["tmp1"]), ptr(w["tmp2"]), ptr(w["tmp3"]), dt,
+                                          p["T_amb"], s), "momentum")
         self._swap("u", "tmp1")
         self._swap("v", "tmp2")
         self._swap("w", "tmp3")
@@ -369,11 +397,13 @@ class Tier3Solver:
                                   ptr(f["Y_fuel"]), 1.0e-3, dt, s), "sponge")
         # --- 7. k-epsilon (spread_3d.py:2409)
         self._phase("k_eps")
-        check(L.fs_k_epsilon(gp, ptr(f["k_turb"]), ptr(f["eps_turb"]), ptr(f["u"]), ptr(f["v"]),
-                             ptr(f["w"]), ptr(f["T_g"]), ptr(f["alpha_s"]), ptr(self.u_inlet),
-                             ptr(self.k_wall), ptr(self.eps_wall), ptr(w["tmp1"]),
-                             ptr(w["tmp2"]), ptr(w["tmp3"]), None, None, p["sav"], dt,
-                             p["T_amb"], p["canopy_beta_p"], p["canopy_beta_d"], s), "k_eps")
+        with self._ktime("k_epsilon"):
+            check(L.fs_k_epsilon(gp, ptr(f["k_turb"]), ptr(f["eps_turb"]), ptr(f["u"]),
+                                 ptr(f["v"]), ptr(f["w"]), ptr(f["T_g"]), ptr(f["alpha_s"]),
+                                 ptr(self.u_inlet), ptr(self.k_wall), ptr(self.eps_wall),
+                                 ptr(w["tmp1"]), ptr(w["tmp2"]), ptr(w["tmp3"]), None, None,
+                                 p["sav"], dt, p["T_amb"], p["canopy_beta_p"],
+                                 p["canopy_beta_d"], s), "k_eps")
         self._swap("k_turb", "tmp1")
         self._swap("eps_turb", "tmp2")
         self._swap("nu_t", "tmp3")
@@ -402,34 +432,38 @@ class Tier3Solver:
                                 ptr(self.active_count), None, s), "active_count")
         # --- 11. gas-temperature advection (:2648)
         self._phase("gas_adv")
-        check(L.fs_gas_energy_adv(gp, ptr(f["T_g"]), ptr(f["u"]), ptr(f["v"]), ptr(f["w"]),
-                                  ptr(w["tmp1"]), dt, 2.0e-5, p["T_amb"], s), "gas_adv")
+        with self._ktime("gas_energy_adv"):
+            check(L.fs_gas_energy_adv(gp, ptr(f["T_g"]), ptr(f["u"]), ptr(f["v"]), ptr(f["w"]),
+                                      ptr(w["tmp1"]), dt, 2.0e-5, p["T_amb"], s), "gas_adv")
         self._swap("T_g", "tmp1")
         # --- 12. ten chemistry/transport sub-steps (:2678-3196)
         self._phase("substeps")
         dt_sub = dt / N_SUB
-        n_sc, dts_sc = self._nsub(SC_T, dt_sub)
-        n_pr, dts_pr = self._nsub(PR_T, dt_sub)
+        nu_in = self._maxes([f["nu_t"]], [2])[0]
+        n_sc, dts_sc = self._nsub_from(nu_in, SC_T, dt_sub)
+        n_pr, dts_pr = self._nsub_from(nu_in, PR_T, dt_sub)
         d.n_sub_sc, d.n_sub_pr = n_sc, n_pr
         drip = int(ign)
         for _sub in range(N_SUB):
             self._phase("edc")
-            check(L.fs_edc(self.n, ptr(f["rho"]), ptr(f["T_g"]), ptr(f["Y_fuel"]),
-                           ptr(f["Y_O2"]), ptr(f["k_turb"]), ptr(f["eps_turb"]),
-                           ptr(f["Y_H2O"]), ptr(w["omega"]), p["chi_rad"], 1100.0, dt_sub,
-                           1, 1.3, 17_000_000.0, int(p["edc_extinction_enable"]),
-                           ptr(self.edc_scratch), s), "edc")
+            with self._ktime("edc"):
+                check(L.fs_edc(self.n, ptr(f["rho"]), ptr(f["T_g"]), ptr(f["Y_fuel"]),
+                               ptr(f["Y_O2"]), ptr(f["k_turb"]), ptr(f["eps_turb"]),
+                               ptr(f["Y_H2O"]), ptr(w["omega"]), p["chi_rad"], 1100.0, dt_sub,
+                               1, 1.3, 17_000_000.0, int(p["edc_extinction_enable"]),
+                               ptr(self.edc_scratch), s), "edc")
             self._phase("species")
             check(L.fs_species_sources(self.n, ptr(Sp), ptr(Sd), ptr(f["Y_fuel"]),
                                        ptr(f["Y_O2"]), ptr(f["Y_H2O"]), ptr(w["S_F"]),
                                        ptr(w["S_O2"]), ptr(w["S_H2O"]), s), "sources")
             Ys = [f["Y_fuel"], f["Y_O2"], f["Y_H2O"]]
             Yo = [w["tmp1"], w["tmp2"], w["tmp3"]]
-            check(L.fs_species_transport(gp, 3, ptr_array(Ys), ptr_array(Yo),
-                                         ptr_array([w["S_F"], w["S_O2"], w["S_H2O"]]),
-                                         dbl_array([0.0, 0.232, 0.0]), ptr(f["rho"]),
-                                         ptr(f["u"]), ptr(f["v"]), ptr(f["w"]), dt_sub, 1.0e-5,
-                                         s), "species")
+            with self._ktime("species_transport"):
+                check(L.fs_species_transport(gp, 3, ptr_array(Ys), ptr_array(Yo),
+                                             ptr_array([w["S_F"], w["S_O2"], w["S_H2O"]]),
+                                             dbl_array([0.0, 0.232, 0.0]), ptr(f["rho"]),
+                                             ptr(f["u"]), ptr(f["v"]), ptr(f["w"]), dt_sub,
+                                             1.0e-5, s), "species")
             self._swap("Y_fuel", "tmp1")
             self._swap("Y_O2", "tmp2")
             self._swap("Y_H2O", "tmp3")
@@ -440,10 +474,11 @@ class Tier3Solver:
                     last = q == n_sc - 1
                     Ys = [f["Y_fuel"], f["Y_O2"], f["Y_H2O"]]
                     Yo = [w["tmp1"], w["tmp2"], w["tmp3"]]
-                    check(L.fs_turb_diffusion_substep(
-                        gp, 3, ptr_array(Ys), ptr_array(Yo), ptr(f["nu_t"]), SC_T, dts_sc,
-                        int(last), dbl_array([0.0, 0.0, 0.0]), dbl_array([1.0, 0.232, 1.0]),
-                        s), "turb_diff_Y")
+                    with self._ktime("turb_diffusion_Y"):
+                        check(L.fs_turb_diffusion_substep(
+                            gp, 3, ptr_array(Ys), ptr_array(Yo), ptr(f["nu_t"]), SC_T, dts_sc,
+                            int(last), dbl_array([0.0, 0.0, 0.0]),
+                            dbl_array([1.0, 0.232, 1.0]), s), "turb_diff_Y")
                     self._swap("Y_fuel", "tmp1")
                     self._swap("Y_O2", "tmp2")
                     self._swap("Y_H2O", "tmp3")
@@ -508,6 +543,30 @@ class Tier3Solver:
         drho = (f["rho"] - w["rho_prev"]) / dt
         torch.div((Sp + Sd) - drho, torch.clamp(f["rho"], min=0.1), out=w["div_target"])
 
+    def _maxes(self, tensors, modes):
+        res = (_C.c_double * len(tensors))()
+        md = (_C.c_int * len(modes))(*modes)
+        check(self.lib.fs_field_max_multi(self.gp, len(tensors), ptr_array(tensors), md, res,
+                                          ptr(self.max_scratch), self._s()), "maxima")
+        return list(res)
+
+    def _nsub_from(self, nu_max, sc, dt):
+        """turbulence_3d.py:880-915 sub-step count from the interior nu_t maximum."""
+        g = self.grid
+        dz_min = self.p["dz_min"]
+        h_min2 = min(g.dx * g.dx, min(g.dy * g.dy, dz_min * dz_min))
+        D_max = nu_max / sc
+        if D_max <= 1.0e-12 or not math.isfinite(D_max):
+            return 0, 0.0
+        dt_sub_max = 0.4 * h_min2 / D_max
+        if dt_sub_max <= 0.0:
+            return 0, 0.0
+        target = dt / dt_sub_max
+        if target > 1000:
+            return 0, 0.0
+        n = max(1, int(math.ceil(target)))
+        return n, dt / n
+
     def _nsub(self, sc, dt_sub):
         n = _ctypes_int()
         dts = _ctypes_double()
@@ -566,6 +625,30 @@ class Tier3Solver:
 
 # ---- small ctypes helpers --------------------------------------------------
 import ctypes as _C  # noqa: E402
+
+
+class _NullCtx:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+class _KernelTimer:
+    def __init__(self, store, label):
+        self.store, self.label = store, label
+
+    def __enter__(self):
+        self.e0 = torch.cuda.Event(enable_timing=True)
+        self.e1 = torch.cuda.Event(enable_timing=True)
+        self.e0.record()
+        return self
+
+    def __exit__(self, *a):
+        self.e1.record()
+        self.store.setdefault(self.label, []).append((self.e0, self.e1))
+        return False
 
 
 def _ctypes_ref(obj):

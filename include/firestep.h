@@ -74,6 +74,8 @@ typedef struct FsBedParams {
 
 const char* fs_last_error(void);
 int fs_version(void);
+/* number of kernel launches this library has issued since it was loaded */
+unsigned long long fs_launch_count(void);
 
 /* species_3d.py:41 step_species_transport, up to 3 species in one pass,
  * out-of-place (Y -> Y_out, clipped to [0,1]). */
@@ -196,6 +198,9 @@ int fs_dom_solve(void* handle, const double* T_s, const double* T_g, const doubl
                  double* q_rad_gas, double* q_in_soil, void* stream);
 double* fs_dom_intensity(void* handle);
 int fs_dom_iterations(void* handle);
+/* enable >= 0 turns per-sweep event timing on/off (and resets it); the
+ * accumulated sweep time and sweep count are returned when pointers are given */
+int fs_dom_sweep_timing(void* handle, int enable, double* total_ms, long long* sweeps);
 
 /* lagrangian_bed_3d.py:594 step_bed_particles (sources overwritten only in
  * occupied cells; zero the grids once), :501 aggregate_particles_to_T_s_grid
@@ -225,6 +230,10 @@ int fs_active_count(int64_t n, const double* omega, const double* T_g, const dou
 /* max reductions: mode 0 max|f|, 1 max f (NaN propagates), 2 interior max
  * ignoring NaN from 0 (turbulence_3d.py:894-900); results to host. */
 int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, void* stream);
+/* several maxima in one pass; scratch: >= 256 bytes of device memory;
+ * results: nf doubles in host memory (synchronises once). */
+int fs_field_max_multi(const FsGrid* g, int nf, const double* const* f, const int* modes,
+                       double* results, void* scratch, void* stream);
 
 #ifdef __cplusplus
 }

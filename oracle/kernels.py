@@ -943,17 +943,79 @@ def divergence(u, v, w, dx, dy, dz, u_in):
     return div
 
 
-def project(u, v, w, rho, dt, div_target, dx, dy, dz, da, db, u_in):
-    """projection_3d.py:677-844 project, with the Poisson system solved
-    directly (the reference's BiCGSTAB at tight tolerance converges to the
-    same solution).  Returns (u, v, w, p)."""
+class SeparablePoisson:
+    """Exact inverse of the constant-coefficient operator, used by the
+    reference as the Krylov preconditioner (fft_poisson_3d.py:45-228):
+    eigen-decompositions of the 1D x and (sqrt(dz)-symmetrised) z Laplacians,
+    FFT along periodic y."""
+
+    def __init__(self, nz, ny, nx, dx, dy, dz, da, db, eps_reg=1.0e-6):
+        from scipy.linalg import eigh
+        dz = np.asarray(dz, dtype=np.float64)
+        Lx = np.zeros((nx, nx))
+        c = 1.0 / (dx * dx)
+        for i in range(nx):
+            if 0 < i < nx - 1:
+                Lx[i, i], Lx[i, i + 1], Lx[i, i - 1] = -2.0 * c, c, c
+            elif i == 0:
+                Lx[0, 0], Lx[0, 1] = -c, c
+            else:
+                Lx[i, i], Lx[i, i - 1] = -3.0 * c, c
+        Lz = np.zeros((nz, nz))
+        for k in range(nz):
+            idz = 1.0 / dz[k]
+            if 0 < k < nz - 1:
+                ca, cb = idz / da[k], idz / db[k]
+                Lz[k, k], Lz[k, k + 1], Lz[k, k - 1] = -ca - cb, ca, cb
+            elif k == 0:
+                ca = idz / da[0]
+                Lz[0, 0], Lz[0, 1] = -ca, ca
+            else:
+                cb = idz / db[k]
+                Lz[k, k], Lz[k, k - 1] = -2.0 * idz * idz - cb, cb
+        D = np.sqrt(dz)
+        lx, self.Ux = eigh(Lx)
+        lz, self.Uz = eigh((D[:, None] * Lz) / D[None, :])
+        ly = (2.0 / (dy * dy)) * (np.cos(2.0 * np.pi * np.arange(ny) / ny) - 1.0)
+        self.inv = 1.0 / (lz[:, None, None] + ly[None, :, None] + lx[None, None, :] - eps_reg)
+        self.D = D
+        self.shape = (nz, ny, nx)
+
+    def solve(self, r):
+        nz, ny, nx = self.shape
+        q = r.reshape(self.shape) * self.D[:, None, None]
+        q = (q.reshape(nz * ny, nx) @ self.Ux).reshape(self.shape)
+        q = np.fft.fft(q, axis=1)
+        q = (self.Uz.T @ q.reshape(nz, ny * nx)).reshape(self.shape) * self.inv
+        q = (self.Uz @ q.reshape(nz, ny * nx)).reshape(self.shape)
+        q = np.fft.ifft(q, axis=1).real
+        q = (q.reshape(nz * ny, nx) @ self.Ux.T).reshape(self.shape)
+        return (q / self.D[:, None, None]).reshape(-1)
+
+
+def project(u, v, w, rho, dt, div_target, dx, dy, dz, da, db, u_in, solver="direct",
+            rtol=1.0e-6, x0=None, precond=None):
+    """projection_3d.py:677-844 project.  ``solver='direct'`` solves the
+    Poisson system exactly (what the reference's BiCGSTAB reaches at tight
+    tolerance); ``'bicgstab'`` is the reference's own iteration (scipy
+    BiCGSTAB, warm start x0, separable preconditioner, rtol).
+    Returns (u, v, w, p)."""
     import scipy.sparse.linalg as spla
     A, ir = poisson_matrix(rho, dx, dy, dz, da, db)
     div = divergence(u, v, w, dx, dy, dz, u_in)
     if div_target is not None:
         div = div - div_target
     rhs = (div / dt).reshape(-1)
-    p = spla.spsolve(A.tocsc(), rhs).reshape(u.shape)
+    if solver == "direct":
+        p = spla.spsolve(A.tocsc(), rhs).reshape(u.shape)
+    else:
+        nz, ny, nx = u.shape
+        pre = precond or SeparablePoisson(nz, ny, nx, dx, dy, dz, da, db)
+        M = spla.LinearOperator(A.shape, matvec=pre.solve)
+        p, info = spla.bicgstab(A, rhs, x0=x0, M=M, rtol=rtol, maxiter=200)
+        if info != 0:
+            raise RuntimeError(f"BiCGSTAB did not converge (info={info})")
+        p = p.reshape(u.shape)
     u = u.copy(); v = v.copy(); w = w.copy()
     nz, ny, nx = u.shape
     if nx > 2:

@@ -49,6 +49,11 @@ class OracleState:
         self.src = None
         self.M_local = np.zeros(shp)
         self.q_in_soil = np.zeros(shp[1:])
+        self.proj_solver = "direct"
+        self.proj_rtol = 1.0e-6
+        self.precond = None
+        self.pressure = (np.array(snap["p_prev"], dtype=np.float64) if "p_prev" in snap
+                         else None)
 
     def snapshot(self):
         out = dict(self.f)
@@ -118,9 +123,15 @@ def step(S: OracleState):
     drho = (f["rho"] - rho_prev) / dt
     tgt = ((Sp + Sd) - drho) / np.maximum(f["rho"], 0.1)
     n_it = 0
+    if S.proj_solver != "direct" and S.precond is None:
+        S.precond = K.SeparablePoisson(nz, ny, nx, dx, dy, dz, da, db)
     for _ in range(p["proj_max_iter"]):
+        x0 = None if S.pressure is None else S.pressure.reshape(-1)
         f["u"], f["v"], f["w"], pres = K.project(f["u"], f["v"], f["w"], f["rho"], dt, tgt,
-                                                 dx, dy, dz, da, db, g["u_inlet"])
+                                                 dx, dy, dz, da, db, g["u_inlet"],
+                                                 solver=S.proj_solver, rtol=S.proj_rtol,
+                                                 x0=x0, precond=S.precond)
+        S.pressure = pres
         d = K.divergence(f["u"], f["v"], f["w"], dx, dy, dz, g["u_inlet"]) - tgt
         n_it += 1
         if float(np.max(np.abs(d))) < p["proj_div_tol"]:
