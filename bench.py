@@ -24,7 +24,6 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -56,28 +55,43 @@ def _dist():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled while the timed region runs."""
+    """SM clocks and clock-event reasons sampled (NVML, read-only queries,
+    every 200 ms) while the timed region runs."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.rows = []
+    def __init__(self, cuda_index):
+        self.idx = cuda_index
+        self.samples = []
         self._stop = threading.Event()
         self._th = None
+        self.handle = None
+        self.max_mhz = None
+        try:
+            import pynvml as nv
+            import torch
+            nv.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(cuda_index).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            self.nv = nv
+            self.handle = nv.nvmlDeviceGetHandleByUUID(uuid)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.handle, nv.NVML_CLOCK_SM))
+        except Exception:
+            self.handle = None
 
     def start(self):
+        if self.handle is None:
+            return
+
         def run():
+            nv = self.nv
             while not self._stop.is_set():
                 try:
-                    out = subprocess.run(
-                        ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                         "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                        timeout=5).stdout.strip()
-                    if out:
-                        self.rows.append([x.strip() for x in out.split(",")])
+                    sm = nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                    self.samples.append((float(sm), int(rs)))
                 except Exception:
                     pass
                 self._stop.wait(0.2)
@@ -87,20 +101,13 @@ class ClockSampler:
     def stop(self):
         self._stop.set()
         if self._th:
-            self._th.join(timeout=6)
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            for n, v in zip(names, r[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+            self._th.join(timeout=2)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        reasons = sorted({n for _, r in self.samples for n, bit in self.REASONS if r & bit})
+        return {"sm_mhz": statistics.median(s for s, _ in self.samples),
+                "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml"}
 
 
 def _oracle_slice(case_nx, seed=0):
