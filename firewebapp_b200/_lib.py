@@ -80,6 +80,7 @@ SIGNATURES = {
     "fs_proj_project": (I, [P, P, P, P, P, P, D, D, I, C.POINTER(I), P]),
     "fs_proj_pressure": (P, [P]),
     "fs_proj_apply": (I, [P, P, P, P]),
+    "fs_proj_configure": (I, [P, I, D]),
     "fs_divergence_max": (I, [_G, P, P, P, P, P, P, C.POINTER(D), P]),
     "fs_dom_create": (I, [_G, I, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(D), D,
                           PP]),
@@ -87,6 +88,9 @@ SIGNATURES = {
     "fs_dom_solve": (I, [P, P, P, P, P, D, D, P, P, P, P, P, P, P, P]),
     "fs_dom_intensity": (P, [P]),
     "fs_dom_iterations": (I, [P]),
+    "fs_dom_set_sweep_mode": (I, [P, I, I]),
+    "fs_dom_sweep_mode": (I, [P]),
+    "fs_dom_load_intensity": (I, [P, P, P]),
     "fs_dom_sweep_timing": (I, [P, I, C.POINTER(D), C.POINTER(C.c_longlong)]),
     "fs_bed_step": (I, [_G, C.POINTER(FsBedParticles), C.POINTER(FsBedSegments),
                         C.POINTER(FsBedSources), C.POINTER(FsBedParams), P, P, P]),
@@ -95,6 +99,7 @@ SIGNATURES = {
                          C.POINTER(FsBedSegments), P, P]),
     "fs_levelset": (I, [_G, P, P, P, D, I, P]),
     "fs_active_count": (I, [I64, P, P, P, P, P, P]),
+    "fs_copy_to_host": (I, [P, P, I64, P]),
     "fs_field_max": (I, [_G, P, I, C.POINTER(D), P]),
     "fs_field_max_multi": (I, [_G, I, PP, C.POINTER(I), C.POINTER(D), P, P]),
 }

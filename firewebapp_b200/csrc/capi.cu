@@ -19,6 +19,20 @@ void fs_set_error(const char* fmt, ...) {
   va_end(ap);
 }
 
+// Host wait for a stream through a blocking-sync event: the calling thread
+// sleeps instead of spinning, so waits do not consume the process's CPU time
+// (spinning threads can get a CPU-quota-limited process throttled).
+int fs_stream_wait(cudaStream_t st) {
+  static thread_local cudaEvent_t ev[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FS_ECUDA;
+  if (!ev[dev] && cudaEventCreateWithFlags(&ev[dev], cudaEventBlockingSync |
+                                                          cudaEventDisableTiming) != cudaSuccess)
+    return FS_ECUDA;
+  if (cudaEventRecord(ev[dev], st) != cudaSuccess) return FS_ECUDA;
+  return cudaEventSynchronize(ev[dev]) == cudaSuccess ? FS_OK : FS_ECUDA;
+}
+
 static int check(int st, const char* where) {
   if (st == FS_OK) return st;
   cudaError_t e = cudaGetLastError();
@@ -94,6 +108,13 @@ int fs_gas_energy_adv(const FsGrid* g, const double* T_g, const double* u, const
                "fs_gas_energy_adv");
 }
 
+int fs_copy_to_host(void* dst, const void* src, int64_t bytes, void* stream) {
+  if (!dst || !src || bytes < 0) return FS_EARG;
+  if (cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyDeviceToHost, ST(stream)) != cudaSuccess)
+    return check(FS_ECUDA, "fs_copy_to_host");
+  return check(fs_stream_wait(ST(stream)), "fs_copy_to_host");
+}
+
 int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, void* stream) {
   GRID("fs_field_max");
   unsigned long long* key = nullptr;
@@ -109,7 +130,7 @@ int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, voi
   cudaMemcpyAsync(result, dres, sizeof(double), cudaMemcpyDeviceToHost, ST(stream));
   cudaFreeAsync(key, ST(stream));
   cudaFreeAsync(dres, ST(stream));
-  if (cudaStreamSynchronize(ST(stream)) != cudaSuccess) return check(FS_ECUDA, "fs_field_max");
+  if (fs_stream_wait(ST(stream)) != FS_OK) return check(FS_ECUDA, "fs_field_max");
   return FS_OK;
 }
 
@@ -126,8 +147,7 @@ int fs_field_max_multi(const FsGrid* g, int nf, const double* const* f, const in
   for (int q = 0; q < nf; ++q) launch_max(gd, f[q], modes[q], key + q, ST(stream));
   launch_keys_to_double(key, dres, nf, ST(stream));
   cudaMemcpyAsync(results, dres, sizeof(double) * nf, cudaMemcpyDeviceToHost, ST(stream));
-  if (cudaStreamSynchronize(ST(stream)) != cudaSuccess)
-    return check(FS_ECUDA, "fs_field_max_multi");
+  if (fs_stream_wait(ST(stream)) != FS_OK) return check(FS_ECUDA, "fs_field_max_multi");
   return check(cuda_status(), "fs_field_max_multi");
 }
 
@@ -298,6 +318,11 @@ int fs_proj_project(void* handle, double* u, double* v, double* w, const double*
 
 double* fs_proj_pressure(void* handle) { return handle ? proj_pressure(handle) : nullptr; }
 
+int fs_proj_configure(void* handle, int nu, double omega) {
+  if (!handle) return FS_EARG;
+  return check(proj_configure(handle, nu, omega), "fs_proj_configure");
+}
+
 int fs_proj_apply(void* handle, const double* x, double* y, void* stream) {
   if (!handle) return FS_EARG;
   return check(proj_apply(handle, x, y, ST(stream)), "fs_proj_apply");
@@ -314,7 +339,7 @@ int fs_divergence_max(const FsGrid* g, const double* u, const double* v, const d
   unsigned long long hk = 0;
   cudaMemcpyAsync(&hk, key, sizeof(hk), cudaMemcpyDeviceToHost, ST(stream));
   cudaFreeAsync(key, ST(stream));
-  if (cudaStreamSynchronize(ST(stream)) != cudaSuccess) return check(FS_ECUDA, "fs_divergence_max");
+  if (fs_stream_wait(ST(stream)) != FS_OK) return check(FS_ECUDA, "fs_divergence_max");
   memcpy(result, &hk, sizeof(double));
   return check(st, "fs_divergence_max");
 }
@@ -344,6 +369,18 @@ int fs_dom_solve(void* handle, const double* T_s, const double* T_g, const doubl
 }
 
 double* fs_dom_intensity(void* handle) { return handle ? dom_intensity(handle) : nullptr; }
+
+int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas) {
+  if (!handle) return FS_EARG;
+  return check(dom_set_mode(handle, mode, cluster_ctas), "fs_dom_set_sweep_mode");
+}
+
+int fs_dom_sweep_mode(void* handle) { return handle ? dom_mode(handle) : -1; }
+
+int fs_dom_load_intensity(void* handle, const double* I_full, void* stream) {
+  if (!handle || !I_full) return FS_EARG;
+  return check(dom_load_intensity(handle, I_full, ST(stream)), "fs_dom_load_intensity");
+}
 
 int fs_dom_sweep_timing(void* handle, int enable, double* total_ms, long long* sweeps) {
   if (!handle) return FS_EARG;

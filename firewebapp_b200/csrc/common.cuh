@@ -86,3 +86,5 @@ void fs_set_error(const char* fmt, ...);
 
 // Count of kernel launches issued by this library (fs_launch_count()).
 void fs_count_launch();
+// wait for a stream with a blocking-sync event (no host spinning)
+int fs_stream_wait(cudaStream_t st);

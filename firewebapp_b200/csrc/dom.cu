@@ -3,15 +3,33 @@
 // Each source iteration sweeps every ordinate with step differencing
 // (dom_3d.py:147-211).  Within one ordinate the upwind dependencies run along
 // +-x, +-y, +-z, so all cells on a hyperplane i'+j'+k' = d (sweep-direction
-// coordinates) are independent; one launch per hyperplane processes that
-// plane for all ordinates of all octants at once.  The y-periodic inflow at
-// the first row reads the intensity left by the previous sweep at the other
-// end of the row, exactly as the reference's in-place sweep does (the source
-// cell sits on a later hyperplane, so it is still the previous value).
-// Intensities persist across calls (the reference keeps I_set).
+// coordinates) are independent.  The y-periodic inflow at the first row reads
+// the intensity left by the previous sweep at the other end of the row, as
+// the reference's in-place sweep does (that cell lies on a later hyperplane).
+// That wrap row is the only part of the intensities that a later sweep reads,
+// and it persists across calls as the reference's I_set does.
+//
+// Sweep paths (chosen at the first solve, or forced by fs_dom_set_sweep_mode):
+//   1 octant clusters: one thread-block cluster per octant, the
+//     cluster's CTAs split the k' rows; every thread owns one pencil (j',k')
+//     and advances all ordinates of the octant on each hyperplane, reading
+//     the previous hyperplane from shared memory.  The row below a CTA's
+//     first row arrives from the upstream CTA through distributed shared
+//     memory, handed over with mbarriers (point to point, so the CTAs run
+//     as a skewed pipeline).  Kappa and kappa*B are loaded once per cell for
+//     all ordinates of the octant, and the sweep emits the octant's partial
+//     G (and ground flux) instead of storing intensities.
+//   4 (default) as 1, with one cluster-wide barrier per hyperplane instead.
+//   2 one CTA per ordinate with the full intensity field stored (then G is
+//     summed over ordinates in ordinate order).
+//   3 one launch per hyperplane (any grid size).
+// G in paths 1 and 4 is summed within each octant in ordinate order and then over
+// octants in octant order (the reference sums all ordinates in one sequence;
+// the two orders differ only by rounding).
 #include <vector>
 #include <cstring>
 #include <utility>
+#include <cooperative_groups.h>
 #include "common.cuh"
 #include "kernels.h"
 
@@ -23,7 +41,16 @@ struct DomCtx {
   int M;
   double *ox, *oy, *oz, *w;  // device ordinates and weights
   std::vector<double> hox, hoy, hoz, hw;
-  double* I;                  // M * N
+  double* I;                  // M * N (paths 2/3 only)
+  double* wrap;               // M * Nz * Nx y-periodic inflow rows (path 1)
+  double2* kb;                // (kappa, kappa*B) per cell (path 1)
+  double* Goct;               // 8 * N octant partial G (path 1)
+  double* Qoct;               // 8 * (Ny*Nx) octant partial ground flux (path 1)
+  int mode;                   // resolved path: 0 not yet, 1 clusters, 2 block/ordinate, 3 planes
+  int mode_req, force_C;      // requested path (0 auto) and cluster size (0 auto)
+  int Mo, cl_C, cl_rows, cl_threads;
+  size_t cl_smem;
+  int down_slot[8];
   double *G, *Gp;             // current / previous G
   double *ks, *kg, *ksafe, *B;
   double *Ig_out, *Isoil, *qin;  // (Ny, Nx)
@@ -49,7 +76,8 @@ __global__ void k_dom_setup(GridDev g, const double* __restrict__ Ts, const doub
                             const double* __restrict__ as, const double* __restrict__ om,
                             const double* __restrict__ YH, const double* __restrict__ rho,
                             const double* __restrict__ Mloc, double sigma, double Tamb4,
-                            double kgmax, double* ks, double* kg, double* ksafe, double* B) {
+                            double kgmax, double* ks, double* kg, double* ksafe, double* B,
+                            double2* kb) {
   int64_t n = ncells_dev(g);
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -68,10 +96,12 @@ __global__ void k_dom_setup(GridDev g, const double* __restrict__ Ts, const doub
   } else {
     T4 = Tamb4;
   }
+  const double Bc = SIGMA_SB_D * T4 / PI_D;
   ks[c] = ksol;
   kg[c] = kgas;
   ksafe[c] = ksf;
-  B[c] = SIGMA_SB_D * T4 / PI_D;
+  B[c] = Bc;
+  if (kb) kb[c] = make_double2(ksf, ksf * Bc);
 }
 
 __global__ void k_dom_ground_init(int n2, const double* __restrict__ Tsoil, double eps_w,
@@ -127,8 +157,8 @@ __global__ void k_dom_plane(GridDev g, SweepArgs a) {
   } else {
     Iz = k < nz - 1 ? I[c + sz] : a.I_amb;
   }
-  const double ix = fabs(xi) * a.inv_dx;
-  const double iy = fabs(eta) * a.inv_dy;
+  const double ix = fabs(xi) / g.dx;
+  const double iy = fabs(eta) / g.dy;
   const double iz = fabs(mu) / g.dz[k];
   const double kap = a.ksafe[c];
   double num = kap * a.B[c] + ix * Ix + iy * Iy + iz * Iz;
@@ -153,8 +183,8 @@ __global__ void __launch_bounds__(1024) k_dom_sweep_block(GridDev g, SweepArgs a
   const int n = blockIdx.x;
   const double xi = a.ox[n], eta = a.oy[n], mu = a.oz[n];
   const bool fx = xi >= 0.0, fy = eta >= 0.0, fz = mu >= 0.0;
-  const double ix = fabs(xi) * a.inv_dx;
-  const double iy = fabs(eta) * a.inv_dy;
+  const double ix = fabs(xi) / g.dx;
+  const double iy = fabs(eta) / g.dy;
   const double amu = fabs(mu);
   const int64_t N = ncells_dev(g);
   double* I = a.I + (int64_t)n * N;
@@ -244,6 +274,471 @@ __global__ void k_dom_ground(int n2, int M, const double* __restrict__ oz,
   Ig[q] = relax * Inew + (1.0 - relax) * Ig[q];
 }
 
+// ---- path 1: octant clusters -------------------------------------------------
+namespace cg = cooperative_groups;
+
+struct OctArgs {
+  const double2* kb;
+  const double *ox, *oy, *oz, *w;
+  const double* Ig;
+  double *Goct, *Qoct, *wrap;
+  double I_amb;
+  int Mo, C, rows, periodic;
+  unsigned down_slots;  // 4 bits per octant: ground-flux slot, 15 = upward octant
+  int* err;             // set when a bounded wait gives up (pipelined sweep)
+};
+
+// Dynamic shared memory: two hyperplane buffers of Mo x (rows*Ny) doubles,
+// then |mu|/dz_k (Mo x Nz), |xi|/dx, |eta|/dy, w, w*|mu| (Mo each).
+__host__ __device__ inline size_t oct_smem_bytes(int Mo, int rows, int ny, int nz) {
+  return sizeof(double) * ((size_t)2 * Mo * rows * ny + (size_t)Mo * nz + 4 * (size_t)Mo);
+}
+// pipelined sweep: mbarriers (2 x OCT_RING) + inbox ring (OCT_RING x Mo x Ny) in front
+#define OCT_RING 4
+// and a ring of OCT_AHEAD hyperplanes of prefetched inputs per thread:
+// (kappa, kappa*B) 16 B, the y-inflow wrap values Mo x 8 B, the ground intensity 8 B
+#define OCT_AHEAD 4
+__host__ __device__ inline size_t oct_pipe_smem_bytes(int Mo, int rows, int ny, int nz) {
+  const size_t nthr = (size_t)rows * ny;
+  return 16 * (size_t)OCT_RING + sizeof(double) * (size_t)OCT_RING * Mo * ny +
+         (size_t)OCT_AHEAD * nthr * 16 + (size_t)OCT_AHEAD * rows * Mo * 8 +
+         (size_t)OCT_AHEAD * ny * 8 + oct_smem_bytes(Mo, rows, ny, nz);
+}
+
+__device__ __forceinline__ void cluster_arrive_release() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait_acquire() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+#define OCT_MAX_THREADS 512
+// One thread per pencil (rows*Ny <= OCT_MAX_THREADS).  Per hyperplane:
+// wait for the previous plane of the whole cluster, compute all MO
+// ordinates of the thread's cell from shared memory (the neighbour CTA's
+// last row through DSMEM), arrive, then store the octant partials and
+// prefetch the next plane's kappa / inflow values while the others finish.
+template <int MO>
+__global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant(GridDev g, OctArgs a) {
+  extern __shared__ double sh[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int rank = (int)cl.block_rank();
+  const int oct = blockIdx.x / a.C;
+  const int n0 = oct * MO;
+  const int S = a.rows * ny;
+  double* buf0 = sh;
+  double* buf1 = sh + (size_t)MO * S;
+  double* izt = buf1 + (size_t)MO * S;
+  double* cix = izt + (size_t)MO * nz;
+  double* ciy = cix + MO;
+  double* cw = ciy + MO;
+  double* cwm = cw + MO;
+  for (int t = threadIdx.x; t < MO * nz; t += blockDim.x) {
+    const int m = t / nz, k = t - m * nz;
+    izt[t] = fabs(a.oz[n0 + m]) / g.dz[k];
+  }
+  for (int m = threadIdx.x; m < MO; m += blockDim.x) {
+    cix[m] = fabs(a.ox[n0 + m]) / g.dx;
+    ciy[m] = fabs(a.oy[n0 + m]) / g.dy;
+    cw[m] = a.w[n0 + m];
+    cwm[m] = a.w[n0 + m] * fabs(a.oz[n0 + m]);
+  }
+  const bool fx = a.ox[n0] >= 0.0, fy = a.oy[n0] >= 0.0, fz = a.oz[n0] >= 0.0;
+  const int r0 = rank * a.rows;
+  const int nrows = min(a.rows, nz - r0);
+  const int npen = nrows > 0 ? nrows * ny : 0;
+  const int q = threadIdx.x;
+  const bool has = q < npen;
+  const int kl = has ? q / ny : 0;
+  const int jp = has ? q - kl * ny : 0;
+  const int kp = r0 + kl;
+  const int j = fy ? jp : ny - 1 - jp;
+  const int k = fz ? kp : nz - 1 - kp;
+  const int64_t N = ncells_dev(g);
+  const int64_t n2 = (int64_t)nx * ny;
+  const int slot_bits = (int)((a.down_slots >> (4 * oct)) & 15u);
+  const int slot = slot_bits == 15 ? -1 : slot_bits;
+  double* Go = a.Goct + (int64_t)oct * N;
+  const int64_t wstride = (int64_t)nz * nx;
+  double* wrap0 = a.wrap + (int64_t)n0 * wstride;
+  const bool ground_out = has && !fz && k == 0 && slot >= 0;
+  const bool z_in_ground = has && fz && kp == 0;
+  const bool z_remote = has && kl == 0 && kp > 0;
+  const bool y_wrap = has && jp == 0 && a.periodic;
+  const bool y_wrap_out = has && jp == ny - 1 && a.periodic;
+  const double* nbase = nullptr;
+  const int nplanes = nx + ny + nz - 2;
+  // prefetched values for the coming plane
+  double2 kab = make_double2(0.0, 0.0);
+  double win[MO];
+  double Igc = 0.0;
+  auto prefetch = [&](int d) {
+    const int ip = d - jp - kp;
+    if (!has || ip < 0 || ip >= nx) return;
+    const int i = fx ? ip : nx - 1 - ip;
+    kab = a.kb[((int64_t)k * ny + j) * nx + i];
+    if (y_wrap) {
+#pragma unroll
+      for (int m = 0; m < MO; ++m) win[m] = wrap0[m * wstride + (int64_t)k * nx + i];
+    }
+    if (z_in_ground) Igc = a.Ig[(int64_t)j * nx + i];
+  };
+#pragma unroll
+  for (int m = 0; m < MO; ++m) win[m] = a.I_amb;
+  __syncthreads();
+  prefetch(0);
+  for (int d = 0; d < nplanes; ++d) {
+    double* cur = (d & 1) ? buf1 : buf0;
+    const double* prev = (d & 1) ? buf0 : buf1;
+    if (d > 0) cluster_wait_acquire();
+    const int ip = d - jp - kp;
+    const bool act = has && ip >= 0 && ip < nx;
+    double v[MO];
+    double gs = 0.0, qs = 0.0;
+    if (act) {
+      if (z_remote) nbase = cl.map_shared_rank(const_cast<double*>(prev), rank - 1) +
+                            (size_t)(a.rows - 1) * ny + jp;
+      double zr[MO];
+      if (z_remote) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) zr[m] = nbase[(size_t)m * S];
+      }
+#pragma unroll
+      for (int m = 0; m < MO; ++m) {
+        const double* pm = prev + (size_t)m * S;
+        const double Ix = ip > 0 ? pm[q] : a.I_amb;
+        const double Iy = jp > 0 ? pm[q - 1] : (a.periodic ? win[m] : a.I_amb);
+        double Iz;
+        if (kl > 0) Iz = pm[q - ny];
+        else if (kp > 0) Iz = zr[m];
+        else Iz = fz ? Igc : a.I_amb;
+        const double ix = cix[m], iy = ciy[m], iz = izt[m * nz + k];
+        const double num = kab.y + ix * Ix + iy * Iy + iz * Iz;
+        const double den = kab.x + ix + iy + iz;
+        v[m] = num / den;
+        cur[(size_t)m * S + q] = v[m];
+        gs = gs + cw[m] * v[m];
+        if (ground_out) qs = qs + cwm[m] * v[m];
+      }
+    }
+    cluster_arrive_release();
+    if (act) {
+      const int i = fx ? ip : nx - 1 - ip;
+      Go[((int64_t)k * ny + j) * nx + i] = gs;
+      if (y_wrap_out) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) wrap0[m * wstride + (int64_t)k * nx + i] = v[m];
+      }
+      if (ground_out) a.Qoct[(int64_t)slot * n2 + (int64_t)j * nx + i] = qs;
+    }
+    if (d + 1 < nplanes) prefetch(d + 1);
+  }
+  cluster_wait_acquire();
+}
+
+// ---- pipelined variant: point-to-point hand-off between neighbouring CTAs ----
+// CTA r needs, on hyperplane d, the last row of CTA r-1 from hyperplane d-1.
+// Instead of a cluster-wide barrier per hyperplane, CTA r-1's last-row
+// threads store those values straight into an inbox ring in CTA r's shared
+// memory (distributed shared memory) and arrive on that slot's "full"
+// mbarrier; CTA r's first-row threads wait on it, read, and arrive on the
+// producer's "empty" mbarrier for the slot.  Each CTA then only waits for
+// its upstream neighbour and the CTAs run as a skewed pipeline; inside a
+// CTA one __syncthreads per hyperplane orders the shared buffers.  Every
+// wait is bounded: on expiry the kernel records the failure in *err and
+// runs to completion without waiting further.
+#define OCT_WAIT_LIMIT 2000000
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint32_t cluster_map_u32(uint32_t a, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t remote_a) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote_a)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; false (and *err set) if it gave up or an earlier wait had
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t a, uint32_t parity, int* err) {
+  if (mbar_try_wait(a, parity)) return true;
+  for (int it = 1; it < OCT_WAIT_LIMIT; ++it) {
+    if (mbar_try_wait(a, parity)) return true;
+    if ((it & 1023) == 0 && *(volatile int*)err) return false;  // another wait gave up
+  }
+  atomicExch(err, 1);
+  return false;
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int MO>
+__global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_pipe(GridDev g, OctArgs a) {
+  extern __shared__ __align__(16) unsigned char shraw[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int rank = (int)cl.block_rank();
+  const int C = a.C;
+  const int oct = blockIdx.x / C;
+  const int n0 = oct * MO;
+  const int rows = a.rows;
+  const int S = rows * ny;
+  unsigned long long* mb_full = (unsigned long long*)shraw;   // this CTA's inbox slots
+  unsigned long long* mb_empty = mb_full + OCT_RING;          // this CTA's outbox slots
+  double* inbox = (double*)(shraw + 16 * OCT_RING);           // OCT_RING x MO x ny
+  double2* kab_ring = (double2*)(inbox + (size_t)OCT_RING * MO * ny);  // OCT_AHEAD x S
+  double* wrap_ring = (double*)(kab_ring + (size_t)OCT_AHEAD * S);     // OCT_AHEAD x MO x rows
+  double* ig_ring = wrap_ring + (size_t)OCT_AHEAD * MO * rows;         // OCT_AHEAD x ny
+  double* buf0 = ig_ring + (size_t)OCT_AHEAD * ny;
+  double* buf1 = buf0 + (size_t)MO * S;
+  double* izt = buf1 + (size_t)MO * S;
+  double* cix = izt + (size_t)MO * nz;
+  double* ciy = cix + MO;
+  double* cw = ciy + MO;
+  double* cwm = cw + MO;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < OCT_RING; ++s) {
+      mbar_init(smem_u32(mb_full + s), (uint32_t)ny);
+      mbar_init(smem_u32(mb_empty + s), (uint32_t)ny);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int t = threadIdx.x; t < MO * nz; t += blockDim.x) {
+    const int m = t / nz, k = t - m * nz;
+    izt[t] = fabs(a.oz[n0 + m]) / g.dz[k];
+  }
+  for (int m = threadIdx.x; m < MO; m += blockDim.x) {
+    cix[m] = fabs(a.ox[n0 + m]) / g.dx;
+    ciy[m] = fabs(a.oy[n0 + m]) / g.dy;
+    cw[m] = a.w[n0 + m];
+    cwm[m] = a.w[n0 + m] * fabs(a.oz[n0 + m]);
+  }
+  const bool fx = a.ox[n0] >= 0.0, fy = a.oy[n0] >= 0.0, fz = a.oz[n0] >= 0.0;
+  const int r0 = rank * rows;
+  const int nrows = min(rows, nz - r0);
+  const int npen = nrows > 0 ? nrows * ny : 0;
+  const int q = threadIdx.x;
+  const bool has = q < npen;
+  const int kl = has ? q / ny : 0;
+  const int jp = has ? q - kl * ny : 0;
+  const int kp = r0 + kl;
+  const int j = fy ? jp : ny - 1 - jp;
+  const int k = fz ? kp : nz - 1 - kp;
+  const int64_t N = ncells_dev(g);
+  const int64_t n2 = (int64_t)nx * ny;
+  const int slot_bits = (int)((a.down_slots >> (4 * oct)) & 15u);
+  const int slot = slot_bits == 15 ? -1 : slot_bits;
+  double* Go = a.Goct + (int64_t)oct * N;
+  const int64_t wstride = (int64_t)nz * nx;
+  double* wrap0 = a.wrap + (int64_t)n0 * wstride;
+  const bool ground_out = has && !fz && k == 0 && slot >= 0;
+  const bool z_in_ground = has && fz && kp == 0;
+  const bool consumer = has && kl == 0 && rank > 0;
+  const bool producer = has && kl == rows - 1 && rank < C - 1;
+  const bool y_wrap = has && jp == 0 && a.periodic;
+  const bool y_wrap_out = has && jp == ny - 1 && a.periodic;
+  double* down_inbox = producer ? cl.map_shared_rank(inbox, rank + 1) : nullptr;
+  const uint32_t full_u32 = smem_u32(mb_full), empty_u32 = smem_u32(mb_empty);
+  const uint32_t down_full = producer ? cluster_map_u32(full_u32, rank + 1) : 0u;
+  const uint32_t up_empty = consumer ? cluster_map_u32(empty_u32, rank - 1) : 0u;
+  const int nplanes = nx + ny + nz - 2;
+  const int64_t row_base = ((int64_t)k * ny + j) * nx;
+  // asynchronous copies of plane d's inputs into ring slot d % OCT_AHEAD (one group per plane)
+  auto prefetch = [&](int d) {
+    const int ip = d - jp - kp;
+    if (has && ip >= 0 && ip < nx) {
+      const int i = fx ? ip : nx - 1 - ip;
+      const int sl = d % OCT_AHEAD;
+      cp_async16(&kab_ring[(size_t)sl * S + q], &a.kb[row_base + i]);
+      if (y_wrap) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m)
+          cp_async8(&wrap_ring[((size_t)sl * MO + m) * rows + kl],
+                    &wrap0[m * wstride + (int64_t)k * nx + i]);
+      }
+      if (z_in_ground) cp_async8(&ig_ring[(size_t)sl * ny + jp], &a.Ig[(int64_t)j * nx + i]);
+    }
+    cp_async_commit();
+  };
+  for (int d = 0; d < OCT_AHEAD - 1; ++d) prefetch(d);
+  // every CTA's barriers are initialised before anyone arrives remotely
+  cluster_arrive_release();
+  cluster_wait_acquire();
+  for (int d = 0; d < nplanes; ++d) {
+    prefetch(d + OCT_AHEAD - 1);   // an empty group past the last plane
+    double* cur = (d & 1) ? buf1 : buf0;
+    const double* prev = (d & 1) ? buf0 : buf1;
+    const int ip = d - jp - kp;
+    const bool act = has && ip >= 0 && ip < nx;
+    double zr[MO];
+    if (consumer && d > 0) {
+      const int sl = (d - 1) % OCT_RING;
+      mbar_wait_bounded(full_u32 + 8u * sl, (uint32_t)(((d - 1) / OCT_RING) & 1), a.err);
+      if (act) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) zr[m] = inbox[((size_t)sl * MO + m) * ny + jp];
+      }
+      mbar_arrive_cluster(up_empty + 8u * sl);
+    }
+    cp_async_wait<OCT_AHEAD - 1>();   // this plane's group has landed
+    double v[MO];
+    double gs = 0.0, qs = 0.0;
+    if (act) {
+      const int sl = d % OCT_AHEAD;
+      const double2 kab = kab_ring[(size_t)sl * S + q];
+#pragma unroll
+      for (int m = 0; m < MO; ++m) {
+        const double* pm = prev + (size_t)m * S;
+        const double Ix = ip > 0 ? pm[q] : a.I_amb;
+        double Iy;
+        if (jp > 0) Iy = pm[q - 1];
+        else Iy = a.periodic ? wrap_ring[((size_t)sl * MO + m) * rows + kl] : a.I_amb;
+        double Iz;
+        if (kl > 0) Iz = pm[q - ny];
+        else if (kp > 0) Iz = zr[m];
+        else Iz = fz ? ig_ring[(size_t)sl * ny + jp] : a.I_amb;
+        const double ix = cix[m], iy = ciy[m], iz = izt[m * nz + k];
+        const double num = kab.y + ix * Ix + iy * Iy + iz * Iz;
+        const double den = kab.x + ix + iy + iz;
+        v[m] = num / den;
+        cur[(size_t)m * S + q] = v[m];
+        gs = gs + cw[m] * v[m];
+        if (ground_out) qs = qs + cwm[m] * v[m];
+      }
+    }
+    if (producer) {
+      const int sl = d % OCT_RING;
+      if (d >= OCT_RING)
+        mbar_wait_bounded(empty_u32 + 8u * sl, (uint32_t)(((d / OCT_RING) - 1) & 1), a.err);
+      if (act) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) down_inbox[((size_t)sl * MO + m) * ny + jp] = v[m];
+      }
+      mbar_arrive_cluster(down_full + 8u * sl);
+    }
+    if (act) {
+      const int i = fx ? ip : nx - 1 - ip;
+      Go[row_base + i] = gs;
+      if (y_wrap_out) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) wrap0[m * wstride + (int64_t)k * nx + i] = v[m];
+      }
+      if (ground_out) a.Qoct[(int64_t)slot * n2 + (int64_t)j * nx + i] = qs;
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+  // nobody leaves while a neighbour may still touch its shared memory
+  cluster_arrive_release();
+  cluster_wait_acquire();
+}
+
+template <int MO>
+static cudaError_t launch_octant_kernel(const GridDev& g, const OctArgs& a, cudaLaunchConfig_t* cfg) {
+  return cudaLaunchKernelEx(cfg, k_dom_octant<MO>, g, a);
+}
+
+template <int MO>
+static cudaError_t launch_octant_pipe_kernel(const GridDev& g, const OctArgs& a,
+                                             cudaLaunchConfig_t* cfg) {
+  return cudaLaunchKernelEx(cfg, k_dom_octant_pipe<MO>, g, a);
+}
+
+// pipe: the point-to-point pipelined kernel (path 1), else the cluster-barrier one (path 4)
+static const void* octant_kernel_ptr(int Mo, bool pipe) {
+  switch (Mo) {
+    case 3: return pipe ? (const void*)k_dom_octant_pipe<3> : (const void*)k_dom_octant<3>;
+    case 6: return pipe ? (const void*)k_dom_octant_pipe<6> : (const void*)k_dom_octant<6>;
+    case 10: return pipe ? (const void*)k_dom_octant_pipe<10> : (const void*)k_dom_octant<10>;
+    default: return nullptr;
+  }
+}
+
+// G = sum over octants of the octant partials (octant order); max G and max |G - G_prev|
+__global__ void k_dom_G_oct(int64_t N, const double* __restrict__ Goct, double* G,
+                            const double* __restrict__ Gp, unsigned long long* keys) {
+  unsigned long long bg = 0, bd = 0;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < N;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int o = 0; o < 8; ++o) s += Goct[(int64_t)o * N + c];
+    G[c] = s;
+    double d = fabs(s - Gp[c]);
+    unsigned long long ks = (s != s) ? 0x7ff8000000000000ull
+                                     : (unsigned long long)__double_as_longlong(s > 0.0 ? s : 0.0);
+    unsigned long long kd = (d != d) ? 0x7ff8000000000000ull
+                                     : (unsigned long long)__double_as_longlong(d);
+    bg = ks > bg ? ks : bg;
+    bd = kd > bd ? kd : bd;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long y = __shfl_xor_sync(0xffffffffu, bg, o);
+    bg = y > bg ? y : bg;
+    y = __shfl_xor_sync(0xffffffffu, bd, o);
+    bd = y > bd ? y : bd;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(keys, bg);
+    atomicMax(keys + 1, bd);
+  }
+}
+
+// q_in at the ground from the downward octants' partial fluxes; ground intensity relaxation
+__global__ void k_dom_ground_oct(int n2, int nslots, const double* __restrict__ Qoct,
+                                 const double* __restrict__ Isoil, double refl, double relax,
+                                 double* Ig, double* qin) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n2) return;
+  double s = 0.0;
+  for (int o = 0; o < nslots; ++o) s += Qoct[(int64_t)o * n2 + q];
+  qin[q] = s;
+  double Inew = Isoil[q] + refl * s;
+  Ig[q] = relax * Inew + (1.0 - relax) * Ig[q];
+}
+
+// wrap rows from a full intensity field: wrap[n][k][i] = I[n][k][j_far][i]
+__global__ void k_dom_extract_wrap(GridDev g, int M, const double* __restrict__ oy,
+                                   const double* __restrict__ I, double* wrap) {
+  const int64_t tot = (int64_t)M * g.nz * g.nx;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= tot) return;
+  const int n = (int)(t / ((int64_t)g.nz * g.nx));
+  const int64_t r = t - (int64_t)n * g.nz * g.nx;
+  const int k = (int)(r / g.nx);
+  const int i = (int)(r - (int64_t)k * g.nx);
+  const int jf = oy[n] >= 0.0 ? g.ny - 1 : 0;
+  wrap[t] = I[(int64_t)n * ncells_dev(g) + cidx(g, k, jf, i)];
+}
+
 __global__ void k_dom_finish(GridDev g, const double* __restrict__ ks, const double* __restrict__ kg,
                              const double* __restrict__ ksafe, const double* __restrict__ B,
                              const double* __restrict__ G, double* qs, double* qg) {
@@ -279,8 +774,8 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   cudaMemcpy(D->oy, oy, sizeof(double) * M, cudaMemcpyHostToDevice);
   cudaMemcpy(D->oz, oz, sizeof(double) * M, cudaMemcpyHostToDevice);
   cudaMemcpy(D->w, w, sizeof(double) * M, cudaMemcpyHostToDevice);
-  cudaMalloc(&D->I, sizeof(double) * N * M);
-  cudaMemset(D->I, 0, sizeof(double) * N * M);
+  D->I = nullptr; D->wrap = nullptr; D->kb = nullptr; D->Goct = nullptr; D->Qoct = nullptr;
+  D->mode = 0; D->mode_req = 0; D->force_C = 0;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemset(D->G, 0, sizeof(double) * N);
   cudaMalloc(&D->ks, sizeof(double) * N); cudaMalloc(&D->kg, sizeof(double) * N);
@@ -307,6 +802,7 @@ void dom_destroy(void* h) {
   DomCtx* D = (DomCtx*)h;
   if (!D) return;
   cudaFree(D->ox); cudaFree(D->oy); cudaFree(D->oz); cudaFree(D->w); cudaFree(D->I);
+  cudaFree(D->wrap); cudaFree(D->kb); cudaFree(D->Goct); cudaFree(D->Qoct);
   cudaFree(D->G); cudaFree(D->Gp); cudaFree(D->ks); cudaFree(D->kg); cudaFree(D->ksafe);
   cudaFree(D->B); cudaFree(D->Ig_out); cudaFree(D->Isoil); cudaFree(D->qin); cudaFree(D->keys);
   cudaFreeHost(D->h_keys);
@@ -315,6 +811,140 @@ void dom_destroy(void* h) {
     cudaEventDestroy(D->ev1[q]);
   }
   delete D;
+}
+
+// Octant grouping required by path 1: M = 8*Mo, ordinates octant-major, every
+// ordinate of a group with the same signs and no zero component.
+static bool octant_grouping(const DomCtx* D) {
+  if (D->M % 8 != 0) return false;
+  const int Mo = D->M / 8;
+  for (int o = 0; o < 8; ++o) {
+    const int n0 = o * Mo;
+    for (int m = 0; m < Mo; ++m) {
+      const int n = n0 + m;
+      if (D->hox[n] == 0.0 || D->hoy[n] == 0.0 || D->hoz[n] == 0.0) return false;
+      if ((D->hox[n] > 0) != (D->hox[n0] > 0) || (D->hoy[n] > 0) != (D->hoy[n0] > 0) ||
+          (D->hoz[n] > 0) != (D->hoz[n0] > 0))
+        return false;
+    }
+  }
+  return true;
+}
+
+// Pick the cluster size (CTAs per octant) and launch shape for path 1; false if none fits.
+static bool plan_clusters(DomCtx* D, int force_C, bool pipe) {
+  const GridDev& g = D->g;
+  const int Mo = D->M / 8;
+  int dev = 0, optin = 0, smem_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  const void* fn = octant_kernel_ptr(Mo, pipe);
+  if (!fn) return false;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  double best = 1e300;
+  bool found = false;
+  for (int C = 16; C >= 1; --C) {
+    if (force_C > 0 && C != force_C) continue;
+    const int rows = (g.nz + C - 1) / C;
+    if ((g.nz + rows - 1) / rows != C) continue;  // same split as a smaller cluster
+    int threads = ((rows * g.ny + 31) / 32) * 32;
+    if (threads > OCT_MAX_THREADS) continue;
+    const size_t need = pipe ? oct_pipe_smem_bytes(Mo, rows, g.ny, g.nz)
+                             : oct_smem_bytes(Mo, rows, g.ny, g.nz);
+    if (need > (size_t)optin) continue;
+    // ask for more than half an SM's shared memory so that no two CTAs share an SM,
+    // unless that leaves fewer than 8 clusters resident
+    size_t pad = (size_t)smem_sm / 2 + 1024;
+    size_t trial[2] = {need > pad ? need : (pad <= (size_t)optin ? pad : need), need};
+    for (int t = 0; t < 2; ++t) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(8 * C); cfg.blockDim = dim3(threads);
+      cfg.dynamicSmemBytes = trial[t]; cfg.attrs = at; cfg.numAttrs = 1;
+      int active = 0;
+      if (cudaOccupancyMaxActiveClusters(&active, fn, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        active = 0;
+      }
+      if (active < 1) continue;
+      const int waves = (8 + active - 1) / active;
+      const int per_thread = (rows * g.ny + threads - 1) / threads;
+      double cost = (double)waves * per_thread * (t == 0 ? 1.0 : (active >= 8 ? 1.5 : 2.0));
+      if (cost < best) {
+        best = cost; found = true;
+        D->cl_C = C; D->cl_rows = rows; D->cl_threads = threads; D->cl_smem = trial[t];
+      }
+      if (t == 0 && active >= 8) break;
+    }
+  }
+  return found;
+}
+
+static int dom_prepare(DomCtx* D) {
+  if (D->mode != 0) return FS_OK;
+  const GridDev& g = D->g;
+  const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
+  const int want = D->mode_req;
+  // auto picks the cluster-barrier sweep (path 4), measured faster than path 1
+  if ((want == 0 || want == 1 || want == 4) && octant_grouping(D) &&
+      plan_clusters(D, D->force_C, want == 1)) {
+    D->mode = want == 1 ? 1 : 4;
+    D->Mo = D->M / 8;
+    int slot = 0;
+    for (int o = 0; o < 8; ++o) D->down_slot[o] = D->hoz[o * D->Mo] < 0.0 ? slot++ : -1;
+    cudaMalloc(&D->kb, sizeof(double2) * N);
+    cudaMalloc(&D->Goct, sizeof(double) * 8 * N);
+    cudaMalloc(&D->Qoct, sizeof(double) * 8 * n2);
+    cudaMalloc(&D->wrap, sizeof(double) * D->M * g.nz * g.nx);
+    cudaMemset(D->wrap, 0, sizeof(double) * D->M * g.nz * g.nx);
+    return cuda_status();
+  }
+  if (want == 1 || want == 4) {
+    fs_set_error("octant-cluster sweep not possible for this grid or quadrature");
+    return FS_EARG;
+  }
+  const size_t smem = sizeof(double) * 2 * (size_t)g.ny * g.nz;
+  int max_smem = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  D->mode = (want == 3 || smem > (size_t)max_smem) ? 3 : 2;
+  cudaMalloc(&D->I, sizeof(double) * N * D->M);
+  cudaMemset(D->I, 0, sizeof(double) * N * D->M);
+  return cuda_status();
+}
+
+int dom_set_mode(void* h, int mode, int cluster_ctas) {
+  DomCtx* D = (DomCtx*)h;
+  if (mode < 0 || mode > 4 || cluster_ctas < 0 || cluster_ctas > 16) return FS_EARG;
+  if (D->mode != 0) {
+    fs_set_error("sweep mode must be set before the first solve or intensity load");
+    return FS_EARG;
+  }
+  D->mode_req = mode;
+  D->force_C = cluster_ctas;
+  return FS_OK;
+}
+
+int dom_mode(void* h) { return ((DomCtx*)h)->mode; }
+
+int dom_load_intensity(void* h, const double* I_full, cudaStream_t st) {
+  DomCtx* D = (DomCtx*)h;
+  int rc = dom_prepare(D);
+  if (rc != FS_OK) return rc;
+  const GridDev& g = D->g;
+  if (D->mode == 1 || D->mode == 4) {
+    const int64_t tot = (int64_t)D->M * g.nz * g.nx;
+    k_dom_extract_wrap<<<blocks_for(tot, 256), 256, 0, st>>>(g, D->M, D->oy, I_full, D->wrap);
+    fs_count_launch();
+  } else {
+    cudaMemcpyAsync(D->I, I_full, sizeof(double) * ncells(g) * D->M, cudaMemcpyDeviceToDevice,
+                    st);
+  }
+  return cuda_status();
 }
 
 void dom_set_timing(void* h, int on) {
@@ -340,58 +970,119 @@ static double key_to_double(unsigned long long k) {
   return d;
 }
 
+static int launch_octant_sweep(DomCtx* D, const OctArgs& a, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = D->cl_C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(8 * D->cl_C);
+  cfg.blockDim = dim3(D->cl_threads);
+  cfg.dynamicSmemBytes = D->cl_smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaError_t e;
+  const bool pipe = D->mode == 1;
+  switch (D->Mo) {
+    case 3: e = pipe ? launch_octant_pipe_kernel<3>(D->g, a, &cfg)
+                     : launch_octant_kernel<3>(D->g, a, &cfg); break;
+    case 6: e = pipe ? launch_octant_pipe_kernel<6>(D->g, a, &cfg)
+                     : launch_octant_kernel<6>(D->g, a, &cfg); break;
+    case 10: e = pipe ? launch_octant_pipe_kernel<10>(D->g, a, &cfg)
+                      : launch_octant_kernel<10>(D->g, a, &cfg); break;
+    default: e = cudaErrorInvalidValue;
+  }
+  fs_count_launch();
+  return e == cudaSuccess ? FS_OK : FS_ECUDA;
+}
+
 int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, const double* om,
               double sigma, double T_amb, const double* Tsoil0, const double* YH, const double* rho,
               const double* Mloc, double* q_solid, double* q_gas, double* q_in_soil,
               cudaStream_t st) {
   DomCtx* D = (DomCtx*)h;
+  int rc = dom_prepare(D);
+  if (rc != FS_OK) return rc;
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
   const int M = D->M;
+  const bool octp = D->mode == 1 || D->mode == 4;
   const double Tamb4 = pow(T_amb, 4.0);
   k_dom_setup<<<blocks_for(N, 256), 256, 0, st>>>(g, Ts, Tg, as, om, YH, rho, Mloc, sigma, Tamb4,
-                                                  D->kgmax, D->ks, D->kg, D->ksafe, D->B); fs_count_launch();
+                                                  D->kgmax, D->ks, D->kg, D->ksafe, D->B,
+                                                  octp ? D->kb : nullptr);
+  fs_count_launch();
   const double I_amb = SIGMA_SB_D * Tamb4 / PI_D;
   k_dom_ground_init<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, Tsoil0, D->eps_w, I_amb, D->Isoil,
-                                                        D->Ig_out); fs_count_launch();
+                                                        D->Ig_out);
+  fs_count_launch();
   SweepArgs a{};
   a.ox = D->ox; a.oy = D->oy; a.oz = D->oz; a.I = D->I; a.ksafe = D->ksafe; a.B = D->B;
   a.Ig = D->Ig_out; a.I_amb = I_amb; a.inv_dx = 1.0 / g.dx; a.inv_dy = 1.0 / g.dy; a.M = M;
   a.periodic = 1;
+  OctArgs oa{};
+  if (octp) {
+    oa.kb = D->kb; oa.ox = D->ox; oa.oy = D->oy; oa.oz = D->oz; oa.w = D->w; oa.Ig = D->Ig_out;
+    oa.Goct = D->Goct; oa.Qoct = D->Qoct; oa.wrap = D->wrap; oa.I_amb = I_amb; oa.Mo = D->Mo;
+    oa.C = D->cl_C; oa.rows = D->cl_rows; oa.periodic = 1;
+    oa.err = (int*)(D->keys + 2);
+    oa.down_slots = 0;
+    for (int o = 0; o < 8; ++o)
+      oa.down_slots |= (unsigned)(D->down_slot[o] >= 0 ? D->down_slot[o] : 15) << (4 * o);
+  }
+  int nslots = 0;
+  for (int o = 0; o < 8; ++o) nslots += (octp && D->down_slot[o] >= 0) ? 1 : 0;
   const int nplanes = g.nx + g.ny + g.nz - 2;
   const int64_t nthr = (int64_t)g.ny * g.nz * M;
   const double refl = (1.0 - D->eps_w) / PI_D;
-  int it;
   const size_t smem = sizeof(double) * 2 * (size_t)g.ny * g.nz;
-  int max_smem = 0, dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const bool block_sweep = smem <= (size_t)max_smem;
-  if (block_sweep)
+  if (D->mode == 2)
     cudaFuncSetAttribute(k_dom_sweep_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
+  cudaMemsetAsync(D->keys + 2, 0, sizeof(unsigned long long), st);
+  int it;
   for (it = 0; it < D->max_iter; ++it) {
     std::swap(D->G, D->Gp);
-    if (block_sweep) {
-      if (D->timing) cudaEventRecord(D->ev0[it], st);
-      k_dom_sweep_block<<<M, 1024, smem, st>>>(g, a); fs_count_launch();
-      if (D->timing) cudaEventRecord(D->ev1[it], st);
+    if (D->timing) cudaEventRecord(D->ev0[it], st);
+    if (octp) {
+      rc = launch_octant_sweep(D, oa, st);
+      if (rc != FS_OK) return rc;
+    } else if (D->mode == 2) {
+      k_dom_sweep_block<<<M, 1024, smem, st>>>(g, a);
+      fs_count_launch();
     } else {
       for (int d = 0; d < nplanes; ++d) {
         a.plane = d;
-        k_dom_plane<<<blocks_for(nthr, 256), 256, 0, st>>>(g, a); fs_count_launch();
+        k_dom_plane<<<blocks_for(nthr, 256), 256, 0, st>>>(g, a);
+        fs_count_launch();
       }
     }
-    cudaMemsetAsync(D->keys, 0, sizeof(unsigned long long) * 2, st);
+    if (D->timing) cudaEventRecord(D->ev1[it], st);
+    cudaMemsetAsync(D->keys, 0, sizeof(unsigned long long) * 2, st);  // keys[2] keeps the wait flag
     unsigned nb = blocks_for(N, 256);
     if (nb > 1184) nb = 1184;
-    k_dom_G<<<nb, 256, 0, st>>>(N, M, D->w, D->I, D->G, D->Gp, D->keys); fs_count_launch();
-    k_dom_ground<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, M, D->oz, D->w, D->I, N, D->Isoil,
-                                                      refl, D->relax, D->Ig_out, D->qin); fs_count_launch();
+    if (octp) {
+      k_dom_G_oct<<<nb, 256, 0, st>>>(N, D->Goct, D->G, D->Gp, D->keys);
+      fs_count_launch();
+      k_dom_ground_oct<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, nslots, D->Qoct, D->Isoil,
+                                                            refl, D->relax, D->Ig_out, D->qin);
+      fs_count_launch();
+    } else {
+      k_dom_G<<<nb, 256, 0, st>>>(N, M, D->w, D->I, D->G, D->Gp, D->keys);
+      fs_count_launch();
+      k_dom_ground<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, M, D->oz, D->w, D->I, N,
+                                                        D->Isoil, refl, D->relax, D->Ig_out,
+                                                        D->qin);
+      fs_count_launch();
+    }
     if (it > 0) {
-      cudaMemcpyAsync(D->h_keys, D->keys, sizeof(unsigned long long) * 2, cudaMemcpyDeviceToHost,
+      cudaMemcpyAsync(D->h_keys, D->keys, sizeof(unsigned long long) * 3, cudaMemcpyDeviceToHost,
                       st);
-      if (cudaStreamSynchronize(st) != cudaSuccess) return FS_ECUDA;
+      if (fs_stream_wait(st) != FS_OK) return FS_ECUDA;
+      if ((int)D->h_keys[2] != 0) {
+        fs_set_error("fs_dom_solve: pipelined sweep wait gave up (hand-off between CTAs stalled)");
+        return FS_ETIMEOUT;
+      }
       double Gmax = key_to_double(D->h_keys[0]);
       double dmax = key_to_double(D->h_keys[1]);
       if (Gmax != Gmax || dmax != dmax) return FS_ENONFINITE;
@@ -400,7 +1091,7 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
     }
   }
   D->last_iters = it;
-  if (D->timing && block_sweep) {
+  if (D->timing) {
     cudaEventSynchronize(D->ev1[it - 1]);
     for (int q = 0; q < it; ++q) {
       float ms = 0.f;
@@ -410,8 +1101,11 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
     }
   }
   k_dom_finish<<<blocks_for(N, 256), 256, 0, st>>>(g, D->ks, D->kg, D->ksafe, D->B, D->G, q_solid,
-                                                   q_gas); fs_count_launch();
+                                                   q_gas);
+  fs_count_launch();
   if (q_in_soil) {
-    k_scale2<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, D->qin, D->eps_w, q_in_soil); fs_count_launch(); }
+    k_scale2<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, D->qin, D->eps_w, q_in_soil);
+    fs_count_launch();
+  }
   return cuda_status();
 }

@@ -88,6 +88,7 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
                  const double* target, double dt, double rtol, int maxiter, int* iters,
                  cudaStream_t st);
 int proj_apply(void* h, const double* x, double* y, cudaStream_t st);
+int proj_configure(void* h, int nu, double omega);
 int launch_div_resid_max(const GridDev& g, const double* u, const double* v, const double* w,
                          const double* u_in, const double* target, double* div_out,
                          unsigned long long* out_key, cudaStream_t st);
@@ -96,6 +97,9 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
                  const double* w, double kgmax);
 void dom_destroy(void* h);
 double* dom_intensity(void* h);
+int dom_set_mode(void* h, int mode, int cluster_ctas);
+int dom_mode(void* h);
+int dom_load_intensity(void* h, const double* I_full, cudaStream_t st);
 double* dom_G(void* h);
 int dom_last_iters(void* h);
 void dom_set_timing(void* h, int on);

@@ -53,11 +53,44 @@ __global__ void k_edc_agg(int64_t n, const double* __restrict__ Yf, const double
   if (threadIdx.x == 0) agg[blockIdx.x] = (signed char)(v < 0 ? -1 : (v & 1));
 }
 
-__global__ void k_edc_carry(int nb, const signed char* agg, signed char* carry,
-                            const signed char* carry_in) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  signed char cur = carry_in ? carry_in[0] : 0;
-  for (int b = 0; b < nb; ++b) {
+// Carry of the last assigned flag into every block: each thread folds a
+// contiguous run of blocks, a block-wide max-scan of (block << 1 | flag)
+// gives every run its incoming flag, then each thread writes its run.
+#define EDC_CARRY_THREADS 1024
+__global__ void __launch_bounds__(EDC_CARRY_THREADS)
+k_edc_carry(int nb, const signed char* agg, signed char* carry, const signed char* carry_in) {
+  __shared__ int incl[EDC_CARRY_THREADS];
+  __shared__ int wsum[32];
+  const int t = threadIdx.x;
+  const int per = (nb + EDC_CARRY_THREADS - 1) / EDC_CARRY_THREADS;
+  const int b0 = t * per;
+  const int b1 = min(nb, b0 + per);
+  int last = -1;
+  for (int b = b0; b < b1; ++b)
+    if (agg[b] >= 0) last = (b << 1) | agg[b];
+  const int lane = t & 31, wid = t >> 5;
+  int v = last;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v = max(v, y);
+  }
+  if (lane == 31) wsum[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    int w = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w = max(w, y);
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  if (wid > 0) v = max(v, wsum[wid - 1]);
+  incl[t] = v;
+  __syncthreads();
+  const int before = t > 0 ? incl[t - 1] : -1;
+  signed char cur = before >= 0 ? (signed char)(before & 1) : (carry_in ? carry_in[0] : 0);
+  for (int b = b0; b < b1; ++b) {
     carry[b] = cur;
     if (agg[b] >= 0) cur = agg[b];
   }
@@ -183,7 +216,7 @@ int launch_edc(int64_t n, const double* rho, double* Tg, double* Yf, double* YO,
   signed char* agg = (signed char*)scratch;
   signed char* carry = agg + nb;
   k_edc_agg<<<(unsigned)nb, EDC_BLK, 0, st>>>(n, Yf, YO, YH, agg); fs_count_launch();
-  k_edc_carry<<<1, 32, 0, st>>>((int)nb, agg, carry, nullptr); fs_count_launch();
+  k_edc_carry<<<1, EDC_CARRY_THREADS, 0, st>>>((int)nb, agg, carry, nullptr); fs_count_launch();
   EdcArgs a{};
   a.rho = rho; a.Tg = Tg; a.Yf = Yf; a.YO = YO; a.kt = kt; a.et = et; a.YH = YH;
   a.omega = omega; a.carry = carry;

@@ -14,7 +14,7 @@
 //   * coarse cells aggregate 2x2x2 fine cells (odd tails keep 1);
 //   * coarse operator = 1/2 (P^T S P) with piecewise-constant P, which keeps
 //     the face-conductance form (coarse face = sum of fine faces across it);
-//   * 2 pre- and 2 post-sweeps of damped Jacobi (omega = 0.8);
+//   * nu pre- and nu post-sweeps of damped Jacobi (default nu = 4, omega = 0.8);
 //   * the coarsest level (<= 64 cells) is solved with a dense inverse built
 //     at each rebuild.
 // The stopping test mirrors scipy's: ||b - A x||_2 < rtol ||b||_2 on the
@@ -26,15 +26,24 @@
 
 #define PROJ_EPS 1.0e-6
 #define MG_OMEGA 0.8
+#define MG_NU_DEFAULT 4
 #define MG_COARSE_MAX 48
 #define RED_BLOCKS 296
 #define RED_THREADS 256
+// Device scalar slots: 0 rz, 1 pq, 2 rz_new, 4 ||b_A||^2, 5 ||r_A||^2,
+// 6 (rtol ||b_A||)^2, 7 converged flag, 8 iterations done.
+#define SC_DONE 7
+#define SC_IT 8
+// Kernels of a PCG iteration return at once when the solve has converged,
+// so iterations queued past convergence change nothing.
+#define PCG_SKIP(done) \
+  if ((done) && *(done) != 0.0) return;
 
 struct MGLevel {
   int nx, ny, nz;
   int64_t n;
   double *gx, *gy, *gz, *e, *dinv;  // conductances, per-cell term, 1/diag
-  double *x, *b, *t;                // correction, rhs, temp
+  double *x, *b, *t, *s;            // correction, rhs, temps
 };
 
 struct ProjCtx {
@@ -53,6 +62,13 @@ struct ProjCtx {
   double* p_prev;     // warm start / solution (owned)
   double* ir;         // 1/max(rho, 0.01)
   int have_prev;
+  int last_iters;     // CG iterations of the previous solve (batch size hint)
+  cudaStream_t cs;    // private stream for graph capture
+  cudaGraphExec_t iter_exec;  // one captured PCG iteration (0 until captured)
+  int iter_kernels;   // kernels in that graph
+  int graph_failed;
+  int nu;             // Jacobi sweeps before and after the coarse correction
+  double omega;       // Jacobi damping
 };
 
 // ---------------------------------------------------------------------------
@@ -230,7 +246,8 @@ __global__ void k_mg_coarse_inverse(int nx, int ny, int nz, const double* __rest
 }
 
 __global__ void k_mg_coarse_solve(int n, const double* __restrict__ Ainv,
-                                  const double* __restrict__ b, double* x) {
+                                  const double* __restrict__ b, double* x, const double* done) {
+  PCG_SKIP(done);
   int r = threadIdx.x;
   if (r >= n) return;
   double s = 0.0;
@@ -243,7 +260,8 @@ __global__ void k_mg_jacobi(int nx, int ny, int nz, const double* __restrict__ g
                             const double* __restrict__ gy, const double* __restrict__ gz,
                             const double* __restrict__ e, const double* __restrict__ dinv,
                             const double* __restrict__ b, const double* __restrict__ x, double* xo,
-                            double w) {
+                            double w, const double* done) {
+  PCG_SKIP(done);
   int64_t n = (int64_t)nx * ny * nz;
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -264,7 +282,8 @@ __global__ void k_mg_restrict_residual(int fx, int fy, int fz, const double* __r
                                        const double* __restrict__ gz,
                                        const double* __restrict__ e, const double* __restrict__ b,
                                        const double* __restrict__ x, int cx, int cy, int cz,
-                                       double* bc) {
+                                       double* bc, const double* done) {
+  PCG_SKIP(done);
   int64_t n = (int64_t)cx * cy * cz;
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= n) return;
@@ -284,7 +303,8 @@ __global__ void k_mg_restrict_residual(int fx, int fy, int fz, const double* __r
 
 // x_f += P x_c (piecewise constant)
 __global__ void k_mg_prolong(int fx, int fy, int fz, double* x, int cx, int cy,
-                             const double* __restrict__ xc) {
+                             const double* __restrict__ xc, const double* done) {
+  PCG_SKIP(done);
   int64_t n = (int64_t)fx * fy * fz;
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -322,7 +342,9 @@ __device__ __forceinline__ void block_sums_store(double (&v)[NV], double* partia
   }
 }
 
-__global__ void k_finish_sums(const double* __restrict__ partial, int nv, double* out) {
+__global__ void k_finish_sums(const double* __restrict__ partial, int nv, double* out,
+                              const double* done) {
+  PCG_SKIP(done);
   int q = threadIdx.x >> 5;
   int lane = threadIdx.x & 31;
   if (q >= nv) return;
@@ -367,7 +389,8 @@ __global__ void k_proj_rhs(GridDev g, const double* __restrict__ u, const double
 __global__ void k_pcg_matvec(int nx, int ny, int nz, const double* __restrict__ gx,
                              const double* __restrict__ gy, const double* __restrict__ gz,
                              const double* __restrict__ e, const double* __restrict__ p, double* q,
-                             double* partial) {
+                             double* partial, const double* done) {
+  PCG_SKIP(done);
   const int64_t n = (int64_t)nx * ny * nz;
   double acc[1] = {0.0};
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
@@ -407,6 +430,7 @@ __global__ void k_pcg_residual(GridDev g, const double* __restrict__ gx,
 __global__ void k_pcg_update(GridDev g, const double* __restrict__ scal, double* x, double* r,
                              const double* __restrict__ p, const double* __restrict__ q,
                              double* partial) {
+  PCG_SKIP(scal + SC_DONE);
   const int64_t n = ncells_dev(g);
   const double alpha = scal[0] / scal[1];
   const int64_t sz = (int64_t)g.nx * g.ny;
@@ -424,7 +448,8 @@ __global__ void k_pcg_update(GridDev g, const double* __restrict__ scal, double*
 
 // partial of r.z
 __global__ void k_dot(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
-                      double* partial) {
+                      double* partial, const double* done) {
+  PCG_SKIP(done);
   double acc[1] = {0.0};
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)RED_BLOCKS * blockDim.x)
@@ -432,17 +457,41 @@ __global__ void k_dot(int64_t n, const double* __restrict__ a, const double* __r
   block_sums_store<1>(acc, partial);
 }
 
-// p = z + beta p, beta = rz_new / rz_old ; first iteration (flag) p = z
+// p = z + beta p, beta = rz_new / rz_old ; first iteration p = z
 __global__ void k_pcg_dir(int64_t n, const double* __restrict__ scal, const double* __restrict__ z,
-                          double* p, int first) {
+                          double* p) {
+  PCG_SKIP(scal + SC_DONE);
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
-  if (first) { p[c] = z[c]; return; }
+  if (scal[SC_IT] == 0.0) { p[c] = z[c]; return; }
   double beta = scal[2] / scal[0];
   p[c] = z[c] + beta * p[c];
 }
 
-__global__ void k_set_scal(double* scal, int dst, int src) { scal[dst] = scal[src]; }
+__global__ void k_set_scal(double* scal, int dst, int src) {
+  PCG_SKIP(scal + SC_DONE);
+  scal[dst] = scal[src];
+}
+
+// end of an iteration: count it and test ||r_A|| < rtol ||b_A||
+__global__ void k_pcg_check(double* scal) {
+  if (scal[SC_DONE] != 0.0) return;
+  scal[SC_IT] += 1.0;
+  if (scal[5] < scal[6]) scal[SC_DONE] = 1.0;
+}
+
+// start of a solve: tolerance, initial test, iteration count; b == 0 -> x = 0
+__global__ void k_pcg_init(double* scal, double rtol2) {
+  scal[6] = rtol2 * scal[4];
+  scal[SC_IT] = 0.0;
+  scal[SC_DONE] = (scal[5] < scal[6] || scal[4] == 0.0) ? 1.0 : 0.0;
+}
+
+__global__ void k_zero_if_zero_rhs(int64_t n, const double* __restrict__ scal, double* x) {
+  if (scal[4] != 0.0) return;
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c < n) x[c] = 0.0;
+}
 
 // ---------------------------------------------------------------------------
 // velocity correction (projection_3d.py:818-842)
@@ -530,6 +579,7 @@ void* proj_create(const GridDev& g) {
     lv.nx = nx; lv.ny = ny; lv.nz = nz; lv.n = (int64_t)nx * ny * nz;
     lv.gx = dalloc(lv.n); lv.gy = dalloc(lv.n); lv.gz = dalloc(lv.n); lv.e = dalloc(lv.n);
     lv.dinv = dalloc(lv.n); lv.x = dalloc(lv.n); lv.b = dalloc(lv.n); lv.t = dalloc(lv.n);
+    lv.s = dalloc(lv.n);
     ++L;
     if (lv.n <= MG_COARSE_MAX || L >= 16) break;
     int cx = (nx + 1) / 2, cy = (ny + 1) / 2, cz = (nz + 1) / 2;
@@ -548,7 +598,15 @@ void* proj_create(const GridDev& g) {
   P->p_prev = dalloc(n0);
   P->ir = dalloc(n0);
   cudaMemset(P->p_prev, 0, sizeof(double) * n0);
+  cudaMemset(P->scal, 0, sizeof(double) * 16);
   P->have_prev = 0;
+  P->last_iters = 0;
+  P->iter_exec = nullptr;
+  P->iter_kernels = 0;
+  P->graph_failed = 0;
+  P->nu = MG_NU_DEFAULT;
+  P->omega = MG_OMEGA;
+  cudaStreamCreateWithFlags(&P->cs, cudaStreamNonBlocking);
   if (cudaGetLastError() != cudaSuccess || !P->p_prev) {
     proj_destroy(P);
     return nullptr;
@@ -562,8 +620,10 @@ void proj_destroy(void* h) {
   for (int l = 0; l < P->nlev; ++l) {
     MGLevel& lv = P->lev[l];
     cudaFree(lv.gx); cudaFree(lv.gy); cudaFree(lv.gz); cudaFree(lv.e); cudaFree(lv.dinv);
-    cudaFree(lv.x); cudaFree(lv.b); cudaFree(lv.t);
+    cudaFree(lv.x); cudaFree(lv.b); cudaFree(lv.t); cudaFree(lv.s);
   }
+  if (P->iter_exec) cudaGraphExecDestroy(P->iter_exec);
+  if (P->cs) cudaStreamDestroy(P->cs);
   cudaFree(P->Ainv); cudaFree(P->pc_r); cudaFree(P->pc_z); cudaFree(P->pc_p); cudaFree(P->pc_q);
   cudaFree(P->rhs); cudaFree(P->partial); cudaFree(P->scal); cudaFreeHost(P->h_scal);
   cudaFree(P->p_prev); cudaFree(P->ir);
@@ -594,54 +654,145 @@ int proj_rebuild(void* h, const double* rho, cudaStream_t st) {
   }
   MGLevel& c = P->lev[P->nlev - 1];
   if (c.n <= MG_COARSE_MAX) {
-    k_mg_coarse_inverse<<<1, 64, 0, st>>>(c.nx, c.ny, c.nz, c.gx, c.gy, c.gz, c.e, P->Ainv); fs_count_launch(); }
+    k_mg_coarse_inverse<<<1, 64, 0, st>>>(c.nx, c.ny, c.nz, c.gx, c.gy, c.gz, c.e, P->Ainv);
+    fs_count_launch();
+  }
   return cuda_status();
 }
 
-// z = V-cycle(r) on level l (b = rhs, x = result)
-static void vcycle(ProjCtx* P, int l, const double* b, double* x, cudaStream_t st) {
+// z = V-cycle(r) on level l (b = rhs, x = result); returns kernels launched
+static int vcycle(ProjCtx* P, int l, const double* b, double* x, const double* done,
+                  cudaStream_t st) {
   MGLevel& f = P->lev[l];
+  int nk = 0;
   if (l == P->nlev - 1) {
     if (f.n <= MG_COARSE_MAX) {
-      k_mg_coarse_solve<<<1, 64, 0, st>>>((int)f.n, P->Ainv, b, x); fs_count_launch();
+      k_mg_coarse_solve<<<1, 64, 0, st>>>((int)f.n, P->Ainv, b, x, done);
+      ++nk;
     } else {
       // not coarsenable and too large for the dense solve: smoothing only
       k_mg_jacobi<<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e,
-                                                       f.dinv, b, nullptr, x, MG_OMEGA); fs_count_launch();
+                                                       f.dinv, b, nullptr, x, MG_OMEGA, done);
+      ++nk;
       for (int s = 0; s < 8; ++s) {
+        const double* src = (s & 1) ? f.t : x;
+        double* dst = (s & 1) ? x : f.t;
         k_mg_jacobi<<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz,
-                                                         f.e, f.dinv, b, x, f.t, MG_OMEGA); fs_count_launch();
-        cudaMemcpyAsync(x, f.t, sizeof(double) * f.n, cudaMemcpyDeviceToDevice, st);
+                                                         f.e, f.dinv, b, src, dst, MG_OMEGA, done);
+        ++nk;
       }
     }
-    return;
+    return nk;
   }
   MGLevel& cl = P->lev[l + 1];
   unsigned nb = blocks_for(f.n, 256);
-  // pre-smoothing: x = w b/d ; t = x + w (b - S x)/d
-  k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, nullptr, x,
-                                  MG_OMEGA); fs_count_launch();
-  k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, x, f.t,
-                                  MG_OMEGA); fs_count_launch();
+  const int nu = P->nu;
+  const double om = P->omega;
+  // pre-smoothing from x = 0, ending in t:  sweep i writes t when (nu-1-i) is even, else s
+  const double* src = nullptr;
+  for (int i = 0; i < nu; ++i) {
+    double* dst = ((nu - 1 - i) % 2 == 0) ? f.t : f.s;
+    k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, src, dst,
+                                    om, done);
+    src = dst;
+    ++nk;
+  }
   k_mg_restrict_residual<<<blocks_for(cl.n, 128), 128, 0, st>>>(
-      f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, b, f.t, cl.nx, cl.ny, cl.nz, cl.b); fs_count_launch();
-  vcycle(P, l + 1, cl.b, cl.x, st);
-  k_mg_prolong<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.t, cl.nx, cl.ny, cl.x); fs_count_launch();
-  // post-smoothing: x = t + w(b - S t)/d ; out = x + w(b - S x)/d
-  k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, f.t, x,
-                                  MG_OMEGA); fs_count_launch();
-  k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, x, f.t,
-                                  MG_OMEGA); fs_count_launch();
-  cudaMemcpyAsync(x, f.t, sizeof(double) * f.n, cudaMemcpyDeviceToDevice, st);
+      f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, b, f.t, cl.nx, cl.ny, cl.nz, cl.b, done);
+  ++nk;
+  nk += vcycle(P, l + 1, cl.b, cl.x, done, st);
+  k_mg_prolong<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.t, cl.nx, cl.ny, cl.x, done);
+  ++nk;
+  // post-smoothing from t, ending in x:  s, t, s, ... then x
+  src = f.t;
+  for (int i = 0; i < nu; ++i) {
+    double* dst = (i == nu - 1) ? x : ((i % 2 == 0) ? f.s : f.t);
+    k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, src, dst,
+                                    om, done);
+    src = dst;
+    ++nk;
+  }
+  return nk;
+}
+
+int proj_configure(void* h, int nu, double omega) {
+  ProjCtx* P = (ProjCtx*)h;
+  if (nu < 1 || nu > 16 || !(omega > 0.0 && omega < 2.0)) return FS_EARG;
+  if (nu != P->nu || omega != P->omega) {
+    P->nu = nu;
+    P->omega = omega;
+    if (P->iter_exec) cudaGraphExecDestroy(P->iter_exec);
+    P->iter_exec = nullptr;
+    P->graph_failed = 0;
+  }
+  return FS_OK;
+}
+
+// One preconditioned-CG iteration, every kernel a no-op once converged.
+static int pcg_iteration(ProjCtx* P, double* x, cudaStream_t st) {
+  MGLevel& l0 = P->lev[0];
+  const int64_t n = l0.n;
+  const double* done = P->scal + SC_DONE;
+  int nk = vcycle(P, 0, P->pc_r, P->pc_z, done, st);
+  k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, P->pc_r, P->pc_z, P->partial, done);
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 2, done);  // rz_new
+  k_pcg_dir<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, P->pc_z, P->pc_p);
+  k_set_scal<<<1, 1, 0, st>>>(P->scal, 0, 2);  // rz = rz_new
+  k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.nx, l0.ny, l0.nz, l0.gx, l0.gy, l0.gz,
+                                                   l0.e, P->pc_p, P->pc_q, P->partial, done);
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 1, done);  // pq
+  k_pcg_update<<<RED_BLOCKS, RED_THREADS, 0, st>>>(P->g, P->scal, x, P->pc_r, P->pc_p, P->pc_q,
+                                                   P->partial);
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5, done);  // ||r_A||^2
+  k_pcg_check<<<1, 1, 0, st>>>(P->scal);
+  return nk + 10;
+}
+
+// Capture one iteration as a CUDA graph (on the context's private stream).
+static void capture_iteration(ProjCtx* P) {
+  cudaGraph_t graph = nullptr;
+  if (cudaStreamBeginCapture(P->cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    P->graph_failed = 1;
+    return;
+  }
+  int nk = pcg_iteration(P, P->p_prev, P->cs);
+  if (cudaStreamEndCapture(P->cs, &graph) != cudaSuccess || !graph) {
+    cudaGetLastError();
+    P->graph_failed = 1;
+    return;
+  }
+  if (cudaGraphInstantiate(&P->iter_exec, graph, 0) != cudaSuccess) {
+    cudaGetLastError();
+    P->iter_exec = nullptr;
+    P->graph_failed = 1;
+  }
+  cudaGraphDestroy(graph);
+  P->iter_kernels = nk;
+}
+
+static int launch_iterations(ProjCtx* P, int count, cudaStream_t st) {
+  for (int q = 0; q < count; ++q) {
+    if (P->iter_exec) {
+      if (cudaGraphLaunch(P->iter_exec, st) != cudaSuccess) return FS_ECUDA;
+      for (int k = 0; k < P->iter_kernels; ++k) fs_count_launch();
+    } else {
+      int nk = pcg_iteration(P, P->p_prev, st);
+      for (int k = 0; k < nk; ++k) fs_count_launch();
+    }
+  }
+  return FS_OK;
 }
 
 static int fetch(ProjCtx* P, int n, cudaStream_t st) {
   cudaMemcpyAsync(P->h_scal, P->scal, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess) return FS_ECUDA;
+  if (fs_stream_wait(st) != FS_OK) return FS_ECUDA;
   return FS_OK;
 }
 
-// Solve for the pressure and correct u, v, w in place.
+// Solve for the pressure and correct u, v, w in place.  The iterations run
+// as graph launches in batches (sized from the previous solve's count); the
+// host reads the converged flag once per batch.
 int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
                  const double* target, double dt, double rtol, int maxiter, int* iters,
                  cudaStream_t st) {
@@ -652,44 +803,31 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
   *iters = 0;
   k_proj_rhs<<<RED_BLOCKS, RED_THREADS, 0, st>>>(g, u, v, w, u_in, target, dt, P->rhs,
                                                  P->partial); fs_count_launch();
-  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 4); fs_count_launch();  // ||b_A||^2
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 4, nullptr); fs_count_launch();
   double* x = P->p_prev;
   k_pcg_residual<<<RED_BLOCKS, RED_THREADS, 0, st>>>(g, l0.gx, l0.gy, l0.gz, l0.e, P->rhs, x,
                                                      P->pc_r, P->partial); fs_count_launch();
-  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5); fs_count_launch();  // ||r_A||^2
-  int stt = fetch(P, 6, st);
-  if (stt) return stt;
-  double bn = sqrt(P->h_scal[4]);
-  if (!(bn == bn)) return FS_ENONFINITE;
-  if (bn == 0.0) {
-    cudaMemsetAsync(x, 0, sizeof(double) * n, st);
-  } else {
-    double atol = rtol * bn;
-    double rn = sqrt(P->h_scal[5]);
-    int it = 0;
-    bool done = rn < atol;
-    while (!done) {
-      if (it >= maxiter) return FS_ENOCONV;
-      vcycle(P, 0, P->pc_r, P->pc_z, st);
-      k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, P->pc_r, P->pc_z, P->partial); fs_count_launch();
-      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 2); fs_count_launch();  // rz_new
-      k_pcg_dir<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, P->pc_z, P->pc_p, it == 0); fs_count_launch();
-      k_set_scal<<<1, 1, 0, st>>>(P->scal, 0, 2); fs_count_launch();  // rz = rz_new
-      k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.nx, l0.ny, l0.nz, l0.gx, l0.gy, l0.gz,
-                                                       l0.e, P->pc_p, P->pc_q, P->partial); fs_count_launch();
-      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 1); fs_count_launch();  // pq
-      k_pcg_update<<<RED_BLOCKS, RED_THREADS, 0, st>>>(g, P->scal, x, P->pc_r, P->pc_p, P->pc_q,
-                                                       P->partial); fs_count_launch();
-      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5); fs_count_launch();
-      ++it;
-      stt = fetch(P, 6, st);
-      if (stt) return stt;
-      rn = sqrt(P->h_scal[5]);
-      if (!(rn == rn)) return FS_ENONFINITE;
-      done = rn < atol;
-    }
-    *iters = it;
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5, nullptr); fs_count_launch();
+  k_pcg_init<<<1, 1, 0, st>>>(P->scal, rtol * rtol); fs_count_launch();
+  k_zero_if_zero_rhs<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, x); fs_count_launch();
+  if (!P->iter_exec && !P->graph_failed) capture_iteration(P);
+  int launched = 0;
+  int batch = P->last_iters > 2 ? P->last_iters - 2 : 1;
+  while (true) {
+    int stt = fetch(P, 9, st);
+    if (stt) return stt;
+    const double bn2 = P->h_scal[4], rn2 = P->h_scal[5];
+    if (!(bn2 == bn2) || !(rn2 == rn2)) return FS_ENONFINITE;
+    if (P->h_scal[SC_DONE] != 0.0) break;
+    if (launched >= maxiter) return FS_ENOCONV;
+    if (batch > maxiter - launched) batch = maxiter - launched;
+    stt = launch_iterations(P, batch, st);
+    if (stt) return stt;
+    launched += batch;
+    batch = 2;
   }
+  *iters = (int)P->h_scal[SC_IT];
+  P->last_iters = *iters;
   P->have_prev = 1;
   Launch3 L = launch_cells(g);
   k_proj_correct<<<L.grid, L.block, 0, st>>>(g, u, v, w, x, P->ir, dt); fs_count_launch();
@@ -712,6 +850,6 @@ int proj_apply(void* h, const double* x, double* y, cudaStream_t st) {
   ProjCtx* P = (ProjCtx*)h;
   MGLevel& l0 = P->lev[0];
   k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.nx, l0.ny, l0.nz, l0.gx, l0.gy, l0.gz, l0.e,
-                                                   x, y, P->partial); fs_count_launch();
+                                                   x, y, P->partial, nullptr); fs_count_launch();
   return cuda_status();
 }

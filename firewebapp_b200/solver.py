@@ -90,7 +90,7 @@ class Tier3Solver:
               "k_turb", "eps_turb", "nu_t", "phi")
 
     def __init__(self, case: dict, device="cuda", projection_cg_rtol: float = 1.0e-6,
-                 proj_maxiter: int = 200):
+                 proj_maxiter: int = 200, mg_sweeps: int | None = None):
         self.lib = _lib.lib()
         self.dev = torch.device(device)
         self.case = dict(case)
@@ -135,6 +135,9 @@ class Tier3Solver:
         self.edc_scratch = torch.zeros(int(self.lib.fs_edc_scratch_bytes(self.n)) + 64,
                                        dtype=torch.uint8, device=dev)
         self.active_count = torch.zeros(1, dtype=torch.int64, device=dev)
+        # pinned host mirrors for the per-step scalar reads
+        self.h_count = torch.zeros(1, dtype=torch.int64).pin_memory()
+        self.h_row = torch.zeros(g.Nx, dtype=torch.float64).pin_memory()
         self.max_scratch = torch.zeros(64, dtype=torch.float64, device=dev)
         # soil
         so = su.soil
@@ -150,6 +153,8 @@ class Tier3Solver:
         h = _ctypes_void()
         check(self.lib.fs_proj_create(self.gp, _ctypes_byref(h)), "fs_proj_create")
         self.proj = h
+        if mg_sweeps is not None:
+            check(self.lib.fs_proj_configure(self.proj, int(mg_sweeps), 0.8), "fs_proj_configure")
         om, wq = level_symmetric(self.p["n_quadrature"])
         self.Omega, self.weights = om, wq
         h2 = _ctypes_void()
@@ -223,8 +228,10 @@ class Tier3Solver:
             pp = torch.as_tensor(np.ascontiguousarray(snap["p_prev"]).reshape(-1))
             self.pressure_view().copy_(pp)
         if "I_set" in snap:
-            I = torch.as_tensor(np.ascontiguousarray(snap["I_set"]).reshape(-1))
-            self.intensity_view().copy_(I)
+            I = torch.as_tensor(np.ascontiguousarray(snap["I_set"]).reshape(-1)).to(self.dev)
+            check(self.lib.fs_dom_load_intensity(self.dom, ptr(I), self._s()), "dom_load")
+            torch.cuda.current_stream().synchronize()
+            del I
         self.t = float(t)
         self.dt = float(dt_prev)
         self.step_count = int(step)
@@ -375,6 +382,8 @@ class Tier3Solver:
         check(L.fs_proj_rebuild(self.proj, ptr(f["rho"]), s), "proj_rebuild")
         n_it = 0
         div_max = 0.0
+        ktp = self._ktime("projection")
+        ktp.__enter__()
         for _it in range(p["proj_max_iter"]):
             its = _ctypes_int()
             check(L.fs_proj_project(self.proj, ptr(f["u"]), ptr(f["v"]), ptr(f["w"]),
@@ -389,6 +398,7 @@ class Tier3Solver:
             n_it = _it + 1
             if div_max < p["proj_div_tol"]:
                 break
+        ktp.__exit__(None, None, None)
         d.proj_iters = n_it
         d.proj_div_max = div_max
         # --- 6. outflow sponge (spread_3d.py:2369)
@@ -510,7 +520,9 @@ class Tier3Solver:
         self.lset_step += 1
         if self.lset_step % 10 == 0:
             self._reinit_levelset()
-        n_active = int(self.active_count.item())
+        check(self.lib.fs_copy_to_host(self.h_count.data_ptr(), ptr(self.active_count), 8,
+                                       self._s()), "active_count")
+        n_active = int(self.h_count[0])
         front_lset = self._front_x(1, g.Ny // 2)
         exit_now = False
         if n_active == 0 and t > p["ignition_duration_s"] + 2.0:
@@ -586,7 +598,10 @@ class Tier3Solver:
             self._swap("phi", "tmp5")
 
     def _front_x(self, k, j):
-        row = self.f["phi"][k, j, :].cpu().numpy()
+        src = self.f["phi"][k, j, :]
+        check(self.lib.fs_copy_to_host(self.h_row.data_ptr(), src.data_ptr(),
+                                       8 * self.grid.Nx, self._s()), "front_row")
+        row = self.h_row.numpy()
         for i in range(row.size - 1):
             a, b = row[i], row[i + 1]
             if a < 0.0 < b or b < 0.0 < a:
@@ -609,8 +624,10 @@ class Tier3Solver:
         for k, v in self.part.items():
             out["p_" + k] = v.cpu().numpy().copy()
         out["p_prev"] = self.pressure_view().cpu().numpy().reshape(self.shape).copy()
-        M = self.Omega.shape[0]
-        out["I_set"] = self.intensity_view().cpu().numpy().reshape((M,) + self.shape).copy()
+        iv = self.intensity_view()
+        if iv is not None:
+            M = self.Omega.shape[0]
+            out["I_set"] = iv.cpu().numpy().reshape((M,) + self.shape).copy()
         return out
 
     def pressure_view(self):
@@ -618,9 +635,13 @@ class Tier3Solver:
         return _DeviceBuffer(self.lib.fs_proj_pressure(self.proj), self.n, self.dev).tensor()
 
     def intensity_view(self):
-        """Zero-copy view of the DOM intensities (M x cells)."""
+        """Zero-copy view of the full DOM intensities (M x cells), or None when
+        the sweep path keeps only the periodic inflow rows."""
+        addr = self.lib.fs_dom_intensity(self.dom)
+        if not addr:
+            return None
         M = self.Omega.shape[0]
-        return _DeviceBuffer(self.lib.fs_dom_intensity(self.dom), self.n * M, self.dev).tensor()
+        return _DeviceBuffer(addr, self.n * M, self.dev).tensor()
 
 
 # ---- small ctypes helpers --------------------------------------------------

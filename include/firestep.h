@@ -182,6 +182,11 @@ int fs_proj_project(void* handle, double* u, double* v, double* w, const double*
                     void* stream);
 double* fs_proj_pressure(void* handle);
 int fs_proj_apply(void* handle, const double* x, double* y, void* stream);
+/* Multigrid preconditioner: nu damped-Jacobi sweeps (weight omega) before and
+ * after each coarse correction (default 4 and 0.8).  The reference's
+ * preconditioner (projection_3d.py:236-246, an FFT solve) has no such knob;
+ * only the converged solution is shared. */
+int fs_proj_configure(void* handle, int nu, double omega);
 /* max |div(u) - target| to *result (synchronises); div_out optional. */
 int fs_divergence_max(const FsGrid* g, const double* u, const double* v, const double* w,
                       const double* u_inlet, const double* div_target, double* div_out,
@@ -196,7 +201,23 @@ int fs_dom_solve(void* handle, const double* T_s, const double* T_g, const doubl
                  const double* omega, double sigma_sav, double T_amb, const double* T_soil0,
                  const double* Y_H2O, const double* rho, const double* M_local, double* q_rad_solid,
                  double* q_rad_gas, double* q_in_soil, void* stream);
+/* Full intensity field (M x Nz x Ny x Nx) for sweep paths 2 and 3; NULL for the
+ * default octant-cluster path, which keeps only the y-periodic inflow rows
+ * (the part of I_set that a later sweep reads, dom_3d.py:147-211). */
 double* fs_dom_intensity(void* handle);
+/* Sweep path: 0 auto (path 4 when the quadrature is octant-major and the
+ * grid fits, else one CTA per ordinate, else one launch per hyperplane),
+ * 1 octant clusters with point-to-point hand-off between CTAs,
+ * 2 one CTA per ordinate, 3 hyperplane launches, 4 octant clusters with a
+ * cluster barrier per hyperplane; cluster_ctas 0 = automatic, else CTAs per
+ * octant (1..16).  Only before the first solve or intensity load.  Path 1
+ * bounds its waits: a stalled hand-off returns FS_ETIMEOUT. */
+int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
+/* The path in use (0 before the first solve or intensity load). */
+int fs_dom_sweep_mode(void* handle);
+/* Load the persistent intensity state from a full device field
+ * (M x Nz x Ny x Nx), as a reference I_set would seed the next solve. */
+int fs_dom_load_intensity(void* handle, const double* I_full, void* stream);
 int fs_dom_iterations(void* handle);
 /* enable >= 0 turns per-sweep event timing on/off (and resets it); the
  * accumulated sweep time and sweep count are returned when pointers are given */
@@ -227,6 +248,10 @@ int fs_levelset(const FsGrid* g, const double* phi, const double* aux, double* o
 int fs_active_count(int64_t n, const double* omega, const double* T_g, const double* Y_F,
                     unsigned long long* count, unsigned char* mask, void* stream);
 
+/* Copy device bytes to host memory and wait (the thread sleeps on a
+ * blocking-sync event rather than spinning).  Host-side reads of the
+ * reference loop's scalars (active-flame count, front row) go through it. */
+int fs_copy_to_host(void* dst, const void* src, int64_t bytes, void* stream);
 /* max reductions: mode 0 max|f|, 1 max f (NaN propagates), 2 interior max
  * ignoring NaN from 0 (turbulence_3d.py:894-900); results to host. */
 int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, void* stream);

@@ -160,6 +160,31 @@ def test_edc(vectors):
         assert rel_l2(host(om), c["omega_out"]) <= LIBM, name
 
 
+def test_edc_flag_scan_many_blocks():
+    """Sparse reacting cells over ~3000 blocks: the carried flag matches the
+    oracle's flat-order forward fill everywhere."""
+    from oracle import kernels as K
+    rng = np.random.default_rng(7)
+    n = 3_000_000
+    rho = rng.uniform(0.3, 1.2, n)
+    k = rng.uniform(1e-3, 1.0, n)
+    e = rng.uniform(1e-3, 1.0, n)
+    Tg0 = rng.uniform(300.0, 1800.0, n)
+    Yf0 = np.where(rng.random(n) < 2e-4, rng.uniform(0.0, 0.2, n), 0.0)
+    YO0 = rng.uniform(0.0, 0.232, n)
+    YH0 = rng.uniform(0.0, 0.2, n)
+    want = K.edc(rho, Tg0, Yf0, YO0, k, e, YH0, 0.34, 1100.0, 2e-3, 1, 1.3, 17e6, 0)
+    Tg, Yf, YO = dev(Tg0), dev(Yf0), dev(YO0)
+    rho_d, k_d, e_d, YH_d = dev(rho), dev(k), dev(e), dev(YH0)   # keep alive across the call
+    om = torch.zeros_like(Tg)
+    scratch = torch.zeros(int(lib().fs_edc_scratch_bytes(n)) + 16, dtype=torch.uint8,
+                          device="cuda")
+    call("fs_edc", n, ptr(rho_d), ptr(Tg), ptr(Yf), ptr(YO), ptr(k_d), ptr(e_d), ptr(YH_d),
+         ptr(om), 0.34, 1100.0, 2e-3, 1, 1.3, 17e6, 0, ptr(scratch), stream())
+    for got, exp in zip((Tg, Yf, YO, om), want):
+        assert rel_l2(host(got), exp) <= LIBM
+
+
 def test_edc_flag_leak_crosses_blocks():
     """Cells without fuel inherit the quench flag of the previous reacting cell
     in flat order, across thread-block boundaries (edc.py:223)."""
@@ -224,7 +249,10 @@ def test_k_epsilon(vectors):
         assert rel_l2(host(nuo), c["nu_t_out"]) <= LIBM, name
 
 
-def test_dom(vectors):
+@pytest.mark.parametrize("mode", [1, 2, 3, 4])
+def test_dom(vectors, mode):
+    """Every sweep path (pipelined octant clusters, CTA per ordinate, hyperplane
+    launches, octant clusters with cluster barriers)."""
     from firewebapp_b200.quadrature import level_symmetric
     om, wq = level_symmetric(4)
     for name in vectors.cases("dom"):
@@ -235,6 +263,7 @@ def test_dom(vectors):
         call("fs_dom_create", g.ref, om.shape[0], dbl_array(om[:, 0]), dbl_array(om[:, 1]),
              dbl_array(om[:, 2]), dbl_array(wq), 0.5, C.byref(h))
         try:
+            call("fs_dom_set_sweep_mode", h, mode, 0)
             Ts, Tg, a, omg, M = (dev(c[x]) for x in ("T_s", "T_g", "alpha_s", "omega_comb",
                                                      "bed_moisture"))
             YH = dev(c["Y_H2O"]) if "Y_H2O" in c else None
@@ -248,6 +277,7 @@ def test_dom(vectors):
             assert rel_l2(host(qs), c["q_rad_solid"]) <= LIBM, name
             assert rel_l2(host(qg), c["q_rad_gas"]) <= LIBM, name
             assert rel_l2(host(qsoil), c["q_in_soil"]) <= LIBM, name
+            assert lib().fs_dom_sweep_mode(h) == mode
         finally:
             lib().fs_dom_destroy(h)
 
