@@ -69,6 +69,7 @@ SIGNATURES = {
     "fs_k_epsilon": (I, [_G, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, D, D, D, D, D, P]),
     "fs_edc_scratch_bytes": (I64, [I64]),
     "fs_edc": (I, [I64, P, P, P, P, P, P, P, P, D, D, D, I, D, D, I, P, P]),
+    "fs_edc_noalloc": (I, [I64, P, P, P, P, P, P, P, P, D, D, D, I, D, D, I, P]),
     "fs_gas_energy_update": (I, [_G, P, P, P, P, P, P, P, P, P, D, D, D, I, I, I, I, P]),
     "fs_eos": (I, [_G, P, P, P, P, D, P]),
     "fs_clip": (I, [I64, P, D, D, P]),

@@ -145,6 +145,19 @@ int fs_edc(int64_t n, const double* rho, double* T_g, double* Y_F, double* Y_O2,
            double dt, int n_substeps, double s_stoich, double hoc_J, int extinction, void* scratch,
            void* stream);
 
+/* No counterpart in the reference: fs_edc for callers that cannot allocate
+ * device memory.  Same arguments and results as fs_edc without the scratch
+ * buffer; the flag scan uses a static device array sized for at most
+ * FS_EDC_NOALLOC_MAX_CELLS cells (larger n is rejected with FS_EARG).  The
+ * first call on a device looks the array up (make it before any stream
+ * capture); all calls share the array, so calls whose kernels overlap on the
+ * GPU race.  It calls no allocation routine. */
+#define FS_EDC_NOALLOC_MAX_CELLS (1LL << 27)
+int fs_edc_noalloc(int64_t n, const double* rho, double* T_g, double* Y_F, double* Y_O2,
+                   const double* k, const double* eps, const double* Y_H2O, double* omega,
+                   double chi_rad, double cp_g, double dt, int n_substeps, double s_stoich,
+                   double hoc_J, int extinction, void* stream);
+
 /* spread_3d.py:2916-2957 + 3104-3146: drip + q_rad_gas into Q_comb and the
  * Lagrangian-branch gas-energy update, in place. */
 int fs_gas_energy_update(const FsGrid* g, double* T_g, const double* rho, const double* Y_H2O,
