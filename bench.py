@@ -20,6 +20,7 @@ not shard); value = cell-steps/s summed over ranks, time = max over ranks.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import math
 import os
@@ -249,6 +250,10 @@ def main():
             dist.barrier()
 
     # ---- timed region: device-resident state, CUDA events on the stream
+    # Objects alive now (torch, numpy, the solver) move to the permanent GC
+    # generation, so a full collection during the steps scans only new ones.
+    gc.collect()
+    gc.freeze()
     solver.enable_kernel_timers(True)
     lib = _lib.lib()
     clocks = ClockSampler(local) if not args.no_clocks else None

@@ -82,6 +82,7 @@ SIGNATURES = {
     "fs_proj_pressure": (P, [P]),
     "fs_proj_apply": (I, [P, P, P, P]),
     "fs_proj_configure": (I, [P, I, D]),
+    "fs_proj_stats": (I, [P, C.POINTER(D)]),
     "fs_divergence_max": (I, [_G, P, P, P, P, P, P, C.POINTER(D), P]),
     "fs_dom_create": (I, [_G, I, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(D), D,
                           PP]),

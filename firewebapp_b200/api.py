@@ -17,6 +17,7 @@ warm-start pressure, DOM intensities) stay on the device, as the reference's
 """
 from __future__ import annotations
 
+import gc
 import json
 import math
 from dataclasses import dataclass, field
@@ -166,6 +167,10 @@ def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | 
     if n_steps is None and t_end is None:
         raise ValueError("run_3d_spread_gpu needs n_steps or t_end")
     s = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol)
+    # long-lived objects out of the collector's way: full collections during the
+    # run then scan only objects made by the run itself
+    gc.collect()
+    gc.freeze()
     try:
         g = s.grid
         res = Spread3DResultGPU(ros_m_s=0.0, n_cells_ignited=0, front_t=s.front_t,
@@ -256,6 +261,8 @@ def run_3d_spread_gpu_e2e(case: dict, steps: int, warmup: int = 1,
     """Time ``steps`` host-buffer outer steps (uploads and downloads inside
     the timed region), after ``warmup`` untimed ones."""
     hs = HostStepper(case, projection_cg_rtol=projection_cg_rtol)
+    gc.collect()
+    gc.freeze()
     try:
         for _ in range(warmup):
             hs.step()

@@ -1,5 +1,6 @@
 // extern "C" entry points of libfirestep.so (declared in include/firestep.h).
 #include <cstdarg>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include "common.cuh"
@@ -31,6 +32,37 @@ int fs_stream_wait(cudaStream_t st) {
     return FS_ECUDA;
   if (cudaEventRecord(ev[dev], st) != cudaSuccess) return FS_ECUDA;
   return cudaEventSynchronize(ev[dev]) == cudaSuccess ? FS_OK : FS_ECUDA;
+}
+
+// One-time per-device scratch for the synchronous reductions (a few device
+// words and a pinned host staging area), so the hot-path reductions neither
+// allocate per call nor copy into pageable memory.  The mutex is held for the
+// whole call, which also makes those entry points safe across threads.
+struct SmallScratch {
+  unsigned long long* dkey;  // 32 words
+  double* dres;              // 32 doubles
+  double* hpin;              // 32 doubles, pinned
+};
+static std::mutex g_small_mu;
+static SmallScratch g_small[64];
+
+static SmallScratch* small_scratch() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  SmallScratch& sc = g_small[dev];
+  if (!sc.dkey) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, 64 * sizeof(double)) != cudaSuccess) return nullptr;
+    void* h = nullptr;
+    if (cudaMallocHost(&h, 32 * sizeof(double)) != cudaSuccess) {
+      cudaFree(p);
+      return nullptr;
+    }
+    sc.dkey = (unsigned long long*)p;
+    sc.dres = (double*)p + 32;
+    sc.hpin = (double*)h;
+  }
+  return &sc;
 }
 
 static int check(int st, const char* where) {
@@ -117,21 +149,19 @@ int fs_copy_to_host(void* dst, const void* src, int64_t bytes, void* stream) {
 
 int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, void* stream) {
   GRID("fs_field_max");
-  unsigned long long* key = nullptr;
-  double* dres = nullptr;
-  if (cudaMallocAsync(&key, sizeof(unsigned long long), ST(stream)) != cudaSuccess ||
-      cudaMallocAsync(&dres, sizeof(double), ST(stream)) != cudaSuccess) {
-    fs_set_error("fs_field_max: allocation failed");
+  std::lock_guard<std::mutex> lock(g_small_mu);
+  SmallScratch* sc = small_scratch();
+  if (!sc) {
+    fs_set_error("fs_field_max: scratch allocation failed");
     return FS_ECUDA;
   }
-  launch_init_keys(key, 1, mode == 2 ? 1 : 0, ST(stream));
-  launch_max(gd, f, mode, key, ST(stream));
-  launch_keys_to_double(key, dres, 1, ST(stream));
-  cudaMemcpyAsync(result, dres, sizeof(double), cudaMemcpyDeviceToHost, ST(stream));
-  cudaFreeAsync(key, ST(stream));
-  cudaFreeAsync(dres, ST(stream));
+  launch_init_keys(sc->dkey, 1, mode == 2 ? 1 : 0, ST(stream));
+  launch_max(gd, f, mode, sc->dkey, ST(stream));
+  launch_keys_to_double(sc->dkey, sc->dres, 1, ST(stream));
+  cudaMemcpyAsync(sc->hpin, sc->dres, sizeof(double), cudaMemcpyDeviceToHost, ST(stream));
   if (fs_stream_wait(ST(stream)) != FS_OK) return check(FS_ECUDA, "fs_field_max");
-  return FS_OK;
+  *result = sc->hpin[0];
+  return check(cuda_status(), "fs_field_max");
 }
 
 int fs_field_max_multi(const FsGrid* g, int nf, const double* const* f, const int* modes,
@@ -146,8 +176,15 @@ int fs_field_max_multi(const FsGrid* g, int nf, const double* const* f, const in
   launch_init_keys(key, nf, mask2, ST(stream));
   for (int q = 0; q < nf; ++q) launch_max(gd, f[q], modes[q], key + q, ST(stream));
   launch_keys_to_double(key, dres, nf, ST(stream));
-  cudaMemcpyAsync(results, dres, sizeof(double) * nf, cudaMemcpyDeviceToHost, ST(stream));
+  std::lock_guard<std::mutex> lock(g_small_mu);
+  SmallScratch* sc = small_scratch();
+  if (!sc) {
+    fs_set_error("fs_field_max_multi: scratch allocation failed");
+    return FS_ECUDA;
+  }
+  cudaMemcpyAsync(sc->hpin, dres, sizeof(double) * nf, cudaMemcpyDeviceToHost, ST(stream));
   if (fs_stream_wait(ST(stream)) != FS_OK) return check(FS_ECUDA, "fs_field_max_multi");
+  for (int q = 0; q < nf; ++q) results[q] = sc->hpin[q];
   return check(cuda_status(), "fs_field_max_multi");
 }
 
@@ -157,12 +194,17 @@ int fs_turb_diffusion_nsub(const FsGrid* g, const double* nu_t, double sc_t, dou
   // turbulence_3d.py:880-915
   double dz_min = 0.0;
   {
-    double* h = new double[gd.nz];
-    cudaMemcpy(h, gd.dz, sizeof(double) * gd.nz, cudaMemcpyDeviceToHost);
+    double* h = nullptr;
+    if (cudaMallocHost(&h, sizeof(double) * gd.nz) != cudaSuccess) return check(FS_ECUDA, "nsub");
+    cudaMemcpyAsync(h, gd.dz, sizeof(double) * gd.nz, cudaMemcpyDeviceToHost, ST(stream));
+    if (fs_stream_wait(ST(stream)) != FS_OK) {
+      cudaFreeHost(h);
+      return check(FS_ECUDA, "nsub");
+    }
     dz_min = h[0];
     for (int k = 1; k < gd.nz; ++k)
       if (h[k] < dz_min) dz_min = h[k];
-    delete[] h;
+    cudaFreeHost(h);
   }
   double dx2 = gd.dx * gd.dx, dy2 = gd.dy * gd.dy, dz2 = dz_min * dz_min;
   double h_min2 = dx2 < (dy2 < dz2 ? dy2 : dz2) ? dx2 : (dy2 < dz2 ? dy2 : dz2);
@@ -318,6 +360,12 @@ int fs_proj_project(void* handle, double* u, double* v, double* w, const double*
 
 double* fs_proj_pressure(void* handle) { return handle ? proj_pressure(handle) : nullptr; }
 
+int fs_proj_stats(void* handle, double* out8) {
+  if (!handle || !out8) return FS_EARG;
+  proj_stats(handle, out8);
+  return FS_OK;
+}
+
 int fs_proj_configure(void* handle, int nu, double omega) {
   if (!handle) return FS_EARG;
   return check(proj_configure(handle, nu, omega), "fs_proj_configure");
@@ -332,15 +380,16 @@ int fs_divergence_max(const FsGrid* g, const double* u, const double* v, const d
                       const double* u_inlet, const double* div_target, double* div_out,
                       double* result, void* stream) {
   GRID("fs_divergence_max");
-  unsigned long long* key = nullptr;
-  if (cudaMallocAsync(&key, sizeof(unsigned long long), ST(stream)) != cudaSuccess)
-    return check(FS_ECUDA, "fs_divergence_max");
-  int st = launch_div_resid_max(gd, u, v, w, u_inlet, div_target, div_out, key, ST(stream));
-  unsigned long long hk = 0;
-  cudaMemcpyAsync(&hk, key, sizeof(hk), cudaMemcpyDeviceToHost, ST(stream));
-  cudaFreeAsync(key, ST(stream));
+  std::lock_guard<std::mutex> lock(g_small_mu);
+  SmallScratch* sc = small_scratch();
+  if (!sc) {
+    fs_set_error("fs_divergence_max: scratch allocation failed");
+    return FS_ECUDA;
+  }
+  int st = launch_div_resid_max(gd, u, v, w, u_inlet, div_target, div_out, sc->dkey, ST(stream));
+  cudaMemcpyAsync(sc->hpin, sc->dkey, sizeof(double), cudaMemcpyDeviceToHost, ST(stream));
   if (fs_stream_wait(ST(stream)) != FS_OK) return check(FS_ECUDA, "fs_divergence_max");
-  memcpy(result, &hk, sizeof(double));
+  memcpy(result, sc->hpin, sizeof(double));
   return check(st, "fs_divergence_max");
 }
 

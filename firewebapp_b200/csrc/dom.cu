@@ -226,6 +226,124 @@ __global__ void __launch_bounds__(1024) k_dom_sweep_block(GridDev g, SweepArgs a
   }
 }
 
+// Path 5: one CTA per ordinate (as path 2) with every thread owning a fixed
+// set of PPT pencils.  Per hyperplane each thread first loads its cells'
+// kappa and kappa*B (all pencils at once, one load latency), then the upwind
+// values from the shared previous-plane buffer, and writes the new values to
+// the shared current-plane buffer and to the intensity field; the y-periodic
+// inflow of the first row and the ground intensity of the bottom row are
+// staged in shared memory one hyperplane ahead by the first threads.  One
+// __syncthreads per hyperplane, no cross-CTA traffic; G is then summed over
+// all ordinates in ordinate order, as the reference does.
+struct OrdArgs {
+  const double *ox, *oy, *oz;
+  double* I;                // M x N intensities (natural layout)
+  const double2* kb;        // (kappa, kappa*B)
+  const double* Ig;         // ground intensity (ny, nx)
+  double I_amb;
+  int periodic;
+};
+
+__host__ __device__ inline size_t ord_smem_bytes(int ny, int nz) {
+  return sizeof(double) * ((size_t)2 * ny * nz + (size_t)nz + 2 * (size_t)nz + 2 * (size_t)ny);
+}
+
+template <int PPT, int TPB>
+__global__ void __launch_bounds__(TPB, 1) k_dom_ord(GridDev g, OrdArgs a) {
+  extern __shared__ double sh[];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int npen = ny * nz;
+  double* bufA = sh;
+  double* bufB = sh + npen;
+  double* izt = bufB + npen;            // |mu| / dz_k
+  double* wrapbuf = izt + nz;           // 2 x nz: y inflow of the row (kp, jp = 0)
+  double* igbuf = wrapbuf + 2 * nz;     // 2 x ny: ground intensity under (kp = 0, jp)
+  const int n = blockIdx.x;
+  const double xi = a.ox[n], eta = a.oy[n], mu = a.oz[n];
+  const bool fx = xi >= 0.0, fy = eta >= 0.0, fz = mu >= 0.0;
+  const double ix = fabs(xi) / g.dx;
+  const double iy = fabs(eta) / g.dy;
+  for (int k = threadIdx.x; k < nz; k += TPB) izt[k] = fabs(mu) / g.dz[k];
+  const int64_t N = ncells_dev(g);
+  double* I = a.I + (int64_t)n * N;
+  const int nplanes = nx + ny + nz - 2;
+  // pencils q = tid + r*TPB, walked incrementally: (kp, jp) += (TPB / ny, TPB % ny)
+  const int kp0 = threadIdx.x / ny, jp0 = threadIdx.x - kp0 * ny;
+  const int dkp = TPB / ny, djp = TPB - dkp * ny;
+  auto stage = [&](int d) {
+    const int t = threadIdx.x;
+    if (t < nz && a.periodic) {  // row kp = t, jp = 0: previous sweep's value at the far end
+      const int ip = d - t;
+      if (ip >= 0 && ip < nx) {
+        const int i = fx ? ip : nx - 1 - ip;
+        const int k = fz ? t : nz - 1 - t;
+        const int jf = fy ? ny - 1 : 0;
+        wrapbuf[(d & 1) * nz + t] = I[((int64_t)k * ny + jf) * nx + i];
+      }
+    }
+    if (fz && t >= nz && t < nz + ny) {  // bottom row kp = 0, jp = t - nz
+      const int jp = t - nz;
+      const int ip = d - jp;
+      if (ip >= 0 && ip < nx) {
+        const int i = fx ? ip : nx - 1 - ip;
+        const int j = fy ? jp : ny - 1 - jp;
+        igbuf[(d & 1) * ny + jp] = a.Ig[(int64_t)j * nx + i];
+      }
+    }
+  };
+  stage(0);
+  __syncthreads();
+  for (int d = 0; d < nplanes; ++d) {
+    double* cur = (d & 1) ? bufB : bufA;
+    const double* prev = (d & 1) ? bufA : bufB;
+    const double* wrp = wrapbuf + (d & 1) * nz;
+    const double* igp = igbuf + (d & 1) * ny;
+    // this plane's (kappa, kappa*B) for all pencils first: one load latency per plane
+    double2 kab[PPT];
+    {
+      int kp = kp0, jp = jp0;
+#pragma unroll
+      for (int r = 0; r < PPT; ++r) {
+        const int ip = d - jp - kp;
+        if (kp < nz && ip >= 0 && ip < nx) {
+          const int i = fx ? ip : nx - 1 - ip;
+          const int j = fy ? jp : ny - 1 - jp;
+          const int k = fz ? kp : nz - 1 - kp;
+          kab[r] = a.kb[((int64_t)k * ny + j) * nx + i];
+        }
+        kp += dkp; jp += djp;
+        if (jp >= ny) { jp -= ny; ++kp; }
+      }
+    }
+    int kp = kp0, jp = jp0;
+#pragma unroll
+    for (int r = 0; r < PPT; ++r) {
+      const int ip = d - jp - kp;
+      if (kp < nz && ip >= 0 && ip < nx) {
+        const int q = threadIdx.x + r * TPB;
+        const int i = fx ? ip : nx - 1 - ip;
+        const int j = fy ? jp : ny - 1 - jp;
+        const int k = fz ? kp : nz - 1 - kp;
+        const double Ix = ip > 0 ? prev[q] : a.I_amb;
+        const double Iy = jp > 0 ? prev[q - 1] : (a.periodic ? wrp[kp] : a.I_amb);
+        double Iz;
+        if (kp > 0) Iz = prev[q - ny];
+        else Iz = fz ? (mu > 0.0 ? igp[jp] : 0.0) : a.I_amb;
+        const double iz = izt[k];
+        const double num = kab[r].y + ix * Ix + iy * Iy + iz * Iz;
+        const double den = kab[r].x + ix + iy + iz;
+        const double v = num / den;
+        cur[q] = v;
+        I[((int64_t)k * ny + j) * nx + i] = v;
+      }
+      kp += dkp; jp += djp;
+      if (jp >= ny) { jp -= ny; ++kp; }
+    }
+    if (d + 1 < nplanes) stage(d + 1);
+    __syncthreads();
+  }
+}
+
 // G = sum_n w_n I_n (ordinate order); also max G and max |G - G_prev|
 __global__ void k_dom_G(int64_t N, int M, const double* __restrict__ w,
                         const double* __restrict__ I, double* G, const double* __restrict__ Gp,
@@ -615,6 +733,7 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_pipe(GridDev 
     if (act) {
       const int sl = d % OCT_AHEAD;
       const double2 kab = kab_ring[(size_t)sl * S + q];
+      double den[MO];
 #pragma unroll
       for (int m = 0; m < MO; ++m) {
         const double* pm = prev + (size_t)m * S;
@@ -627,9 +746,13 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_pipe(GridDev 
         else if (kp > 0) Iz = zr[m];
         else Iz = fz ? ig_ring[(size_t)sl * ny + jp] : a.I_amb;
         const double ix = cix[m], iy = ciy[m], iz = izt[m * nz + k];
-        const double num = kab.y + ix * Ix + iy * Iy + iz * Iz;
-        const double den = kab.x + ix + iy + iz;
-        v[m] = num / den;
+        v[m] = kab.y + ix * Ix + iy * Iy + iz * Iz;
+        den[m] = kab.x + ix + iy + iz;
+      }
+#pragma unroll
+      for (int m = 0; m < MO; ++m) v[m] = v[m] / den[m];
+#pragma unroll
+      for (int m = 0; m < MO; ++m) {
         cur[(size_t)m * S + q] = v[m];
         gs = gs + cw[m] * v[m];
         if (ground_out) qs = qs + cwm[m] * v[m];
@@ -911,7 +1034,18 @@ static int dom_prepare(DomCtx* D) {
   int max_smem = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  D->mode = (want == 3 || smem > (size_t)max_smem) ? 3 : 2;
+  const bool ord_ok = ord_smem_bytes(g.ny, g.nz) <= (size_t)max_smem &&
+                      (int64_t)g.ny * g.nz <= 8 * 1024 && g.ny + g.nz <= 1024;
+  if (want == 5 && !ord_ok) {
+    fs_set_error("per-ordinate register sweep not possible for this grid");
+    return FS_EARG;
+  }
+  if (want == 5) {
+    D->mode = 5;
+    cudaMalloc(&D->kb, sizeof(double2) * N);
+  } else {
+    D->mode = (want == 3 || smem > (size_t)max_smem) ? 3 : 2;
+  }
   cudaMalloc(&D->I, sizeof(double) * N * D->M);
   cudaMemset(D->I, 0, sizeof(double) * N * D->M);
   return cuda_status();
@@ -919,7 +1053,7 @@ static int dom_prepare(DomCtx* D) {
 
 int dom_set_mode(void* h, int mode, int cluster_ctas) {
   DomCtx* D = (DomCtx*)h;
-  if (mode < 0 || mode > 4 || cluster_ctas < 0 || cluster_ctas > 16) return FS_EARG;
+  if (mode < 0 || mode > 5 || cluster_ctas < 0 || cluster_ctas > 16) return FS_EARG;
   if (D->mode != 0) {
     fs_set_error("sweep mode must be set before the first solve or intensity load");
     return FS_EARG;
@@ -996,6 +1130,32 @@ static int launch_octant_sweep(DomCtx* D, const OctArgs& a, cudaStream_t st) {
   return e == cudaSuccess ? FS_OK : FS_ECUDA;
 }
 
+template <int PPT, int TPB>
+static void ord_launch(DomCtx* D, const OrdArgs& oa, size_t smem, cudaStream_t st) {
+  cudaFuncSetAttribute(k_dom_ord<PPT, TPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  k_dom_ord<PPT, TPB><<<D->M, TPB, smem, st>>>(D->g, oa);
+}
+
+static int launch_ord_sweep(DomCtx* D, double I_amb, cudaStream_t st) {
+  const GridDev& g = D->g;
+  const int npen = g.ny * g.nz;
+  OrdArgs oa{};
+  oa.ox = D->ox; oa.oy = D->oy; oa.oz = D->oz; oa.I = D->I; oa.kb = D->kb; oa.Ig = D->Ig_out;
+  oa.I_amb = I_amb; oa.periodic = 1;
+  const size_t smem = ord_smem_bytes(g.ny, g.nz);
+  // pencils per thread at 1024 threads per ordinate (the staging threads need ny+nz)
+  if (g.ny + g.nz > 1024) return FS_EARG;
+  const int need = (npen + 1023) / 1024;
+  if (need <= 1) ord_launch<1, 1024>(D, oa, smem, st);
+  else if (need <= 2) ord_launch<2, 1024>(D, oa, smem, st);
+  else if (need <= 4) ord_launch<4, 1024>(D, oa, smem, st);
+  else if (need <= 8) ord_launch<8, 1024>(D, oa, smem, st);
+  else return FS_EARG;
+  fs_count_launch();
+  return cudaGetLastError() == cudaSuccess ? FS_OK : FS_ECUDA;
+}
+
 int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, const double* om,
               double sigma, double T_amb, const double* Tsoil0, const double* YH, const double* rho,
               const double* Mloc, double* q_solid, double* q_gas, double* q_in_soil,
@@ -1010,7 +1170,7 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   const double Tamb4 = pow(T_amb, 4.0);
   k_dom_setup<<<blocks_for(N, 256), 256, 0, st>>>(g, Ts, Tg, as, om, YH, rho, Mloc, sigma, Tamb4,
                                                   D->kgmax, D->ks, D->kg, D->ksafe, D->B,
-                                                  octp ? D->kb : nullptr);
+                                                  (octp || D->mode == 5) ? D->kb : nullptr);
   fs_count_launch();
   const double I_amb = SIGMA_SB_D * Tamb4 / PI_D;
   k_dom_ground_init<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, Tsoil0, D->eps_w, I_amb, D->Isoil,
@@ -1046,6 +1206,9 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
     if (D->timing) cudaEventRecord(D->ev0[it], st);
     if (octp) {
       rc = launch_octant_sweep(D, oa, st);
+      if (rc != FS_OK) return rc;
+    } else if (D->mode == 5) {
+      rc = launch_ord_sweep(D, I_amb, st);
       if (rc != FS_OK) return rc;
     } else if (D->mode == 2) {
       k_dom_sweep_block<<<M, 1024, smem, st>>>(g, a);

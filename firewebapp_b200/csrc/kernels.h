@@ -89,6 +89,7 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
                  cudaStream_t st);
 int proj_apply(void* h, const double* x, double* y, cudaStream_t st);
 int proj_configure(void* h, int nu, double omega);
+void proj_stats(void* h, double* out8);
 int launch_div_resid_max(const GridDev& g, const double* u, const double* v, const double* w,
                          const double* u_in, const double* target, double* div_out,
                          unsigned long long* out_key, cudaStream_t st);

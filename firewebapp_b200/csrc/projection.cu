@@ -20,6 +20,7 @@
 // The stopping test mirrors scipy's: ||b - A x||_2 < rtol ||b||_2 on the
 // unsymmetrised system, warm-started from the previous solution.
 #include <vector>
+#include <chrono>
 #include <cstdlib>
 #include "common.cuh"
 #include "kernels.h"
@@ -69,6 +70,9 @@ struct ProjCtx {
   int graph_failed;
   int nu;             // Jacobi sweeps before and after the coarse correction
   double omega;       // Jacobi damping
+  // host-side statistics of the last solve (ms): total, fetch waits (sum, max),
+  // graph-launch calls (sum, max), fetches, iteration launches, iterations
+  double stats[8];
 };
 
 // ---------------------------------------------------------------------------
@@ -605,6 +609,7 @@ void* proj_create(const GridDev& g) {
   P->iter_kernels = 0;
   P->graph_failed = 0;
   P->nu = MG_NU_DEFAULT;
+  for (int q = 0; q < 8; ++q) P->stats[q] = 0.0;
   P->omega = MG_OMEGA;
   cudaStreamCreateWithFlags(&P->cs, cudaStreamNonBlocking);
   if (cudaGetLastError() != cudaSuccess || !P->p_prev) {
@@ -715,6 +720,11 @@ static int vcycle(ProjCtx* P, int l, const double* b, double* x, const double* d
   return nk;
 }
 
+void proj_stats(void* h, double* out8) {
+  ProjCtx* P = (ProjCtx*)h;
+  for (int q = 0; q < 8; ++q) out8[q] = P->stats[q];
+}
+
 int proj_configure(void* h, int nu, double omega) {
   ProjCtx* P = (ProjCtx*)h;
   if (nu < 1 || nu > 16 || !(omega > 0.0 && omega < 2.0)) return FS_EARG;
@@ -784,10 +794,20 @@ static int launch_iterations(ProjCtx* P, int count, cudaStream_t st) {
   return FS_OK;
 }
 
+using Clock = std::chrono::steady_clock;
+static double ms_since(Clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
 static int fetch(ProjCtx* P, int n, cudaStream_t st) {
+  const auto t0 = Clock::now();
   cudaMemcpyAsync(P->h_scal, P->scal, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
-  if (fs_stream_wait(st) != FS_OK) return FS_ECUDA;
-  return FS_OK;
+  const int rc = fs_stream_wait(st) != FS_OK ? FS_ECUDA : FS_OK;
+  const double w = ms_since(t0);
+  P->stats[1] += w;
+  if (w > P->stats[2]) P->stats[2] = w;
+  P->stats[5] += 1.0;
+  return rc;
 }
 
 // Solve for the pressure and correct u, v, w in place.  The iterations run
@@ -800,6 +820,8 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
   const GridDev& g = P->g;
   MGLevel& l0 = P->lev[0];
   const int64_t n = l0.n;
+  const auto t_start = Clock::now();
+  for (int q = 0; q < 8; ++q) P->stats[q] = 0.0;
   *iters = 0;
   k_proj_rhs<<<RED_BLOCKS, RED_THREADS, 0, st>>>(g, u, v, w, u_in, target, dt, P->rhs,
                                                  P->partial); fs_count_launch();
@@ -821,13 +843,20 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
     if (P->h_scal[SC_DONE] != 0.0) break;
     if (launched >= maxiter) return FS_ENOCONV;
     if (batch > maxiter - launched) batch = maxiter - launched;
+    const auto tl = Clock::now();
     stt = launch_iterations(P, batch, st);
+    const double lw = ms_since(tl);
+    P->stats[3] += lw;
+    if (lw > P->stats[4]) P->stats[4] = lw;
     if (stt) return stt;
     launched += batch;
+    P->stats[6] += batch;
     batch = 2;
   }
   *iters = (int)P->h_scal[SC_IT];
   P->last_iters = *iters;
+  P->stats[7] = *iters;
+  P->stats[0] = ms_since(t_start);
   P->have_prev = 1;
   Launch3 L = launch_cells(g);
   k_proj_correct<<<L.grid, L.block, 0, st>>>(g, u, v, w, x, P->ir, dt); fs_count_launch();

@@ -19,17 +19,23 @@ struct SpeciesArgs {
   int nspec;
 };
 
-__global__ void k_species(GridDev g, SpeciesArgs a, const double* __restrict__ rho,
-                          const double* __restrict__ u, const double* __restrict__ v,
-                          const double* __restrict__ w, double dt, double D,
-                          double inv_dx, double inv_dy, double inv_dx2, double inv_dy2) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int k = blockIdx.z;
-  if (i >= g.nx || j >= g.ny) return;
+// One thread per cell over the flattened grid (no idle lanes at the x edge);
+// the species loop is unrolled so the loads of all species are in flight
+// together.
+template <int NS>
+__global__ void __launch_bounds__(256, 4)
+k_species(GridDev g, SpeciesArgs a, const double* __restrict__ rho,
+          const double* __restrict__ u, const double* __restrict__ v,
+          const double* __restrict__ w, double dt, double D, double inv_dx, double inv_dy,
+          double inv_dx2, double inv_dy2) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int64_t sx = 1, sy = nx, sz = (int64_t)nx * ny;
-  const int64_t c = cidx(g, k, j, i);
+  const int64_t sy = nx, sz = (int64_t)nx * ny;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= sz * nz) return;
+  const int k = (int)(c / sz);
+  const int64_t rem = c - (int64_t)k * sz;
+  const int j = (int)(rem / nx);
+  const int i = (int)(rem - (int64_t)j * nx);
   const int jm2 = wrapj(j - 2, ny), jm1 = wrapj(j - 1, ny);
   const int jp1 = wrapj(j + 1, ny), jp2 = wrapj(j + 2, ny);
   const int64_t crow = c - (int64_t)j * sy;
@@ -41,11 +47,12 @@ __global__ void k_species(GridDev g, SpeciesArgs a, const double* __restrict__ r
   const double hz = 0.5 * (g.da[k] + g.db[k]);
   const bool mx = (i >= 2 && i <= nx - 3);
   const bool mz = (k >= 2 && k <= nz - 3);
-  for (int s = 0; s < a.nspec; ++s) {
-    const double* Y = a.Y[s];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double* __restrict__ Y = a.Y[s];
     const double Yi = Y[c];
-    const double YL_x = (i == 0) ? a.Y_inlet[s] : Y[c - sx];
-    const double YR_x = (i == nx - 1) ? Yi : Y[c + sx];
+    const double YL_x = (i == 0) ? a.Y_inlet[s] : Y[c - 1];
+    const double YR_x = (i == nx - 1) ? Yi : Y[c + 1];
     const double YL_z = (k == 0) ? Yi : Y[c - sz];
     const double YR_z = (k == nz - 1) ? Yi : Y[c + sz];
     double flux_x, flux_z;
@@ -93,9 +100,16 @@ int launch_species(const GridDev& g, int nspec, const double* const* Y, double* 
     a.Y[s] = Y[s]; a.Yo[s] = Yo[s]; a.S[s] = S[s]; a.Y_inlet[s] = Y_inlet[s];
   }
   double inv_dx = 1.0 / g.dx, inv_dy = 1.0 / g.dy;
-  Launch3 L = launch_cells(g);
-  k_species<<<L.grid, L.block, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
-                                        inv_dx * inv_dx, inv_dy * inv_dy); fs_count_launch();
+  const unsigned nb = blocks_for(ncells(g), 256);
+  switch (nspec) {
+    case 1: k_species<1><<<nb, 256, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
+                                             inv_dx * inv_dx, inv_dy * inv_dy); break;
+    case 2: k_species<2><<<nb, 256, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
+                                             inv_dx * inv_dx, inv_dy * inv_dy); break;
+    default: k_species<3><<<nb, 256, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
+                                              inv_dx * inv_dx, inv_dy * inv_dy); break;
+  }
+  fs_count_launch();
   return cuda_status();
 }
 

@@ -200,6 +200,10 @@ int fs_proj_apply(void* handle, const double* x, double* y, void* stream);
  * preconditioner (projection_3d.py:236-246, an FFT solve) has no such knob;
  * only the converged solution is shared. */
 int fs_proj_configure(void* handle, int nu, double omega);
+/* Host-side timings of the last fs_proj_project (ms): total, fetch waits
+ * (sum, max), iteration launch calls (sum, max), then the number of fetches,
+ * queued iterations and CG iterations (diagnostics; no reference counterpart). */
+int fs_proj_stats(void* handle, double* out8);
 /* max |div(u) - target| to *result (synchronises); div_out optional. */
 int fs_divergence_max(const FsGrid* g, const double* u, const double* v, const double* w,
                       const double* u_inlet, const double* div_target, double* div_out,
