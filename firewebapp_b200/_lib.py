@@ -93,6 +93,9 @@ SIGNATURES = {
     "fs_dom_set_sweep_mode": (I, [P, I, I]),
     "fs_dom_sweep_mode": (I, [P]),
     "fs_dom_load_intensity": (I, [P, P, P]),
+    "fs_dom_wrap_size": (I64, [P]),
+    "fs_dom_get_wrap": (I, [P, P, P]),
+    "fs_dom_set_wrap": (I, [P, P, P]),
     "fs_dom_sweep_timing": (I, [P, I, C.POINTER(D), C.POINTER(C.c_longlong)]),
     "fs_bed_step": (I, [_G, C.POINTER(FsBedParticles), C.POINTER(FsBedSegments),
                         C.POINTER(FsBedSources), C.POINTER(FsBedParams), P, P, P]),

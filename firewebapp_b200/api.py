@@ -279,3 +279,64 @@ def run_3d_spread_gpu_e2e(case: dict, steps: int, warmup: int = 1,
                 "h2d_bytes": nb * steps, "d2h_bytes": nb * steps}
     finally:
         hs.close()
+
+
+# ---------------------------------------------------------------- checkpoints
+_CKPT_WORK = ("omega", "q_rad", "q_rad_gas", "M_local")
+_CKPT_PARTS = ("x", "y", "z", "alive", "m_solid", "m_water", "m_char", "T_s", "m_water_0",
+               "sav", "m_char_max")
+
+
+def save_checkpoint(solver: Tier3Solver, path) -> Path:
+    """Write everything a later step reads: the state fields, the fields
+    carried between steps (omega, q_rad, q_rad_gas, M_local), soil, particles,
+    the projection's warm-start pressure, the DOM inflow rows and the clock.
+    The reference has no checkpoint; a run restored from this file continues
+    bit-identically."""
+    s = solver
+    torch.cuda.synchronize()
+    path = Path(path)
+    if not str(path).endswith(".npz"):
+        path = path.with_suffix(".npz")
+    path.parent.mkdir(parents=True, exist_ok=True)
+    arrays = {"f_" + k: s.f[k].cpu().numpy() for k in Tier3Solver.FIELDS}
+    arrays.update({"w_" + k: s.w[k].cpu().numpy() for k in _CKPT_WORK})
+    arrays.update({"p_" + k: s.part[k].cpu().numpy() for k in _CKPT_PARTS})
+    arrays["T_soil"] = s.T_soil.cpu().numpy()
+    arrays["pressure"] = s.pressure_view().cpu().numpy()
+    nw = int(s.lib.fs_dom_wrap_size(s.dom))
+    wrap = torch.empty(nw, dtype=torch.float64, device=s.dev)
+    check(s.lib.fs_dom_get_wrap(s.dom, ptr(wrap), s._s()), "fs_dom_get_wrap")
+    arrays["dom_wrap"] = wrap.cpu().numpy()
+    meta = {"case": s.case, "t": s.t, "dt": s.dt, "step_count": s.step_count,
+            "lset_step": s.lset_step, "extinct_count": s.extinct_count,
+            "front_t": list(s.front_t), "front_x": list(s.front_x),
+            "rtol": s.rtol, "proj_maxiter": s.proj_maxiter}
+    np.savez(path, _meta_json=np.array(json.dumps(meta)), **arrays)
+    return path
+
+
+def load_checkpoint(path, device="cuda") -> Tier3Solver:
+    """A solver restored from :func:`save_checkpoint`."""
+    z = np.load(Path(path), allow_pickle=False)
+    meta = json.loads(str(z["_meta_json"]))
+    s = Tier3Solver(meta["case"], device=device, projection_cg_rtol=meta["rtol"],
+                    proj_maxiter=meta["proj_maxiter"])
+    for k in Tier3Solver.FIELDS:
+        s.f[k].copy_(torch.as_tensor(z["f_" + k]))
+    for k in _CKPT_WORK:
+        s.w[k].copy_(torch.as_tensor(z["w_" + k]))
+    for k in _CKPT_PARTS:
+        s.part[k].copy_(torch.as_tensor(z["p_" + k]))
+    s.T_soil.copy_(torch.as_tensor(z["T_soil"]))
+    s.pressure_view().copy_(torch.as_tensor(z["pressure"]))
+    wrap = torch.as_tensor(z["dom_wrap"]).to(s.dev)
+    if wrap.numel() != int(s.lib.fs_dom_wrap_size(s.dom)):
+        raise ValueError("checkpoint DOM state does not match the case's grid and quadrature")
+    check(s.lib.fs_dom_set_wrap(s.dom, ptr(wrap), s._s()), "fs_dom_set_wrap")
+    s.t, s.dt = float(meta["t"]), float(meta["dt"])
+    s.step_count, s.lset_step = int(meta["step_count"]), int(meta["lset_step"])
+    s.extinct_count = int(meta["extinct_count"])
+    s.front_t, s.front_x = list(meta["front_t"]), list(meta["front_x"])
+    torch.cuda.synchronize()
+    return s

@@ -426,6 +426,18 @@ int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas) {
 
 int fs_dom_sweep_mode(void* handle) { return handle ? dom_mode(handle) : -1; }
 
+int64_t fs_dom_wrap_size(void* handle) { return handle ? dom_wrap_size(handle) : -1; }
+
+int fs_dom_get_wrap(void* handle, double* dst, void* stream) {
+  if (!handle || !dst) return FS_EARG;
+  return check(dom_get_wrap(handle, dst, ST(stream)), "fs_dom_get_wrap");
+}
+
+int fs_dom_set_wrap(void* handle, const double* src, void* stream) {
+  if (!handle || !src) return FS_EARG;
+  return check(dom_set_wrap(handle, src, ST(stream)), "fs_dom_set_wrap");
+}
+
 int fs_dom_load_intensity(void* handle, const double* I_full, void* stream) {
   if (!handle || !I_full) return FS_EARG;
   return check(dom_load_intensity(handle, I_full, ST(stream)), "fs_dom_load_intensity");

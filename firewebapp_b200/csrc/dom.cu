@@ -23,6 +23,8 @@
 //   2 one CTA per ordinate with the full intensity field stored (then G is
 //     summed over ordinates in ordinate order).
 //   3 one launch per hyperplane (any grid size).
+//   5 one CTA per ordinate (as 2) with fixed pencils per thread, the inputs
+//     of a hyperplane loaded in batches and the inflow rows staged ahead.
 // G in paths 1 and 4 is summed within each octant in ordinate order and then over
 // octants in octant order (the reference sums all ordinates in one sequence;
 // the two orders differ only by rounding).
@@ -48,6 +50,7 @@ struct DomCtx {
   double* Qoct;               // 8 * (Ny*Nx) octant partial ground flux (path 1)
   int mode;                   // resolved path: 0 not yet, 1 clusters, 2 block/ordinate, 3 planes
   int mode_req, force_C;      // requested path (0 auto) and cluster size (0 auto)
+  int groups;                 // ordinate groups per octant (clusters per octant), paths 4/6
   int Mo, cl_C, cl_rows, cl_threads;
   size_t cl_smem;
   int down_slot[8];
@@ -65,6 +68,30 @@ struct DomCtx {
   double sweep_ms;
   long long sweep_count;
 };
+
+// L2 eviction-priority hints: (kappa, kappa*B) is re-read by every ordinate of
+// a sweep and should stay in L2, while intensities and partial sums are
+// written once per sweep and should leave it first.
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ double2 ld_hint(const double2* p, uint64_t pol) {
+  double2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+               : "=d"(v.x), "=d"(v.y)
+               : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_stream(double* p, double v) {
+  asm volatile("st.global.cs.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
 
 __device__ __forceinline__ double clip01(double x) {
   if (x < 0.0) x = 0.0;
@@ -264,82 +291,83 @@ __global__ void __launch_bounds__(TPB, 1) k_dom_ord(GridDev g, OrdArgs a) {
   const double ix = fabs(xi) / g.dx;
   const double iy = fabs(eta) / g.dy;
   for (int k = threadIdx.x; k < nz; k += TPB) izt[k] = fabs(mu) / g.dz[k];
-  const int64_t N = ncells_dev(g);
-  double* I = a.I + (int64_t)n * N;
+  // cell index of sweep coordinates (ip, jp, kp) = base + ip*si + jp*sj + kp*sk (32-bit; the
+  // host checks that Nx*Ny*Nz fits)
+  const int si = fx ? 1 : -1;
+  const int sj = fy ? nx : -nx;
+  const int sk = fz ? nx * ny : -(nx * ny);
+  const int base = (fz ? 0 : (nz - 1) * nx * ny) + (fy ? 0 : (ny - 1) * nx) + (fx ? 0 : nx - 1);
+  const int wrap_off = fy ? (ny - 1) * nx : -(ny - 1) * nx;   // jp = 0 -> far end of the row
+  double* I = a.I + (int64_t)n * ncells_dev(g);
   const int nplanes = nx + ny + nz - 2;
-  // pencils q = tid + r*TPB, walked incrementally: (kp, jp) += (TPB / ny, TPB % ny)
   const int kp0 = threadIdx.x / ny, jp0 = threadIdx.x - kp0 * ny;
   const int dkp = TPB / ny, djp = TPB - dkp * ny;
-  auto stage = [&](int d) {
-    const int t = threadIdx.x;
-    if (t < nz && a.periodic) {  // row kp = t, jp = 0: previous sweep's value at the far end
-      const int ip = d - t;
-      if (ip >= 0 && ip < nx) {
-        const int i = fx ? ip : nx - 1 - ip;
-        const int k = fz ? t : nz - 1 - t;
-        const int jf = fy ? ny - 1 : 0;
-        wrapbuf[(d & 1) * nz + t] = I[((int64_t)k * ny + jf) * nx + i];
-      }
-    }
-    if (fz && t >= nz && t < nz + ny) {  // bottom row kp = 0, jp = t - nz
-      const int jp = t - nz;
-      const int ip = d - jp;
-      if (ip >= 0 && ip < nx) {
-        const int i = fx ? ip : nx - 1 - ip;
-        const int j = fy ? jp : ny - 1 - jp;
-        igbuf[(d & 1) * ny + jp] = a.Ig[(int64_t)j * nx + i];
-      }
-    }
-  };
-  stage(0);
-  __syncthreads();
-  for (int d = 0; d < nplanes; ++d) {
-    double* cur = (d & 1) ? bufB : bufA;
-    const double* prev = (d & 1) ? bufA : bufB;
-    const double* wrp = wrapbuf + (d & 1) * nz;
-    const double* igp = igbuf + (d & 1) * ny;
-    // this plane's (kappa, kappa*B) for all pencils first: one load latency per plane
-    double2 kab[PPT];
+  constexpr int CH = PPT < 4 ? PPT : 4;   // pencils whose loads are in flight together
+  const uint64_t keep = l2_policy_evict_last();
+  for (int d = -1; d < nplanes; ++d) {
+    // stage the inflow values of plane d+1 (plane 0 before the loop proper)
     {
+      const int dn = d + 1;
+      const int t = threadIdx.x;
+      if (dn < nplanes) {
+        if (t < nz && a.periodic) {
+          const int ip = dn - t;
+          if (ip >= 0 && ip < nx) wrapbuf[(dn & 1) * nz + t] = I[base + ip * si + t * sk + wrap_off];
+        }
+        if (fz && t >= nz && t < nz + ny) {
+          const int jp = t - nz;
+          const int ip = dn - jp;
+          if (ip >= 0 && ip < nx) {
+            const int i = fx ? ip : nx - 1 - ip;
+            const int j = fy ? jp : ny - 1 - jp;
+            igbuf[(dn & 1) * ny + jp] = a.Ig[j * nx + i];
+          }
+        }
+      }
+    }
+    if (d >= 0) {
+      double* cur = (d & 1) ? bufB : bufA;
+      const double* prev = (d & 1) ? bufA : bufB;
+      const double* wrp = wrapbuf + (d & 1) * nz;
+      const double* igp = igbuf + (d & 1) * ny;
       int kp = kp0, jp = jp0;
 #pragma unroll
-      for (int r = 0; r < PPT; ++r) {
-        const int ip = d - jp - kp;
-        if (kp < nz && ip >= 0 && ip < nx) {
-          const int i = fx ? ip : nx - 1 - ip;
-          const int j = fy ? jp : ny - 1 - jp;
-          const int k = fz ? kp : nz - 1 - kp;
-          kab[r] = a.kb[((int64_t)k * ny + j) * nx + i];
-        }
-        kp += dkp; jp += djp;
-        if (jp >= ny) { jp -= ny; ++kp; }
-      }
-    }
-    int kp = kp0, jp = jp0;
+      for (int r0 = 0; r0 < PPT; r0 += CH) {
+        double2 kab[CH];
+        int cc[CH];
+        {
+          int kq = kp, jq = jp;
 #pragma unroll
-    for (int r = 0; r < PPT; ++r) {
-      const int ip = d - jp - kp;
-      if (kp < nz && ip >= 0 && ip < nx) {
-        const int q = threadIdx.x + r * TPB;
-        const int i = fx ? ip : nx - 1 - ip;
-        const int j = fy ? jp : ny - 1 - jp;
-        const int k = fz ? kp : nz - 1 - kp;
-        const double Ix = ip > 0 ? prev[q] : a.I_amb;
-        const double Iy = jp > 0 ? prev[q - 1] : (a.periodic ? wrp[kp] : a.I_amb);
-        double Iz;
-        if (kp > 0) Iz = prev[q - ny];
-        else Iz = fz ? (mu > 0.0 ? igp[jp] : 0.0) : a.I_amb;
-        const double iz = izt[k];
-        const double num = kab[r].y + ix * Ix + iy * Iy + iz * Iz;
-        const double den = kab[r].x + ix + iy + iz;
-        const double v = num / den;
-        cur[q] = v;
-        I[((int64_t)k * ny + j) * nx + i] = v;
+          for (int r = 0; r < CH; ++r) {
+            const int ip = d - jq - kq;
+            cc[r] = (kq < nz && ip >= 0 && ip < nx) ? base + ip * si + jq * sj + kq * sk : -1;
+            if (cc[r] >= 0) kab[r] = ld_hint(a.kb + cc[r], keep);
+            kq += dkp; jq += djp;
+            if (jq >= ny) { jq -= ny; ++kq; }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < CH; ++r) {
+          if (cc[r] >= 0) {
+            const int ip = d - jp - kp;
+            const int q = threadIdx.x + (r0 + r) * TPB;
+            const double Ix = ip > 0 ? prev[q] : a.I_amb;
+            const double Iy = jp > 0 ? prev[q - 1] : (a.periodic ? wrp[kp] : a.I_amb);
+            double Iz;
+            if (kp > 0) Iz = prev[q - ny];
+            else Iz = fz ? (mu > 0.0 ? igp[jp] : 0.0) : a.I_amb;
+            const double iz = izt[fz ? kp : nz - 1 - kp];
+            const double num = kab[r].y + ix * Ix + iy * Iy + iz * Iz;
+            const double den = kab[r].x + ix + iy + iz;
+            const double v = num / den;
+            cur[q] = v;
+            st_stream(I + cc[r], v);
+          }
+          kp += dkp; jp += djp;
+          if (jp >= ny) { jp -= ny; ++kp; }
+        }
       }
-      kp += dkp; jp += djp;
-      if (jp >= ny) { jp -= ny; ++kp; }
     }
-    if (d + 1 < nplanes) stage(d + 1);
     __syncthreads();
   }
 }
@@ -404,6 +432,7 @@ struct OctArgs {
   int Mo, C, rows, periodic;
   unsigned down_slots;  // 4 bits per octant: ground-flux slot, 15 = upward octant
   int* err;             // set when a bounded wait gives up (pipelined sweep)
+  int groups;           // clusters per octant, each with MO of its ordinates (barrier path)
 };
 
 // Dynamic shared memory: two hyperplane buffers of Mo x (rows*Ny) doubles,
@@ -436,14 +465,16 @@ __device__ __forceinline__ void cluster_wait_acquire() {
 // ordinates of the thread's cell from shared memory (the neighbour CTA's
 // last row through DSMEM), arrive, then store the octant partials and
 // prefetch the next plane's kappa / inflow values while the others finish.
-template <int MO>
-__global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant(GridDev g, OctArgs a) {
+template <int MO, int MINB = 1>
+__global__ void __launch_bounds__(OCT_MAX_THREADS, MINB) k_dom_octant(GridDev g, OctArgs a) {
   extern __shared__ double sh[];
   cg::cluster_group cl = cg::this_cluster();
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int rank = (int)cl.block_rank();
-  const int oct = blockIdx.x / a.C;
-  const int n0 = oct * MO;
+  const int part = blockIdx.x / a.C;      // (octant, ordinate group)
+  const int oct = part / a.groups;
+  const int grp = part - oct * a.groups;
+  const int n0 = (oct * a.groups + grp) * MO;
   const int S = a.rows * ny;
   double* buf0 = sh;
   double* buf1 = sh + (size_t)MO * S;
@@ -476,8 +507,8 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant(GridDev g, Oc
   const int64_t N = ncells_dev(g);
   const int64_t n2 = (int64_t)nx * ny;
   const int slot_bits = (int)((a.down_slots >> (4 * oct)) & 15u);
-  const int slot = slot_bits == 15 ? -1 : slot_bits;
-  double* Go = a.Goct + (int64_t)oct * N;
+  const int slot = slot_bits == 15 ? -1 : slot_bits * a.groups + grp;
+  double* Go = a.Goct + (int64_t)part * N;
   const int64_t wstride = (int64_t)nz * nx;
   double* wrap0 = a.wrap + (int64_t)n0 * wstride;
   const bool ground_out = has && !fz && k == 0 && slot >= 0;
@@ -487,6 +518,7 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant(GridDev g, Oc
   const bool y_wrap_out = has && jp == ny - 1 && a.periodic;
   const double* nbase = nullptr;
   const int nplanes = nx + ny + nz - 2;
+  const uint64_t keep = l2_policy_evict_last();
   // prefetched values for the coming plane
   double2 kab = make_double2(0.0, 0.0);
   double win[MO];
@@ -495,7 +527,7 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant(GridDev g, Oc
     const int ip = d - jp - kp;
     if (!has || ip < 0 || ip >= nx) return;
     const int i = fx ? ip : nx - 1 - ip;
-    kab = a.kb[((int64_t)k * ny + j) * nx + i];
+    kab = ld_hint(a.kb + ((int64_t)k * ny + j) * nx + i, keep);
     if (y_wrap) {
 #pragma unroll
       for (int m = 0; m < MO; ++m) win[m] = wrap0[m * wstride + (int64_t)k * nx + i];
@@ -543,7 +575,7 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant(GridDev g, Oc
     cluster_arrive_release();
     if (act) {
       const int i = fx ? ip : nx - 1 - ip;
-      Go[((int64_t)k * ny + j) * nx + i] = gs;
+      st_stream(Go + ((int64_t)k * ny + j) * nx + i, gs);
       if (y_wrap_out) {
 #pragma unroll
         for (int m = 0; m < MO; ++m) wrap0[m * wstride + (int64_t)k * nx + i] = v[m];
@@ -785,9 +817,9 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_pipe(GridDev 
   cluster_wait_acquire();
 }
 
-template <int MO>
+template <int MO, int MINB = 1>
 static cudaError_t launch_octant_kernel(const GridDev& g, const OctArgs& a, cudaLaunchConfig_t* cfg) {
-  return cudaLaunchKernelEx(cfg, k_dom_octant<MO>, g, a);
+  return cudaLaunchKernelEx(cfg, k_dom_octant<MO, MINB>, g, a);
 }
 
 template <int MO>
@@ -796,24 +828,40 @@ static cudaError_t launch_octant_pipe_kernel(const GridDev& g, const OctArgs& a,
   return cudaLaunchKernelEx(cfg, k_dom_octant_pipe<MO>, g, a);
 }
 
-// pipe: the point-to-point pipelined kernel (path 1), else the cluster-barrier one (path 4)
-static const void* octant_kernel_ptr(int Mo, bool pipe) {
+// pipe: the point-to-point pipelined kernel (path 1), else the cluster-barrier one (paths 4
+// and 6, the latter with two clusters per octant of half the ordinates, two CTAs per SM)
+static const void* octant_kernel_ptr(int Mo, bool pipe, int groups = 1) {
+  if (pipe) {
+    switch (Mo) {
+      case 3: return (const void*)k_dom_octant_pipe<3>;
+      case 6: return (const void*)k_dom_octant_pipe<6>;
+      case 10: return (const void*)k_dom_octant_pipe<10>;
+      default: return nullptr;
+    }
+  }
+  if (groups == 2) {
+    switch (Mo / 2) {
+      case 3: return (const void*)k_dom_octant<3, 2>;
+      case 5: return (const void*)k_dom_octant<5, 2>;
+      default: return nullptr;
+    }
+  }
   switch (Mo) {
-    case 3: return pipe ? (const void*)k_dom_octant_pipe<3> : (const void*)k_dom_octant<3>;
-    case 6: return pipe ? (const void*)k_dom_octant_pipe<6> : (const void*)k_dom_octant<6>;
-    case 10: return pipe ? (const void*)k_dom_octant_pipe<10> : (const void*)k_dom_octant<10>;
+    case 3: return (const void*)k_dom_octant<3>;
+    case 6: return (const void*)k_dom_octant<6>;
+    case 10: return (const void*)k_dom_octant<10>;
     default: return nullptr;
   }
 }
 
 // G = sum over octants of the octant partials (octant order); max G and max |G - G_prev|
-__global__ void k_dom_G_oct(int64_t N, const double* __restrict__ Goct, double* G,
+__global__ void k_dom_G_oct(int64_t N, int nparts, const double* __restrict__ Goct, double* G,
                             const double* __restrict__ Gp, unsigned long long* keys) {
   unsigned long long bg = 0, bd = 0;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < N;
        c += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int o = 0; o < 8; ++o) s += Goct[(int64_t)o * N + c];
+    for (int o = 0; o < nparts; ++o) s += Goct[(int64_t)o * N + c];
     G[c] = s;
     double d = fabs(s - Gp[c]);
     unsigned long long ks = (s != s) ? 0x7ff8000000000000ull
@@ -849,6 +897,20 @@ __global__ void k_dom_ground_oct(int n2, int nslots, const double* __restrict__ 
 }
 
 // wrap rows from a full intensity field: wrap[n][k][i] = I[n][k][j_far][i]
+// inverse of k_dom_extract_wrap: write the wrap rows into a full intensity field
+__global__ void k_dom_scatter_wrap(GridDev g, int M, const double* __restrict__ oy,
+                                   const double* __restrict__ wrap, double* I) {
+  const int64_t tot = (int64_t)M * g.nz * g.nx;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= tot) return;
+  const int n = (int)(t / ((int64_t)g.nz * g.nx));
+  const int64_t r = t - (int64_t)n * g.nz * g.nx;
+  const int k = (int)(r / g.nx);
+  const int i = (int)(r - (int64_t)k * g.nx);
+  const int jf = oy[n] >= 0.0 ? g.ny - 1 : 0;
+  I[(int64_t)n * ncells_dev(g) + cidx(g, k, jf, i)] = wrap[t];
+}
+
 __global__ void k_dom_extract_wrap(GridDev g, int M, const double* __restrict__ oy,
                                    const double* __restrict__ I, double* wrap) {
   const int64_t tot = (int64_t)M * g.nz * g.nx;
@@ -898,7 +960,7 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   cudaMemcpy(D->oz, oz, sizeof(double) * M, cudaMemcpyHostToDevice);
   cudaMemcpy(D->w, w, sizeof(double) * M, cudaMemcpyHostToDevice);
   D->I = nullptr; D->wrap = nullptr; D->kb = nullptr; D->Goct = nullptr; D->Qoct = nullptr;
-  D->mode = 0; D->mode_req = 0; D->force_C = 0;
+  D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemset(D->G, 0, sizeof(double) * N);
   cudaMalloc(&D->ks, sizeof(double) * N); cudaMalloc(&D->kg, sizeof(double) * N);
@@ -955,14 +1017,14 @@ static bool octant_grouping(const DomCtx* D) {
 }
 
 // Pick the cluster size (CTAs per octant) and launch shape for path 1; false if none fits.
-static bool plan_clusters(DomCtx* D, int force_C, bool pipe) {
+static bool plan_clusters(DomCtx* D, int force_C, bool pipe, int groups = 1) {
   const GridDev& g = D->g;
-  const int Mo = D->M / 8;
+  const int Mo = D->M / 8 / groups;
   int dev = 0, optin = 0, smem_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-  const void* fn = octant_kernel_ptr(Mo, pipe);
+  const void* fn = octant_kernel_ptr(Mo * groups, pipe, groups);
   if (!fn) return false;
   cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
@@ -979,14 +1041,14 @@ static bool plan_clusters(DomCtx* D, int force_C, bool pipe) {
     if (need > (size_t)optin) continue;
     // ask for more than half an SM's shared memory so that no two CTAs share an SM,
     // unless that leaves fewer than 8 clusters resident
-    size_t pad = (size_t)smem_sm / 2 + 1024;
+    size_t pad = groups > 1 ? need : (size_t)smem_sm / 2 + 1024;
     size_t trial[2] = {need > pad ? need : (pad <= (size_t)optin ? pad : need), need};
     for (int t = 0; t < 2; ++t) {
       cudaLaunchConfig_t cfg = {};
       cudaLaunchAttribute at[1];
       at[0].id = cudaLaunchAttributeClusterDimension;
       at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-      cfg.gridDim = dim3(8 * C); cfg.blockDim = dim3(threads);
+      cfg.gridDim = dim3(8 * groups * C); cfg.blockDim = dim3(threads);
       cfg.dynamicSmemBytes = trial[t]; cfg.attrs = at; cfg.numAttrs = 1;
       int active = 0;
       if (cudaOccupancyMaxActiveClusters(&active, fn, &cfg) != cudaSuccess) {
@@ -997,6 +1059,7 @@ static bool plan_clusters(DomCtx* D, int force_C, bool pipe) {
       const int waves = (8 + active - 1) / active;
       const int per_thread = (rows * g.ny + threads - 1) / threads;
       double cost = (double)waves * per_thread * (t == 0 ? 1.0 : (active >= 8 ? 1.5 : 2.0));
+      if (groups > 1) cost = (double)((8 * groups + active - 1) / active) * 0.5;
       if (cost < best) {
         best = cost; found = true;
         D->cl_C = C; D->cl_rows = rows; D->cl_threads = threads; D->cl_smem = trial[t];
@@ -1013,20 +1076,22 @@ static int dom_prepare(DomCtx* D) {
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
   const int want = D->mode_req;
   // auto picks the cluster-barrier sweep (path 4), measured faster than path 1
-  if ((want == 0 || want == 1 || want == 4) && octant_grouping(D) &&
-      plan_clusters(D, D->force_C, want == 1)) {
-    D->mode = want == 1 ? 1 : 4;
+  const int groups = (want == 6 && D->M % 16 == 0) ? 2 : 1;
+  if ((want == 0 || want == 1 || want == 4 || want == 6) && octant_grouping(D) &&
+      plan_clusters(D, D->force_C, want == 1, groups)) {
+    D->mode = want == 1 ? 1 : (want == 6 ? 6 : 4);
+    D->groups = groups;
     D->Mo = D->M / 8;
     int slot = 0;
     for (int o = 0; o < 8; ++o) D->down_slot[o] = D->hoz[o * D->Mo] < 0.0 ? slot++ : -1;
     cudaMalloc(&D->kb, sizeof(double2) * N);
-    cudaMalloc(&D->Goct, sizeof(double) * 8 * N);
-    cudaMalloc(&D->Qoct, sizeof(double) * 8 * n2);
+    cudaMalloc(&D->Goct, sizeof(double) * 8 * groups * N);
+    cudaMalloc(&D->Qoct, sizeof(double) * 8 * groups * n2);
     cudaMalloc(&D->wrap, sizeof(double) * D->M * g.nz * g.nx);
     cudaMemset(D->wrap, 0, sizeof(double) * D->M * g.nz * g.nx);
     return cuda_status();
   }
-  if (want == 1 || want == 4) {
+  if (want == 1 || want == 4 || want == 6) {
     fs_set_error("octant-cluster sweep not possible for this grid or quadrature");
     return FS_EARG;
   }
@@ -1053,7 +1118,7 @@ static int dom_prepare(DomCtx* D) {
 
 int dom_set_mode(void* h, int mode, int cluster_ctas) {
   DomCtx* D = (DomCtx*)h;
-  if (mode < 0 || mode > 5 || cluster_ctas < 0 || cluster_ctas > 16) return FS_EARG;
+  if (mode < 0 || mode > 6 || cluster_ctas < 0 || cluster_ctas > 16) return FS_EARG;
   if (D->mode != 0) {
     fs_set_error("sweep mode must be set before the first solve or intensity load");
     return FS_EARG;
@@ -1070,13 +1135,48 @@ int dom_load_intensity(void* h, const double* I_full, cudaStream_t st) {
   int rc = dom_prepare(D);
   if (rc != FS_OK) return rc;
   const GridDev& g = D->g;
-  if (D->mode == 1 || D->mode == 4) {
+  if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
     const int64_t tot = (int64_t)D->M * g.nz * g.nx;
     k_dom_extract_wrap<<<blocks_for(tot, 256), 256, 0, st>>>(g, D->M, D->oy, I_full, D->wrap);
     fs_count_launch();
   } else {
     cudaMemcpyAsync(D->I, I_full, sizeof(double) * ncells(g) * D->M, cudaMemcpyDeviceToDevice,
                     st);
+  }
+  return cuda_status();
+}
+
+int64_t dom_wrap_size(void* h) {
+  DomCtx* D = (DomCtx*)h;
+  return (int64_t)D->M * D->g.nz * D->g.nx;
+}
+
+// The persistent part of the intensities (the y-inflow rows a later sweep
+// reads), M x Nz x Nx, out of or into whichever storage the sweep path uses.
+int dom_get_wrap(void* h, double* dst, cudaStream_t st) {
+  DomCtx* D = (DomCtx*)h;
+  int rc = dom_prepare(D);
+  if (rc != FS_OK) return rc;
+  const int64_t tot = dom_wrap_size(h);
+  if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
+    cudaMemcpyAsync(dst, D->wrap, sizeof(double) * tot, cudaMemcpyDeviceToDevice, st);
+  } else {
+    k_dom_extract_wrap<<<blocks_for(tot, 256), 256, 0, st>>>(D->g, D->M, D->oy, D->I, dst);
+    fs_count_launch();
+  }
+  return cuda_status();
+}
+
+int dom_set_wrap(void* h, const double* src, cudaStream_t st) {
+  DomCtx* D = (DomCtx*)h;
+  int rc = dom_prepare(D);
+  if (rc != FS_OK) return rc;
+  const int64_t tot = dom_wrap_size(h);
+  if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
+    cudaMemcpyAsync(D->wrap, src, sizeof(double) * tot, cudaMemcpyDeviceToDevice, st);
+  } else {
+    k_dom_scatter_wrap<<<blocks_for(tot, 256), 256, 0, st>>>(D->g, D->M, D->oy, src, D->I);
+    fs_count_launch();
   }
   return cuda_status();
 }
@@ -1109,7 +1209,7 @@ static int launch_octant_sweep(DomCtx* D, const OctArgs& a, cudaStream_t st) {
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = D->cl_C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-  cfg.gridDim = dim3(8 * D->cl_C);
+  cfg.gridDim = dim3(8 * D->groups * D->cl_C);
   cfg.blockDim = dim3(D->cl_threads);
   cfg.dynamicSmemBytes = D->cl_smem;
   cfg.stream = st;
@@ -1117,6 +1217,15 @@ static int launch_octant_sweep(DomCtx* D, const OctArgs& a, cudaStream_t st) {
   cfg.numAttrs = 1;
   cudaError_t e;
   const bool pipe = D->mode == 1;
+  if (D->groups == 2) {
+    switch (D->Mo / 2) {
+      case 3: e = launch_octant_kernel<3, 2>(D->g, a, &cfg); break;
+      case 5: e = launch_octant_kernel<5, 2>(D->g, a, &cfg); break;
+      default: e = cudaErrorInvalidValue;
+    }
+    fs_count_launch();
+    return e == cudaSuccess ? FS_OK : FS_ECUDA;
+  }
   switch (D->Mo) {
     case 3: e = pipe ? launch_octant_pipe_kernel<3>(D->g, a, &cfg)
                      : launch_octant_kernel<3>(D->g, a, &cfg); break;
@@ -1145,7 +1254,7 @@ static int launch_ord_sweep(DomCtx* D, double I_amb, cudaStream_t st) {
   oa.I_amb = I_amb; oa.periodic = 1;
   const size_t smem = ord_smem_bytes(g.ny, g.nz);
   // pencils per thread at 1024 threads per ordinate (the staging threads need ny+nz)
-  if (g.ny + g.nz > 1024) return FS_EARG;
+  if (g.ny + g.nz > 1024 || ncells(g) >= (int64_t)1 << 31) return FS_EARG;
   const int need = (npen + 1023) / 1024;
   if (need <= 1) ord_launch<1, 1024>(D, oa, smem, st);
   else if (need <= 2) ord_launch<2, 1024>(D, oa, smem, st);
@@ -1166,7 +1275,7 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
   const int M = D->M;
-  const bool octp = D->mode == 1 || D->mode == 4;
+  const bool octp = D->mode == 1 || D->mode == 4 || D->mode == 6;
   const double Tamb4 = pow(T_amb, 4.0);
   k_dom_setup<<<blocks_for(N, 256), 256, 0, st>>>(g, Ts, Tg, as, om, YH, rho, Mloc, sigma, Tamb4,
                                                   D->kgmax, D->ks, D->kg, D->ksafe, D->B,
@@ -1185,13 +1294,14 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
     oa.kb = D->kb; oa.ox = D->ox; oa.oy = D->oy; oa.oz = D->oz; oa.w = D->w; oa.Ig = D->Ig_out;
     oa.Goct = D->Goct; oa.Qoct = D->Qoct; oa.wrap = D->wrap; oa.I_amb = I_amb; oa.Mo = D->Mo;
     oa.C = D->cl_C; oa.rows = D->cl_rows; oa.periodic = 1;
+    oa.groups = D->groups;
     oa.err = (int*)(D->keys + 2);
     oa.down_slots = 0;
     for (int o = 0; o < 8; ++o)
       oa.down_slots |= (unsigned)(D->down_slot[o] >= 0 ? D->down_slot[o] : 15) << (4 * o);
   }
   int nslots = 0;
-  for (int o = 0; o < 8; ++o) nslots += (octp && D->down_slot[o] >= 0) ? 1 : 0;
+  for (int o = 0; o < 8; ++o) nslots += (octp && D->down_slot[o] >= 0) ? D->groups : 0;
   const int nplanes = g.nx + g.ny + g.nz - 2;
   const int64_t nthr = (int64_t)g.ny * g.nz * M;
   const double refl = (1.0 - D->eps_w) / PI_D;
@@ -1225,7 +1335,7 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
     unsigned nb = blocks_for(N, 256);
     if (nb > 1184) nb = 1184;
     if (octp) {
-      k_dom_G_oct<<<nb, 256, 0, st>>>(N, D->Goct, D->G, D->Gp, D->keys);
+      k_dom_G_oct<<<nb, 256, 0, st>>>(N, 8 * D->groups, D->Goct, D->G, D->Gp, D->keys);
       fs_count_launch();
       k_dom_ground_oct<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, nslots, D->Qoct, D->Isoil,
                                                             refl, D->relax, D->Ig_out, D->qin);

@@ -101,6 +101,9 @@ double* dom_intensity(void* h);
 int dom_set_mode(void* h, int mode, int cluster_ctas);
 int dom_mode(void* h);
 int dom_load_intensity(void* h, const double* I_full, cudaStream_t st);
+int64_t dom_wrap_size(void* h);
+int dom_get_wrap(void* h, double* dst, cudaStream_t st);
+int dom_set_wrap(void* h, const double* src, cudaStream_t st);
 double* dom_G(void* h);
 int dom_last_iters(void* h);
 void dom_set_timing(void* h, int on);

@@ -264,23 +264,27 @@ struct DiffArgs {
   int clip;
 };
 
-__global__ void k_turb_diff(GridDev g, DiffArgs a, const double* __restrict__ nu_t, double sc_t,
-                            double dt_sub, double inv_dx2, double inv_dy2) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int k = blockIdx.z;
-  if (i >= g.nx || j >= g.ny) return;
+template <int NF>
+__global__ void __launch_bounds__(256, 4)
+k_turb_diff(GridDev g, DiffArgs a, const double* __restrict__ nu_t, double sc_t, double dt_sub,
+            double inv_dx2, double inv_dy2) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int64_t sy = nx, sz = (int64_t)nx * ny;
-  const int64_t c = cidx(g, k, j, i);
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= sz * nz) return;
+  const int k = (int)(c / sz);
+  const int64_t rem = c - (int64_t)k * sz;
+  const int j = (int)(rem / nx);
+  const int i = (int)(rem - (int64_t)j * nx);
   const int64_t crow = c - (int64_t)j * sy;
   const int64_t cjp = crow + wrapj(j + 1, ny) * sy, cjm = crow + wrapj(j - 1, ny) * sy;
   const double inv_dz_k = 1.0 / g.dz[k];
   const double inv_d_above = 1.0 / g.da[k];
   const double inv_d_below = 1.0 / g.db[k];
   const double D_t = nu_t[c] / sc_t;
-  for (int s = 0; s < a.nfield; ++s) {
-    const double* f = a.f[s];
+#pragma unroll
+  for (int s = 0; s < NF; ++s) {
+    const double* __restrict__ f = a.f[s];
     const double fc = f[c];
     const double fxL = (i == 0) ? fc : f[c - 1];
     const double fxR = (i == nx - 1) ? fc : f[c + 1];
@@ -311,9 +315,15 @@ int launch_turb_diff(const GridDev& g, int nfield, const double* const* f, doubl
     a.lo[s] = clip ? lo[s] : 0.0;
     a.hi[s] = clip ? hi[s] : 0.0;
   }
-  Launch3 L = launch_cells(g);
-  k_turb_diff<<<L.grid, L.block, 0, st>>>(g, a, nu_t, sc_t, dt_sub, 1.0 / (g.dx * g.dx),
-                                          1.0 / (g.dy * g.dy)); fs_count_launch();
+  const unsigned nb = blocks_for(ncells(g), 256);
+  const double ix2 = 1.0 / (g.dx * g.dx), iy2 = 1.0 / (g.dy * g.dy);
+  switch (nfield) {
+    case 1: k_turb_diff<1><<<nb, 256, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
+    case 2: k_turb_diff<2><<<nb, 256, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
+    case 3: k_turb_diff<3><<<nb, 256, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
+    default: k_turb_diff<4><<<nb, 256, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
+  }
+  fs_count_launch();
   return cuda_status();
 }
 

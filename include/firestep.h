@@ -226,7 +226,9 @@ double* fs_dom_intensity(void* handle);
  * grid fits, else one CTA per ordinate, else one launch per hyperplane),
  * 1 octant clusters with point-to-point hand-off between CTAs,
  * 2 one CTA per ordinate, 3 hyperplane launches, 4 octant clusters with a
- * cluster barrier per hyperplane; cluster_ctas 0 = automatic, else CTAs per
+ * cluster barrier per hyperplane, 5 one CTA per ordinate with per-thread
+ * pencils and batched loads, 6 as 4 with two clusters per octant (half the
+ * ordinates each, two CTAs per SM); cluster_ctas 0 = automatic, else CTAs per
  * octant (1..16).  Only before the first solve or intensity load.  Path 1
  * bounds its waits: a stalled hand-off returns FS_ETIMEOUT. */
 int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
@@ -235,6 +237,14 @@ int fs_dom_sweep_mode(void* handle);
 /* Load the persistent intensity state from a full device field
  * (M x Nz x Ny x Nx), as a reference I_set would seed the next solve. */
 int fs_dom_load_intensity(void* handle, const double* I_full, void* stream);
+/* The persistent DOM state for checkpoints: the y-periodic inflow rows
+ * (M x Nz x Nx doubles, device memory), read out of or written into
+ * whichever storage the sweep path uses.  The reference keeps the whole
+ * I_set between calls (dom_3d.py:286-300); these rows are the part of it a
+ * later sweep reads. */
+int64_t fs_dom_wrap_size(void* handle);
+int fs_dom_get_wrap(void* handle, double* dst, void* stream);
+int fs_dom_set_wrap(void* handle, const double* src, void* stream);
 int fs_dom_iterations(void* handle);
 /* enable >= 0 turns per-sweep event timing on/off (and resets it); the
  * accumulated sweep time and sweep count are returned when pointers are given */

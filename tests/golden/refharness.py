@@ -126,13 +126,15 @@ PART_FIELDS = ("x", "y", "z", "alive", "m_solid", "m_water", "m_char", "T_s",
 
 
 def run_reference(case: dict, n_steps: int, capture_steps=None,
-                  projection_cg_rtol: float = 1e-12, verbose=False):
+                  projection_cg_rtol: float = 1e-12, verbose=False, step_hook=None):
     """Run the reference for ``n_steps`` outer steps; return per-step snapshots.
 
     Returns ``(init, snaps, trace)``: ``init`` is the state right after the
     driver's initialisation (before step 1), ``snaps[n]`` the state after step
     ``n`` for every ``n`` in ``capture_steps`` and ``trace`` per-step scalars
-    (dt, projection iterations, DOM source iterations).
+    (dt, projection iterations, DOM source iterations).  ``step_hook(n,
+    state, extras)``, if given, is called after every step with the
+    reference's state object and the captured extra fields.
     """
     R = load_reference()
     S, T, D, P, L, soil, F, C = (R[k] for k in "S T D P L soil F C".split())
@@ -279,6 +281,8 @@ def run_reference(case: dict, n_steps: int, capture_steps=None,
         trace["dom_sweeps"].append(counters["sweeps"])
         counters["proj"] = 0
         counters["sweeps"] = 0
+        if step_hook is not None:
+            step_hook(n, cap["state"], cap)
         if n in capture_steps:
             snaps[n] = snapshot()
             if "dom" in cap:

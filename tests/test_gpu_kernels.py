@@ -249,7 +249,7 @@ def test_k_epsilon(vectors):
         assert rel_l2(host(nuo), c["nu_t_out"]) <= LIBM, name
 
 
-@pytest.mark.parametrize("mode", [1, 2, 3, 4])
+@pytest.mark.parametrize("mode", [1, 2, 3, 4, 5, 6])
 def test_dom(vectors, mode):
     """Every sweep path (pipelined octant clusters, CTA per ordinate, hyperplane
     launches, octant clusters with cluster barriers)."""
