@@ -48,6 +48,20 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def job_totals(cells_steps: float, seconds: float, device="cpu"):
+    """Whole-job work and time over the ranks: cell-steps summed, time the
+    maximum (the slowest rank bounds the job).  Single process: unchanged."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(cells_steps), float(seconds)
+    w = torch.tensor([float(cells_steps)], dtype=torch.float64, device=device)
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(w.item()), float(t.item())
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -275,11 +289,9 @@ def main():
     ms = e0.elapsed_time(e1) / args.steps
     kt = solver.kernel_times()
     solver.enable_kernel_timers(False)
-    if ws > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = ws * cells / (ms * 1e-3)
+    work, sec = job_totals(cells * args.steps, ms * 1e-3 * args.steps, device="cuda")
+    ms = 1e3 * sec / args.steps
+    value = work / sec
 
     # ---- roofline of the dominant bracketed kernel
     peak, peak_src = _peaks()
@@ -351,13 +363,8 @@ def measure_e2e(case, steps, ws):
     import torch
     from firewebapp_b200.api import run_3d_spread_gpu_e2e
     res = run_3d_spread_gpu_e2e(case, steps)
-    sec = res["seconds"]
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([sec], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sec = float(t.item())
-    return {"value": ws * res["cells"] * steps / sec, "unit": UNIT,
+    work, sec = job_totals(res["cells"] * steps, res["seconds"], device="cuda")
+    return {"value": work / sec, "unit": UNIT,
             "h2d_bytes_per_step": res["h2d_bytes"] / steps,
             "d2h_bytes_per_step": res["d2h_bytes"] / steps}
 

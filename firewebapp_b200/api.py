@@ -160,10 +160,13 @@ class _Diag:
 
 def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | None = None,
                       snapshot_every_s: float = 1.0, device="cuda",
-                      projection_cg_rtol: float = 1.0e-6) -> Spread3DResultGPU:
+                      projection_cg_rtol: float = 1.0e-6, snapshot_dir=None,
+                      snapshot_interval_s: float = 1.0) -> Spread3DResultGPU:
     """Device-resident ``run_3d_spread`` for a case; stops at ``n_steps``
     outer steps, at ``t_end`` simulated seconds or at the reference's own
-    exit tests, whichever comes first."""
+    exit tests, whichever comes first.  With ``snapshot_dir`` it writes
+    ``snap_NNNN.npz`` files every ``snapshot_interval_s`` of simulated time,
+    as the reference does (spread_3d.py:3537-3669)."""
     if n_steps is None and t_end is None:
         raise ValueError("run_3d_spread_gpu needs n_steps or t_end")
     s = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol)
@@ -177,6 +180,10 @@ def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | 
                                 front_x=s.front_x, grid=g, state_final={})
         dg = _Diag(s)
         snap_t, snap_x = [], []
+        last_snap_t, snap_idx = -1.0e30, 0
+        if snapshot_dir is not None:
+            snapshot_dir = Path(snapshot_dir)
+            snapshot_dir.mkdir(parents=True, exist_ok=True)
         next_snap = snapshot_every_s
         hrr_peak = 0.0
         k = 0
@@ -194,6 +201,11 @@ def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | 
                 snap_t.append(s.t)
                 snap_x.append(dg.lead_x_Ts())
                 next_snap += snapshot_every_s
+            if snapshot_dir is not None and s.t - last_snap_t >= snapshot_interval_s:
+                last_snap_t = s.t
+                write_snapshot(s, snapshot_dir / f"snap_{snap_idx:04d}.npz",
+                               float(case.get("wind_speed_m_s", 0.0)))
+                snap_idx += 1
         st = s.state()
         res.state_final = st
         res.k_turb_final = st["k_turb"]
@@ -279,6 +291,85 @@ def run_3d_spread_gpu_e2e(case: dict, steps: int, warmup: int = 1,
                 "h2d_bytes": nb * steps, "d2h_bytes": nb * steps}
     finally:
         hs.close()
+
+
+# ------------------------------------------------------------------ snapshots
+OMEGA_MIN_FLAME = 1.0e-3   # flame_front_3d.py:751-753 active-flame thresholds
+T_PLUME_MIN = 1000.0
+Y_F_MIN_PLUME = 1.0e-3
+
+
+def phi_flame_from_state(omega, T_g, Y_fuel, dx, dy, dz_arr):
+    """Signed distance to the active-flame region, negative inside
+    (``compute_phi_flame_from_state``, flame_front_3d.py:756-800): Euclidean
+    distance transforms of the active mask with sampling (mean dz, dy, dx)."""
+    from scipy import ndimage
+    active = (omega > OMEGA_MIN_FLAME) | ((T_g > T_PLUME_MIN) & (Y_fuel > Y_F_MIN_PLUME))
+    sampling = (float(np.mean(dz_arr)), dy, dx)
+    if active.any() and (~active).any():
+        d_out = ndimage.distance_transform_edt(~active, sampling=sampling)
+        d_in = ndimage.distance_transform_edt(active, sampling=sampling)
+        return np.where(active, -d_in, d_out)
+    return np.full(active.shape, -1.0e6 if active.all() else 1.0e6)
+
+
+def bed_particles_per_cell(parts, grid):
+    """Per-cell particle count, masses and mass-weighted T_s of the live
+    particles (the snapshot aggregation of spread_3d.py:3567-3606): x and y
+    cells by truncation, z by the first face above the particle."""
+    shape = grid.shape
+    alive = np.asarray(parts["alive"]) != 0
+    xi = np.trunc(np.asarray(parts["x"]) / grid.dx).astype(np.int64)
+    yj = np.trunc(np.asarray(parts["y"]) / grid.dy).astype(np.int64)
+    zz = np.asarray(parts["z"])
+    zk = np.searchsorted(np.asarray(grid.z_face)[1:], zz, side="right")
+    ok = alive & (xi >= 0) & (xi < grid.Nx) & (yj >= 0) & (yj < grid.Ny) & (zk < grid.Nz)
+    idx = (zk[ok], yj[ok], xi[ok])
+    out = {}
+    cnt = np.zeros(shape); np.add.at(cnt, idx, 1.0)
+    ms, mw, mc = (np.asarray(parts[k])[ok] for k in ("m_solid", "m_water", "m_char"))
+    mt = ms + mw + mc
+    for name, v in (("bp_m_solid", ms), ("bp_m_water", mw), ("bp_m_char", mc)):
+        a = np.zeros(shape); np.add.at(a, idx, v); out[name] = a.astype(np.float32)
+    tw = np.zeros(shape); np.add.at(tw, idx, np.asarray(parts["T_s"])[ok] * mt)
+    mm = np.zeros(shape); np.add.at(mm, idx, mt)
+    out["bp_count"] = cnt.astype(np.float32)
+    out["bp_T_s_avg"] = np.where(mm > 0.0, tw / np.maximum(mm, 1e-30), 0.0).astype(np.float32)
+    return out
+
+
+def write_snapshot(solver: Tier3Solver, path, wind_speed_m_s: float):
+    """One animation snapshot with the reference's key set
+    (spread_3d.py:3613-3669).  Fields this production path does not carry
+    (mixing time, level-set drive fields, tendril inventory) are zeros, as
+    the reference writes for passive level-set runs without tendrils."""
+    s = solver
+    g = s.grid
+    st = s.state()
+    f32 = lambda a: np.asarray(a, dtype=np.float32)  # noqa: E731
+    zeros3 = np.zeros(g.shape, np.float32)
+    zeros2 = np.zeros((g.Ny, g.Nx), np.float32)
+    parts = {k[2:]: v for k, v in st.items() if k.startswith("p_") and k != "p_prev"}
+    phi_flame = phi_flame_from_state(st["omega"], st["T_g"], st["Y_fuel"], g.dx, g.dy, g.dz_arr)
+    arrays = dict(
+        t=np.float64(s.t), step=np.int64(s.step_count),
+        T_g=f32(st["T_g"]), T_s=f32(st["T_s"]), Y_fuel=f32(st["Y_fuel"]), Y_O2=f32(st["Y_O2"]),
+        Y_H2O=f32(st["Y_H2O"]), u=f32(st["u"]), v=f32(st["v"]), w=f32(st["w"]),
+        rho=f32(st["rho"]), omega=f32(st["omega"]),
+        S_pyro=f32(np.asarray(st["S_pyro_b"]) + np.asarray(st["S_dry_b"])),
+        k_turb=f32(st["k_turb"]), eps_turb=f32(st["eps_turb"]), nu_t=f32(st["nu_t"]),
+        tau_mix=zeros3, phi_bed=f32(st["phi"]) if g.n_z_bed > 0 else zeros3,
+        phi_flame=f32(phi_flame), front_x=np.float64(s.front_x[-1] if s.front_x else 0.0),
+        q_dom_fwd_3d=zeros3, q_frankman_3d=zeros3, q_in_at_front_2d=zeros2, v_n_2d=zeros2,
+        ft_sink_M=zeros3, ft_sink_E=zeros3, ft_dep_M=zeros3, ft_dep_E=zeros3,
+        ft_sink_t_rem=zeros3, ft_dep_t_rem=zeros3,
+        x_mid=f32(g.x_mid), z_mid=f32(g.z_mid), dx=np.float64(g.dx), dy=np.float64(g.dy),
+        dz_arr=f32(g.dz_arr), wind_U=np.float64(wind_speed_m_s),
+        closure=np.array(["edc"], dtype=object),
+    )
+    arrays.update(bed_particles_per_cell(parts, g))
+    np.savez_compressed(path, **arrays)
+    return path
 
 
 # ---------------------------------------------------------------- checkpoints
