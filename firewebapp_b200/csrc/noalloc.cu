@@ -1,5 +1,12 @@
 // EDC entry point for callers that cannot allocate device memory.
 //
+// Some hosts of this library may not call cudaMalloc themselves or let a
+// plugin call it: a framework whose own allocator owns all device memory (a
+// fixed arena sized at start-up, or a caching allocator that must see every
+// byte), or a time-step loop that cannot take the device-wide
+// synchronisation a cudaMalloc/cudaFree can cause.  fs_edc needs a scratch
+// buffer from its caller; this variant needs none.
+//
 // fs_edc_noalloc runs the same three EDC kernels as fs_edc, with the flag
 // scan's scratch in a file-scope device array instead of a caller buffer.
 // The array's address is looked up once per device, with that device

@@ -146,8 +146,11 @@ int fs_edc(int64_t n, const double* rho, double* T_g, double* Y_F, double* Y_O2,
            void* stream);
 
 /* No counterpart in the reference: fs_edc for callers that cannot allocate
- * device memory.  Same arguments and results as fs_edc without the scratch
- * buffer; the flag scan uses a static device array sized for at most
+ * device memory, such as a host whose own allocator owns all device memory
+ * (fixed arena, caching allocator) or a loop that cannot afford the
+ * synchronisation of cudaMalloc.  Same arguments and results as fs_edc
+ * without the scratch buffer; the flag scan uses a static device array (about
+ * 256 KiB per GPU that loads the library, held until exit) sized for at most
  * FS_EDC_NOALLOC_MAX_CELLS cells (larger n is rejected with FS_EARG).  The
  * first call on a device looks the array up (make it before any stream
  * capture); all calls share the array, so calls whose kernels overlap on the

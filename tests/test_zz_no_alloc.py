@@ -1,6 +1,8 @@
 """fs_edc_noalloc: the EDC step with its flag-scan scratch in a static device
-array (no allocation by the library).  Its results must equal fs_edc's, also
-on a second call that finds the first call's scratch contents.
+array, for callers that may not allocate device memory (a host whose own
+allocator owns the GPU's memory, or a loop that cannot take cudaMalloc's
+synchronisation).  Its results must equal fs_edc's, also on a second call
+that finds the first call's scratch contents.
 
 Collected last on purpose: it must pass in a fresh process and after the
 other GPU tests.
