@@ -38,6 +38,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "3D solver cell-steps/s on 1 B200 (plain FP64 Tier-3 step)"
 UNIT = "cell-steps/s"
 WORKLOAD = "tier3_step_400x120x60_S8_fp64"
+# measured DRAM bytes per cell of one launch (see the traffic comment in main)
+TRAFFIC_PER_CELL = {"dom_sweep": 18.44e6 / 720000.0}
 
 
 def _peaks():
@@ -227,6 +229,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--form", default="plain", choices=["plain", "mixed"],
+                    help="plain: FP64 throughout; mixed: FP32 DOM sweep and multigrid "
+                         "preconditioner, pressure tolerance 1e-8")
     ap.add_argument("--no-clocks", action="store_true",
                     help="skip the clock sampler (diagnostics only; the line then has no clocks)")
     ap.add_argument("--nx", type=int, default=None,
@@ -253,7 +258,7 @@ def main():
     if args.nx:
         from firewebapp_b200.cases import scaled
         case = dict(scaled(CFG2, nx=args.nx), jitter_seed=rank)
-    solver = Tier3Solver(case, projection_cg_rtol=1.0e-6)
+    solver = Tier3Solver(case, form=args.form)
     cells = solver.n
     for _ in range(args.warmup):
         solver.step()
@@ -299,10 +304,11 @@ def main():
     M = solver.Omega.shape[0]
     dom_mode = lib.fs_dom_sweep_mode(solver.dom)
     alg = {  # algorithmic bytes per launch (distinct fields read + written, 8 B each)
-        # octant-cluster sweep (path 1): reads (kappa, kappa*B) once, writes the
-        # 8 octant partial G fields (wrap rows and ground partials < 1% more);
-        # per-ordinate paths write every intensity
-        "dom_sweep": N * (16.0 + 8.0 * 8) if dom_mode in (1, 4) else N * (8.0 * M + 16.0),
+        # octant-cluster sweeps (paths 1, 4): read (kappa, kappa*B) once and write
+        # the 8 octant partial G fields (FP32 in the mixed form; wrap rows and
+        # ground partials < 1% more); per-ordinate paths write every intensity
+        "dom_sweep": (N * (8.0 + 4.0 * 8) if args.form == "mixed" else
+                      N * (16.0 + 8.0 * 8) if dom_mode in (1, 4) else N * (8.0 * M + 16.0)),
         "species_transport": N * 8.0 * 12,
         "edc": N * 8.0 * 11,
         "turb_diffusion_Y": N * 8.0 * 7,
@@ -314,10 +320,12 @@ def main():
     tot_ms, nl = kt[dom_k]
     avg_ms = tot_ms / max(nl, 1)
     achieved = alg[dom_k] / (avg_ms * 1e-3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get(dom_k)
+    # DRAM bytes per launch of the dominant kernel from an ncu capture of the
+    # 100x120x60 slice of this workload (dram__bytes_read.sum + write.sum),
+    # scaled by the cell count to a full 400x120x60 launch
+    traffic = TRAFFIC_PER_CELL.get(dom_k) if args.form == "plain" else None
+    if traffic is not None:
+        traffic *= N
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "kernel": dom_k,
                 "peak_source": peak_src, "launches": nl, "avg_launch_ms": avg_ms,
@@ -327,7 +335,7 @@ def main():
     # ---- end to end through the public API: host state in, result out
     e2e = None
     if not args.no_e2e:
-        e2e = measure_e2e(case, args.steps, ws)
+        e2e = measure_e2e(case, args.steps, ws, args.form)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -341,12 +349,15 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.form == "plain" else "f64+f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD if not args.nx else
-                       f"tier3_step_{args.nx}x120x60_S8_fp64", "cells": cells, "ordinates": M,
+            "config": {"workload": (WORKLOAD if not args.nx else
+                                    f"tier3_step_{args.nx}x120x60_S8_fp64").replace(
+                                        "fp64", "fp64" if args.form == "plain" else "mixed"),
+                       "form": args.form, "cells": cells, "ordinates": M,
                        "parallelism": f"replicas{ws}", "l2": "inputs larger than L2",
-                       "projection_rtol": 1e-6},
+                       "projection_rtol": solver.rtol},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,
             "gpu_launches": launches,
         }
@@ -356,13 +367,13 @@ def main():
         dist.destroy_process_group()
 
 
-def measure_e2e(case, steps, ws):
+def measure_e2e(case, steps, ws, form="plain"):
     """Cell-steps/s through the public host-buffer API: every step uploads the
     caller's state (fields, particles, soil) from pinned host memory, advances
     one outer step and downloads the state again; max time over ranks."""
     import torch
     from firewebapp_b200.api import run_3d_spread_gpu_e2e
-    res = run_3d_spread_gpu_e2e(case, steps)
+    res = run_3d_spread_gpu_e2e(case, steps, form=form)
     work, sec = job_totals(res["cells"] * steps, res["seconds"], device="cuda")
     return {"value": work / sec, "unit": UNIT,
             "h2d_bytes_per_step": res["h2d_bytes"] / steps,

@@ -82,6 +82,7 @@ SIGNATURES = {
     "fs_proj_pressure": (P, [P]),
     "fs_proj_apply": (I, [P, P, P, P]),
     "fs_proj_configure": (I, [P, I, D]),
+    "fs_proj_set_precision": (I, [P, I]),
     "fs_proj_stats": (I, [P, C.POINTER(D)]),
     "fs_divergence_max": (I, [_G, P, P, P, P, P, P, C.POINTER(D), P]),
     "fs_dom_create": (I, [_G, I, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(D), D,
@@ -92,6 +93,7 @@ SIGNATURES = {
     "fs_dom_iterations": (I, [P]),
     "fs_dom_set_sweep_mode": (I, [P, I, I]),
     "fs_dom_sweep_mode": (I, [P]),
+    "fs_dom_set_precision": (I, [P, I]),
     "fs_dom_load_intensity": (I, [P, P, P]),
     "fs_dom_wrap_size": (I64, [P]),
     "fs_dom_get_wrap": (I, [P, P, P]),

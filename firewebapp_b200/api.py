@@ -160,8 +160,8 @@ class _Diag:
 
 def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | None = None,
                       snapshot_every_s: float = 1.0, device="cuda",
-                      projection_cg_rtol: float = 1.0e-6, snapshot_dir=None,
-                      snapshot_interval_s: float = 1.0) -> Spread3DResultGPU:
+                      projection_cg_rtol: float | None = None, snapshot_dir=None,
+                      snapshot_interval_s: float = 1.0, form: str = "plain") -> Spread3DResultGPU:
     """Device-resident ``run_3d_spread`` for a case; stops at ``n_steps``
     outer steps, at ``t_end`` simulated seconds or at the reference's own
     exit tests, whichever comes first.  With ``snapshot_dir`` it writes
@@ -169,7 +169,7 @@ def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | 
     as the reference does (spread_3d.py:3537-3669)."""
     if n_steps is None and t_end is None:
         raise ValueError("run_3d_spread_gpu needs n_steps or t_end")
-    s = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol)
+    s = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol, form=form)
     # long-lived objects out of the collector's way: full collections during the
     # run then scan only objects made by the run itself
     gc.collect()
@@ -229,8 +229,10 @@ class HostStepper:
     PARTS = ("x", "y", "z", "alive", "m_solid", "m_water", "m_char", "T_s", "m_water_0",
              "sav", "m_char_max")
 
-    def __init__(self, case: dict, device="cuda", projection_cg_rtol: float = 1.0e-6):
-        self.solver = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol)
+    def __init__(self, case: dict, device="cuda", projection_cg_rtol: float | None = None,
+                 form: str = "plain"):
+        self.solver = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol,
+                                  form=form)
         s = self.solver
         self.host = {}
         for k in self.FIELDS:
@@ -269,10 +271,10 @@ class HostStepper:
 
 
 def run_3d_spread_gpu_e2e(case: dict, steps: int, warmup: int = 1,
-                          projection_cg_rtol: float = 1.0e-6):
+                          projection_cg_rtol: float | None = None, form: str = "plain"):
     """Time ``steps`` host-buffer outer steps (uploads and downloads inside
     the timed region), after ``warmup`` untimed ones."""
-    hs = HostStepper(case, projection_cg_rtol=projection_cg_rtol)
+    hs = HostStepper(case, projection_cg_rtol=projection_cg_rtol, form=form)
     gc.collect()
     gc.freeze()
     try:
@@ -402,7 +404,7 @@ def save_checkpoint(solver: Tier3Solver, path) -> Path:
     meta = {"case": s.case, "t": s.t, "dt": s.dt, "step_count": s.step_count,
             "lset_step": s.lset_step, "extinct_count": s.extinct_count,
             "front_t": list(s.front_t), "front_x": list(s.front_x),
-            "rtol": s.rtol, "proj_maxiter": s.proj_maxiter}
+            "rtol": s.rtol, "proj_maxiter": s.proj_maxiter, "form": s.form}
     np.savez(path, _meta_json=np.array(json.dumps(meta)), **arrays)
     return path
 
@@ -412,7 +414,7 @@ def load_checkpoint(path, device="cuda") -> Tier3Solver:
     z = np.load(Path(path), allow_pickle=False)
     meta = json.loads(str(z["_meta_json"]))
     s = Tier3Solver(meta["case"], device=device, projection_cg_rtol=meta["rtol"],
-                    proj_maxiter=meta["proj_maxiter"])
+                    proj_maxiter=meta["proj_maxiter"], form=meta.get("form", "plain"))
     for k in Tier3Solver.FIELDS:
         s.f[k].copy_(torch.as_tensor(z["f_" + k]))
     for k in _CKPT_WORK:

@@ -366,6 +366,11 @@ int fs_proj_stats(void* handle, double* out8) {
   return FS_OK;
 }
 
+int fs_proj_set_precision(void* handle, int fp32) {
+  if (!handle) return FS_EARG;
+  return check(proj_set_precision(handle, fp32), "fs_proj_set_precision");
+}
+
 int fs_proj_configure(void* handle, int nu, double omega) {
   if (!handle) return FS_EARG;
   return check(proj_configure(handle, nu, omega), "fs_proj_configure");
@@ -425,6 +430,11 @@ int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas) {
 }
 
 int fs_dom_sweep_mode(void* handle) { return handle ? dom_mode(handle) : -1; }
+
+int fs_dom_set_precision(void* handle, int fp32) {
+  if (!handle) return FS_EARG;
+  return check(dom_set_precision(handle, fp32), "fs_dom_set_precision");
+}
 
 int64_t fs_dom_wrap_size(void* handle) { return handle ? dom_wrap_size(handle) : -1; }
 

@@ -51,6 +51,9 @@ struct DomCtx {
   int mode;                   // resolved path: 0 not yet, 1 clusters, 2 block/ordinate, 3 planes
   int mode_req, force_C;      // requested path (0 auto) and cluster size (0 auto)
   int groups;                 // ordinate groups per octant (clusters per octant), paths 4/6
+  int fp32;                   // single-precision sweep (path 4 only)
+  float2* kb32;
+  float *Goct32, *Qoct32, *wrap32;
   int Mo, cl_C, cl_rows, cl_threads;
   size_t cl_smem;
   int down_slot[8];
@@ -104,7 +107,7 @@ __global__ void k_dom_setup(GridDev g, const double* __restrict__ Ts, const doub
                             const double* __restrict__ YH, const double* __restrict__ rho,
                             const double* __restrict__ Mloc, double sigma, double Tamb4,
                             double kgmax, double* ks, double* kg, double* ksafe, double* B,
-                            double2* kb) {
+                            double2* kb, float2* kb32) {
   int64_t n = ncells_dev(g);
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -129,6 +132,7 @@ __global__ void k_dom_setup(GridDev g, const double* __restrict__ Ts, const doub
   ksafe[c] = ksf;
   B[c] = Bc;
   if (kb) kb[c] = make_double2(ksf, ksf * Bc);
+  if (kb32) kb32[c] = make_float2((float)ksf, (float)(ksf * Bc));
 }
 
 __global__ void k_dom_ground_init(int n2, const double* __restrict__ Tsoil, double eps_w,
@@ -587,6 +591,208 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, MINB) k_dom_octant(GridDev g,
   cluster_wait_acquire();
 }
 
+// ---- single-precision form of path 4 (the mixed-precision solver) -----------
+// Same sweep, with kappa, kappa*B, the hyperplane buffers, the inflow rows and
+// the octant partials in FP32; the octant partials are summed into G in FP64.
+struct OctArgs32 {
+  const float2* kb;
+  const double *ox, *oy, *oz, *w;
+  const double* Ig;
+  float *Goct, *Qoct, *wrap;
+  float I_amb;
+  int C, rows, periodic;
+  unsigned down_slots;
+};
+
+__device__ __forceinline__ float2 ld_hint_f2(const float2* p, uint64_t pol) {
+  float2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+               : "=f"(v.x), "=f"(v.y)
+               : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_stream_f(float* p, float v) {
+  asm volatile("st.global.cs.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
+template <int MO>
+__global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_f32(GridDev g, OctArgs32 a) {
+  extern __shared__ float shf[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int rank = (int)cl.block_rank();
+  const int oct = blockIdx.x / a.C;
+  const int n0 = oct * MO;
+  const int S = a.rows * ny;
+  float* buf0 = shf;
+  float* buf1 = shf + (size_t)MO * S;
+  float* izt = buf1 + (size_t)MO * S;
+  float* cix = izt + (size_t)MO * nz;
+  float* ciy = cix + MO;
+  float* cw = ciy + MO;
+  float* cwm = cw + MO;
+  for (int t = threadIdx.x; t < MO * nz; t += blockDim.x) {
+    const int m = t / nz, k = t - m * nz;
+    izt[t] = (float)(fabs(a.oz[n0 + m]) / g.dz[k]);
+  }
+  for (int m = threadIdx.x; m < MO; m += blockDim.x) {
+    cix[m] = (float)(fabs(a.ox[n0 + m]) / g.dx);
+    ciy[m] = (float)(fabs(a.oy[n0 + m]) / g.dy);
+    cw[m] = (float)a.w[n0 + m];
+    cwm[m] = (float)(a.w[n0 + m] * fabs(a.oz[n0 + m]));
+  }
+  const bool fx = a.ox[n0] >= 0.0, fy = a.oy[n0] >= 0.0, fz = a.oz[n0] >= 0.0;
+  const int r0 = rank * a.rows;
+  const int nrows = min(a.rows, nz - r0);
+  const int npen = nrows > 0 ? nrows * ny : 0;
+  const int q = threadIdx.x;
+  const bool has = q < npen;
+  const int kl = has ? q / ny : 0;
+  const int jp = has ? q - kl * ny : 0;
+  const int kp = r0 + kl;
+  const int j = fy ? jp : ny - 1 - jp;
+  const int k = fz ? kp : nz - 1 - kp;
+  const int64_t N = ncells_dev(g);
+  const int64_t n2 = (int64_t)nx * ny;
+  const int slot_bits = (int)((a.down_slots >> (4 * oct)) & 15u);
+  const int slot = slot_bits == 15 ? -1 : slot_bits;
+  float* Go = a.Goct + (int64_t)oct * N;
+  const int64_t wstride = (int64_t)nz * nx;
+  float* wrap0 = a.wrap + (int64_t)n0 * wstride;
+  const bool ground_out = has && !fz && k == 0 && slot >= 0;
+  const bool z_in_ground = has && fz && kp == 0;
+  const bool z_remote = has && kl == 0 && kp > 0;
+  const bool y_wrap = has && jp == 0 && a.periodic;
+  const bool y_wrap_out = has && jp == ny - 1 && a.periodic;
+  const float* nbase = nullptr;
+  const int nplanes = nx + ny + nz - 2;
+  const uint64_t keep = l2_policy_evict_last();
+  float2 kab = make_float2(0.f, 0.f);
+  float win[MO];
+  float Igc = 0.f;
+  auto prefetch = [&](int d) {
+    const int ip = d - jp - kp;
+    if (!has || ip < 0 || ip >= nx) return;
+    const int i = fx ? ip : nx - 1 - ip;
+    kab = ld_hint_f2(a.kb + ((int64_t)k * ny + j) * nx + i, keep);
+    if (y_wrap) {
+#pragma unroll
+      for (int m = 0; m < MO; ++m) win[m] = wrap0[m * wstride + (int64_t)k * nx + i];
+    }
+    if (z_in_ground) Igc = (float)a.Ig[(int64_t)j * nx + i];
+  };
+#pragma unroll
+  for (int m = 0; m < MO; ++m) win[m] = a.I_amb;
+  __syncthreads();
+  prefetch(0);
+  for (int d = 0; d < nplanes; ++d) {
+    float* cur = (d & 1) ? buf1 : buf0;
+    const float* prev = (d & 1) ? buf0 : buf1;
+    if (d > 0) cluster_wait_acquire();
+    const int ip = d - jp - kp;
+    const bool act = has && ip >= 0 && ip < nx;
+    float v[MO];
+    float gs = 0.f, qs = 0.f;
+    if (act) {
+      if (z_remote) nbase = cl.map_shared_rank(const_cast<float*>(prev), rank - 1) +
+                            (size_t)(a.rows - 1) * ny + jp;
+      float zr[MO];
+      if (z_remote) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) zr[m] = nbase[(size_t)m * S];
+      }
+#pragma unroll
+      for (int m = 0; m < MO; ++m) {
+        const float* pm = prev + (size_t)m * S;
+        const float Ix = ip > 0 ? pm[q] : a.I_amb;
+        const float Iy = jp > 0 ? pm[q - 1] : (a.periodic ? win[m] : a.I_amb);
+        float Iz;
+        if (kl > 0) Iz = pm[q - ny];
+        else if (kp > 0) Iz = zr[m];
+        else Iz = fz ? Igc : a.I_amb;
+        const float ix = cix[m], iy = ciy[m], iz = izt[m * nz + k];
+        const float num = kab.y + ix * Ix + iy * Iy + iz * Iz;
+        const float den = kab.x + ix + iy + iz;
+        v[m] = num / den;
+        cur[(size_t)m * S + q] = v[m];
+        gs = gs + cw[m] * v[m];
+        if (ground_out) qs = qs + cwm[m] * v[m];
+      }
+    }
+    cluster_arrive_release();
+    if (act) {
+      const int i = fx ? ip : nx - 1 - ip;
+      st_stream_f(Go + ((int64_t)k * ny + j) * nx + i, gs);
+      if (y_wrap_out) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) wrap0[m * wstride + (int64_t)k * nx + i] = v[m];
+      }
+      if (ground_out) a.Qoct[(int64_t)slot * n2 + (int64_t)j * nx + i] = qs;
+    }
+    if (d + 1 < nplanes) prefetch(d + 1);
+  }
+  cluster_wait_acquire();
+}
+
+static const void* octant_f32_ptr(int Mo) {
+  switch (Mo) {
+    case 3: return (const void*)k_dom_octant_f32<3>;
+    case 6: return (const void*)k_dom_octant_f32<6>;
+    case 10: return (const void*)k_dom_octant_f32<10>;
+    default: return nullptr;
+  }
+}
+
+// G (FP64) from FP32 octant partials; max G and max |G - G_prev|
+__global__ void k_dom_G_oct32(int64_t N, const float* __restrict__ Goct, double* G,
+                              const double* __restrict__ Gp, unsigned long long* keys) {
+  unsigned long long bg = 0, bd = 0;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < N;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int o = 0; o < 8; ++o) s += (double)Goct[(int64_t)o * N + c];
+    G[c] = s;
+    double d = fabs(s - Gp[c]);
+    unsigned long long ks = (s != s) ? 0x7ff8000000000000ull
+                                     : (unsigned long long)__double_as_longlong(s > 0.0 ? s : 0.0);
+    unsigned long long kd = (d != d) ? 0x7ff8000000000000ull
+                                     : (unsigned long long)__double_as_longlong(d);
+    bg = ks > bg ? ks : bg;
+    bd = kd > bd ? kd : bd;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long y = __shfl_xor_sync(0xffffffffu, bg, o);
+    bg = y > bg ? y : bg;
+    y = __shfl_xor_sync(0xffffffffu, bd, o);
+    bd = y > bd ? y : bd;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(keys, bg);
+    atomicMax(keys + 1, bd);
+  }
+}
+
+__global__ void k_dom_ground_oct32(int n2, int nslots, const float* __restrict__ Qoct,
+                                   const double* __restrict__ Isoil, double refl, double relax,
+                                   double* Ig, double* qin) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n2) return;
+  double s = 0.0;
+  for (int o = 0; o < nslots; ++o) s += (double)Qoct[(int64_t)o * n2 + q];
+  qin[q] = s;
+  double Inew = Isoil[q] + refl * s;
+  Ig[q] = relax * Inew + (1.0 - relax) * Ig[q];
+}
+
+__global__ void k_f32_to_f64(int64_t n, const float* __restrict__ a, double* b) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < n) b[t] = (double)a[t];
+}
+__global__ void k_f64_to_f32(int64_t n, const double* __restrict__ a, float* b) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < n) b[t] = (float)a[t];
+}
+
 // ---- pipelined variant: point-to-point hand-off between neighbouring CTAs ----
 // CTA r needs, on hyperplane d, the last row of CTA r-1 from hyperplane d-1.
 // Instead of a cluster-wide barrier per hyperplane, CTA r-1's last-row
@@ -911,8 +1117,9 @@ __global__ void k_dom_scatter_wrap(GridDev g, int M, const double* __restrict__ 
   I[(int64_t)n * ncells_dev(g) + cidx(g, k, jf, i)] = wrap[t];
 }
 
+template <typename T>
 __global__ void k_dom_extract_wrap(GridDev g, int M, const double* __restrict__ oy,
-                                   const double* __restrict__ I, double* wrap) {
+                                   const double* __restrict__ I, T* wrap) {
   const int64_t tot = (int64_t)M * g.nz * g.nx;
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= tot) return;
@@ -921,7 +1128,7 @@ __global__ void k_dom_extract_wrap(GridDev g, int M, const double* __restrict__ 
   const int k = (int)(r / g.nx);
   const int i = (int)(r - (int64_t)k * g.nx);
   const int jf = oy[n] >= 0.0 ? g.ny - 1 : 0;
-  wrap[t] = I[(int64_t)n * ncells_dev(g) + cidx(g, k, jf, i)];
+  wrap[t] = (T)I[(int64_t)n * ncells_dev(g) + cidx(g, k, jf, i)];
 }
 
 __global__ void k_dom_finish(GridDev g, const double* __restrict__ ks, const double* __restrict__ kg,
@@ -961,6 +1168,7 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   cudaMemcpy(D->w, w, sizeof(double) * M, cudaMemcpyHostToDevice);
   D->I = nullptr; D->wrap = nullptr; D->kb = nullptr; D->Goct = nullptr; D->Qoct = nullptr;
   D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1;
+  D->fp32 = 0; D->kb32 = nullptr; D->Goct32 = nullptr; D->Qoct32 = nullptr; D->wrap32 = nullptr;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemset(D->G, 0, sizeof(double) * N);
   cudaMalloc(&D->ks, sizeof(double) * N); cudaMalloc(&D->kg, sizeof(double) * N);
@@ -988,6 +1196,7 @@ void dom_destroy(void* h) {
   if (!D) return;
   cudaFree(D->ox); cudaFree(D->oy); cudaFree(D->oz); cudaFree(D->w); cudaFree(D->I);
   cudaFree(D->wrap); cudaFree(D->kb); cudaFree(D->Goct); cudaFree(D->Qoct);
+  cudaFree(D->kb32); cudaFree(D->Goct32); cudaFree(D->Qoct32); cudaFree(D->wrap32);
   cudaFree(D->G); cudaFree(D->Gp); cudaFree(D->ks); cudaFree(D->kg); cudaFree(D->ksafe);
   cudaFree(D->B); cudaFree(D->Ig_out); cudaFree(D->Isoil); cudaFree(D->qin); cudaFree(D->keys);
   cudaFreeHost(D->h_keys);
@@ -1024,7 +1233,7 @@ static bool plan_clusters(DomCtx* D, int force_C, bool pipe, int groups = 1) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-  const void* fn = octant_kernel_ptr(Mo * groups, pipe, groups);
+  const void* fn = D->fp32 ? octant_f32_ptr(Mo) : octant_kernel_ptr(Mo * groups, pipe, groups);
   if (!fn) return false;
   cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
@@ -1037,7 +1246,8 @@ static bool plan_clusters(DomCtx* D, int force_C, bool pipe, int groups = 1) {
     int threads = ((rows * g.ny + 31) / 32) * 32;
     if (threads > OCT_MAX_THREADS) continue;
     const size_t need = pipe ? oct_pipe_smem_bytes(Mo, rows, g.ny, g.nz)
-                             : oct_smem_bytes(Mo, rows, g.ny, g.nz);
+                             : (D->fp32 ? oct_smem_bytes(Mo, rows, g.ny, g.nz) / 2
+                                        : oct_smem_bytes(Mo, rows, g.ny, g.nz));
     if (need > (size_t)optin) continue;
     // ask for more than half an SM's shared memory so that no two CTAs share an SM,
     // unless that leaves fewer than 8 clusters resident
@@ -1075,6 +1285,23 @@ static int dom_prepare(DomCtx* D) {
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
   const int want = D->mode_req;
+  if (D->fp32) {
+    if ((want != 0 && want != 4) || !octant_grouping(D) || !plan_clusters(D, D->force_C, false)) {
+      fs_set_error("single-precision sweep needs the octant-cluster path (4) on this grid");
+      return FS_EARG;
+    }
+    D->mode = 4;
+    D->groups = 1;
+    D->Mo = D->M / 8;
+    int slot = 0;
+    for (int o = 0; o < 8; ++o) D->down_slot[o] = D->hoz[o * D->Mo] < 0.0 ? slot++ : -1;
+    cudaMalloc(&D->kb32, sizeof(float2) * N);
+    cudaMalloc(&D->Goct32, sizeof(float) * 8 * N);
+    cudaMalloc(&D->Qoct32, sizeof(float) * 8 * n2);
+    cudaMalloc(&D->wrap32, sizeof(float) * D->M * g.nz * g.nx);
+    cudaMemset(D->wrap32, 0, sizeof(float) * D->M * g.nz * g.nx);
+    return cuda_status();
+  }
   // auto picks the cluster-barrier sweep (path 4), measured faster than path 1
   const int groups = (want == 6 && D->M % 16 == 0) ? 2 : 1;
   if ((want == 0 || want == 1 || want == 4 || want == 6) && octant_grouping(D) &&
@@ -1130,14 +1357,30 @@ int dom_set_mode(void* h, int mode, int cluster_ctas) {
 
 int dom_mode(void* h) { return ((DomCtx*)h)->mode; }
 
+int dom_set_precision(void* h, int fp32) {
+  DomCtx* D = (DomCtx*)h;
+  if (D->mode != 0) {
+    fs_set_error("precision must be set before the first solve or intensity load");
+    return FS_EARG;
+  }
+  D->fp32 = fp32 ? 1 : 0;
+  return FS_OK;
+}
+
 int dom_load_intensity(void* h, const double* I_full, cudaStream_t st) {
   DomCtx* D = (DomCtx*)h;
   int rc = dom_prepare(D);
   if (rc != FS_OK) return rc;
   const GridDev& g = D->g;
-  if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
+  if (D->fp32) {
     const int64_t tot = (int64_t)D->M * g.nz * g.nx;
-    k_dom_extract_wrap<<<blocks_for(tot, 256), 256, 0, st>>>(g, D->M, D->oy, I_full, D->wrap);
+    k_dom_extract_wrap<float><<<blocks_for(tot, 256), 256, 0, st>>>(g, D->M, D->oy, I_full,
+                                                                   D->wrap32);
+    fs_count_launch();
+  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
+    const int64_t tot = (int64_t)D->M * g.nz * g.nx;
+    k_dom_extract_wrap<double><<<blocks_for(tot, 256), 256, 0, st>>>(g, D->M, D->oy, I_full,
+                                                                    D->wrap);
     fs_count_launch();
   } else {
     cudaMemcpyAsync(D->I, I_full, sizeof(double) * ncells(g) * D->M, cudaMemcpyDeviceToDevice,
@@ -1158,10 +1401,14 @@ int dom_get_wrap(void* h, double* dst, cudaStream_t st) {
   int rc = dom_prepare(D);
   if (rc != FS_OK) return rc;
   const int64_t tot = dom_wrap_size(h);
-  if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
+  if (D->fp32) {
+    k_f32_to_f64<<<blocks_for(tot, 256), 256, 0, st>>>(tot, D->wrap32, dst);
+    fs_count_launch();
+  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
     cudaMemcpyAsync(dst, D->wrap, sizeof(double) * tot, cudaMemcpyDeviceToDevice, st);
   } else {
-    k_dom_extract_wrap<<<blocks_for(tot, 256), 256, 0, st>>>(D->g, D->M, D->oy, D->I, dst);
+    k_dom_extract_wrap<double><<<blocks_for(tot, 256), 256, 0, st>>>(D->g, D->M, D->oy, D->I,
+                                                                    dst);
     fs_count_launch();
   }
   return cuda_status();
@@ -1172,7 +1419,10 @@ int dom_set_wrap(void* h, const double* src, cudaStream_t st) {
   int rc = dom_prepare(D);
   if (rc != FS_OK) return rc;
   const int64_t tot = dom_wrap_size(h);
-  if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
+  if (D->fp32) {
+    k_f64_to_f32<<<blocks_for(tot, 256), 256, 0, st>>>(tot, src, D->wrap32);
+    fs_count_launch();
+  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
     cudaMemcpyAsync(D->wrap, src, sizeof(double) * tot, cudaMemcpyDeviceToDevice, st);
   } else {
     k_dom_scatter_wrap<<<blocks_for(tot, 256), 256, 0, st>>>(D->g, D->M, D->oy, src, D->I);
@@ -1279,7 +1529,8 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   const double Tamb4 = pow(T_amb, 4.0);
   k_dom_setup<<<blocks_for(N, 256), 256, 0, st>>>(g, Ts, Tg, as, om, YH, rho, Mloc, sigma, Tamb4,
                                                   D->kgmax, D->ks, D->kg, D->ksafe, D->B,
-                                                  (octp || D->mode == 5) ? D->kb : nullptr);
+                                                  (!D->fp32 && (octp || D->mode == 5)) ? D->kb : nullptr,
+                                                  D->fp32 ? D->kb32 : nullptr);
   fs_count_launch();
   const double I_amb = SIGMA_SB_D * Tamb4 / PI_D;
   k_dom_ground_init<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, Tsoil0, D->eps_w, I_amb, D->Isoil,
@@ -1314,7 +1565,28 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   for (it = 0; it < D->max_iter; ++it) {
     std::swap(D->G, D->Gp);
     if (D->timing) cudaEventRecord(D->ev0[it], st);
-    if (octp) {
+    if (D->fp32) {
+      OctArgs32 o3{};
+      o3.kb = D->kb32; o3.ox = D->ox; o3.oy = D->oy; o3.oz = D->oz; o3.w = D->w;
+      o3.Ig = D->Ig_out; o3.Goct = D->Goct32; o3.Qoct = D->Qoct32; o3.wrap = D->wrap32;
+      o3.I_amb = (float)I_amb; o3.C = D->cl_C; o3.rows = D->cl_rows; o3.periodic = 1;
+      o3.down_slots = oa.down_slots;
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = D->cl_C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(8 * D->cl_C); cfg.blockDim = dim3(D->cl_threads);
+      cfg.dynamicSmemBytes = D->cl_smem; cfg.stream = st; cfg.attrs = at; cfg.numAttrs = 1;
+      cudaError_t e;
+      switch (D->Mo) {
+        case 3: e = cudaLaunchKernelEx(&cfg, k_dom_octant_f32<3>, g, o3); break;
+        case 6: e = cudaLaunchKernelEx(&cfg, k_dom_octant_f32<6>, g, o3); break;
+        case 10: e = cudaLaunchKernelEx(&cfg, k_dom_octant_f32<10>, g, o3); break;
+        default: e = cudaErrorInvalidValue;
+      }
+      fs_count_launch();
+      if (e != cudaSuccess) return FS_ECUDA;
+    } else if (octp) {
       rc = launch_octant_sweep(D, oa, st);
       if (rc != FS_OK) return rc;
     } else if (D->mode == 5) {
@@ -1334,7 +1606,14 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
     cudaMemsetAsync(D->keys, 0, sizeof(unsigned long long) * 2, st);  // keys[2] keeps the wait flag
     unsigned nb = blocks_for(N, 256);
     if (nb > 1184) nb = 1184;
-    if (octp) {
+    if (D->fp32) {
+      k_dom_G_oct32<<<nb, 256, 0, st>>>(N, D->Goct32, D->G, D->Gp, D->keys);
+      fs_count_launch();
+      k_dom_ground_oct32<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, nslots, D->Qoct32,
+                                                              D->Isoil, refl, D->relax,
+                                                              D->Ig_out, D->qin);
+      fs_count_launch();
+    } else if (octp) {
       k_dom_G_oct<<<nb, 256, 0, st>>>(N, 8 * D->groups, D->Goct, D->G, D->Gp, D->keys);
       fs_count_launch();
       k_dom_ground_oct<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, nslots, D->Qoct, D->Isoil,

@@ -89,6 +89,7 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
                  cudaStream_t st);
 int proj_apply(void* h, const double* x, double* y, cudaStream_t st);
 int proj_configure(void* h, int nu, double omega);
+int proj_set_precision(void* h, int fp32);
 void proj_stats(void* h, double* out8);
 int launch_div_resid_max(const GridDev& g, const double* u, const double* v, const double* w,
                          const double* u_in, const double* target, double* div_out,
@@ -100,6 +101,7 @@ void dom_destroy(void* h);
 double* dom_intensity(void* h);
 int dom_set_mode(void* h, int mode, int cluster_ctas);
 int dom_mode(void* h);
+int dom_set_precision(void* h, int fp32);
 int dom_load_intensity(void* h, const double* I_full, cudaStream_t st);
 int64_t dom_wrap_size(void* h);
 int dom_get_wrap(void* h, double* dst, cudaStream_t st);

@@ -143,7 +143,10 @@ __global__ void k_edc_main(int64_t n, EdcArgs a) {
   if (e_t < 1.0e-6) e_t = 1.0e-6;
   double ratio = 1.5e-5 * e_t / (k_t * k_t);
   if (ratio < 1e-30) ratio = 1e-30;
-  double gx = 2.1377 * pow(ratio, 0.25);
+  // ratio**0.25 as two square roots: each is correctly rounded, so the
+  // fourth root is within about one ulp of the correctly rounded power, the
+  // accuracy of a libm pow, at a fraction of pow's cost
+  double gx = 2.1377 * sqrt(sqrt(ratio));
   double gamma_star = gx * (gx * gx);
   if (gamma_star > 1.0) gamma_star = 1.0;
   double tau_star = 0.4083 * sqrt(1.5e-5 / e_t);

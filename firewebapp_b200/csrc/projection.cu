@@ -40,12 +40,14 @@
 #define PCG_SKIP(done) \
   if ((done) && *(done) != 0.0) return;
 
-struct MGLevel {
+template <typename T>
+struct MGLevelT {
   int nx, ny, nz;
   int64_t n;
-  double *gx, *gy, *gz, *e, *dinv;  // conductances, per-cell term, 1/diag
-  double *x, *b, *t, *s;            // correction, rhs, temps
+  T *gx, *gy, *gz, *e, *dinv;  // conductances, per-cell term, 1/diag
+  T *x, *b, *t, *s;            // correction, rhs, temps
 };
+using MGLevel = MGLevelT<double>;
 
 struct ProjCtx {
   GridDev g;
@@ -70,6 +72,12 @@ struct ProjCtx {
   int graph_failed;
   int nu;             // Jacobi sweeps before and after the coarse correction
   double omega;       // Jacobi damping
+  // mixed-precision form: the V-cycle in FP32 (levels, coarse inverse, the
+  // residual it smooths and the correction it returns); CG stays FP64
+  int fp32;
+  MGLevelT<float> lev32[16];
+  float* Ainv32;
+  float *r32, *z32;
   // host-side statistics of the last solve (ms): total, fetch waits (sum, max),
   // graph-launch calls (sum, max), fetches, iteration launches, iterations
   double stats[8];
@@ -120,9 +128,10 @@ __global__ void k_proj_level0(GridDev g, const double* __restrict__ rho, double*
 }
 
 // diagonal of a face-conductance operator -> 1/diag
-__global__ void k_mg_diag(int nx, int ny, int nz, const double* __restrict__ gx,
-                          const double* __restrict__ gy, const double* __restrict__ gz,
-                          const double* __restrict__ e, double* dinv) {
+template <typename T>
+__global__ void k_mg_diag(int nx, int ny, int nz, const T* __restrict__ gx,
+                          const T* __restrict__ gy, const T* __restrict__ gz,
+                          const T* __restrict__ e, T* dinv) {
   int64_t n = (int64_t)nx * ny * nz;
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -130,26 +139,27 @@ __global__ void k_mg_diag(int nx, int ny, int nz, const double* __restrict__ gx,
   int j = (int)((c / nx) % ny);
   int k = (int)(c / ((int64_t)nx * ny));
   int64_t sy = nx, sz = (int64_t)nx * ny;
-  double d = e[c] + gx[c] + gy[c] + gz[c];
+  T d = e[c] + gx[c] + gy[c] + gz[c];
   if (i > 0) d += gx[c - 1];
   if (ny > 1) {
     int jm = j > 0 ? j - 1 : ny - 1;
     d += gy[c - (int64_t)j * sy + (int64_t)jm * sy];
   }
   if (k > 0) d += gz[c - sz];
-  dinv[c] = 1.0 / d;
+  dinv[c] = T(1) / d;
 }
 
 // (S x)_c for a face-conductance operator
-__device__ __forceinline__ double mg_apply(int nx, int ny, int nz, const double* __restrict__ gx,
-                                           const double* __restrict__ gy,
-                                           const double* __restrict__ gz,
-                                           const double* __restrict__ e,
-                                           const double* __restrict__ x, int64_t c, int i, int j,
+template <typename T>
+__device__ __forceinline__ T mg_apply(int nx, int ny, int nz, const T* __restrict__ gx,
+                                           const T* __restrict__ gy,
+                                           const T* __restrict__ gz,
+                                           const T* __restrict__ e,
+                                           const T* __restrict__ x, int64_t c, int i, int j,
                                            int k) {
   const int64_t sy = nx, sz = (int64_t)nx * ny;
-  const double xc = x[c];
-  double y = e[c] * xc;
+  const T xc = x[c];
+  T y = e[c] * xc;
   if (i < nx - 1) y += gx[c] * (xc - x[c + 1]);
   if (i > 0) y += gx[c - 1] * (xc - x[c - 1]);
   if (ny > 1) {
@@ -166,10 +176,11 @@ __device__ __forceinline__ double mg_apply(int nx, int ny, int nz, const double*
 }
 
 // Galerkin aggregation of level f into level c (coarse = scale * P^T S_f P)
-__global__ void k_mg_coarsen(int fx, int fy, int fz, const double* __restrict__ gxf,
-                             const double* __restrict__ gyf, const double* __restrict__ gzf,
-                             const double* __restrict__ ef, int cx, int cy, int cz, double* gxc,
-                             double* gyc, double* gzc, double* ec, double scale) {
+template <typename T>
+__global__ void k_mg_coarsen(int fx, int fy, int fz, const T* __restrict__ gxf,
+                             const T* __restrict__ gyf, const T* __restrict__ gzf,
+                             const T* __restrict__ ef, int cx, int cy, int cz, T* gxc,
+                             T* gyc, T* gzc, T* ec, double scale_) {
   int64_t n = (int64_t)cx * cy * cz;
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= n) return;
@@ -180,7 +191,7 @@ __global__ void k_mg_coarsen(int fx, int fy, int fz, const double* __restrict__ 
   int i0 = 2 * I, i1 = min(2 * I + 1, fx - 1);
   int j0 = 2 * J, j1 = min(2 * J + 1, fy - 1);
   int k0 = 2 * K, k1 = min(2 * K + 1, fz - 1);
-  double se = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+  T se = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
   for (int k = k0; k <= k1; ++k)
     for (int j = j0; j <= j1; ++j)
       for (int i = i0; i <= i1; ++i) se += ef[(int64_t)k * fsz + (int64_t)j * fsy + i];
@@ -196,6 +207,7 @@ __global__ void k_mg_coarsen(int fx, int fy, int fz, const double* __restrict__ 
     for (int j = j0; j <= j1; ++j)
       for (int i = i0; i <= i1; ++i) sz += gzf[(int64_t)k1 * fsz + (int64_t)j * fsy + i];
   }
+  const T scale = (T)scale_;
   gxc[q] = scale * sx;
   gyc[q] = scale * sy;
   gzc[q] = scale * sz;
@@ -203,10 +215,11 @@ __global__ void k_mg_coarsen(int fx, int fy, int fz, const double* __restrict__ 
 }
 
 // Dense inverse of the coarsest operator (Gauss-Jordan in shared memory, n <= 64).
-__global__ void k_mg_coarse_inverse(int nx, int ny, int nz, const double* __restrict__ gx,
-                                    const double* __restrict__ gy, const double* __restrict__ gz,
-                                    const double* __restrict__ e, double* Ainv) {
-  __shared__ double M[MG_COARSE_MAX][2 * MG_COARSE_MAX + 1];
+template <typename T>
+__global__ void k_mg_coarse_inverse(int nx, int ny, int nz, const T* __restrict__ gx,
+                                    const T* __restrict__ gy, const T* __restrict__ gz,
+                                    const T* __restrict__ e, T* Ainv) {
+  __shared__ T M[MG_COARSE_MAX][2 * MG_COARSE_MAX + 1];
   const int n = nx * ny * nz;
   const int t = threadIdx.x;
   for (int r = t; r < n; r += blockDim.x) {
@@ -233,13 +246,13 @@ __global__ void k_mg_coarse_inverse(int nx, int ny, int nz, const double* __rest
   }
   __syncthreads();
   for (int piv = 0; piv < n; ++piv) {
-    double d = M[piv][piv];
+    T d = M[piv][piv];
     __syncthreads();
     for (int q = t; q < 2 * n; q += blockDim.x) M[piv][q] /= d;
     __syncthreads();
     for (int r = t; r < n; r += blockDim.x) {
       if (r == piv) continue;
-      double f = M[r][piv];
+      T f = M[r][piv];
       if (f != 0.0)
         for (int q = 0; q < 2 * n; ++q) M[r][q] -= f * M[piv][q];
     }
@@ -249,23 +262,26 @@ __global__ void k_mg_coarse_inverse(int nx, int ny, int nz, const double* __rest
     for (int q = 0; q < n; ++q) Ainv[r * n + q] = M[r][n + q];
 }
 
-__global__ void k_mg_coarse_solve(int n, const double* __restrict__ Ainv,
-                                  const double* __restrict__ b, double* x, const double* done) {
+template <typename T>
+__global__ void k_mg_coarse_solve(int n, const T* __restrict__ Ainv,
+                                  const T* __restrict__ b, T* x, const double* done) {
   PCG_SKIP(done);
   int r = threadIdx.x;
   if (r >= n) return;
-  double s = 0.0;
+  T s = 0.0;
   for (int q = 0; q < n; ++q) s += Ainv[r * n + q] * b[q];
   x[r] = s;
 }
 
 // damped Jacobi sweep: xo = x + w (b - S x) / d ; x == null means x = 0
-__global__ void k_mg_jacobi(int nx, int ny, int nz, const double* __restrict__ gx,
-                            const double* __restrict__ gy, const double* __restrict__ gz,
-                            const double* __restrict__ e, const double* __restrict__ dinv,
-                            const double* __restrict__ b, const double* __restrict__ x, double* xo,
-                            double w, const double* done) {
+template <typename T>
+__global__ void k_mg_jacobi(int nx, int ny, int nz, const T* __restrict__ gx,
+                            const T* __restrict__ gy, const T* __restrict__ gz,
+                            const T* __restrict__ e, const T* __restrict__ dinv,
+                            const T* __restrict__ b, const T* __restrict__ x, T* xo,
+                            double w_, const double* done) {
   PCG_SKIP(done);
+  const T w = (T)w_;
   int64_t n = (int64_t)nx * ny * nz;
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -276,17 +292,18 @@ __global__ void k_mg_jacobi(int nx, int ny, int nz, const double* __restrict__ g
   int i = (int)(c % nx);
   int j = (int)((c / nx) % ny);
   int k = (int)(c / ((int64_t)nx * ny));
-  double r = b[c] - mg_apply(nx, ny, nz, gx, gy, gz, e, x, c, i, j, k);
+  T r = b[c] - mg_apply(nx, ny, nz, gx, gy, gz, e, x, c, i, j, k);
   xo[c] = x[c] + w * r * dinv[c];
 }
 
 // coarse rhs = sum over children of the fine residual (b - S x)
-__global__ void k_mg_restrict_residual(int fx, int fy, int fz, const double* __restrict__ gx,
-                                       const double* __restrict__ gy,
-                                       const double* __restrict__ gz,
-                                       const double* __restrict__ e, const double* __restrict__ b,
-                                       const double* __restrict__ x, int cx, int cy, int cz,
-                                       double* bc, const double* done) {
+template <typename T>
+__global__ void k_mg_restrict_residual(int fx, int fy, int fz, const T* __restrict__ gx,
+                                       const T* __restrict__ gy,
+                                       const T* __restrict__ gz,
+                                       const T* __restrict__ e, const T* __restrict__ b,
+                                       const T* __restrict__ x, int cx, int cy, int cz,
+                                       T* bc, const double* done) {
   PCG_SKIP(done);
   int64_t n = (int64_t)cx * cy * cz;
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -295,7 +312,7 @@ __global__ void k_mg_restrict_residual(int fx, int fy, int fz, const double* __r
   int J = (int)((q / cx) % cy);
   int K = (int)(q / ((int64_t)cx * cy));
   const int64_t fsy = fx, fsz = (int64_t)fx * fy;
-  double s = 0.0;
+  T s = 0.0;
   for (int k = 2 * K; k <= min(2 * K + 1, fz - 1); ++k)
     for (int j = 2 * J; j <= min(2 * J + 1, fy - 1); ++j)
       for (int i = 2 * I; i <= min(2 * I + 1, fx - 1); ++i) {
@@ -306,8 +323,9 @@ __global__ void k_mg_restrict_residual(int fx, int fy, int fz, const double* __r
 }
 
 // x_f += P x_c (piecewise constant)
-__global__ void k_mg_prolong(int fx, int fy, int fz, double* x, int cx, int cy,
-                             const double* __restrict__ xc, const double* done) {
+template <typename T>
+__global__ void k_mg_prolong(int fx, int fy, int fz, T* x, int cx, int cy,
+                             const T* __restrict__ xc, const double* done) {
   PCG_SKIP(done);
   int64_t n = (int64_t)fx * fy * fz;
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -609,6 +627,9 @@ void* proj_create(const GridDev& g) {
   P->iter_kernels = 0;
   P->graph_failed = 0;
   P->nu = MG_NU_DEFAULT;
+  P->fp32 = 0;
+  P->Ainv32 = nullptr; P->r32 = nullptr; P->z32 = nullptr;
+  for (int l = 0; l < 16; ++l) P->lev32[l] = MGLevelT<float>{};
   for (int q = 0; q < 8; ++q) P->stats[q] = 0.0;
   P->omega = MG_OMEGA;
   cudaStreamCreateWithFlags(&P->cs, cudaStreamNonBlocking);
@@ -627,6 +648,12 @@ void proj_destroy(void* h) {
     cudaFree(lv.gx); cudaFree(lv.gy); cudaFree(lv.gz); cudaFree(lv.e); cudaFree(lv.dinv);
     cudaFree(lv.x); cudaFree(lv.b); cudaFree(lv.t); cudaFree(lv.s);
   }
+  for (int l = 0; l < P->nlev; ++l) {
+    MGLevelT<float>& lv = P->lev32[l];
+    cudaFree(lv.gx); cudaFree(lv.gy); cudaFree(lv.gz); cudaFree(lv.e); cudaFree(lv.dinv);
+    cudaFree(lv.x); cudaFree(lv.b); cudaFree(lv.t); cudaFree(lv.s);
+  }
+  cudaFree(P->Ainv32); cudaFree(P->r32); cudaFree(P->z32);
   if (P->iter_exec) cudaGraphExecDestroy(P->iter_exec);
   if (P->cs) cudaStreamDestroy(P->cs);
   cudaFree(P->Ainv); cudaFree(P->pc_r); cudaFree(P->pc_z); cudaFree(P->pc_p); cudaFree(P->pc_q);
@@ -639,6 +666,39 @@ double* proj_pressure(void* h) { return ((ProjCtx*)h)->p_prev; }
 const double* proj_inv_rho(void* h) { return ((ProjCtx*)h)->ir; }
 int proj_nlevels(void* h) { return ((ProjCtx*)h)->nlev; }
 
+__global__ void k_cvt_d2f(int64_t n, const double* __restrict__ a, float* b, const double* done) {
+  PCG_SKIP(done);
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c < n) b[c] = (float)a[c];
+}
+__global__ void k_cvt_f2d(int64_t n, const float* __restrict__ a, double* b, const double* done) {
+  PCG_SKIP(done);
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c < n) b[c] = (double)a[c];
+}
+
+template <typename T>
+static void rebuild_levels(ProjCtx* P, MGLevelT<T>* lev, T* Ainv, cudaStream_t st) {
+  for (int l = 0; l < P->nlev; ++l) {
+    MGLevelT<T>& f = lev[l];
+    if (l > 0) {
+      MGLevelT<T>& pf = lev[l - 1];
+      k_mg_coarsen<T><<<blocks_for(f.n, 128), 128, 0, st>>>(pf.nx, pf.ny, pf.nz, pf.gx, pf.gy,
+                                                           pf.gz, pf.e, f.nx, f.ny, f.nz, f.gx,
+                                                           f.gy, f.gz, f.e, 0.5);
+      fs_count_launch();
+    }
+    k_mg_diag<T><<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e,
+                                                       f.dinv);
+    fs_count_launch();
+  }
+  MGLevelT<T>& c = lev[P->nlev - 1];
+  if (c.n <= MG_COARSE_MAX) {
+    k_mg_coarse_inverse<T><<<1, 64, 0, st>>>(c.nx, c.ny, c.nz, c.gx, c.gy, c.gz, c.e, Ainv);
+    fs_count_launch();
+  }
+}
+
 int proj_rebuild(void* h, const double* rho, cudaStream_t st) {
   ProjCtx* P = (ProjCtx*)h;
   const GridDev& g = P->g;
@@ -646,79 +706,108 @@ int proj_rebuild(void* h, const double* rho, cudaStream_t st) {
   Launch3 L = launch_cells(g);
   k_proj_level0<<<L.grid, L.block, 0, st>>>(g, rho, P->ir, l0.gx, l0.gy, l0.gz, l0.e,
                                             g.dx * g.dx, g.dy * g.dy); fs_count_launch();
-  for (int l = 0; l < P->nlev; ++l) {
-    MGLevel& f = P->lev[l];
-    if (l > 0) {
-      MGLevel& pf = P->lev[l - 1];
-      k_mg_coarsen<<<blocks_for(f.n, 128), 128, 0, st>>>(pf.nx, pf.ny, pf.nz, pf.gx, pf.gy, pf.gz,
-                                                        pf.e, f.nx, f.ny, f.nz, f.gx, f.gy, f.gz,
-                                                        f.e, 0.5); fs_count_launch();
+  if (P->fp32) {
+    // the FP64 level-0 operator stays the CG's; the preconditioner gets an FP32 copy
+    MGLevelT<float>& f0 = P->lev32[0];
+    const double* src[4] = {l0.gx, l0.gy, l0.gz, l0.e};
+    float* dst[4] = {f0.gx, f0.gy, f0.gz, f0.e};
+    for (int q = 0; q < 4; ++q) {
+      k_cvt_d2f<<<blocks_for(l0.n, 256), 256, 0, st>>>(l0.n, src[q], dst[q], nullptr);
+      fs_count_launch();
     }
-    k_mg_diag<<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e,
-                                                    f.dinv); fs_count_launch();
-  }
-  MGLevel& c = P->lev[P->nlev - 1];
-  if (c.n <= MG_COARSE_MAX) {
-    k_mg_coarse_inverse<<<1, 64, 0, st>>>(c.nx, c.ny, c.nz, c.gx, c.gy, c.gz, c.e, P->Ainv);
-    fs_count_launch();
+    rebuild_levels<float>(P, P->lev32, P->Ainv32, st);
+  } else {
+    rebuild_levels<double>(P, P->lev, P->Ainv, st);
   }
   return cuda_status();
 }
 
+int proj_set_precision(void* h, int fp32) {
+  ProjCtx* P = (ProjCtx*)h;
+  fp32 = fp32 ? 1 : 0;
+  if (fp32 == P->fp32) return FS_OK;
+  if (fp32 && !P->lev32[0].gx) {
+    for (int l = 0; l < P->nlev; ++l) {
+      MGLevelT<float>& lv = P->lev32[l];
+      const MGLevel& ld = P->lev[l];
+      lv.nx = ld.nx; lv.ny = ld.ny; lv.nz = ld.nz; lv.n = ld.n;
+      float** arrs[9] = {&lv.gx, &lv.gy, &lv.gz, &lv.e, &lv.dinv, &lv.x, &lv.b, &lv.t, &lv.s};
+      for (float** a : arrs)
+        if (cudaMalloc(a, sizeof(float) * (size_t)(lv.n > 0 ? lv.n : 1)) != cudaSuccess)
+          return FS_ECUDA;
+    }
+    const int64_t nc = P->lev[P->nlev - 1].n;
+    if (cudaMalloc(&P->Ainv32, sizeof(float) * (size_t)(nc <= MG_COARSE_MAX ? nc * nc : 1)) !=
+            cudaSuccess ||
+        cudaMalloc(&P->r32, sizeof(float) * P->lev[0].n) != cudaSuccess ||
+        cudaMalloc(&P->z32, sizeof(float) * P->lev[0].n) != cudaSuccess)
+      return FS_ECUDA;
+  }
+  P->fp32 = fp32;
+  if (P->iter_exec) cudaGraphExecDestroy(P->iter_exec);  // the iteration graph changes
+  P->iter_exec = nullptr;
+  P->graph_failed = 0;
+  return FS_OK;
+}
+
 // z = V-cycle(r) on level l (b = rhs, x = result); returns kernels launched
-static int vcycle(ProjCtx* P, int l, const double* b, double* x, const double* done,
-                  cudaStream_t st) {
-  MGLevel& f = P->lev[l];
+template <typename T>
+static int vcycle(ProjCtx* P, MGLevelT<T>* lev, const T* Ainv, int l, const T* b, T* x,
+                  const double* done, cudaStream_t st) {
+  MGLevelT<T>& f = lev[l];
   int nk = 0;
   if (l == P->nlev - 1) {
     if (f.n <= MG_COARSE_MAX) {
-      k_mg_coarse_solve<<<1, 64, 0, st>>>((int)f.n, P->Ainv, b, x, done);
+      k_mg_coarse_solve<T><<<1, 64, 0, st>>>((int)f.n, Ainv, b, x, done);
       ++nk;
     } else {
       // not coarsenable and too large for the dense solve: smoothing only
-      k_mg_jacobi<<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e,
-                                                       f.dinv, b, nullptr, x, MG_OMEGA, done);
+      k_mg_jacobi<T><<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz,
+                                                          f.e, f.dinv, b, nullptr, x, MG_OMEGA,
+                                                          done);
       ++nk;
       for (int s = 0; s < 8; ++s) {
-        const double* src = (s & 1) ? f.t : x;
-        double* dst = (s & 1) ? x : f.t;
-        k_mg_jacobi<<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz,
-                                                         f.e, f.dinv, b, src, dst, MG_OMEGA, done);
+        const T* src = (s & 1) ? f.t : x;
+        T* dst = (s & 1) ? x : f.t;
+        k_mg_jacobi<T><<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz,
+                                                            f.e, f.dinv, b, src, dst, MG_OMEGA,
+                                                            done);
         ++nk;
       }
     }
     return nk;
   }
-  MGLevel& cl = P->lev[l + 1];
+  MGLevelT<T>& cl = lev[l + 1];
   unsigned nb = blocks_for(f.n, 256);
   const int nu = P->nu;
   const double om = P->omega;
   // pre-smoothing from x = 0, ending in t:  sweep i writes t when (nu-1-i) is even, else s
-  const double* src = nullptr;
+  const T* src = nullptr;
   for (int i = 0; i < nu; ++i) {
-    double* dst = ((nu - 1 - i) % 2 == 0) ? f.t : f.s;
-    k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, src, dst,
-                                    om, done);
+    T* dst = ((nu - 1 - i) % 2 == 0) ? f.t : f.s;
+    k_mg_jacobi<T><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, src,
+                                       dst, om, done);
     src = dst;
     ++nk;
   }
-  k_mg_restrict_residual<<<blocks_for(cl.n, 128), 128, 0, st>>>(
+  k_mg_restrict_residual<T><<<blocks_for(cl.n, 128), 128, 0, st>>>(
       f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, b, f.t, cl.nx, cl.ny, cl.nz, cl.b, done);
   ++nk;
-  nk += vcycle(P, l + 1, cl.b, cl.x, done, st);
-  k_mg_prolong<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.t, cl.nx, cl.ny, cl.x, done);
+  nk += vcycle<T>(P, lev, Ainv, l + 1, cl.b, cl.x, done, st);
+  k_mg_prolong<T><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.t, cl.nx, cl.ny, cl.x, done);
   ++nk;
   // post-smoothing from t, ending in x:  s, t, s, ... then x
   src = f.t;
   for (int i = 0; i < nu; ++i) {
-    double* dst = (i == nu - 1) ? x : ((i % 2 == 0) ? f.s : f.t);
-    k_mg_jacobi<<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, src, dst,
-                                    om, done);
+    T* dst = (i == nu - 1) ? x : ((i % 2 == 0) ? f.s : f.t);
+    k_mg_jacobi<T><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, src,
+                                       dst, om, done);
     src = dst;
     ++nk;
   }
   return nk;
 }
+
 
 void proj_stats(void* h, double* out8) {
   ProjCtx* P = (ProjCtx*)h;
@@ -743,7 +832,15 @@ static int pcg_iteration(ProjCtx* P, double* x, cudaStream_t st) {
   MGLevel& l0 = P->lev[0];
   const int64_t n = l0.n;
   const double* done = P->scal + SC_DONE;
-  int nk = vcycle(P, 0, P->pc_r, P->pc_z, done, st);
+  int nk;
+  if (P->fp32) {
+    k_cvt_d2f<<<blocks_for(n, 256), 256, 0, st>>>(n, P->pc_r, P->r32, done);
+    nk = vcycle<float>(P, P->lev32, P->Ainv32, 0, P->r32, P->z32, done, st);
+    k_cvt_f2d<<<blocks_for(n, 256), 256, 0, st>>>(n, P->z32, P->pc_z, done);
+    nk += 2;
+  } else {
+    nk = vcycle<double>(P, P->lev, P->Ainv, 0, P->pc_r, P->pc_z, done, st);
+  }
   k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, P->pc_r, P->pc_z, P->partial, done);
   k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 2, done);  // rz_new
   k_pcg_dir<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, P->pc_z, P->pc_p);

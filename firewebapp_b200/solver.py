@@ -84,13 +84,18 @@ class StepDiag:
 
 
 class Tier3Solver:
-    """The Tier-3 step on one GPU, from a case dict (deck keys + wind speed)."""
+    """The Tier-3 step on one GPU, from a case dict (deck keys + wind speed).
+
+    ``form="plain"`` is FP64 throughout.  ``form="mixed"`` runs the DOM sweep
+    and the multigrid preconditioner in FP32; the state, every other kernel,
+    the CG (operator, residuals, dot products), the divergence test and all
+    reductions stay FP64."""
 
     FIELDS = ("rho", "u", "v", "w", "T_g", "Y_fuel", "Y_O2", "Y_H2O", "T_s", "alpha_s",
               "k_turb", "eps_turb", "nu_t", "phi")
 
-    def __init__(self, case: dict, device="cuda", projection_cg_rtol: float = 1.0e-6,
-                 proj_maxiter: int = 200, mg_sweeps: int | None = None):
+    def __init__(self, case: dict, device="cuda", projection_cg_rtol: float | None = None,
+                 proj_maxiter: int = 200, mg_sweeps: int | None = None, form: str = "plain"):
         self.lib = _lib.lib()
         self.dev = torch.device(device)
         self.case = dict(case)
@@ -99,6 +104,13 @@ class Tier3Solver:
         g = su.grid
         self.grid = g
         self.p = dict(su.params)
+        if form not in ("plain", "mixed"):
+            raise ValueError(f"unknown solver form {form!r} (plain or mixed)")
+        self.form = form
+        if projection_cg_rtol is None:
+            # the reference's production tolerance for the plain form; the
+            # mixed form's pressure tolerance is 1e-8 relative
+            projection_cg_rtol = 1.0e-6 if form == "plain" else 1.0e-8
         self.rtol = float(projection_cg_rtol)
         self.proj_maxiter = int(proj_maxiter)
         dev = self.dev
@@ -155,6 +167,8 @@ class Tier3Solver:
         self.proj = h
         if mg_sweeps is not None:
             check(self.lib.fs_proj_configure(self.proj, int(mg_sweeps), 0.8), "fs_proj_configure")
+        if form == "mixed":
+            check(self.lib.fs_proj_set_precision(self.proj, 1), "fs_proj_set_precision")
         om, wq = level_symmetric(self.p["n_quadrature"])
         self.Omega, self.weights = om, wq
         h2 = _ctypes_void()
@@ -162,6 +176,8 @@ class Tier3Solver:
                                      dbl_array(om[:, 1]), dbl_array(om[:, 2]), dbl_array(wq),
                                      KAPPA_SOOT_HOT, _ctypes_byref(h2)), "fs_dom_create")
         self.dom = h2
+        if form == "mixed":
+            check(self.lib.fs_dom_set_precision(self.dom, 1), "fs_dom_set_precision")
         # clock
         self.t = 0.0
         self.dt = float(self.p["dt0"])

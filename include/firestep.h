@@ -203,6 +203,12 @@ int fs_proj_apply(void* handle, const double* x, double* y, void* stream);
  * preconditioner (projection_3d.py:236-246, an FFT solve) has no such knob;
  * only the converged solution is shared. */
 int fs_proj_configure(void* handle, int nu, double omega);
+/* fp32 = 1: the mixed-precision form of the preconditioner (V-cycle
+ * coefficients, vectors and coarse inverse in FP32); the CG itself, its
+ * operator, residuals, dot products and the solution stay FP64, so the
+ * tolerance still applies to the FP64 residual.  No counterpart in the
+ * reference. */
+int fs_proj_set_precision(void* handle, int fp32);
 /* Host-side timings of the last fs_proj_project (ms): total, fetch waits
  * (sum, max), iteration launch calls (sum, max), then the number of fetches,
  * queued iterations and CG iterations (diagnostics; no reference counterpart). */
@@ -237,6 +243,11 @@ double* fs_dom_intensity(void* handle);
 int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
 /* The path in use (0 before the first solve or intensity load). */
 int fs_dom_sweep_mode(void* handle);
+/* fp32 = 1: the mixed-precision form of the sweep (path 4 with kappa,
+ * kappa*B, intensities and octant partials in FP32; G, the ground exchange
+ * and all outputs in FP64).  No counterpart in the reference, which is FP64
+ * throughout.  Only before the first solve or intensity load. */
+int fs_dom_set_precision(void* handle, int fp32);
 /* Load the persistent intensity state from a full device field
  * (M x Nz x Ny x Nx), as a reference I_set would seed the next solve. */
 int fs_dom_load_intensity(void* handle, const double* I_full, void* stream);

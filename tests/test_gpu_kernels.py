@@ -282,6 +282,36 @@ def test_dom(vectors, mode):
             lib().fs_dom_destroy(h)
 
 
+def test_dom_fp32_form(vectors):
+    """The mixed-precision sweep (FP32 intensities) against the FP64 golden
+    vectors: relative error at FP32 level."""
+    from firewebapp_b200.quadrature import level_symmetric
+    om, wq = level_symmetric(4)
+    for name in vectors.cases("dom"):
+        c = vectors.case("dom", name)
+        nz, ny, nx = c["nz"], c["ny"], c["nx"]
+        g = Grid(nz, ny, nx, c["dx"], c["dy"], c["dz_arr"])
+        h = C.c_void_p()
+        call("fs_dom_create", g.ref, om.shape[0], dbl_array(om[:, 0]), dbl_array(om[:, 1]),
+             dbl_array(om[:, 2]), dbl_array(wq), 0.5, C.byref(h))
+        try:
+            call("fs_dom_set_precision", h, 1)
+            Ts, Tg, a, omg, M = (dev(c[x]) for x in ("T_s", "T_g", "alpha_s", "omega_comb",
+                                                     "bed_moisture"))
+            YH = dev(c["Y_H2O"]) if "Y_H2O" in c else None
+            rho = dev(c["rho"]) if "rho" in c else None
+            Tsoil = dev(c["T_soil"].reshape(ny, nx))
+            qs, qg = torch.zeros_like(Ts), torch.zeros_like(Ts)
+            qsoil = torch.zeros((ny, nx), dtype=torch.float64, device="cuda")
+            call("fs_dom_solve", h, ptr(Ts), ptr(Tg), ptr(a), ptr(omg), c["sigma_sav"],
+                 c["T_amb"], ptr(Tsoil), ptr(YH), ptr(rho), ptr(M), ptr(qs), ptr(qg),
+                 ptr(qsoil), stream())
+            for got, key in ((qs, "q_rad_solid"), (qg, "q_rad_gas"), (qsoil, "q_in_soil")):
+                assert rel_l2(host(got), c[key]) <= 1e-5, (name, key)
+        finally:
+            lib().fs_dom_destroy(h)
+
+
 def _segments(x, y, z, dx, dy, z_face, nz, ny, nx, alive):
     from firewebapp_b200.solver import build_segments, locate_particle_cells
     cell = locate_particle_cells(x, y, z, dx, dy, z_face, nx, ny, nz)

@@ -1,0 +1,61 @@
+"""The mixed-precision form (FP32 DOM sweep and multigrid preconditioner,
+everything else FP64) against the FP64 path: per-field error after ten
+steps, and the whole-run derived quantities within 2 % of the reference's
+FP64 run (the form's acceptance criterion)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "ref_cfg1_run.npz"
+FIELDS = ("rho", "u", "v", "w", "T_g", "Y_fuel", "Y_O2", "Y_H2O", "T_s", "k_turb", "eps_turb",
+          "nu_t", "omega", "q_rad", "q_rad_gas", "T_soil", "p_T_s", "p_m_solid", "p_m_water")
+# FP32 intensities carry ~1e-7 relative error into q_rad; after ten coupled
+# steps the fields differ from the FP64 path by far less than this bound
+TOL = 1e-4
+
+
+def test_mixed_form_error_against_fp64_after_ten_steps():
+    from firewebapp_b200.cases import TINY
+    from firewebapp_b200.solver import Tier3Solver
+    a = Tier3Solver(TINY, projection_cg_rtol=1e-10)
+    b = Tier3Solver(TINY, projection_cg_rtol=1e-10, form="mixed")
+    for _ in range(10):
+        a.step()
+        b.step()
+    sa, sb = a.state(), b.state()
+    errs = {k: rel_l2(sb[k], sa[k]) for k in FIELDS}
+    print("mixed vs fp64 rel-L2 after 10 steps:", {k: f"{v:.2e}" for k, v in errs.items()})
+    assert all(v <= TOL for v in errs.values()), errs
+    assert a.t == b.t
+    a.close()
+    b.close()
+
+
+def test_mixed_form_full_run_within_two_percent():
+    import torch
+    from firewebapp_b200.cases import CFG1
+    from firewebapp_b200.solver import Tier3Solver
+    ref = np.load(GOLDEN)
+    n = len(ref["dt"])
+    s = Tier3Solver(CFG1, form="mixed")
+    g = s.grid
+    dzk = s.dz_t.view(-1, 1, 1)
+    lead, hrr, t = [], [], []
+    for _ in range(n):
+        assert s.step()
+        hot = torch.nonzero((s.f["T_s"] >= 600.0).any(dim=0).any(dim=0))
+        lead.append((float(hot.max()) + 0.5) * g.dx if hot.numel() else np.nan)
+        hrr.append(float(((s.w["omega"] * dzk).sum(dim=(0, 1)) * 1.7e7 * g.dy / g.Ly).max()))
+        t.append(s.t)
+    s.close()
+    t, lead = np.asarray(t), np.asarray(lead)
+    ok, okr = (t >= 1.0) & np.isfinite(lead), (ref["t"] >= 1.0) & np.isfinite(ref["lead_x_Ts600"])
+    ros = np.polyfit(t[ok], lead[ok], 1)[0]
+    ros_ref = np.polyfit(ref["t"][okr], ref["lead_x_Ts600"][okr], 1)[0]
+    assert abs(ros - ros_ref) <= 0.02 * ros_ref, (ros, ros_ref)
+    assert abs(max(hrr) - ref["hrr_peak_x"].max()) <= 0.02 * ref["hrr_peak_x"].max()
