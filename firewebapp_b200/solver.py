@@ -95,9 +95,12 @@ class Tier3Solver:
               "k_turb", "eps_turb", "nu_t", "phi")
 
     def __init__(self, case: dict, device="cuda", projection_cg_rtol: float | None = None,
-                 proj_maxiter: int = 200, mg_sweeps: int | None = None, form: str = "plain"):
+                 proj_maxiter: int = 200, mg_sweeps: int | None = None, form: str = "plain",
+                 overlap_dom: bool = True):
         self.lib = _lib.lib()
         self.dev = torch.device(device)
+        if self.dev.type == "cuda" and self.dev.index is None:
+            self.dev = torch.device("cuda", torch.cuda.current_device())
         self.case = dict(case)
         su = build_setup(case)
         self.setup = su
@@ -176,6 +179,16 @@ class Tier3Solver:
                                      dbl_array(om[:, 1]), dbl_array(om[:, 2]), dbl_array(wq),
                                      KAPPA_SOOT_HOT, _ctypes_byref(h2)), "fs_dom_create")
         self.dom = h2
+        # The DOM solve reads only fields that momentum, projection, sponge and
+        # k-epsilon leave untouched (T_s, T_g, alpha_s, omega, Y_H2O, rho,
+        # M_local) and writes only fields they do not read, so it runs on a
+        # second stream from a worker thread, concurrently with them.
+        self.overlap_dom = bool(overlap_dom)
+        self.s_dom = torch.cuda.Stream(device=dev) if self.overlap_dom else None
+        self._pool = None
+        if self.overlap_dom:
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(max_workers=1, thread_name_prefix="dom")
         if form == "mixed":
             check(self.lib.fs_dom_set_precision(self.dom, 1), "fs_dom_set_precision")
         # clock
@@ -255,6 +268,9 @@ class Tier3Solver:
         torch.cuda.synchronize()
 
     def close(self):
+        if getattr(self, "_pool", None) is not None:
+            self._pool.shutdown(wait=True)
+            self._pool = None
         if getattr(self, "proj", None):
             self.lib.fs_proj_destroy(self.proj)
             self.proj = None
@@ -380,6 +396,16 @@ class Tier3Solver:
                              _ctypes_ref(self.fs_parts), _ctypes_ref(self.fs_segs),
                              ptr(self.seg_of_cell), s), "bed_hcond")
         Sp, Sd = self.bed_out["S_pyro"], self.bed_out["S_drying"]
+        # --- 8 (started here). DOM + M_local aggregation on the second stream
+        dom_now = self.step_count % max(p["dom_subcycle_every"], 1) == 0
+        dom_job = None
+        if dom_now and self.overlap_dom:
+            ready = torch.cuda.Event()
+            ready.record(torch.cuda.current_stream(self.dev))
+            dom_args = (ptr(f["T_s"]), ptr(f["T_g"]), ptr(f["alpha_s"]), ptr(w["omega"]),
+                        ptr(f["Y_H2O"]), ptr(f["rho"]), ptr(w["M_local"]), ptr(w["q_rad"]),
+                        ptr(w["q_rad_gas"]))
+            dom_job = self._pool.submit(self._dom_job, ready, dom_args)
         # --- 3/4. drag + tentative momentum (spread_3d.py:2223-2276)
         self._phase("momentum")
         with self._ktime("momentum_drag"):
@@ -435,7 +461,11 @@ class Tier3Solver:
         self._swap("nu_t", "tmp3")
         # --- 8. DOM (every dom_subcycle_every steps) + soil (spread_3d.py:2472-2514)
         self._phase("dom")
-        if self.step_count % max(p["dom_subcycle_every"], 1) == 0:
+        if dom_job is not None:
+            done = dom_job.result()
+            torch.cuda.current_stream(self.dev).wait_event(done)
+            d.dom_iters = L.fs_dom_iterations(self.dom)
+        elif dom_now:
             check(L.fs_bed_aggregate(_ctypes_ref(self.fs_parts), _ctypes_ref(self.fs_segs),
                                      ptr(w["M_local"]), 1, s), "bed_aggregate_M")
             check(L.fs_dom_solve(self.dom, ptr(f["T_s"]), ptr(f["T_g"]), ptr(f["alpha_s"]),
@@ -563,6 +593,25 @@ class Tier3Solver:
         d.t, d.dt = self.t, dt
         self.diag = d
         return True
+
+    def _dom_job(self, ready, a):
+        """M_local aggregation and the DOM solve on the second stream, after
+        the bed work queued before ``ready``; returns the event that marks the
+        end of that work."""
+        torch.cuda.set_device(self.dev)
+        st = self.s_dom
+        st.wait_event(ready)
+        sp = st.cuda_stream
+        L, p = self.lib, self.p
+        Ts, Tg, a_s, om, YH, rho, Ml, qr, qrg = a
+        check(L.fs_bed_aggregate(_ctypes_ref(self.fs_parts), _ctypes_ref(self.fs_segs), Ml, 1,
+                                 sp), "bed_aggregate_M")
+        check(L.fs_dom_solve(self.dom, Ts, Tg, a_s, om, p["sav"], p["T_amb"],
+                             ptr(self.T_soil[0]), YH, rho, Ml, qr, qrg, ptr(self.q_in_soil), sp),
+              "dom_solve")
+        done = torch.cuda.Event()
+        done.record(st)
+        return done
 
     def _div_target(self, dt):
         # (S_pyro - (rho - rho_prev)/dt) / max(rho, 0.1), S_pyro = Sp + Sd (:2147, :2317)
