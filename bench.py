@@ -236,6 +236,8 @@ def main():
                     help="skip the clock sampler (diagnostics only; the line then has no clocks)")
     ap.add_argument("--nx", type=int, default=None,
                     help="run the workload cut to its first NX x-cells (profiling)")
+    ap.add_argument("--dom-sweep", type=int, default=0,
+                    help="force a DOM sweep path (fs_dom_set_sweep_mode); 0 picks automatically")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -258,7 +260,7 @@ def main():
     if args.nx:
         from firewebapp_b200.cases import scaled
         case = dict(scaled(CFG2, nx=args.nx), jitter_seed=rank)
-    solver = Tier3Solver(case, form=args.form)
+    solver = Tier3Solver(case, form=args.form, dom_sweep=args.dom_sweep)
     cells = solver.n
     for _ in range(args.warmup):
         solver.step()
@@ -308,7 +310,7 @@ def main():
         # the 8 octant partial G fields (FP32 in the mixed form; wrap rows and
         # ground partials < 1% more); per-ordinate paths write every intensity
         "dom_sweep": (N * (8.0 + 4.0 * 8) if args.form == "mixed" else
-                      N * (16.0 + 8.0 * 8) if dom_mode in (1, 4) else N * (8.0 * M + 16.0)),
+                      N * (16.0 + 8.0 * 8) if dom_mode in (1, 4, 6, 7) else N * (8.0 * M + 16.0)),
         "species_transport": N * 8.0 * 12,
         "edc": N * 8.0 * 11,
         "turb_diffusion_Y": N * 8.0 * 7,

@@ -25,7 +25,9 @@
 //   3 one launch per hyperplane (any grid size).
 //   5 one CTA per ordinate (as 2) with fixed pencils per thread, the inputs
 //     of a hyperplane loaded in batches and the inflow rows staged ahead.
-// G in paths 1 and 4 is summed within each octant in ordinate order and then over
+//   7 as 4 without clusters: a cooperative launch of self-timed CTAs that
+//     hand their last row downstream through a ring in global memory.
+// G in paths 1, 4, 6 and 7 is summed within each octant in ordinate order and then over
 // octants in octant order (the reference sums all ordinates in one sequence;
 // the two orders differ only by rounding).
 #include <vector>
@@ -54,7 +56,10 @@ struct DomCtx {
   int fp32;                   // single-precision sweep (path 4 only)
   float2* kb32;
   float *Goct32, *Qoct32, *wrap32;
-  int Mo, cl_C, cl_rows, cl_threads;
+  int Mo, cl_C, cl_rows, cl_threads, cl_lg_ring;
+  void* st_ring;              // path 7 hand-off ring, then the read counters
+  size_t st_ring_bytes;       // ring and counters (filled with 0xff before each sweep)
+  size_t st_cnt_offset;
   size_t cl_smem;
   int down_slot[8];
   double *G, *Gp;             // current / previous G
@@ -591,6 +596,12 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, MINB) k_dom_octant(GridDev g,
   cluster_wait_acquire();
 }
 
+// The division of the sweep: correctly rounded in FP64 (the reference's
+// arithmetic); in the single-precision form the reciprocal-based quotient of
+// __fdividef (about 2 ulp), which keeps each ordinate's dependent chain short.
+__device__ __forceinline__ double sweep_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float sweep_div(float a, float b) { return __fdividef(a, b); }
+
 // ---- single-precision form of path 4 (the mixed-precision solver) -----------
 // Same sweep, with kappa, kappa*B, the hyperplane buffers, the inflow rows and
 // the octant partials in FP32; the octant partials are summed into G in FP64.
@@ -713,7 +724,7 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_f32(GridDev g
         const float ix = cix[m], iy = ciy[m], iz = izt[m * nz + k];
         const float num = kab.y + ix * Ix + iy * Iy + iz * Iz;
         const float den = kab.x + ix + iy + iz;
-        v[m] = num / den;
+        v[m] = sweep_div(num, den);
         cur[(size_t)m * S + q] = v[m];
         gs = gs + cw[m] * v[m];
         if (ground_out) qs = qs + cwm[m] * v[m];
@@ -1023,6 +1034,389 @@ __global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_pipe(GridDev 
   cluster_wait_acquire();
 }
 
+// ---- path 7: self-timed octant pipeline (global-memory hand-off) -------------
+// The row split of path 4 (CTAs of an octant split the k' rows, one thread per
+// pencil, all ordinates of the octant per thread), without clusters and
+// without any barrier between CTAs.  The only value a CTA needs from another
+// is the upstream CTA's last row of the previous hyperplane.  The upstream
+// CTA's last-row threads store that row into a ring of R slots in global
+// memory (L2), and the downstream CTA's first-row threads load it from there.
+// No fence is issued on the hand-off: every word carries its own state.  The
+// intensities are never negative, so the sign bit of each stored word is free
+// and holds the lap parity ((p - a0) / R) mod 2 of hyperplane p, a0 being the
+// first hyperplane of that pencil; the ring is filled with sign-bit-set words
+// before every sweep, so the first lap (parity 0) can never be mistaken for
+// stale contents, and a word two laps old cannot be present when a lap is
+// awaited because the reader has already read the lap in between.  The
+// writer may overwrite a slot once the reader's CTA has published (one
+// relaxed store per hyperplane) that it has read it; those reads have
+// completed by then.  Each CTA therefore runs at its own pace with one
+// __syncthreads per hyperplane, the latency between SMs is paid once per CTA
+// in the pipeline fill, and no cluster has to fit in one GPC, so all eight
+// octants run at once.  The arithmetic of every cell is that of path 4, so the
+// results are identical.  Every wait is bounded as in path 1.
+template <typename T> struct Vec2Of;
+template <> struct Vec2Of<double> { using type = double2; };
+template <> struct Vec2Of<float> { using type = float2; };
+template <typename T> struct WordOf;
+template <> struct WordOf<double> { using type = unsigned long long; };
+template <> struct WordOf<float> { using type = unsigned; };
+
+template <typename T>
+struct StArgs {
+  const typename Vec2Of<T>::type* kb;
+  const double *ox, *oy, *oz, *w;
+  const double* Ig;
+  T *Goct, *Qoct, *wrap;
+  typename WordOf<T>::type* ring;  // 8 x (C-1) x R x Mo x Ny words
+  int* consumed;                   // 8 x (C-1): last hyperplane read by each downstream CTA
+  T I_amb;
+  int C, rows, periodic, lg_ring;
+  unsigned down_slots;
+  int* err;
+};
+#define ST_RING_LG 3  // R = 8 slots
+
+__host__ __device__ inline size_t st_up16(size_t x) { return (x + 15) & ~(size_t)15; }
+// Shared-memory layout of path 7 (byte offsets, each 16-byte aligned): the
+// prefetch rings (OCT_AHEAD hyperplanes of kappa/kappa*B and ground
+// intensity), the y-inflow and y-outflow rows staged in chunks of ST_CHUNK
+// hyperplanes (two chunks each), the z-inflow row from the upstream CTA, the
+// two hyperplane buffers and the per-ordinate constants.
+#define ST_CHUNK 32
+struct StLayout {
+  size_t kab, ig, win, wout, zin, buf0, buf1, izt, cix, total;
+};
+__host__ __device__ inline StLayout st_layout(int tsize, int Mo, int rows, int ny, int nz) {
+  StLayout L;
+  const size_t S = (size_t)rows * ny;
+  const size_t chunk = (size_t)2 * Mo * rows * ST_CHUNK * tsize;
+  size_t o = 0;
+  L.kab = o; o = st_up16(o + (size_t)OCT_AHEAD * S * 2 * tsize);
+  L.ig = o; o = st_up16(o + (size_t)OCT_AHEAD * ny * sizeof(double));
+  L.win = o; o = st_up16(o + chunk);
+  L.wout = o; o = st_up16(o + chunk);
+  L.zin = o; o = st_up16(o + (size_t)Mo * ny * tsize);
+  L.buf0 = o; o = st_up16(o + (size_t)Mo * S * tsize);
+  L.buf1 = o; o = st_up16(o + (size_t)Mo * S * tsize);
+  L.izt = o; o = st_up16(o + (size_t)Mo * nz * tsize);
+  L.cix = o; o = st_up16(o + 4 * (size_t)Mo * tsize);
+  L.total = o;
+  return L;
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(int* p, int v) {
+  asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long word_of(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
+__device__ __forceinline__ unsigned word_of(float v) { return __float_as_uint(v); }
+__device__ __forceinline__ double value_of(unsigned long long w) {
+  return __longlong_as_double((long long)(w & 0x7fffffffffffffffull));
+}
+__device__ __forceinline__ float value_of(unsigned w) { return __uint_as_float(w & 0x7fffffffu); }
+__device__ __forceinline__ unsigned sign_of(unsigned long long w) { return (unsigned)(w >> 63); }
+__device__ __forceinline__ unsigned sign_of(unsigned w) { return w >> 31; }
+__device__ __forceinline__ unsigned long long with_sign(unsigned long long w, unsigned s) {
+  return (w & 0x7fffffffffffffffull) | ((unsigned long long)s << 63);
+}
+__device__ __forceinline__ unsigned with_sign(unsigned w, unsigned s) {
+  return (w & 0x7fffffffu) | (s << 31);
+}
+__device__ __forceinline__ void cp_async_kb(void* dst, const double2* src, uint64_t pol) {
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_kb(void* dst, const float2* src, uint64_t pol) {
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_val(void* dst, const double* src) { cp_async8(dst, src); }
+__device__ __forceinline__ void cp_async_val(void* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void st_cs(double* p, double v) { st_stream(p, v); }
+__device__ __forceinline__ void st_cs(float* p, float v) {
+  asm volatile("st.global.cs.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
+// One thread per pencil.  The y-periodic inflow of a row (read by its first
+// pencil) and outflow (written by its last) run along x over the hyperplanes,
+// so they move through shared memory in chunks of ST_CHUNK hyperplanes with
+// contiguous loads and stores by the whole CTA.  A location's inflow is read
+// (from the previous sweep) before its chunk starts and its outflow is
+// written after the outflow's chunk ends, ny-1 hyperplanes later, so the
+// previous sweep's value is always the one read, as in the reference's
+// in-place sweep.
+template <typename T, int MO>
+__global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_st(GridDev g, StArgs<T> a) {
+  using T2 = typename Vec2Of<T>::type;
+  using W = typename WordOf<T>::type;
+  extern __shared__ __align__(16) unsigned char shraw[];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int C = a.C;
+  const int oct = blockIdx.x / C;
+  const int rank = blockIdx.x - oct * C;
+  const int n0 = oct * MO;
+  const int rows = a.rows;
+  const int S = rows * ny;
+  const int lg = a.lg_ring;
+  const int R = 1 << lg;
+  const StLayout L = st_layout((int)sizeof(T), MO, rows, ny, nz);
+  T2* kab_ring = (T2*)(shraw + L.kab);
+  double* ig_ring = (double*)(shraw + L.ig);
+  T* win = (T*)(shraw + L.win);    // [2 chunks][MO][rows][ST_CHUNK]
+  T* wout = (T*)(shraw + L.wout);  // [2 chunks][MO][rows][ST_CHUNK]
+  T* zin = (T*)(shraw + L.zin);
+  T* buf0 = (T*)(shraw + L.buf0);
+  T* buf1 = (T*)(shraw + L.buf1);
+  T* izt = (T*)(shraw + L.izt);
+  T* cix = (T*)(shraw + L.cix);
+  T* ciy = cix + MO;
+  T* cw = ciy + MO;
+  T* cwm = cw + MO;
+  const int nplanes = nx + ny + nz - 2;
+  for (int t = threadIdx.x; t < MO * nz; t += blockDim.x) {
+    const int m = t / nz, k = t - m * nz;
+    izt[t] = (T)(fabs(a.oz[n0 + m]) / g.dz[k]);
+  }
+  for (int m = threadIdx.x; m < MO; m += blockDim.x) {
+    cix[m] = (T)(fabs(a.ox[n0 + m]) / g.dx);
+    ciy[m] = (T)(fabs(a.oy[n0 + m]) / g.dy);
+    cw[m] = (T)a.w[n0 + m];
+    cwm[m] = (T)(a.w[n0 + m] * fabs(a.oz[n0 + m]));
+  }
+  const bool fx = a.ox[n0] >= 0.0, fy = a.oy[n0] >= 0.0, fz = a.oz[n0] >= 0.0;
+  const int r0 = rank * rows;
+  const int nrows = min(rows, nz - r0);
+  const int npen = nrows > 0 ? nrows * ny : 0;
+  const int q = threadIdx.x;
+  const bool has = q < npen;
+  const int kl = has ? q / ny : 0;
+  const int jp = has ? q - kl * ny : 0;
+  const int kp = r0 + kl;
+  const int j = fy ? jp : ny - 1 - jp;
+  const int k = fz ? kp : nz - 1 - kp;
+  const int64_t N = ncells_dev(g);
+  const int64_t n2 = (int64_t)nx * ny;
+  const int slot_bits = (int)((a.down_slots >> (4 * oct)) & 15u);
+  const int slot = slot_bits == 15 ? -1 : slot_bits;
+  T* Go = a.Goct + (int64_t)oct * N;
+  const int64_t wstride = (int64_t)nz * nx;
+  T* wrap0 = a.wrap + (int64_t)n0 * wstride;
+  const bool ground_out = has && !fz && k == 0 && slot >= 0;
+  const bool z_in_ground = has && fz && kp == 0;
+  const bool consumer = has && kl == 0 && rank > 0;
+  // only a full CTA (every CTA but the last) has a downstream neighbour
+  const bool producer = has && kl == rows - 1 && rank < C - 1;
+  const bool periodic = a.periodic != 0;
+  const bool y_out = has && jp == ny - 1 && periodic;
+  // ring of the boundary below this CTA (read) and above it (written)
+  const size_t slot_words = (size_t)MO * ny;
+  const W* ring_in = consumer
+      ? a.ring + ((size_t)oct * (C - 1) + (rank - 1)) * R * slot_words + jp : nullptr;
+  W* ring_out = producer
+      ? a.ring + ((size_t)oct * (C - 1) + rank) * R * slot_words + jp : nullptr;
+  int* cnt_in = (rank > 0) ? a.consumed + oct * (C - 1) + (rank - 1) : nullptr;
+  const int* cnt_out = producer ? a.consumed + oct * (C - 1) + rank : nullptr;
+  // first hyperplane of a pencil's hand-off words (the row below the consumer's
+  // first row, and the producer's own row): laps are counted from there.  A
+  // one-row CTA is consumer and producer at once.
+  const int a0_in = jp + kp - 1, a0_out = jp + kp;
+  const int64_t row_base = ((int64_t)k * ny + j) * nx;
+  const uint64_t keep = l2_policy_evict_last();
+  const int chunk_elems = MO * rows * ST_CHUNK;
+  // the y-inflow rows of chunk c (hyperplanes c*ST_CHUNK ...), by the whole CTA
+  auto load_inflow = [&](int c) {
+    T* dst = win + (size_t)(c & 1) * chunk_elems;
+    for (int e = threadIdx.x; e < chunk_elems; e += blockDim.x) {
+      const int t = e % ST_CHUNK, rm = e / ST_CHUNK;
+      const int rl = rm % rows, m = rm / rows;
+      const int ip = c * ST_CHUNK + t - (r0 + rl);  // pencil jp = 0 of row rl
+      if (rl < nrows && ip >= 0 && ip < nx) {
+        const int kk = fz ? r0 + rl : nz - 1 - (r0 + rl);
+        const int i = fx ? ip : nx - 1 - ip;
+        cp_async_val(&dst[e], &wrap0[m * wstride + (int64_t)kk * nx + i]);
+      }
+    }
+  };
+  // the y-outflow rows of chunk c, to global memory by the whole CTA
+  auto store_outflow = [&](int c) {
+    const T* src = wout + (size_t)(c & 1) * chunk_elems;
+    for (int e = threadIdx.x; e < chunk_elems; e += blockDim.x) {
+      const int t = e % ST_CHUNK, rm = e / ST_CHUNK;
+      const int rl = rm % rows, m = rm / rows;
+      const int ip = c * ST_CHUNK + t - (ny - 1) - (r0 + rl);  // pencil jp = ny-1 of row rl
+      if (rl < nrows && ip >= 0 && ip < nx) {
+        const int kk = fz ? r0 + rl : nz - 1 - (r0 + rl);
+        const int i = fx ? ip : nx - 1 - ip;
+        wrap0[m * wstride + (int64_t)kk * nx + i] = src[e];
+      }
+    }
+  };
+  // the inputs of hyperplane d (one commit group per hyperplane); the group of
+  // the last hyperplane before a chunk also carries that chunk's inflow rows
+  auto prefetch = [&](int d) {
+    const int ip = d - jp - kp;
+    if (has && ip >= 0 && ip < nx) {
+      const int i = fx ? ip : nx - 1 - ip;
+      const int sl = d % OCT_AHEAD;
+      cp_async_kb(&kab_ring[(size_t)sl * S + q], &a.kb[row_base + i], keep);
+      if (z_in_ground) cp_async8(&ig_ring[(size_t)sl * ny + jp], &a.Ig[(int64_t)j * nx + i]);
+    }
+    if (periodic && (d + 1) % ST_CHUNK == 0 && d + 1 < nplanes) load_inflow((d + 1) / ST_CHUNK);
+    cp_async_commit();
+  };
+  if (periodic) load_inflow(0);
+  for (int d = 0; d < OCT_AHEAD - 1; ++d) prefetch(d);
+  cp_async_wait<OCT_AHEAD - 2>();  // group 0, which holds chunk 0 of the inflow rows
+  __syncthreads();
+  const int Rm = R - 1;
+  W raw[MO];  // the z-inflow words of the coming hyperplane (consumer row)
+#pragma unroll
+  for (int m = 0; m < MO; ++m) raw[m] = 0;
+  int known = -1;    // last hyperplane the downstream CTA is known to have read
+  int pending = -1;  // a load of that count issued on the previous hyperplane
+  for (int d = 0; d < nplanes; ++d) {
+    prefetch(d + OCT_AHEAD - 1);  // an empty group past the last plane
+    // a finished chunk of outflow rows leaves for global memory
+    if (periodic && d > 0 && d % ST_CHUNK == 0) store_outflow(d / ST_CHUNK - 1);
+    T* cur = (d & 1) ? buf1 : buf0;
+    const T* prev = (d & 1) ? buf0 : buf1;
+    const int ip = d - jp - kp;
+    const bool act = has && ip >= 0 && ip < nx;
+    if (consumer) {
+      if (act) {
+        // words of hyperplane d-1, loaded one hyperplane ago; re-read any not yet written
+        const int p = d - 1;
+        const unsigned par = (unsigned)((p - a0_in) >> lg) & 1u;
+        const W* src = ring_in + (size_t)(p & Rm) * slot_words;
+        unsigned bad = 0;
+#pragma unroll
+        for (int m = 0; m < MO; ++m) bad |= sign_of(raw[m]) ^ par;
+        for (int it = 0; bad; ++it) {
+          if (it >= OCT_WAIT_LIMIT) { atomicExch(a.err, 1); break; }
+          if ((it & 1023) == 1023 && *(volatile int*)a.err) break;
+          // all stale words re-read at once
+#pragma unroll
+          for (int m = 0; m < MO; ++m)
+            if (sign_of(raw[m]) != par) raw[m] = ld_relaxed(src + (size_t)m * ny);
+          bad = 0;
+#pragma unroll
+          for (int m = 0; m < MO; ++m) bad |= sign_of(raw[m]) ^ par;
+        }
+#pragma unroll
+        for (int m = 0; m < MO; ++m) zin[(size_t)m * ny + jp] = value_of(raw[m]);
+      }
+      // start loading hyperplane d's words, used on the next hyperplane
+      const int ipn = d + 1 - jp - kp;
+      if (d + 1 < nplanes && ipn >= 0 && ipn < nx) {
+        const W* src = ring_in + (size_t)(d & Rm) * slot_words;
+#pragma unroll
+        for (int m = 0; m < MO; ++m) raw[m] = ld_relaxed(src + (size_t)m * ny);
+      }
+    }
+    cp_async_wait<OCT_AHEAD - 1>();  // this plane's group has landed
+    T v[MO];
+    T gs = (T)0, qs = (T)0;
+    if (act) {
+      const int sl = d % OCT_AHEAD;
+      const int ch = (d / ST_CHUNK) & 1, tt = d % ST_CHUNK;
+      const T2 kab = kab_ring[(size_t)sl * S + q];
+#pragma unroll
+      for (int m = 0; m < MO; ++m) {
+        const T* pm = prev + (size_t)m * S;
+        const T Ix = ip > 0 ? pm[q] : a.I_amb;
+        T Iy;
+        if (jp > 0) Iy = pm[q - 1];
+        else Iy = periodic ? win[((size_t)(ch * MO + m) * rows + kl) * ST_CHUNK + tt] : a.I_amb;
+        T Iz;
+        if (kl > 0) Iz = pm[q - ny];
+        else if (kp > 0) Iz = zin[(size_t)m * ny + jp];
+        else Iz = fz ? (T)ig_ring[(size_t)sl * ny + jp] : a.I_amb;
+        const T ix = cix[m], iy = ciy[m], iz = izt[m * nz + k];
+        const T num = kab.y + ix * Ix + iy * Iy + iz * Iz;
+        const T den = kab.x + ix + iy + iz;
+        v[m] = sweep_div(num, den);
+        cur[(size_t)m * S + q] = v[m];
+        gs = gs + cw[m] * v[m];
+        if (ground_out) qs = qs + cwm[m] * v[m];
+      }
+      if (y_out) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) wout[((size_t)(ch * MO + m) * rows + kl) * ST_CHUNK + tt] = v[m];
+      }
+    }
+    if (producer) {
+      if (pending > known) known = pending;
+      if (act) {
+        // the slot held hyperplane d-R, which the downstream CTA must have read
+        if (d - R > known) {
+          int it = 0;
+          do {
+            known = ld_relaxed(cnt_out);
+          } while (d - R > known && ++it < OCT_WAIT_LIMIT &&
+                   !((it & 1023) == 0 && *(volatile int*)a.err));
+          if (d - R > known && it >= OCT_WAIT_LIMIT) atomicExch(a.err, 1);
+        }
+        const unsigned par = (unsigned)((d - a0_out) >> lg) & 1u;
+        W* dst = ring_out + (size_t)(d & Rm) * slot_words;
+#pragma unroll
+        for (int m = 0; m < MO; ++m)
+          st_relaxed(dst + (size_t)m * ny, with_sign(word_of(v[m]), par));
+      }
+      pending = ld_relaxed(cnt_out);  // used on the next hyperplane
+    }
+    if (act) {
+      const int i = fx ? ip : nx - 1 - ip;
+      st_cs(Go + row_base + i, gs);
+      if (ground_out) a.Qoct[(int64_t)slot * n2 + (int64_t)j * nx + i] = qs;
+    }
+    __syncthreads();
+    // every read of hyperplane d-1's words in this CTA has completed
+    if (threadIdx.x == 0 && rank > 0 && d > 0) st_relaxed(cnt_in, d - 1);
+  }
+  // the last (partial) chunk of outflow rows
+  if (periodic) store_outflow((nplanes - 1) / ST_CHUNK);
+  cp_async_wait<0>();
+}
+
+static const void* octant_st_ptr(bool fp32, int Mo) {
+  switch (Mo) {
+    case 3: return fp32 ? (const void*)k_dom_octant_st<float, 3> : (const void*)k_dom_octant_st<double, 3>;
+    case 6: return fp32 ? (const void*)k_dom_octant_st<float, 6> : (const void*)k_dom_octant_st<double, 6>;
+    case 10: return fp32 ? (const void*)k_dom_octant_st<float, 10> : (const void*)k_dom_octant_st<double, 10>;
+    default: return nullptr;
+  }
+}
+
 template <int MO, int MINB = 1>
 static cudaError_t launch_octant_kernel(const GridDev& g, const OctArgs& a, cudaLaunchConfig_t* cfg) {
   return cudaLaunchKernelEx(cfg, k_dom_octant<MO, MINB>, g, a);
@@ -1169,6 +1563,7 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   D->I = nullptr; D->wrap = nullptr; D->kb = nullptr; D->Goct = nullptr; D->Qoct = nullptr;
   D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1;
   D->fp32 = 0; D->kb32 = nullptr; D->Goct32 = nullptr; D->Qoct32 = nullptr; D->wrap32 = nullptr;
+  D->st_ring = nullptr; D->st_ring_bytes = 0; D->st_cnt_offset = 0;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemset(D->G, 0, sizeof(double) * N);
   cudaMalloc(&D->ks, sizeof(double) * N); cudaMalloc(&D->kg, sizeof(double) * N);
@@ -1197,6 +1592,7 @@ void dom_destroy(void* h) {
   cudaFree(D->ox); cudaFree(D->oy); cudaFree(D->oz); cudaFree(D->w); cudaFree(D->I);
   cudaFree(D->wrap); cudaFree(D->kb); cudaFree(D->Goct); cudaFree(D->Qoct);
   cudaFree(D->kb32); cudaFree(D->Goct32); cudaFree(D->Qoct32); cudaFree(D->wrap32);
+  cudaFree(D->st_ring);
   cudaFree(D->G); cudaFree(D->Gp); cudaFree(D->ks); cudaFree(D->kg); cudaFree(D->ksafe);
   cudaFree(D->B); cudaFree(D->Ig_out); cudaFree(D->Isoil); cudaFree(D->qin); cudaFree(D->keys);
   cudaFreeHost(D->h_keys);
@@ -1226,9 +1622,11 @@ static bool octant_grouping(const DomCtx* D) {
 }
 
 // Pick the cluster size (CTAs per octant) and launch shape for path 1; false if none fits.
-static bool plan_clusters(DomCtx* D, int force_C, bool pipe, int groups = 1) {
+// kind: 4 cluster barrier per hyperplane, 1 mbarrier pipeline
+static bool plan_clusters(DomCtx* D, int force_C, int kind, int groups = 1) {
   const GridDev& g = D->g;
   const int Mo = D->M / 8 / groups;
+  const bool pipe = kind == 1;
   int dev = 0, optin = 0, smem_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -1280,17 +1678,68 @@ static bool plan_clusters(DomCtx* D, int force_C, bool pipe, int groups = 1) {
   return found;
 }
 
+// Launch shape of path 7: CTAs per octant C (k' rows split as in path 4), one
+// CTA per SM, and all 8*C CTAs resident at once (the hand-off waits on other
+// CTAs, so the grid is launched cooperatively); false if it does not fit.
+static bool plan_st(DomCtx* D, int force_C) {
+  const GridDev& g = D->g;
+  const int Mo = D->M / 8;
+  const int tsize = D->fp32 ? (int)sizeof(float) : (int)sizeof(double);
+  if (g.nx + g.ny + g.nz - 2 >= (1 << 30)) return false;
+  int dev = 0, optin = 0, smem_sm = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const void* fn = octant_st_ptr(D->fp32 != 0, Mo);
+  if (!fn) return false;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  // the largest C (fewest rows per CTA) whose 8*C CTAs fit one per SM
+  for (int C = 64; C >= 1; --C) {
+    if (force_C > 0 && C != force_C) continue;
+    const int rows = (g.nz + C - 1) / C;
+    if ((g.nz + rows - 1) / rows != C) continue;
+    const int threads = ((rows * g.ny + 31) / 32) * 32;
+    if (threads > OCT_MAX_THREADS || 8 * C > nsm) continue;
+    const size_t need = st_layout(tsize, Mo, rows, g.ny, g.nz).total;
+    const size_t pad = (size_t)smem_sm / 2 + 1024;  // no two CTAs on one SM
+    const size_t smem = need > pad ? need : pad;
+    if (smem > (size_t)optin) continue;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (per_sm < 1 || (int64_t)per_sm * nsm < 8 * C) continue;
+    D->cl_C = C; D->cl_rows = rows; D->cl_threads = threads; D->cl_smem = smem;
+    D->cl_lg_ring = ST_RING_LG;
+    return true;
+  }
+  return false;
+}
+
+static void alloc_st_ring(DomCtx* D) {
+  const int tsize = D->fp32 ? (int)sizeof(float) : (int)sizeof(double);
+  const size_t bounds = (size_t)8 * (D->cl_C - 1);
+  const size_t words = bounds * ((size_t)1 << D->cl_lg_ring) * D->Mo * D->g.ny;
+  D->st_cnt_offset = (words * tsize + 255) & ~(size_t)255;
+  D->st_ring_bytes = D->st_cnt_offset + sizeof(int) * (bounds > 0 ? bounds : 1);
+  cudaMalloc(&D->st_ring, D->st_ring_bytes);
+}
+
 static int dom_prepare(DomCtx* D) {
   if (D->mode != 0) return FS_OK;
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
   const int want = D->mode_req;
   if (D->fp32) {
-    if ((want != 0 && want != 4) || !octant_grouping(D) || !plan_clusters(D, D->force_C, false)) {
-      fs_set_error("single-precision sweep needs the octant-cluster path (4) on this grid");
+    const int kind = want == 7 ? 7 : 4;
+    if ((want != 0 && want != 4 && want != 7) || !octant_grouping(D) ||
+        !(kind == 7 ? plan_st(D, D->force_C) : plan_clusters(D, D->force_C, kind))) {
+      fs_set_error("single-precision sweep needs an octant-cluster path (4 or 7) on this grid");
       return FS_EARG;
     }
-    D->mode = 4;
+    D->mode = kind;
     D->groups = 1;
     D->Mo = D->M / 8;
     int slot = 0;
@@ -1300,13 +1749,15 @@ static int dom_prepare(DomCtx* D) {
     cudaMalloc(&D->Qoct32, sizeof(float) * 8 * n2);
     cudaMalloc(&D->wrap32, sizeof(float) * D->M * g.nz * g.nx);
     cudaMemset(D->wrap32, 0, sizeof(float) * D->M * g.nz * g.nx);
+    if (D->mode == 7) alloc_st_ring(D);
     return cuda_status();
   }
   // auto picks the cluster-barrier sweep (path 4), measured faster than path 1
   const int groups = (want == 6 && D->M % 16 == 0) ? 2 : 1;
-  if ((want == 0 || want == 1 || want == 4 || want == 6) && octant_grouping(D) &&
-      plan_clusters(D, D->force_C, want == 1, groups)) {
-    D->mode = want == 1 ? 1 : (want == 6 ? 6 : 4);
+  const int kind = (want == 1 || want == 7) ? want : 4;
+  if ((want == 0 || want == 1 || want == 4 || want == 6 || want == 7) && octant_grouping(D) &&
+      (kind == 7 ? plan_st(D, D->force_C) : plan_clusters(D, D->force_C, kind, groups))) {
+    D->mode = want == 1 ? 1 : (want == 6 ? 6 : (want == 7 ? 7 : 4));
     D->groups = groups;
     D->Mo = D->M / 8;
     int slot = 0;
@@ -1316,9 +1767,10 @@ static int dom_prepare(DomCtx* D) {
     cudaMalloc(&D->Qoct, sizeof(double) * 8 * groups * n2);
     cudaMalloc(&D->wrap, sizeof(double) * D->M * g.nz * g.nx);
     cudaMemset(D->wrap, 0, sizeof(double) * D->M * g.nz * g.nx);
+    if (D->mode == 7) alloc_st_ring(D);
     return cuda_status();
   }
-  if (want == 1 || want == 4 || want == 6) {
+  if (want == 1 || want == 4 || want == 6 || want == 7) {
     fs_set_error("octant-cluster sweep not possible for this grid or quadrature");
     return FS_EARG;
   }
@@ -1345,7 +1797,8 @@ static int dom_prepare(DomCtx* D) {
 
 int dom_set_mode(void* h, int mode, int cluster_ctas) {
   DomCtx* D = (DomCtx*)h;
-  if (mode < 0 || mode > 6 || cluster_ctas < 0 || cluster_ctas > 16) return FS_EARG;
+  if (mode < 0 || mode > 7 || cluster_ctas < 0 || cluster_ctas > (mode == 7 ? 64 : 16))
+    return FS_EARG;
   if (D->mode != 0) {
     fs_set_error("sweep mode must be set before the first solve or intensity load");
     return FS_EARG;
@@ -1377,7 +1830,7 @@ int dom_load_intensity(void* h, const double* I_full, cudaStream_t st) {
     k_dom_extract_wrap<float><<<blocks_for(tot, 256), 256, 0, st>>>(g, D->M, D->oy, I_full,
                                                                    D->wrap32);
     fs_count_launch();
-  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
+  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7) {
     const int64_t tot = (int64_t)D->M * g.nz * g.nx;
     k_dom_extract_wrap<double><<<blocks_for(tot, 256), 256, 0, st>>>(g, D->M, D->oy, I_full,
                                                                     D->wrap);
@@ -1404,7 +1857,7 @@ int dom_get_wrap(void* h, double* dst, cudaStream_t st) {
   if (D->fp32) {
     k_f32_to_f64<<<blocks_for(tot, 256), 256, 0, st>>>(tot, D->wrap32, dst);
     fs_count_launch();
-  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
+  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7) {
     cudaMemcpyAsync(dst, D->wrap, sizeof(double) * tot, cudaMemcpyDeviceToDevice, st);
   } else {
     k_dom_extract_wrap<double><<<blocks_for(tot, 256), 256, 0, st>>>(D->g, D->M, D->oy, D->I,
@@ -1422,7 +1875,7 @@ int dom_set_wrap(void* h, const double* src, cudaStream_t st) {
   if (D->fp32) {
     k_f64_to_f32<<<blocks_for(tot, 256), 256, 0, st>>>(tot, src, D->wrap32);
     fs_count_launch();
-  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6) {
+  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7) {
     cudaMemcpyAsync(D->wrap, src, sizeof(double) * tot, cudaMemcpyDeviceToDevice, st);
   } else {
     k_dom_scatter_wrap<<<blocks_for(tot, 256), 256, 0, st>>>(D->g, D->M, D->oy, src, D->I);
@@ -1489,6 +1942,33 @@ static int launch_octant_sweep(DomCtx* D, const OctArgs& a, cudaStream_t st) {
   return e == cudaSuccess ? FS_OK : FS_ECUDA;
 }
 
+template <typename T>
+static int launch_st_sweep(DomCtx* D, StArgs<T> a, cudaStream_t st) {
+  // every word of the ring back to "sign bit set" and every read count to -1
+  if (cudaMemsetAsync(D->st_ring, 0xff, D->st_ring_bytes, st) != cudaSuccess) return FS_ECUDA;
+  a.ring = (typename WordOf<T>::type*)D->st_ring;
+  a.consumed = (int*)((char*)D->st_ring + D->st_cnt_offset);
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.gridDim = dim3(8 * D->cl_C);
+  cfg.blockDim = dim3(D->cl_threads);
+  cfg.dynamicSmemBytes = D->cl_smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaError_t e;
+  switch (D->Mo) {
+    case 3: e = cudaLaunchKernelEx(&cfg, k_dom_octant_st<T, 3>, D->g, a); break;
+    case 6: e = cudaLaunchKernelEx(&cfg, k_dom_octant_st<T, 6>, D->g, a); break;
+    case 10: e = cudaLaunchKernelEx(&cfg, k_dom_octant_st<T, 10>, D->g, a); break;
+    default: e = cudaErrorInvalidValue;
+  }
+  fs_count_launch();
+  return e == cudaSuccess ? FS_OK : FS_ECUDA;
+}
+
 template <int PPT, int TPB>
 static void ord_launch(DomCtx* D, const OrdArgs& oa, size_t smem, cudaStream_t st) {
   cudaFuncSetAttribute(k_dom_ord<PPT, TPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1525,7 +2005,7 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
   const int M = D->M;
-  const bool octp = D->mode == 1 || D->mode == 4 || D->mode == 6;
+  const bool octp = D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7;
   const double Tamb4 = pow(T_amb, 4.0);
   k_dom_setup<<<blocks_for(N, 256), 256, 0, st>>>(g, Ts, Tg, as, om, YH, rho, Mloc, sigma, Tamb4,
                                                   D->kgmax, D->ks, D->kg, D->ksafe, D->B,
@@ -1565,7 +2045,26 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   for (it = 0; it < D->max_iter; ++it) {
     std::swap(D->G, D->Gp);
     if (D->timing) cudaEventRecord(D->ev0[it], st);
-    if (D->fp32) {
+    if (D->mode == 7) {
+      if (D->fp32) {
+        StArgs<float> sa{};
+        sa.kb = D->kb32; sa.Goct = D->Goct32; sa.Qoct = D->Qoct32; sa.wrap = D->wrap32;
+        sa.I_amb = (float)I_amb;
+        sa.ox = D->ox; sa.oy = D->oy; sa.oz = D->oz; sa.w = D->w; sa.Ig = D->Ig_out;
+        sa.C = D->cl_C; sa.rows = D->cl_rows; sa.periodic = 1; sa.lg_ring = D->cl_lg_ring;
+        sa.down_slots = oa.down_slots; sa.err = oa.err;
+        rc = launch_st_sweep(D, sa, st);
+      } else {
+        StArgs<double> sa{};
+        sa.kb = D->kb; sa.Goct = D->Goct; sa.Qoct = D->Qoct; sa.wrap = D->wrap;
+        sa.I_amb = I_amb;
+        sa.ox = D->ox; sa.oy = D->oy; sa.oz = D->oz; sa.w = D->w; sa.Ig = D->Ig_out;
+        sa.C = D->cl_C; sa.rows = D->cl_rows; sa.periodic = 1; sa.lg_ring = D->cl_lg_ring;
+        sa.down_slots = oa.down_slots; sa.err = oa.err;
+        rc = launch_st_sweep(D, sa, st);
+      }
+      if (rc != FS_OK) return rc;
+    } else if (D->fp32) {
       OctArgs32 o3{};
       o3.kb = D->kb32; o3.ox = D->ox; o3.oy = D->oy; o3.oz = D->oz; o3.w = D->w;
       o3.Ig = D->Ig_out; o3.Goct = D->Goct32; o3.Qoct = D->Qoct32; o3.wrap = D->wrap32;

@@ -89,14 +89,15 @@ class Tier3Solver:
     ``form="plain"`` is FP64 throughout.  ``form="mixed"`` runs the DOM sweep
     and the multigrid preconditioner in FP32; the state, every other kernel,
     the CG (operator, residuals, dot products), the divergence test and all
-    reductions stay FP64."""
+    reductions stay FP64.  ``dom_sweep`` forces a DOM sweep path
+    (``fs_dom_set_sweep_mode``; 0 picks automatically)."""
 
     FIELDS = ("rho", "u", "v", "w", "T_g", "Y_fuel", "Y_O2", "Y_H2O", "T_s", "alpha_s",
               "k_turb", "eps_turb", "nu_t", "phi")
 
     def __init__(self, case: dict, device="cuda", projection_cg_rtol: float | None = None,
                  proj_maxiter: int = 200, mg_sweeps: int | None = None, form: str = "plain",
-                 overlap_dom: bool = True):
+                 overlap_dom: bool = True, dom_sweep: int = 0):
         self.lib = _lib.lib()
         self.dev = torch.device(device)
         if self.dev.type == "cuda" and self.dev.index is None:
@@ -191,6 +192,9 @@ class Tier3Solver:
             self._pool = ThreadPoolExecutor(max_workers=1, thread_name_prefix="dom")
         if form == "mixed":
             check(self.lib.fs_dom_set_precision(self.dom, 1), "fs_dom_set_precision")
+        if dom_sweep:
+            check(self.lib.fs_dom_set_sweep_mode(self.dom, int(dom_sweep), 0),
+                  "fs_dom_set_sweep_mode")
         # clock
         self.t = 0.0
         self.dt = float(self.p["dt0"])

@@ -237,16 +237,21 @@ double* fs_dom_intensity(void* handle);
  * 2 one CTA per ordinate, 3 hyperplane launches, 4 octant clusters with a
  * cluster barrier per hyperplane, 5 one CTA per ordinate with per-thread
  * pencils and batched loads, 6 as 4 with two clusters per octant (half the
- * ordinates each, two CTAs per SM); cluster_ctas 0 = automatic, else CTAs per
- * octant (1..16).  Only before the first solve or intensity load.  Path 1
- * bounds its waits: a stalled hand-off returns FS_ETIMEOUT. */
+ * ordinates each, two CTAs per SM), 7 as 4 without clusters: a cooperative
+ * launch of self-timed CTAs that hand their last row on through a ring in
+ * global memory (needs all 8*C CTAs resident at once, one per SM; no other
+ * path-7 sweep may run on the device at the same time); cluster_ctas 0 =
+ * automatic, else CTAs per octant (1..16; up to 64 for path 7).  Only before
+ * the first solve or intensity load.  Paths 1 and 7 bound their waits: a
+ * stalled hand-off returns FS_ETIMEOUT. */
 int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
 /* The path in use (0 before the first solve or intensity load). */
 int fs_dom_sweep_mode(void* handle);
-/* fp32 = 1: the mixed-precision form of the sweep (path 4 with kappa,
- * kappa*B, intensities and octant partials in FP32; G, the ground exchange
- * and all outputs in FP64).  No counterpart in the reference, which is FP64
- * throughout.  Only before the first solve or intensity load. */
+/* fp32 = 1: the mixed-precision form of the sweep (path 4 or 7 with kappa,
+ * kappa*B, intensities and octant partials in FP32 and the quotient of
+ * __fdividef, about 2 ulp; G, the ground exchange and all outputs in FP64).
+ * No counterpart in the reference, which is FP64 throughout.  Only before the
+ * first solve or intensity load. */
 int fs_dom_set_precision(void* handle, int fp32);
 /* Load the persistent intensity state from a full device field
  * (M x Nz x Ny x Nx), as a reference I_set would seed the next solve. */

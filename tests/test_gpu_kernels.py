@@ -249,10 +249,11 @@ def test_k_epsilon(vectors):
         assert rel_l2(host(nuo), c["nu_t_out"]) <= LIBM, name
 
 
-@pytest.mark.parametrize("mode", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("mode", [1, 2, 3, 4, 5, 6, 7])
 def test_dom(vectors, mode):
     """Every sweep path (pipelined octant clusters, CTA per ordinate, hyperplane
-    launches, octant clusters with cluster barriers)."""
+    launches, octant clusters with cluster barriers, self-timed octant
+    pipeline)."""
     from firewebapp_b200.quadrature import level_symmetric
     om, wq = level_symmetric(4)
     for name in vectors.cases("dom"):
@@ -282,7 +283,8 @@ def test_dom(vectors, mode):
             lib().fs_dom_destroy(h)
 
 
-def test_dom_fp32_form(vectors):
+@pytest.mark.parametrize("mode", [4, 7])
+def test_dom_fp32_form(vectors, mode):
     """The mixed-precision sweep (FP32 intensities) against the FP64 golden
     vectors: relative error at FP32 level."""
     from firewebapp_b200.quadrature import level_symmetric
@@ -296,6 +298,7 @@ def test_dom_fp32_form(vectors):
              dbl_array(om[:, 2]), dbl_array(wq), 0.5, C.byref(h))
         try:
             call("fs_dom_set_precision", h, 1)
+            call("fs_dom_set_sweep_mode", h, mode, 0)
             Ts, Tg, a, omg, M = (dev(c[x]) for x in ("T_s", "T_g", "alpha_s", "omega_comb",
                                                      "bed_moisture"))
             YH = dev(c["Y_H2O"]) if "Y_H2O" in c else None
@@ -310,6 +313,57 @@ def test_dom_fp32_form(vectors):
                 assert rel_l2(host(got), c[key]) <= 1e-5, (name, key)
         finally:
             lib().fs_dom_destroy(h)
+
+
+def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2):
+    """q_rad_solid, q_rad_gas, q_in_soil after each of ``calls`` solves of an
+    S8 DOM on seeded random fields (the y-inflow rows persist between calls)."""
+    from firewebapp_b200.quadrature import level_symmetric
+    om, wq = level_symmetric(8)
+    rng = np.random.default_rng(seed)
+    dz = np.concatenate([np.full(nz // 3, 0.05), np.linspace(0.05, 0.4, nz - nz // 3)])
+    g = Grid(nz, ny, nx, 0.5, 0.5, dz)
+    h = C.c_void_p()
+    call("fs_dom_create", g.ref, om.shape[0], dbl_array(om[:, 0]), dbl_array(om[:, 1]),
+         dbl_array(om[:, 2]), dbl_array(wq), 0.5, C.byref(h))
+    out = []
+    try:
+        if fp32:
+            call("fs_dom_set_precision", h, 1)
+        call("fs_dom_set_sweep_mode", h, mode, 0)
+        shape = (nz, ny, nx)
+        for it in range(calls):
+            Ts = dev(300.0 + 900.0 * rng.random(shape) ** 4)
+            Tg = dev(300.0 + 1500.0 * rng.random(shape) ** 6)
+            a = dev(np.where(rng.random(shape) < 0.3, 0.002 * rng.random(shape), 0.0))
+            omg = dev(np.where(rng.random(shape) < 0.05, 0.5 * rng.random(shape), 0.0))
+            M = dev(0.05 + 0.1 * rng.random(shape))
+            YH = dev(0.05 * rng.random(shape))
+            rho = dev(0.8 + 0.4 * rng.random(shape))
+            Tsoil = dev(300.0 + 50.0 * rng.random((ny, nx)))
+            qs, qg = torch.zeros_like(Ts), torch.zeros_like(Ts)
+            qsoil = torch.zeros((ny, nx), dtype=torch.float64, device="cuda")
+            call("fs_dom_solve", h, ptr(Ts), ptr(Tg), ptr(a), ptr(omg), 5000.0, 300.0,
+                 ptr(Tsoil), ptr(YH), ptr(rho), ptr(M), ptr(qs), ptr(qg), ptr(qsoil), stream())
+            out.append((host(qs), host(qg), host(qsoil), lib().fs_dom_iterations(h)))
+        assert lib().fs_dom_sweep_mode(h) == mode
+    finally:
+        lib().fs_dom_destroy(h)
+    return out
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+@pytest.mark.parametrize("dims", [(29, 40, 48), (13, 7, 21), (60, 120, 24)])
+def test_dom_self_timed_equals_barrier_path(fp32, dims):
+    """The self-timed octant pipeline (path 7) reproduces the cluster-barrier
+    sweep (path 4) bit for bit, over two solves, in both precisions, on grids
+    with full and partial last CTAs."""
+    nz, ny, nx = dims
+    a = _dom_solves(4, fp32, nz, ny, nx, seed=5)
+    b = _dom_solves(7, fp32, nz, ny, nx, seed=5)
+    for (qa, ga, sa, ia), (qb, gb, sb, ib) in zip(a, b):
+        assert ia == ib
+        assert np.array_equal(qa, qb) and np.array_equal(ga, gb) and np.array_equal(sa, sb)
 
 
 def _segments(x, y, z, dx, dy, z_face, nz, ny, nx, alive):
