@@ -56,7 +56,7 @@ struct DomCtx {
   int fp32;                   // single-precision sweep (path 4 only)
   float2* kb32;
   float *Goct32, *Qoct32, *wrap32;
-  int Mo, cl_C, cl_rows, cl_threads, cl_lg_ring;
+  int Mo, cl_C, cl_rows, cl_threads, cl_lg_ring, cl_ppt, cl_active;
   void* st_ring;              // path 7 hand-off ring, then the read counters
   size_t st_ring_bytes;       // ring and counters (filled with 0xff before each sweep)
   size_t st_cnt_offset;
@@ -1417,6 +1417,288 @@ static const void* octant_st_ptr(bool fp32, int Mo) {
   }
 }
 
+// ---- path 8: octant clusters sized to run all eight octants at once ----------
+// Path 4's lockstep scheme (a cluster per octant, one cluster barrier per
+// hyperplane, the upstream CTA's last row read through distributed shared
+// memory), with the inputs prefetched into shared memory by cp.async and the
+// y-wrap rows staged in chunks as in path 7, and with PPT pencils per thread
+// so that a cluster can take more k' rows.  A thread-block cluster must fit
+// in one GPC: with one CTA per SM at most 7 clusters of 11-16 CTAs are
+// resident on a B200, but 11 of 10 and 15 of 9, so eight octant clusters of
+// up to 10 CTAs run in one wave instead of two.  Every cell's arithmetic is
+// that of path 4.
+struct ClArgs {
+  const void* kb;
+  const double *ox, *oy, *oz, *w;
+  const double* Ig;
+  void *Goct, *Qoct, *wrap;
+  double I_amb;
+  int C, rows, periodic;
+  unsigned down_slots;
+};
+// The hyperplane buffers carry a ghost row below the CTA's first row and a
+// ghost column left of every row (rows+1 by ny+1 per ordinate): the first
+// row's threads put the z-inflow (upstream CTA, ground or ambient) into the
+// ghost row and the first column's threads the y-inflow into the ghost
+// column, and a pencil's own slot holds the ambient intensity until its
+// first cell, so every cell reads its three upwind neighbours the same way.
+#define CL_CHUNK 16
+struct ClLayout {
+  size_t kab, ig, win, wout, buf0, buf1, izt, cix, total;
+};
+__host__ __device__ inline ClLayout cl_layout(int tsize, int Mo, int rows, int ny, int nz) {
+  ClLayout L;
+  const size_t S = (size_t)rows * ny;
+  const size_t P = (size_t)(rows + 1) * (ny + 1);
+  const size_t chunk = (size_t)2 * Mo * rows * CL_CHUNK * tsize;
+  size_t o = 0;
+  L.kab = o; o = st_up16(o + (size_t)OCT_AHEAD * S * 2 * tsize);
+  L.ig = o; o = st_up16(o + (size_t)OCT_AHEAD * ny * sizeof(double));
+  L.win = o; o = st_up16(o + chunk);
+  L.wout = o; o = st_up16(o + chunk);
+  L.buf0 = o; o = st_up16(o + (size_t)Mo * P * tsize);
+  L.buf1 = o; o = st_up16(o + (size_t)Mo * P * tsize);
+  L.izt = o; o = st_up16(o + (size_t)Mo * nz * tsize);
+  L.cix = o; o = st_up16(o + 4 * (size_t)Mo * tsize);
+  L.total = o;
+  return L;
+}
+
+template <typename T, int MO, int PPT>
+__global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_cl(GridDev g, ClArgs a) {
+  using T2 = typename Vec2Of<T>::type;
+  extern __shared__ __align__(16) unsigned char shraw[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int C = a.C;
+  const int rank = (int)cl.block_rank();
+  const int oct = blockIdx.x / C;
+  const int n0 = oct * MO;
+  const int rows = a.rows;
+  const int S = rows * ny;
+  const int RS = ny + 1;           // padded row stride
+  const int P = (rows + 1) * RS;   // padded plane per ordinate
+  const ClLayout L = cl_layout((int)sizeof(T), MO, rows, ny, nz);
+  T2* kab_ring = (T2*)(shraw + L.kab);
+  double* ig_ring = (double*)(shraw + L.ig);
+  T* win = (T*)(shraw + L.win);
+  T* wout = (T*)(shraw + L.wout);
+  T* buf0 = (T*)(shraw + L.buf0);
+  T* buf1 = (T*)(shraw + L.buf1);
+  T* izt = (T*)(shraw + L.izt);
+  T* cix = (T*)(shraw + L.cix);
+  T* ciy = cix + MO;
+  T* cw = ciy + MO;
+  T* cwm = cw + MO;
+  const T2* kb = (const T2*)a.kb;
+  T* Goct = (T*)a.Goct;
+  T* Qoct = (T*)a.Qoct;
+  T* wrap = (T*)a.wrap;
+  const T I_amb = (T)a.I_amb;
+  const int nplanes = nx + ny + nz - 2;
+  for (int t = threadIdx.x; t < MO * nz; t += blockDim.x) {
+    const int m = t / nz, k = t - m * nz;
+    izt[t] = (T)(fabs(a.oz[n0 + m]) / g.dz[k]);
+  }
+  for (int m = threadIdx.x; m < MO; m += blockDim.x) {
+    cix[m] = (T)(fabs(a.ox[n0 + m]) / g.dx);
+    ciy[m] = (T)(fabs(a.oy[n0 + m]) / g.dy);
+    cw[m] = (T)a.w[n0 + m];
+    cwm[m] = (T)(a.w[n0 + m] * fabs(a.oz[n0 + m]));
+  }
+  for (int t = threadIdx.x; t < MO * P; t += blockDim.x) {
+    buf0[t] = I_amb;
+    buf1[t] = I_amb;
+  }
+  const bool fx = a.ox[n0] >= 0.0, fy = a.oy[n0] >= 0.0, fz = a.oz[n0] >= 0.0;
+  const int r0 = rank * rows;
+  const int nrows = min(rows, nz - r0);
+  const int npen = nrows > 0 ? nrows * ny : 0;
+  const int64_t N = ncells_dev(g);
+  const int64_t n2 = (int64_t)nx * ny;
+  const int slot_bits = (int)((a.down_slots >> (4 * oct)) & 15u);
+  const int slot = slot_bits == 15 ? -1 : slot_bits;
+  T* Go = Goct + (int64_t)oct * N;
+  const int64_t wstride = (int64_t)nz * nx;
+  T* wrap0 = wrap + (int64_t)n0 * wstride;
+  const bool periodic = a.periodic != 0;
+  const int TT = blockDim.x;
+  const uint64_t keep = l2_policy_evict_last();
+  const int chunk_elems = MO * rows * CL_CHUNK;
+  auto load_inflow = [&](int c) {
+    T* dst = win + (size_t)(c & 1) * chunk_elems;
+    for (int e = threadIdx.x; e < chunk_elems; e += TT) {
+      const int t = e % CL_CHUNK, rm = e / CL_CHUNK;
+      const int rl = rm % rows, m = rm / rows;
+      const int ip = c * CL_CHUNK + t - (r0 + rl);
+      if (rl < nrows && ip >= 0 && ip < nx) {
+        const int kk = fz ? r0 + rl : nz - 1 - (r0 + rl);
+        const int i = fx ? ip : nx - 1 - ip;
+        cp_async_val(&dst[e], &wrap0[m * wstride + (int64_t)kk * nx + i]);
+      }
+    }
+  };
+  auto store_outflow = [&](int c) {
+    const T* src = wout + (size_t)(c & 1) * chunk_elems;
+    for (int e = threadIdx.x; e < chunk_elems; e += TT) {
+      const int t = e % CL_CHUNK, rm = e / CL_CHUNK;
+      const int rl = rm % rows, m = rm / rows;
+      const int ip = c * CL_CHUNK + t - (ny - 1) - (r0 + rl);
+      if (rl < nrows && ip >= 0 && ip < nx) {
+        const int kk = fz ? r0 + rl : nz - 1 - (r0 + rl);
+        const int i = fx ? ip : nx - 1 - ip;
+        wrap0[m * wstride + (int64_t)kk * nx + i] = src[e];
+      }
+    }
+  };
+  // per-pencil constants: pencil index, row and column, global row base, roles
+  int pq[PPT], pjp[PPT], pkp[PPT], pk[PPT], pqi[PPT];
+  int64_t prb[PPT];
+  unsigned prole[PPT];  // 1 has, 2 first row, 4 first column, 8 last column, 16 ground flux, 32 ground inflow
+#pragma unroll
+  for (int pp = 0; pp < PPT; ++pp) {
+    const int q = threadIdx.x + pp * TT;
+    const bool has = q < npen;
+    const int kl = has ? q / ny : 0;
+    const int jp = has ? q - kl * ny : 0;
+    const int kp = r0 + kl;
+    const int k = fz ? kp : nz - 1 - kp;
+    const int j = fy ? jp : ny - 1 - jp;
+    pq[pp] = q; pjp[pp] = jp; pkp[pp] = kp; pk[pp] = k;
+    pqi[pp] = (kl + 1) * RS + jp + 1;
+    prb[pp] = ((int64_t)k * ny + j) * nx;
+    prole[pp] = (has ? 1u : 0u) | (has && kl == 0 ? 2u : 0u) | (has && jp == 0 ? 4u : 0u) |
+                (has && jp == ny - 1 ? 8u : 0u) | (has && !fz && k == 0 && slot >= 0 ? 16u : 0u) |
+                (has && fz && kp == 0 ? 32u : 0u);
+  }
+  auto prefetch = [&](int d) {
+#pragma unroll
+    for (int pp = 0; pp < PPT; ++pp) {
+      const int ip = d - pjp[pp] - pkp[pp];
+      if ((prole[pp] & 1u) && ip >= 0 && ip < nx) {
+        const int i = fx ? ip : nx - 1 - ip;
+        const int sl = d % OCT_AHEAD;
+        cp_async_kb(&kab_ring[(size_t)sl * S + pq[pp]], &kb[prb[pp] + i], keep);
+        if (prole[pp] & 32u) {
+          const int j = fy ? pjp[pp] : ny - 1 - pjp[pp];
+          cp_async8(&ig_ring[(size_t)sl * ny + pjp[pp]], &a.Ig[(int64_t)j * nx + i]);
+        }
+      }
+    }
+    if (periodic && (d + 1) % CL_CHUNK == 0 && d + 1 < nplanes) load_inflow((d + 1) / CL_CHUNK);
+    cp_async_commit();
+  };
+  if (periodic) load_inflow(0);
+  for (int d = 0; d < OCT_AHEAD - 1; ++d) prefetch(d);
+  cp_async_wait<OCT_AHEAD - 2>();  // group 0, which holds chunk 0 of the inflow rows
+  // the first cluster barrier also publishes the ambient-filled buffers
+  cluster_arrive_release();
+  // the upstream CTA's shared memory, for the row below this CTA's first row
+  const T* up0 = rank > 0 ? cl.map_shared_rank(buf0, rank - 1) : nullptr;
+  const T* up1 = rank > 0 ? cl.map_shared_rank(buf1, rank - 1) : nullptr;
+  for (int d = 0; d < nplanes; ++d) {
+    prefetch(d + OCT_AHEAD - 1);  // an empty group past the last plane
+    T* cur = (d & 1) ? buf1 : buf0;
+    T* prev = (d & 1) ? buf0 : buf1;
+    const T* uprev = (d & 1) ? up0 : up1;
+    cp_async_wait<OCT_AHEAD - 1>();  // this plane's group has landed
+    cluster_wait_acquire();
+    // a finished chunk of outflow rows leaves for global memory
+    if (periodic && d > 0 && d % CL_CHUNK == 0) store_outflow(d / CL_CHUNK - 1);
+    const int sl = d % OCT_AHEAD;
+    const int ch = (d / CL_CHUNK) & 1, tt = d % CL_CHUNK;
+    T gsv[PPT], qsv[PPT];
+#pragma unroll
+    for (int pp = 0; pp < PPT; ++pp) {
+      const int jp = pjp[pp], kp = pkp[pp], qi = pqi[pp];
+      const int ip = d - jp - kp;
+      const bool act = (prole[pp] & 1u) && ip >= 0 && ip < nx;
+      T gs = (T)0, qs = (T)0;
+      if (act) {
+        // inflow ghosts of this cell: z below the first row, y left of the first column
+        if (prole[pp] & 2u) {
+#pragma unroll
+          for (int m = 0; m < MO; ++m) {
+            T z;
+            if (kp > 0) z = uprev[(size_t)m * P + (size_t)rows * RS + jp + 1];
+            else z = fz ? (T)ig_ring[(size_t)sl * ny + jp] : I_amb;
+            prev[(size_t)m * P + jp + 1] = z;
+          }
+        }
+        if (prole[pp] & 4u) {
+          const int kl = kp - r0;
+#pragma unroll
+          for (int m = 0; m < MO; ++m)
+            prev[(size_t)m * P + (kl + 1) * RS] =
+                periodic ? win[((size_t)(ch * MO + m) * rows + kl) * CL_CHUNK + tt] : I_amb;
+        }
+        const T2 kab = kab_ring[(size_t)sl * S + pq[pp]];
+        const bool ground_out = (prole[pp] & 16u) != 0;
+        const int k = pk[pp];
+#pragma unroll
+        for (int m = 0; m < MO; ++m) {
+          const T* pm = prev + (size_t)m * P + qi;
+          const T Ix = pm[0], Iy = pm[-1], Iz = pm[-RS];
+          const T ix = cix[m], iy = ciy[m], iz = izt[m * nz + k];
+          const T num = kab.y + ix * Ix + iy * Iy + iz * Iz;
+          const T den = kab.x + ix + iy + iz;
+          const T v = sweep_div(num, den);
+          cur[(size_t)m * P + qi] = v;
+          gs = gs + cw[m] * v;
+          if (ground_out) qs = qs + cwm[m] * v;
+        }
+        if (periodic && (prole[pp] & 8u)) {
+          const int kl = kp - r0;
+#pragma unroll
+          for (int m = 0; m < MO; ++m)
+            wout[((size_t)(ch * MO + m) * rows + kl) * CL_CHUNK + tt] = cur[(size_t)m * P + qi];
+        }
+      } else if (prole[pp] & 1u) {
+        // before its first cell a pencil's x-inflow is the ambient intensity
+#pragma unroll
+        for (int m = 0; m < MO; ++m) cur[(size_t)m * P + qi] = I_amb;
+      }
+      gsv[pp] = gs;
+      qsv[pp] = qs;
+    }
+    cluster_arrive_release();
+#pragma unroll
+    for (int pp = 0; pp < PPT; ++pp) {
+      const int ip = d - pjp[pp] - pkp[pp];
+      if ((prole[pp] & 1u) && ip >= 0 && ip < nx) {
+        const int i = fx ? ip : nx - 1 - ip;
+        st_cs(Go + prb[pp] + i, gsv[pp]);
+        if (prole[pp] & 16u) {
+          const int j = fy ? pjp[pp] : ny - 1 - pjp[pp];
+          Qoct[(int64_t)slot * n2 + (int64_t)j * nx + i] = qsv[pp];
+        }
+      }
+    }
+  }
+  cluster_wait_acquire();
+  if (periodic) store_outflow((nplanes - 1) / CL_CHUNK);
+  cp_async_wait<0>();
+}
+
+static const void* octant_cl_ptr(bool fp32, int Mo, int ppt) {
+#define CLP(T, M, P) (const void*)k_dom_octant_cl<T, M, P>
+  if (ppt == 1) {
+    switch (Mo) {
+      case 3: return fp32 ? CLP(float, 3, 1) : CLP(double, 3, 1);
+      case 6: return fp32 ? CLP(float, 6, 1) : CLP(double, 6, 1);
+      case 10: return fp32 ? CLP(float, 10, 1) : CLP(double, 10, 1);
+    }
+  } else if (ppt == 2) {
+    switch (Mo) {
+      case 3: return fp32 ? CLP(float, 3, 2) : CLP(double, 3, 2);
+      case 6: return fp32 ? CLP(float, 6, 2) : CLP(double, 6, 2);
+      case 10: return fp32 ? CLP(float, 10, 2) : CLP(double, 10, 2);
+    }
+  }
+#undef CLP
+  return nullptr;
+}
+
 template <int MO, int MINB = 1>
 static cudaError_t launch_octant_kernel(const GridDev& g, const OctArgs& a, cudaLaunchConfig_t* cfg) {
   return cudaLaunchKernelEx(cfg, k_dom_octant<MO, MINB>, g, a);
@@ -1564,6 +1846,7 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1;
   D->fp32 = 0; D->kb32 = nullptr; D->Goct32 = nullptr; D->Qoct32 = nullptr; D->wrap32 = nullptr;
   D->st_ring = nullptr; D->st_ring_bytes = 0; D->st_cnt_offset = 0;
+  D->cl_ppt = 1; D->cl_active = 0;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemset(D->G, 0, sizeof(double) * N);
   cudaMalloc(&D->ks, sizeof(double) * N); cudaMalloc(&D->kg, sizeof(double) * N);
@@ -1718,6 +2001,56 @@ static bool plan_st(DomCtx* D, int force_C) {
   return false;
 }
 
+// Launch shape of path 8: the largest cluster size C (rows of k' per CTA,
+// pencils per thread 1 or 2, one CTA per SM) for which eight clusters are
+// resident at once; else the largest C that launches at all.
+static bool plan_cl(DomCtx* D, int force_C) {
+  const GridDev& g = D->g;
+  const int Mo = D->M / 8;
+  const int tsize = D->fp32 ? (int)sizeof(float) : (int)sizeof(double);
+  int dev = 0, optin = 0, smem_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  int best_active = 0;
+  for (int C = 16; C >= 1; --C) {
+    if (force_C > 0 && C != force_C) continue;
+    const int rows = (g.nz + C - 1) / C;
+    if ((g.nz + rows - 1) / rows != C) continue;
+    const int ppt = (rows * g.ny + OCT_MAX_THREADS - 1) / OCT_MAX_THREADS;
+    if (ppt > 2) continue;
+    const int threads = ((rows * g.ny + ppt - 1) / ppt + 31) / 32 * 32;
+    const void* fn = octant_cl_ptr(D->fp32 != 0, Mo, ppt);
+    if (!fn) continue;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    const size_t need = cl_layout(tsize, Mo, rows, g.ny, g.nz).total;
+    const size_t pad = (size_t)smem_sm / 2 + 1024;  // no two CTAs on one SM
+    const size_t smem = need > pad ? need : pad;
+    if (smem > (size_t)optin) continue;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(8 * C); cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem; cfg.attrs = at; cfg.numAttrs = 1;
+    int active = 0;
+    if (cudaOccupancyMaxActiveClusters(&active, fn, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      active = 0;
+    }
+    if (active < 1) continue;
+    const int score = active >= 8 ? 8 : active;
+    if (score > best_active) {
+      best_active = score;
+      D->cl_C = C; D->cl_rows = rows; D->cl_threads = threads; D->cl_smem = smem;
+      D->cl_ppt = ppt;
+    }
+  }
+  D->cl_active = best_active;
+  return best_active > 0;
+}
+
 static void alloc_st_ring(DomCtx* D) {
   const int tsize = D->fp32 ? (int)sizeof(float) : (int)sizeof(double);
   const size_t bounds = (size_t)8 * (D->cl_C - 1);
@@ -1732,11 +2065,14 @@ static int dom_prepare(DomCtx* D) {
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
   const int want = D->mode_req;
+  // auto: path 8 when all eight octant clusters can be resident at once, else path 4
+  const bool auto8 = want == 0 && octant_grouping(D) && plan_cl(D, D->force_C) && D->cl_active >= 8;
   if (D->fp32) {
-    const int kind = want == 7 ? 7 : 4;
-    if ((want != 0 && want != 4 && want != 7) || !octant_grouping(D) ||
-        !(kind == 7 ? plan_st(D, D->force_C) : plan_clusters(D, D->force_C, kind))) {
-      fs_set_error("single-precision sweep needs an octant-cluster path (4 or 7) on this grid");
+    const int kind = auto8 ? 8 : ((want == 7 || want == 8) ? want : 4);
+    if ((want != 0 && want != 4 && want != 7 && want != 8) || !octant_grouping(D) ||
+        !(kind == 7 ? plan_st(D, D->force_C)
+                    : (kind == 8 ? plan_cl(D, D->force_C) : plan_clusters(D, D->force_C, kind)))) {
+      fs_set_error("single-precision sweep needs an octant path (4, 7 or 8) on this grid");
       return FS_EARG;
     }
     D->mode = kind;
@@ -1754,10 +2090,12 @@ static int dom_prepare(DomCtx* D) {
   }
   // auto picks the cluster-barrier sweep (path 4), measured faster than path 1
   const int groups = (want == 6 && D->M % 16 == 0) ? 2 : 1;
-  const int kind = (want == 1 || want == 7) ? want : 4;
-  if ((want == 0 || want == 1 || want == 4 || want == 6 || want == 7) && octant_grouping(D) &&
-      (kind == 7 ? plan_st(D, D->force_C) : plan_clusters(D, D->force_C, kind, groups))) {
-    D->mode = want == 1 ? 1 : (want == 6 ? 6 : (want == 7 ? 7 : 4));
+  const int kind = auto8 ? 8 : ((want == 1 || want == 7 || want == 8) ? want : 4);
+  if ((want == 0 || want == 1 || want == 4 || want == 6 || want == 7 || want == 8) &&
+      octant_grouping(D) &&
+      (kind == 7 ? plan_st(D, D->force_C)
+                 : (kind == 8 ? plan_cl(D, D->force_C) : plan_clusters(D, D->force_C, kind, groups)))) {
+    D->mode = kind == 8 ? 8 : (want == 1 ? 1 : (want == 6 ? 6 : (want == 7 ? 7 : 4)));
     D->groups = groups;
     D->Mo = D->M / 8;
     int slot = 0;
@@ -1770,7 +2108,7 @@ static int dom_prepare(DomCtx* D) {
     if (D->mode == 7) alloc_st_ring(D);
     return cuda_status();
   }
-  if (want == 1 || want == 4 || want == 6 || want == 7) {
+  if (want == 1 || want == 4 || want == 6 || want == 7 || want == 8) {
     fs_set_error("octant-cluster sweep not possible for this grid or quadrature");
     return FS_EARG;
   }
@@ -1797,7 +2135,7 @@ static int dom_prepare(DomCtx* D) {
 
 int dom_set_mode(void* h, int mode, int cluster_ctas) {
   DomCtx* D = (DomCtx*)h;
-  if (mode < 0 || mode > 7 || cluster_ctas < 0 || cluster_ctas > (mode == 7 ? 64 : 16))
+  if (mode < 0 || mode > 8 || cluster_ctas < 0 || cluster_ctas > (mode == 7 ? 64 : 16))
     return FS_EARG;
   if (D->mode != 0) {
     fs_set_error("sweep mode must be set before the first solve or intensity load");
@@ -1830,7 +2168,7 @@ int dom_load_intensity(void* h, const double* I_full, cudaStream_t st) {
     k_dom_extract_wrap<float><<<blocks_for(tot, 256), 256, 0, st>>>(g, D->M, D->oy, I_full,
                                                                    D->wrap32);
     fs_count_launch();
-  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7) {
+  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7 || D->mode == 8) {
     const int64_t tot = (int64_t)D->M * g.nz * g.nx;
     k_dom_extract_wrap<double><<<blocks_for(tot, 256), 256, 0, st>>>(g, D->M, D->oy, I_full,
                                                                     D->wrap);
@@ -1857,7 +2195,7 @@ int dom_get_wrap(void* h, double* dst, cudaStream_t st) {
   if (D->fp32) {
     k_f32_to_f64<<<blocks_for(tot, 256), 256, 0, st>>>(tot, D->wrap32, dst);
     fs_count_launch();
-  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7) {
+  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7 || D->mode == 8) {
     cudaMemcpyAsync(dst, D->wrap, sizeof(double) * tot, cudaMemcpyDeviceToDevice, st);
   } else {
     k_dom_extract_wrap<double><<<blocks_for(tot, 256), 256, 0, st>>>(D->g, D->M, D->oy, D->I,
@@ -1875,7 +2213,7 @@ int dom_set_wrap(void* h, const double* src, cudaStream_t st) {
   if (D->fp32) {
     k_f64_to_f32<<<blocks_for(tot, 256), 256, 0, st>>>(tot, src, D->wrap32);
     fs_count_launch();
-  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7) {
+  } else if (D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7 || D->mode == 8) {
     cudaMemcpyAsync(D->wrap, src, sizeof(double) * tot, cudaMemcpyDeviceToDevice, st);
   } else {
     k_dom_scatter_wrap<<<blocks_for(tot, 256), 256, 0, st>>>(D->g, D->M, D->oy, src, D->I);
@@ -1938,6 +2276,33 @@ static int launch_octant_sweep(DomCtx* D, const OctArgs& a, cudaStream_t st) {
                       : launch_octant_kernel<10>(D->g, a, &cfg); break;
     default: e = cudaErrorInvalidValue;
   }
+  fs_count_launch();
+  return e == cudaSuccess ? FS_OK : FS_ECUDA;
+}
+
+static int launch_cl_sweep(DomCtx* D, const ClArgs& a, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = D->cl_C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(8 * D->cl_C);
+  cfg.blockDim = dim3(D->cl_threads);
+  cfg.dynamicSmemBytes = D->cl_smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaErrorInvalidValue;
+  const bool f = D->fp32 != 0;
+#define CLL(T, M, P) e = cudaLaunchKernelEx(&cfg, k_dom_octant_cl<T, M, P>, D->g, a)
+  switch (D->Mo * 4 + D->cl_ppt) {
+    case 3 * 4 + 1: if (f) CLL(float, 3, 1); else CLL(double, 3, 1); break;
+    case 6 * 4 + 1: if (f) CLL(float, 6, 1); else CLL(double, 6, 1); break;
+    case 10 * 4 + 1: if (f) CLL(float, 10, 1); else CLL(double, 10, 1); break;
+    case 3 * 4 + 2: if (f) CLL(float, 3, 2); else CLL(double, 3, 2); break;
+    case 6 * 4 + 2: if (f) CLL(float, 6, 2); else CLL(double, 6, 2); break;
+    case 10 * 4 + 2: if (f) CLL(float, 10, 2); else CLL(double, 10, 2); break;
+  }
+#undef CLL
   fs_count_launch();
   return e == cudaSuccess ? FS_OK : FS_ECUDA;
 }
@@ -2005,7 +2370,7 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
   const int M = D->M;
-  const bool octp = D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7;
+  const bool octp = D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7 || D->mode == 8;
   const double Tamb4 = pow(T_amb, 4.0);
   k_dom_setup<<<blocks_for(N, 256), 256, 0, st>>>(g, Ts, Tg, as, om, YH, rho, Mloc, sigma, Tamb4,
                                                   D->kgmax, D->ks, D->kg, D->ksafe, D->B,
@@ -2045,7 +2410,18 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   for (it = 0; it < D->max_iter; ++it) {
     std::swap(D->G, D->Gp);
     if (D->timing) cudaEventRecord(D->ev0[it], st);
-    if (D->mode == 7) {
+    if (D->mode == 8) {
+      ClArgs ca{};
+      ca.kb = D->fp32 ? (const void*)D->kb32 : (const void*)D->kb;
+      ca.Goct = D->fp32 ? (void*)D->Goct32 : (void*)D->Goct;
+      ca.Qoct = D->fp32 ? (void*)D->Qoct32 : (void*)D->Qoct;
+      ca.wrap = D->fp32 ? (void*)D->wrap32 : (void*)D->wrap;
+      ca.I_amb = I_amb;
+      ca.ox = D->ox; ca.oy = D->oy; ca.oz = D->oz; ca.w = D->w; ca.Ig = D->Ig_out;
+      ca.C = D->cl_C; ca.rows = D->cl_rows; ca.periodic = 1; ca.down_slots = oa.down_slots;
+      rc = launch_cl_sweep(D, ca, st);
+      if (rc != FS_OK) return rc;
+    } else if (D->mode == 7) {
       if (D->fp32) {
         StArgs<float> sa{};
         sa.kb = D->kb32; sa.Goct = D->Goct32; sa.Qoct = D->Qoct32; sa.wrap = D->wrap32;

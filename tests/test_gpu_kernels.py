@@ -249,11 +249,11 @@ def test_k_epsilon(vectors):
         assert rel_l2(host(nuo), c["nu_t_out"]) <= LIBM, name
 
 
-@pytest.mark.parametrize("mode", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("mode", [1, 2, 3, 4, 5, 6, 7, 8])
 def test_dom(vectors, mode):
     """Every sweep path (pipelined octant clusters, CTA per ordinate, hyperplane
     launches, octant clusters with cluster barriers, self-timed octant
-    pipeline)."""
+    pipeline, octant clusters sized to run at once)."""
     from firewebapp_b200.quadrature import level_symmetric
     om, wq = level_symmetric(4)
     for name in vectors.cases("dom"):
@@ -283,7 +283,7 @@ def test_dom(vectors, mode):
             lib().fs_dom_destroy(h)
 
 
-@pytest.mark.parametrize("mode", [4, 7])
+@pytest.mark.parametrize("mode", [4, 7, 8])
 def test_dom_fp32_form(vectors, mode):
     """The mixed-precision sweep (FP32 intensities) against the FP64 golden
     vectors: relative error at FP32 level."""
@@ -352,15 +352,17 @@ def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2):
     return out
 
 
+@pytest.mark.parametrize("mode", [7, 8])
 @pytest.mark.parametrize("fp32", [0, 1])
 @pytest.mark.parametrize("dims", [(29, 40, 48), (13, 7, 21), (60, 120, 24)])
-def test_dom_self_timed_equals_barrier_path(fp32, dims):
-    """The self-timed octant pipeline (path 7) reproduces the cluster-barrier
-    sweep (path 4) bit for bit, over two solves, in both precisions, on grids
-    with full and partial last CTAs."""
+def test_dom_octant_paths_equal_barrier_path(mode, fp32, dims):
+    """The self-timed octant pipeline (path 7) and the co-resident octant
+    clusters (path 8) reproduce the cluster-barrier sweep (path 4) bit for bit,
+    over two solves, in both precisions, on grids with full and partial last
+    CTAs and with one and two pencils per thread."""
     nz, ny, nx = dims
     a = _dom_solves(4, fp32, nz, ny, nx, seed=5)
-    b = _dom_solves(7, fp32, nz, ny, nx, seed=5)
+    b = _dom_solves(mode, fp32, nz, ny, nx, seed=5)
     for (qa, ga, sa, ia), (qb, gb, sb, ib) in zip(a, b):
         assert ia == ib
         assert np.array_equal(qa, qb) and np.array_equal(ga, gb) and np.array_equal(sa, sb)
