@@ -19,7 +19,7 @@
 //     as a skewed pipeline).  Kappa and kappa*B are loaded once per cell for
 //     all ordinates of the octant, and the sweep emits the octant's partial
 //     G (and ground flux) instead of storing intensities.
-//   4 (default) as 1, with one cluster-wide barrier per hyperplane instead.
+//   4 as 1, with one cluster-wide barrier per hyperplane instead.
 //   2 one CTA per ordinate with the full intensity field stored (then G is
 //     summed over ordinates in ordinate order).
 //   3 one launch per hyperplane (any grid size).
@@ -27,7 +27,10 @@
 //     of a hyperplane loaded in batches and the inflow rows staged ahead.
 //   7 as 4 without clusters: a cooperative launch of self-timed CTAs that
 //     hand their last row downstream through a ring in global memory.
-// G in paths 1, 4, 6 and 7 is summed within each octant in ordinate order and then over
+//   8 (default where it fits) as 4 with clusters small enough that all eight
+//     octants are resident at once, two pencils per thread where needed,
+//     inputs prefetched by cp.async and ghost cells for the inflow.
+// G in paths 1, 4, 6, 7 and 8 is summed within each octant in ordinate order and then over
 // octants in octant order (the reference sums all ordinates in one sequence;
 // the two orders differ only by rounding).
 #include <vector>
@@ -1443,6 +1446,8 @@ struct ClArgs {
 // column, and a pencil's own slot holds the ambient intensity until its
 // first cell, so every cell reads its three upwind neighbours the same way.
 #define CL_CHUNK 16
+// one pencil per thread up to this many pencils per CTA (80 registers a thread)
+#define CL_MAX_THREADS_1 768
 struct ClLayout {
   size_t kab, ig, win, wout, buf0, buf1, izt, cix, total;
 };
@@ -1465,7 +1470,8 @@ __host__ __device__ inline ClLayout cl_layout(int tsize, int Mo, int rows, int n
 }
 
 template <typename T, int MO, int PPT>
-__global__ void __launch_bounds__(OCT_MAX_THREADS, 1) k_dom_octant_cl(GridDev g, ClArgs a) {
+__global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : OCT_MAX_THREADS, 1)
+    k_dom_octant_cl(GridDev g, ClArgs a) {
   using T2 = typename Vec2Of<T>::type;
   extern __shared__ __align__(16) unsigned char shraw[];
   cg::cluster_group cl = cg::this_cluster();
@@ -2017,7 +2023,7 @@ static bool plan_cl(DomCtx* D, int force_C) {
     if (force_C > 0 && C != force_C) continue;
     const int rows = (g.nz + C - 1) / C;
     if ((g.nz + rows - 1) / rows != C) continue;
-    const int ppt = (rows * g.ny + OCT_MAX_THREADS - 1) / OCT_MAX_THREADS;
+    const int ppt = rows * g.ny <= CL_MAX_THREADS_1 ? 1 : (rows * g.ny + OCT_MAX_THREADS - 1) / OCT_MAX_THREADS;
     if (ppt > 2) continue;
     const int threads = ((rows * g.ny + ppt - 1) / ppt + 31) / 32 * 32;
     const void* fn = octant_cl_ptr(D->fp32 != 0, Mo, ppt);

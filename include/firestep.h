@@ -231,8 +231,9 @@ int fs_dom_solve(void* handle, const double* T_s, const double* T_g, const doubl
  * default octant-cluster path, which keeps only the y-periodic inflow rows
  * (the part of I_set that a later sweep reads, dom_3d.py:147-211). */
 double* fs_dom_intensity(void* handle);
-/* Sweep path: 0 auto (path 4 when the quadrature is octant-major and the
- * grid fits, else one CTA per ordinate, else one launch per hyperplane),
+/* Sweep path: 0 auto (path 8 when the quadrature is octant-major and eight
+ * octant clusters can be resident at once, else path 4 when the grid fits,
+ * else one CTA per ordinate, else one launch per hyperplane),
  * 1 octant clusters with point-to-point hand-off between CTAs,
  * 2 one CTA per ordinate, 3 hyperplane launches, 4 octant clusters with a
  * cluster barrier per hyperplane, 5 one CTA per ordinate with per-thread
@@ -240,14 +241,16 @@ double* fs_dom_intensity(void* handle);
  * ordinates each, two CTAs per SM), 7 as 4 without clusters: a cooperative
  * launch of self-timed CTAs that hand their last row on through a ring in
  * global memory (needs all 8*C CTAs resident at once, one per SM; no other
- * path-7 sweep may run on the device at the same time); cluster_ctas 0 =
- * automatic, else CTAs per octant (1..16; up to 64 for path 7).  Only before
+ * path-7 sweep may run on the device at the same time), 8 as 4 with clusters
+ * small enough that all eight octants run at once (up to two pencils per
+ * thread); cluster_ctas 0 = automatic, else CTAs per octant (1..16; up to 64
+ * for path 7).  Only before
  * the first solve or intensity load.  Paths 1 and 7 bound their waits: a
  * stalled hand-off returns FS_ETIMEOUT. */
 int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
 /* The path in use (0 before the first solve or intensity load). */
 int fs_dom_sweep_mode(void* handle);
-/* fp32 = 1: the mixed-precision form of the sweep (path 4 or 7 with kappa,
+/* fp32 = 1: the mixed-precision form of the sweep (path 4, 7 or 8 with kappa,
  * kappa*B, intensities and octant partials in FP32 and the quotient of
  * __fdividef, about 2 ulp; G, the ground exchange and all outputs in FP64).
  * No counterpart in the reference, which is FP64 throughout.  Only before the

@@ -315,11 +315,11 @@ def test_dom_fp32_form(vectors, mode):
             lib().fs_dom_destroy(h)
 
 
-def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2):
+def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0):
     """q_rad_solid, q_rad_gas, q_in_soil after each of ``calls`` solves of an
-    S8 DOM on seeded random fields (the y-inflow rows persist between calls)."""
+    S_order DOM on seeded random fields (the y-inflow rows persist between calls)."""
     from firewebapp_b200.quadrature import level_symmetric
-    om, wq = level_symmetric(8)
+    om, wq = level_symmetric(order)
     rng = np.random.default_rng(seed)
     dz = np.concatenate([np.full(nz // 3, 0.05), np.linspace(0.05, 0.4, nz - nz // 3)])
     g = Grid(nz, ny, nx, 0.5, 0.5, dz)
@@ -330,7 +330,7 @@ def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2):
     try:
         if fp32:
             call("fs_dom_set_precision", h, 1)
-        call("fs_dom_set_sweep_mode", h, mode, 0)
+        call("fs_dom_set_sweep_mode", h, mode, cluster_ctas)
         shape = (nz, ny, nx)
         for it in range(calls):
             Ts = dev(300.0 + 900.0 * rng.random(shape) ** 4)
@@ -354,15 +354,18 @@ def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2):
 
 @pytest.mark.parametrize("mode", [7, 8])
 @pytest.mark.parametrize("fp32", [0, 1])
-@pytest.mark.parametrize("dims", [(29, 40, 48), (13, 7, 21), (60, 120, 24)])
-def test_dom_octant_paths_equal_barrier_path(mode, fp32, dims):
+@pytest.mark.parametrize("case", [((29, 40, 48), 8, 0), ((13, 7, 21), 8, 0),
+                                  ((60, 120, 24), 8, 0), ((64, 100, 16), 4, 8)])
+def test_dom_octant_paths_equal_barrier_path(mode, fp32, case):
     """The self-timed octant pipeline (path 7) and the co-resident octant
     clusters (path 8) reproduce the cluster-barrier sweep (path 4) bit for bit,
     over two solves, in both precisions, on grids with full and partial last
-    CTAs and with one and two pencils per thread."""
-    nz, ny, nx = dims
-    a = _dom_solves(4, fp32, nz, ny, nx, seed=5)
-    b = _dom_solves(mode, fp32, nz, ny, nx, seed=5)
+    CTAs; the last case makes path 8 take two pencils per thread (8 CTAs of
+    8 rows of 100 pencils)."""
+    (nz, ny, nx), order, cc = case
+    a = _dom_solves(4, fp32, nz, ny, nx, seed=5, order=order)
+    b = _dom_solves(mode, fp32, nz, ny, nx, seed=5, order=order,
+                    cluster_ctas=cc if mode == 8 else 0)
     for (qa, ga, sa, ia), (qb, gb, sb, ib) in zip(a, b):
         assert ia == ib
         assert np.array_equal(qa, qb) and np.array_equal(ga, gb) and np.array_equal(sa, sb)
