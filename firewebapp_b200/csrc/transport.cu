@@ -21,17 +21,38 @@ struct SpeciesArgs {
 
 // One thread per cell over the flattened grid (no idle lanes at the x edge);
 // the species loop is unrolled so the loads of all species are in flight
-// together.
+// together.  The per-level reciprocals of the z spacings are computed once
+// per block (a block spans at most SP_KLEV levels on grids of 32 or more
+// cells per level; smaller grids compute them per cell), and the divisions by
+// the centred z spacing and by rho are multiplications by one reciprocal per
+// cell, shared by the three species.
+#define SP_KLEV 8
 template <int NS>
 __global__ void __launch_bounds__(256, 4)
 k_species(GridDev g, SpeciesArgs a, const double* __restrict__ rho,
           const double* __restrict__ u, const double* __restrict__ v,
           const double* __restrict__ w, double dt, double D, double inv_dx, double inv_dy,
           double inv_dx2, double inv_dy2) {
+  __shared__ double rk[4][SP_KLEV];  // 1/da, 1/db, 1/dz, 1/hz per level of the block
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int64_t sy = nx, sz = (int64_t)nx * ny;
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= sz * nz) return;
+  const int64_t ncell = sz * nz;
+  const int64_t c0 = (int64_t)blockIdx.x * blockDim.x;
+  const int k0 = (int)(c0 / sz);
+  const int64_t clast = min(c0 + (int64_t)blockDim.x, ncell) - 1;
+  const int nlev = (int)(clast / sz) - k0 + 1;
+  const bool shared_k = nlev <= SP_KLEV;
+  if (shared_k && (int)threadIdx.x < nlev) {
+    const int kk = k0 + threadIdx.x;
+    const double da = g.da[kk], db = g.db[kk];
+    rk[0][threadIdx.x] = 1.0 / da;
+    rk[1][threadIdx.x] = 1.0 / db;
+    rk[2][threadIdx.x] = 1.0 / g.dz[kk];
+    rk[3][threadIdx.x] = 1.0 / (0.5 * (da + db));
+  }
+  __syncthreads();
+  const int64_t c = c0 + threadIdx.x;
+  if (c >= ncell) return;
   const int k = (int)(c / sz);
   const int64_t rem = c - (int64_t)k * sz;
   const int j = (int)(rem / nx);
@@ -40,11 +61,17 @@ k_species(GridDev g, SpeciesArgs a, const double* __restrict__ rho,
   const int jp1 = wrapj(j + 1, ny), jp2 = wrapj(j + 2, ny);
   const int64_t crow = c - (int64_t)j * sy;
   const double ui = u[c], vi = v[c], wi = w[c];
-  const double rhoi = rho[c];
-  const double inv_d_above = 1.0 / g.da[k];
-  const double inv_d_below = 1.0 / g.db[k];
-  const double inv_dz_k = 1.0 / g.dz[k];
-  const double hz = 0.5 * (g.da[k] + g.db[k]);
+  const double inv_rho = 1.0 / rho[c];
+  double inv_d_above, inv_d_below, inv_dz_k, inv_hz;
+  if (shared_k) {
+    const int kl = k - k0;
+    inv_d_above = rk[0][kl]; inv_d_below = rk[1][kl]; inv_dz_k = rk[2][kl]; inv_hz = rk[3][kl];
+  } else {
+    inv_d_above = 1.0 / g.da[k];
+    inv_d_below = 1.0 / g.db[k];
+    inv_dz_k = 1.0 / g.dz[k];
+    inv_hz = 1.0 / (0.5 * (g.da[k] + g.db[k]));
+  }
   const bool mx = (i >= 2 && i <= nx - 3);
   const bool mz = (k >= 2 && k <= nz - 3);
 #pragma unroll
@@ -71,7 +98,7 @@ k_species(GridDev g, SpeciesArgs a, const double* __restrict__ rho,
     if (mz) {
       double fzp = muscl_face(Y[c - sz], Yi, Y[c + sz], Y[c + 2 * sz], wi);
       double fzm = muscl_face(Y[c - 2 * sz], Y[c - sz], Yi, Y[c + sz], wi);
-      flux_z = wi * (fzp - fzm) / hz;
+      flux_z = wi * (fzp - fzm) * inv_hz;
     } else {
       flux_z = (wi >= 0.0) ? wi * (Yi - YL_z) * inv_d_below : wi * (YR_z - Yi) * inv_d_above;
     }
@@ -80,7 +107,7 @@ k_species(GridDev g, SpeciesArgs a, const double* __restrict__ rho,
     double d2y = (Yjp1 - 2.0 * Yi + Yjm1) * inv_dy2;
     double d2z = ((YR_z - Yi) * inv_d_above - (Yi - YL_z) * inv_d_below) * inv_dz_k;
     double diff = D * (d2x + d2y + d2z);
-    double src = a.S[s][c] / rhoi;
+    double src = a.S[s][c] * inv_rho;
     double dY = (adv + diff + src) * dt;
     double nw = Yi + dY;
     if (nw < 0.0) nw = 0.0;
