@@ -39,7 +39,7 @@ METRIC = "3D solver cell-steps/s on 1 B200 (plain FP64 Tier-3 step)"
 UNIT = "cell-steps/s"
 WORKLOAD = "tier3_step_400x120x60_S8_fp64"
 # measured DRAM bytes per cell of one launch (see the traffic comment in main)
-TRAFFIC_PER_CELL = {"dom_sweep": 18.44e6 / 720000.0}
+TRAFFIC_PER_CELL = {"dom_sweep": (16.686848e6 + 4.866304e6) / 720000.0}
 
 
 def _peaks():
@@ -306,11 +306,11 @@ def main():
     M = solver.Omega.shape[0]
     dom_mode = lib.fs_dom_sweep_mode(solver.dom)
     alg = {  # algorithmic bytes per launch (distinct fields read + written, 8 B each)
-        # octant-cluster sweeps (paths 1, 4): read (kappa, kappa*B) once and write
+        # octant sweeps (paths 1, 4, 6, 7, 8): read (kappa, kappa*B) once and write
         # the 8 octant partial G fields (FP32 in the mixed form; wrap rows and
         # ground partials < 1% more); per-ordinate paths write every intensity
         "dom_sweep": (N * (8.0 + 4.0 * 8) if args.form == "mixed" else
-                      N * (16.0 + 8.0 * 8) if dom_mode in (1, 4, 6, 7) else N * (8.0 * M + 16.0)),
+                      N * (16.0 + 8.0 * 8) if dom_mode in (1, 4, 6, 7, 8) else N * (8.0 * M + 16.0)),
         "species_transport": N * 8.0 * 12,
         "edc": N * 8.0 * 11,
         "turb_diffusion_Y": N * 8.0 * 7,
@@ -323,9 +323,10 @@ def main():
     avg_ms = tot_ms / max(nl, 1)
     achieved = alg[dom_k] / (avg_ms * 1e-3) / 1e9
     # DRAM bytes per launch of the dominant kernel from an ncu capture of the
-    # 100x120x60 slice of this workload (dram__bytes_read.sum + write.sum),
-    # scaled by the cell count to a full 400x120x60 launch
-    traffic = TRAFFIC_PER_CELL.get(dom_k) if args.form == "plain" else None
+    # 100x120x60 slice of this workload (dram__bytes_read.sum + write.sum) with
+    # the default sweep (path 8), scaled by the cell count to a full launch
+    traffic = (TRAFFIC_PER_CELL.get(dom_k)
+               if args.form == "plain" and (dom_k != "dom_sweep" or dom_mode == 8) else None)
     if traffic is not None:
         traffic *= N
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
