@@ -221,6 +221,55 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batch_bench(args):
+    """N cases of the batched sweep (``cases.batch_cases``) on each GPU: all
+    stepped concurrently (one stream and host thread per case), and the same
+    cases one after another; both aggregate cell-steps/s over the timed steps,
+    host clock between device-wide synchronisations.  Ranks take disjoint
+    cases (weak scaling, no collective on the data path)."""
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    from firewebapp_b200.batch import time_concurrent
+    from firewebapp_b200.cases import batch_cases
+    cases = batch_cases(args.batch, seed0=rank * args.batch)
+    conc = time_concurrent(cases, args.steps, warmup=args.warmup, form=args.form)
+    seq_work, seq_wall = 0.0, 0.0
+    for c in cases:
+        one = time_concurrent([c], args.steps, warmup=args.warmup, form=args.form)
+        seq_work += one["cell_steps"]
+        seq_wall += one["wall_s"]
+    work, wall = conc["cell_steps"], conc["wall_s"]
+    if ws > 1:
+        t = torch.tensor([work, wall, seq_work, seq_wall], dtype=torch.float64, device="cuda")
+        parts = [torch.zeros_like(t) for _ in range(ws)]
+        dist.all_gather(parts, t)
+        tot = torch.stack(parts)
+        work, seq_work = float(tot[:, 0].sum()), float(tot[:, 2].sum())
+        wall, seq_wall = float(tot[:, 1].max()), float(tot[:, 3].max())
+    if rank == 0:
+        line = {
+            "metric": METRIC.replace("plain FP64 Tier-3 step", "batched sweep"), "value": work / wall,
+            "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * wall / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.form == "plain" else "f64+f32", "data": "synthetic",
+            "config": {"workload": f"tier3_batch_{args.batch}_cases_nx200-600_S8_{args.form}",
+                       "cases_per_gpu": args.batch, "cells": conc["cells"],
+                       "parallelism": f"replicas{ws}", "timing": "host clock between "
+                       "device-wide synchronisations"},
+            "sequential_value": seq_work / seq_wall,
+            "concurrency_gain": (work / wall) / (seq_work / seq_wall),
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -238,11 +287,18 @@ def main():
                     help="run the workload cut to its first NX x-cells (profiling)")
     ap.add_argument("--dom-sweep", type=int, default=0,
                     help="force a DOM sweep path (fs_dom_set_sweep_mode); 0 picks automatically")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="instead of the headline line: N cases of the batched sweep of uneven "
+                         "domains (Nx 200-600) stepped concurrently, against the same cases "
+                         "stepped one after another")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.batch:
+        run_batch_bench(args)
         return
 
     import torch

@@ -87,3 +87,29 @@ def scaled(case: dict, nx: int | None = None, ny: int | None = None,
     if nz is not None:
         out["Lz"] = h + (nz - out["n_z_bed"]) * dz
     return out
+
+
+def batch_cases(n: int = 32, seed0: int = 0, nx_range=(200, 600)) -> list[dict]:
+    """The batched sweep of uneven domains: ``n`` cases with Nx drawn uniformly
+    from ``nx_range`` (inclusive), Ny = 120, Nz = 60, dx = dy = 0.1 m,
+    n_z_bed = 4, dz = h/4 and Lz = 15 h, and per case U10 ~ U(1, 8) m/s,
+    moisture ~ U(0.02, 0.12), bulk density ~ U(0.2, 0.6) kg/m3 and fuel depth
+    h ~ U(0.1, 0.4) m, each case from its own PCG64 stream seeded with
+    ``seed0 + k`` (the seed is also the case's particle-jitter seed)."""
+    import numpy as np
+    out = []
+    for k in range(n):
+        rng = np.random.Generator(np.random.PCG64(seed0 + k))
+        nx = int(rng.integers(nx_range[0], nx_range[1] + 1))
+        u10 = float(rng.uniform(1.0, 8.0))
+        moist = float(rng.uniform(0.02, 0.12))
+        rho_b = float(rng.uniform(0.2, 0.6))
+        h = float(rng.uniform(0.1, 0.4))
+        out.append(dict(
+            CFG2,
+            Lx=nx * 0.1, Ly=12.0, Lz=15.0 * h, dx=0.10, dy=0.10, n_z_bed=4,
+            bed_x_start=1.0, bed_x_end=nx * 0.1,
+            fuel_depth_m=h, bulk_density_kg_m3=rho_b, initial_moisture_frac=moist,
+            wind_speed_m_s=u10, jitter_seed=seed0 + k,
+        ))
+    return out

@@ -34,17 +34,17 @@ int fs_stream_wait(cudaStream_t st) {
   return cudaEventSynchronize(ev[dev]) == cudaSuccess ? FS_OK : FS_ECUDA;
 }
 
-// One-time per-device scratch for the synchronous reductions (a few device
-// words and a pinned host staging area), so the hot-path reductions neither
-// allocate per call nor copy into pageable memory.  The mutex is held for the
-// whole call, which also makes those entry points safe across threads.
+// Per-thread, per-device scratch for the synchronous reductions (a few device
+// words and a pinned host staging area), made on a thread's first call, so the
+// hot-path reductions neither allocate per call nor copy into pageable memory,
+// and threads that step different cases on different streams never wait for
+// each other's streams.
 struct SmallScratch {
   unsigned long long* dkey;  // 32 words
   double* dres;              // 32 doubles
   double* hpin;              // 32 doubles, pinned
 };
-static std::mutex g_small_mu;
-static SmallScratch g_small[64];
+static thread_local SmallScratch g_small[64];
 
 static SmallScratch* small_scratch() {
   int dev = 0;
@@ -149,7 +149,6 @@ int fs_copy_to_host(void* dst, const void* src, int64_t bytes, void* stream) {
 
 int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, void* stream) {
   GRID("fs_field_max");
-  std::lock_guard<std::mutex> lock(g_small_mu);
   SmallScratch* sc = small_scratch();
   if (!sc) {
     fs_set_error("fs_field_max: scratch allocation failed");
@@ -176,7 +175,6 @@ int fs_field_max_multi(const FsGrid* g, int nf, const double* const* f, const in
   launch_init_keys(key, nf, mask2, ST(stream));
   for (int q = 0; q < nf; ++q) launch_max(gd, f[q], modes[q], key + q, ST(stream));
   launch_keys_to_double(key, dres, nf, ST(stream));
-  std::lock_guard<std::mutex> lock(g_small_mu);
   SmallScratch* sc = small_scratch();
   if (!sc) {
     fs_set_error("fs_field_max_multi: scratch allocation failed");
@@ -385,7 +383,6 @@ int fs_divergence_max(const FsGrid* g, const double* u, const double* v, const d
                       const double* u_inlet, const double* div_target, double* div_out,
                       double* result, void* stream) {
   GRID("fs_divergence_max");
-  std::lock_guard<std::mutex> lock(g_small_mu);
   SmallScratch* sc = small_scratch();
   if (!sc) {
     fs_set_error("fs_divergence_max: scratch allocation failed");

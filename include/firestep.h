@@ -302,7 +302,11 @@ int fs_active_count(int64_t n, const double* omega, const double* T_g, const dou
  * reference loop's scalars (active-flame count, front row) go through it. */
 int fs_copy_to_host(void* dst, const void* src, int64_t bytes, void* stream);
 /* max reductions: mode 0 max|f|, 1 max f (NaN propagates), 2 interior max
- * ignoring NaN from 0 (turbulence_3d.py:894-900); results to host. */
+ * ignoring NaN from 0 (turbulence_3d.py:894-900); results to host.  The
+ * synchronous reductions (this, fs_field_max_multi, fs_divergence_max) stage
+ * through per-thread device words and pinned memory made on a thread's first
+ * call, so threads that step different cases on their own streams may call
+ * them at the same time. */
 int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, void* stream);
 /* several maxima in one pass; scratch: >= 256 bytes of device memory;
  * results: nf doubles in host memory (synchronises once). */

@@ -1,0 +1,40 @@
+"""The batched form: case sharding (host) and concurrent stepping of several
+cases on one GPU, which must give each case exactly its single-case result."""
+import numpy as np
+import pytest
+
+
+def test_shard_balances_work_and_covers_every_case():
+    from firewebapp_b200.batch import shard
+    w = [541, 389, 535, 525, 210, 600, 333, 450]
+    parts = [shard(len(w), r, 3, w) for r in range(3)]
+    assert sorted(sum(parts, [])) == list(range(len(w)))
+    loads = [sum(w[i] for i in p) for p in parts]
+    assert max(loads) - min(loads) <= max(w)
+    assert shard(4, 0, 1) == [0, 1, 2, 3]
+
+
+def test_batch_cases_follow_the_sweep_distribution():
+    from firewebapp_b200.cases import batch_cases
+    from firewebapp_b200.grid import build_setup
+    cs = batch_cases(3, seed0=3)
+    assert cs == batch_cases(3, seed0=3)
+    for c in cs:
+        g = build_setup(c).grid
+        assert 200 <= g.Nx <= 600 and g.Ny == 120 and g.Nz == 60 and g.n_z_bed == 4
+        assert 1.0 <= c["wind_speed_m_s"] <= 8.0 and 0.02 <= c["initial_moisture_frac"] <= 0.12
+        assert 0.2 <= c["bulk_density_kg_m3"] <= 0.6 and 0.1 <= c["fuel_depth_m"] <= 0.4
+
+
+@pytest.mark.gpu
+def test_concurrent_cases_match_single_runs():
+    from firewebapp_b200.batch import run_batch
+    from firewebapp_b200.cases import TINY
+    cases = [dict(TINY, wind_speed_m_s=u, jitter_seed=s)
+             for u, s in ((4.0, 0), (6.0, 1), (2.5, 2))]
+    alone = run_batch(cases, steps=6, concurrency=1, keep_state=True)
+    together = run_batch(cases, steps=6, concurrency=3, keep_state=True)
+    for a, b in zip(alone, together):
+        assert a.steps == b.steps == 6 and a.t == b.t
+        for k, v in a.state.items():
+            assert np.array_equal(v, b.state[k]), k
