@@ -72,6 +72,7 @@ struct ProjCtx {
   int graph_failed;
   int nu;             // Jacobi sweeps before and after the coarse correction
   double omega;       // Jacobi damping
+  int tail_on;        // coarse levels in one launch (k_mg_vcycle_tail)
   // mixed-precision form: the V-cycle in FP32 (levels, coarse inverse, the
   // residual it smooths and the correction it returns); CG stays FP64
   int fp32;
@@ -627,6 +628,7 @@ void* proj_create(const GridDev& g) {
   P->iter_kernels = 0;
   P->graph_failed = 0;
   P->nu = MG_NU_DEFAULT;
+  P->tail_on = 1;
   P->fp32 = 0;
   P->Ainv32 = nullptr; P->r32 = nullptr; P->z32 = nullptr;
   for (int l = 0; l < 16; ++l) P->lev32[l] = MGLevelT<float>{};
@@ -751,11 +753,196 @@ int proj_set_precision(void* h, int fp32) {
 }
 
 // z = V-cycle(r) on level l (b = rhs, x = result); returns kernels launched
+// ---------------------------------------------------------------------------
+// The coarse end of the V-cycle in one launch: every level from the first one
+// whose tail fits in shared memory (operator, right-hand sides and vectors of
+// all coarser levels, plus the coarsest level's dense inverse) down to the
+// coarsest and back, in one CTA, with a __syncthreads between the sweeps,
+// instead of one launch per sweep (a few microseconds of launch and drain
+// each for a few hundred cells).  The first tail level's right-hand side
+// comes from global memory and its correction goes back there.  The order of
+// operations and every per-cell expression are those of vcycle() with
+// k_mg_jacobi, k_mg_restrict_residual, k_mg_coarse_solve and k_mg_prolong, so
+// the correction is bit-identical.
+#define MG_TAIL_SMEM (200 * 1024)
+#define MG_TAIL_MAX 10
+#define MG_TAIL_THREADS 512
+template <typename T>
+struct MGTail {
+  MGLevelT<T> lev[MG_TAIL_MAX];  // the tail's levels (global arrays), finest first
+  int nl, nu;
+  double omega;
+  const T* Ainv;
+};
+
+// elements of shared memory the tail of levels lev[0..nl-1] needs
+template <typename T>
+__host__ __device__ inline int64_t tail_smem_elems(const MGLevelT<T>* lev, int nl) {
+  int64_t e = 0;
+  for (int q = 0; q < nl; ++q) e += 9 * lev[q].n;
+  const int64_t nc = lev[nl - 1].n;
+  return e + (nc <= MG_COARSE_MAX ? nc * nc : 0);
+}
+
+template <typename T>
+__device__ __forceinline__ T tail_apply(const MGLevelT<T>& f, const T* x, int64_t c, int i,
+                                        int j, int k) {
+  const int nx = f.nx, ny = f.ny, nz = f.nz;
+  const int64_t sy = nx, sz = (int64_t)nx * ny;
+  const T xc = x[c];
+  T y = f.e[c] * xc;
+  if (i < nx - 1) y += f.gx[c] * (xc - x[c + 1]);
+  if (i > 0) y += f.gx[c - 1] * (xc - x[c - 1]);
+  if (ny > 1) {
+    int jp = j + 1 < ny ? j + 1 : 0;
+    int jm = j > 0 ? j - 1 : ny - 1;
+    int64_t cp = c - (int64_t)j * sy + (int64_t)jp * sy;
+    int64_t cm = c - (int64_t)j * sy + (int64_t)jm * sy;
+    y += f.gy[c] * (xc - x[cp]);
+    y += f.gy[cm] * (xc - x[cm]);
+  }
+  if (k < nz - 1) y += f.gz[c] * (xc - x[c + sz]);
+  if (k > 0) y += f.gz[c - sz] * (xc - x[c - sz]);
+  return y;
+}
+
+template <typename T>
+__device__ __forceinline__ void tail_jacobi(const MGLevelT<T>& f, const T* b, const T* x, T* xo,
+                                            T w) {
+  for (int64_t c = threadIdx.x; c < f.n; c += blockDim.x) {
+    if (!x) {
+      xo[c] = w * b[c] * f.dinv[c];
+      continue;
+    }
+    int i = (int)(c % f.nx);
+    int j = (int)((c / f.nx) % f.ny);
+    int k = (int)(c / ((int64_t)f.nx * f.ny));
+    T r = b[c] - tail_apply(f, x, c, i, j, k);
+    xo[c] = x[c] + w * r * f.dinv[c];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MG_TAIL_THREADS, 1)
+    k_mg_vcycle_tail(MGTail<T> a, const double* done) {
+  PCG_SKIP(done);
+  extern __shared__ __align__(16) unsigned char tsh[];
+  T* sp = (T*)tsh;
+  // the levels in shared memory: operator copied in, vectors private
+  MGLevelT<T> L[MG_TAIL_MAX];
+  for (int q = 0; q < a.nl; ++q) {
+    const MGLevelT<T>& g = a.lev[q];
+    const int64_t n = g.n;
+    MGLevelT<T>& f = L[q];
+    f.nx = g.nx; f.ny = g.ny; f.nz = g.nz; f.n = n;
+    f.gx = sp; f.gy = sp + n; f.gz = sp + 2 * n; f.e = sp + 3 * n; f.dinv = sp + 4 * n;
+    f.b = sp + 5 * n; f.x = sp + 6 * n; f.t = sp + 7 * n; f.s = sp + 8 * n;
+    sp += 9 * n;
+    for (int64_t c = threadIdx.x; c < n; c += blockDim.x) {
+      f.gx[c] = g.gx[c]; f.gy[c] = g.gy[c]; f.gz[c] = g.gz[c]; f.e[c] = g.e[c];
+      f.dinv[c] = g.dinv[c];
+      if (q == 0) f.b[c] = g.b[c];
+    }
+  }
+  const int64_t ncs = L[a.nl - 1].n;
+  T* Ainv = sp;
+  if (ncs <= MG_COARSE_MAX)
+    for (int64_t c = threadIdx.x; c < ncs * ncs; c += blockDim.x) Ainv[c] = a.Ainv[c];
+  __syncthreads();
+  const T w = (T)a.omega;
+  const int nu = a.nu;
+  // down: pre-smoothing from x = 0 ending in t, residual restricted to the next level's b
+  for (int l = 0; l + 1 < a.nl; ++l) {
+    const MGLevelT<T>& f = L[l];
+    const T* src = nullptr;
+    for (int s = 0; s < nu; ++s) {
+      T* dst = ((nu - 1 - s) % 2 == 0) ? f.t : f.s;
+      tail_jacobi(f, f.b, src, dst, w);
+      __syncthreads();
+      src = dst;
+    }
+    const MGLevelT<T>& cl = L[l + 1];
+    const int64_t fsy = f.nx, fsz = (int64_t)f.nx * f.ny;
+    for (int64_t q = threadIdx.x; q < cl.n; q += blockDim.x) {
+      int I = (int)(q % cl.nx);
+      int J = (int)((q / cl.nx) % cl.ny);
+      int K = (int)(q / ((int64_t)cl.nx * cl.ny));
+      T sum = 0.0;
+      for (int k = 2 * K; k <= min(2 * K + 1, f.nz - 1); ++k)
+        for (int j = 2 * J; j <= min(2 * J + 1, f.ny - 1); ++j)
+          for (int i = 2 * I; i <= min(2 * I + 1, f.nx - 1); ++i) {
+            int64_t c = (int64_t)k * fsz + (int64_t)j * fsy + i;
+            sum += f.b[c] - tail_apply(f, f.t, c, i, j, k);
+          }
+      cl.b[q] = sum;
+    }
+    __syncthreads();
+  }
+  // coarsest level: dense solve, or smoothing only when it is too large for it
+  {
+    const MGLevelT<T>& f = L[a.nl - 1];
+    if (f.n <= MG_COARSE_MAX) {
+      for (int r = threadIdx.x; r < (int)f.n; r += blockDim.x) {
+        T sum = 0.0;
+        for (int q = 0; q < (int)f.n; ++q) sum += Ainv[r * f.n + q] * f.b[q];
+        f.x[r] = sum;
+      }
+      __syncthreads();
+    } else {
+      const T wc = (T)MG_OMEGA;
+      tail_jacobi(f, f.b, (const T*)nullptr, f.x, wc);
+      __syncthreads();
+      for (int s = 0; s < 8; ++s) {
+        const T* src = (s & 1) ? f.t : f.x;
+        T* dst = (s & 1) ? f.x : f.t;
+        tail_jacobi(f, f.b, src, dst, wc);
+        __syncthreads();
+      }
+    }
+  }
+  // up: prolongation into t, post-smoothing from t ending in the level's x
+  for (int l = a.nl - 2; l >= 0; --l) {
+    const MGLevelT<T>& f = L[l];
+    const MGLevelT<T>& cl = L[l + 1];
+    for (int64_t c = threadIdx.x; c < f.n; c += blockDim.x) {
+      int i = (int)(c % f.nx);
+      int j = (int)((c / f.nx) % f.ny);
+      int k = (int)(c / ((int64_t)f.nx * f.ny));
+      f.t[c] += cl.x[((int64_t)(k >> 1) * cl.ny + (j >> 1)) * cl.nx + (i >> 1)];
+    }
+    __syncthreads();
+    const T* src = f.t;
+    for (int s = 0; s < nu; ++s) {
+      T* dst = (s == nu - 1) ? f.x : ((s % 2 == 0) ? f.s : f.t);
+      tail_jacobi(f, f.b, src, dst, w);
+      __syncthreads();
+      src = dst;
+    }
+  }
+  // the first tail level's correction back to global memory
+  for (int64_t c = threadIdx.x; c < L[0].n; c += blockDim.x) a.lev[0].x[c] = L[0].x[c];
+}
+
 template <typename T>
 static int vcycle(ProjCtx* P, MGLevelT<T>* lev, const T* Ainv, int l, const T* b, T* x,
                   const double* done, cudaStream_t st) {
   MGLevelT<T>& f = lev[l];
   int nk = 0;
+  // the coarse end in one launch (its first level's b and x are the level's own)
+  if (l > 0 && P->tail_on && P->nlev - l <= MG_TAIL_MAX && b == f.b && x == f.x &&
+      tail_smem_elems(lev + l, P->nlev - l) * (int64_t)sizeof(T) <= MG_TAIL_SMEM) {
+    MGTail<T> ta{};
+    ta.nl = P->nlev - l;
+    for (int q = 0; q < ta.nl; ++q) ta.lev[q] = lev[l + q];
+    ta.nu = P->nu;
+    ta.omega = P->omega;
+    ta.Ainv = Ainv;
+    const size_t smem = (size_t)tail_smem_elems(lev + l, ta.nl) * sizeof(T);
+    cudaFuncSetAttribute(k_mg_vcycle_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         MG_TAIL_SMEM);
+    k_mg_vcycle_tail<T><<<1, MG_TAIL_THREADS, smem, st>>>(ta, done);
+    return 1;
+  }
   if (l == P->nlev - 1) {
     if (f.n <= MG_COARSE_MAX) {
       k_mg_coarse_solve<T><<<1, 64, 0, st>>>((int)f.n, Ainv, b, x, done);
@@ -820,6 +1007,17 @@ int proj_configure(void* h, int nu, double omega) {
   if (nu != P->nu || omega != P->omega) {
     P->nu = nu;
     P->omega = omega;
+    if (P->iter_exec) cudaGraphExecDestroy(P->iter_exec);
+    P->iter_exec = nullptr;
+    P->graph_failed = 0;
+  }
+  return FS_OK;
+}
+
+int proj_set_coarse_tail(void* h, int on) {
+  ProjCtx* P = (ProjCtx*)h;
+  if ((on != 0) != (P->tail_on != 0)) {
+    P->tail_on = on ? 1 : 0;
     if (P->iter_exec) cudaGraphExecDestroy(P->iter_exec);
     P->iter_exec = nullptr;
     P->graph_failed = 0;

@@ -203,6 +203,11 @@ int fs_proj_apply(void* handle, const double* x, double* y, void* stream);
  * preconditioner (projection_3d.py:236-246, an FFT solve) has no such knob;
  * only the converged solution is shared. */
 int fs_proj_configure(void* handle, int nu, double omega);
+/* on = 1 (default): the coarse end of the V-cycle (the levels whose operators
+ * and vectors fit in one CTA's shared memory) runs in one single-CTA launch;
+ * 0: one launch per sweep.  The correction, and so the solve, is
+ * bit-identical either way. */
+int fs_proj_set_coarse_tail(void* handle, int on);
 /* fp32 = 1: the mixed-precision form of the preconditioner (V-cycle
  * coefficients, vectors and coarse inverse in FP32); the CG itself, its
  * operator, residuals, dot products and the solution stay FP64, so the

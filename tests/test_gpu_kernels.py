@@ -492,6 +492,44 @@ def test_projection(vectors):
         lib().fs_proj_destroy(h)
 
 
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_projection_coarse_tail_is_bit_identical(fp32):
+    """The coarse end of the V-cycle in one single-CTA launch gives the same
+    solve, bit for bit, as one launch per sweep (80x48x60: levels of 28800
+    and 3600 cells and below run in the tail)."""
+    from firewebapp_b200.cases import scaled, CFG2
+    from firewebapp_b200.grid import build_setup
+    gr = build_setup(scaled(CFG2, nx=80, ny=48)).grid
+    nz, ny, nx = gr.Nz, gr.Ny, gr.Nx
+    g = Grid(nz, ny, nx, gr.dx, gr.dy, gr.dz_arr, gr.d_face_above, gr.d_face_below)
+    rng = np.random.default_rng(7)
+    shape = (nz, ny, nx)
+    rho = 0.3 + rng.random(shape)
+    u0, v0, w0 = (rng.standard_normal(shape) for _ in range(3))
+    ui = dev(np.full((nz, ny), 1.5))
+    tgt = dev(0.01 * rng.standard_normal(shape))
+    out = []
+    for tail in (1, 0):
+        h = C.c_void_p()
+        call("fs_proj_create", g.ref, C.byref(h))
+        try:
+            if fp32:
+                call("fs_proj_set_precision", h, 1)
+            call("fs_proj_set_coarse_tail", h, tail)
+            call("fs_proj_rebuild", h, ptr(dev(rho)), stream())
+            u, v, w = dev(u0), dev(v0), dev(w0)
+            its = C.c_int()
+            for _ in range(2):
+                call("fs_proj_project", h, ptr(u), ptr(v), ptr(w), ptr(ui), ptr(tgt), 0.01,
+                     1e-8, 200, C.byref(its), stream())
+            out.append((host(u), host(v), host(w), its.value))
+        finally:
+            lib().fs_proj_destroy(h)
+    (ua, va, wa, ia), (ub, vb, wb, ib) = out
+    assert ia == ib
+    assert np.array_equal(ua, ub) and np.array_equal(va, vb) and np.array_equal(wa, wb)
+
+
 def test_level_set(vectors):
     for name in vectors.cases("flame_front"):
         c = vectors.case("flame_front", name)
