@@ -199,6 +199,37 @@ def build_grid_from_case(case):
                       wall_bl_N=int(_pick(case, "wall_bl_N", 0)))
 
 
+# The physics branches this build provides, with the reference driver's
+# defaults (spread_3d.py:597-893) for keys a deck leaves out.  Any other
+# choice raises NotImplementedError, as the reference's JS port does for the
+# branches it lacks, instead of silently running the provided branch.
+SUPPORTED = (
+    ("turbulence_model", "laminar", ("k_epsilon",)),
+    ("combustion_closure", "edc", ("edc",)),
+    ("radiation_solver", "dom", ("dom",)),
+    ("wall_function", False, (False, None)),
+    ("level_set_passive", False, (True,)),
+    ("ignition_T_pin_enable", False, (False,)),
+    ("empirical_ros_enable", False, (False,)),
+    ("finney_tendril_enable", False, (False,)),
+    ("moisture_jump_enable", False, (False,)),
+)
+
+
+def check_supported(case: dict) -> None:
+    """Raise NotImplementedError for a physics branch this build does not provide."""
+    for key, default, ok in SUPPORTED:
+        v = _pick(case, key, default)
+        if isinstance(v, str):
+            v = v.strip().lower()
+        elif v is not None and not isinstance(v, bool):
+            v = bool(v)
+        if v not in ok:
+            raise NotImplementedError(
+                f"{key}={v!r} is not provided by the GPU Tier-3 step (provided: "
+                f"{', '.join(repr(o) for o in ok if o is not None)})")
+
+
 def build_setup(case: dict) -> CaseSetup:
     """Resolve a case (deck keys + ``wind_speed_m_s``) into initial state and constants."""
     g = build_grid_from_case(case)
@@ -230,6 +261,7 @@ def build_setup(case: dict) -> CaseSetup:
 
     if not bool(_pick(case, "lagrangian_bed_enable", False)):
         raise NotImplementedError("the Eulerian bed branch is not provided (Lagrangian bed only)")
+    check_supported(case)
     n_pc = int(_pick(case, "lagrangian_bed_N_per_cell", 50))
     parts = init_bed_particles(f["alpha_s"], rho_b, M_f, T_amb, g.dx, g.dy, g.dz_arr,
                                g.n_z_bed, n_pc, sav, i_bed_start, i_bed_end)

@@ -160,3 +160,20 @@ def test_deck_value_parsing_and_precedence(tmp_path):
     assert case["n_z_bed"] == 8.0        # deck wins (spread_3d.py:1041)
     assert case["Lx"] == 6.0 and "lx" not in case   # keyword wins (_pick)
     assert case["dx"] == 0.1 and case["wind_speed_m_s"] == 3.0
+
+
+def test_unprovided_physics_branches_raise():
+    """Decks that ask for a branch the GPU step does not provide fail at setup
+    instead of silently running the provided one."""
+    from firewebapp_b200.cases import TINY
+    from firewebapp_b200.grid import build_setup
+    build_setup(TINY)
+    for key, bad in (("radiation_solver", "p1"), ("turbulence_model", "smagorinsky"),
+                     ("combustion_closure", "mixing_limited"), ("level_set_passive", False),
+                     ("empirical_ros_enable", True), ("wall_function", True)):
+        with pytest.raises(NotImplementedError, match=key):
+            build_setup(dict(TINY, **{key: bad}))
+    case = dict(TINY)
+    del case["turbulence_model"]  # the reference's default is laminar
+    with pytest.raises(NotImplementedError, match="turbulence_model"):
+        build_setup(case)

@@ -266,3 +266,4 @@ def test_oracle_step_from_reference_state(ref_tiny):
     S = _oracle_state(TINY, ref_tiny["s9"], float(np.sum(dts[:9])), float(dts[8]), 9)
     step(S)
     _compare(S.snapshot(), ref_tiny["s10"], "s9 -> s10")
+
