@@ -430,6 +430,10 @@ int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas) {
   return check(dom_set_mode(handle, mode, cluster_ctas), "fs_dom_set_sweep_mode");
 }
 
+int fs_dom_set_octant_groups(void* handle, int groups) {
+  if (!handle) return check(FS_EARG, "fs_dom_set_octant_groups");
+  return check(dom_set_groups(handle, groups), "fs_dom_set_octant_groups");
+}
 int fs_dom_sweep_mode(void* handle) { return handle ? dom_mode(handle) : -1; }
 
 int fs_dom_set_precision(void* handle, int fp32) {

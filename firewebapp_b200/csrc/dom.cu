@@ -60,6 +60,7 @@ struct DomCtx {
   float2* kb32;
   float *Goct32, *Qoct32, *wrap32;
   int Mo, cl_C, cl_rows, cl_threads, cl_lg_ring, cl_ppt, cl_active;
+  int force_groups;            // path 8: ordinate groups per octant (0 automatic)
   void* st_ring;              // path 7 hand-off ring, then the read counters
   size_t st_ring_bytes;       // ring and counters (filled with 0xff before each sweep)
   size_t st_cnt_offset;
@@ -758,13 +759,13 @@ static const void* octant_f32_ptr(int Mo) {
 }
 
 // G (FP64) from FP32 octant partials; max G and max |G - G_prev|
-__global__ void k_dom_G_oct32(int64_t N, const float* __restrict__ Goct, double* G,
+__global__ void k_dom_G_oct32(int64_t N, int nparts, const float* __restrict__ Goct, double* G,
                               const double* __restrict__ Gp, unsigned long long* keys) {
   unsigned long long bg = 0, bd = 0;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < N;
        c += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int o = 0; o < 8; ++o) s += (double)Goct[(int64_t)o * N + c];
+    for (int o = 0; o < nparts; ++o) s += (double)Goct[(int64_t)o * N + c];
     G[c] = s;
     double d = fabs(s - Gp[c]);
     unsigned long long ks = (s != s) ? 0x7ff8000000000000ull
@@ -1437,6 +1438,7 @@ struct ClArgs {
   void *Goct, *Qoct, *wrap;
   double I_amb;
   int C, rows, periodic;
+  int groups;  // clusters (ordinate groups of MO) per octant
   unsigned down_slots;
 };
 // The hyperplane buffers carry a ghost row below the CTA's first row and a
@@ -1446,8 +1448,10 @@ struct ClArgs {
 // column, and a pencil's own slot holds the ambient intensity until its
 // first cell, so every cell reads its three upwind neighbours the same way.
 #define CL_CHUNK 16
-// one pencil per thread up to this many pencils per CTA (80 registers a thread)
+// one pencil per thread up to this many pencils per CTA (80 registers a thread),
+// else two pencils per thread up to twice this many (at most 96 registers)
 #define CL_MAX_THREADS_1 768
+#define CL_MAX_THREADS_2 640
 struct ClLayout {
   size_t kab, ig, win, wout, buf0, buf1, izt, cix, total;
 };
@@ -1470,7 +1474,7 @@ __host__ __device__ inline ClLayout cl_layout(int tsize, int Mo, int rows, int n
 }
 
 template <typename T, int MO, int PPT>
-__global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : OCT_MAX_THREADS, 1)
+__global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2, 1)
     k_dom_octant_cl(GridDev g, ClArgs a) {
   using T2 = typename Vec2Of<T>::type;
   extern __shared__ __align__(16) unsigned char shraw[];
@@ -1478,8 +1482,10 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : OCT_MAX_THREADS,
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int C = a.C;
   const int rank = (int)cl.block_rank();
-  const int oct = blockIdx.x / C;
-  const int n0 = oct * MO;
+  const int part = blockIdx.x / C;  // (octant, ordinate group)
+  const int oct = part / a.groups;
+  const int grp = part - oct * a.groups;
+  const int n0 = part * MO;
   const int rows = a.rows;
   const int S = rows * ny;
   const int RS = ny + 1;           // padded row stride
@@ -1523,8 +1529,8 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : OCT_MAX_THREADS,
   const int64_t N = ncells_dev(g);
   const int64_t n2 = (int64_t)nx * ny;
   const int slot_bits = (int)((a.down_slots >> (4 * oct)) & 15u);
-  const int slot = slot_bits == 15 ? -1 : slot_bits;
-  T* Go = Goct + (int64_t)oct * N;
+  const int slot = slot_bits == 15 ? -1 : slot_bits * a.groups + grp;
+  T* Go = Goct + (int64_t)part * N;
   const int64_t wstride = (int64_t)nz * nx;
   T* wrap0 = wrap + (int64_t)n0 * wstride;
   const bool periodic = a.periodic != 0;
@@ -1691,12 +1697,14 @@ static const void* octant_cl_ptr(bool fp32, int Mo, int ppt) {
   if (ppt == 1) {
     switch (Mo) {
       case 3: return fp32 ? CLP(float, 3, 1) : CLP(double, 3, 1);
+      case 5: return fp32 ? CLP(float, 5, 1) : CLP(double, 5, 1);
       case 6: return fp32 ? CLP(float, 6, 1) : CLP(double, 6, 1);
       case 10: return fp32 ? CLP(float, 10, 1) : CLP(double, 10, 1);
     }
   } else if (ppt == 2) {
     switch (Mo) {
       case 3: return fp32 ? CLP(float, 3, 2) : CLP(double, 3, 2);
+      case 5: return fp32 ? CLP(float, 5, 2) : CLP(double, 5, 2);
       case 6: return fp32 ? CLP(float, 6, 2) : CLP(double, 6, 2);
       case 10: return fp32 ? CLP(float, 10, 2) : CLP(double, 10, 2);
     }
@@ -1852,7 +1860,7 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1;
   D->fp32 = 0; D->kb32 = nullptr; D->Goct32 = nullptr; D->Qoct32 = nullptr; D->wrap32 = nullptr;
   D->st_ring = nullptr; D->st_ring_bytes = 0; D->st_cnt_offset = 0;
-  D->cl_ppt = 1; D->cl_active = 0;
+  D->cl_ppt = 1; D->cl_active = 0; D->force_groups = 0;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemset(D->G, 0, sizeof(double) * N);
   cudaMalloc(&D->ks, sizeof(double) * N); cudaMalloc(&D->kg, sizeof(double) * N);
@@ -2007,54 +2015,70 @@ static bool plan_st(DomCtx* D, int force_C) {
   return false;
 }
 
-// Launch shape of path 8: the largest cluster size C (rows of k' per CTA,
-// pencils per thread 1 or 2, one CTA per SM) for which eight clusters are
-// resident at once; else the largest C that launches at all.
+// Launch shape of path 8: ordinate groups per octant (1, or 2 when the octant's
+// ordinates split evenly), cluster size C (k' rows per CTA), pencils per
+// thread (1 or 2), one CTA per SM.  One cluster per octant is kept whenever
+// all eight clusters are resident at once: two clusters per octant take more
+// SMs for about the same sweep time, and the SMs left free are the ones the
+// concurrent projection and k-epsilon run on (measured: 23.4 against 22.8 ms
+// per step).  Otherwise the configuration with the fewest waves times work per
+// CTA per hyperplane (pencils x ordinates) wins.  force_C / D->force_groups
+// pin C / the grouping (0: free).
 static bool plan_cl(DomCtx* D, int force_C) {
+  const int force_groups = D->force_groups;
   const GridDev& g = D->g;
-  const int Mo = D->M / 8;
+  const int MoAll = D->M / 8;
   const int tsize = D->fp32 ? (int)sizeof(float) : (int)sizeof(double);
   int dev = 0, optin = 0, smem_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-  int best_active = 0;
-  for (int C = 16; C >= 1; --C) {
-    if (force_C > 0 && C != force_C) continue;
-    const int rows = (g.nz + C - 1) / C;
-    if ((g.nz + rows - 1) / rows != C) continue;
-    const int ppt = rows * g.ny <= CL_MAX_THREADS_1 ? 1 : (rows * g.ny + OCT_MAX_THREADS - 1) / OCT_MAX_THREADS;
-    if (ppt > 2) continue;
-    const int threads = ((rows * g.ny + ppt - 1) / ppt + 31) / 32 * 32;
-    const void* fn = octant_cl_ptr(D->fp32 != 0, Mo, ppt);
-    if (!fn) continue;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    const size_t need = cl_layout(tsize, Mo, rows, g.ny, g.nz).total;
-    const size_t pad = (size_t)smem_sm / 2 + 1024;  // no two CTAs on one SM
-    const size_t smem = need > pad ? need : pad;
-    if (smem > (size_t)optin) continue;
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(8 * C); cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = smem; cfg.attrs = at; cfg.numAttrs = 1;
-    int active = 0;
-    if (cudaOccupancyMaxActiveClusters(&active, fn, &cfg) != cudaSuccess) {
-      cudaGetLastError();
-      active = 0;
-    }
-    if (active < 1) continue;
-    const int score = active >= 8 ? 8 : active;
-    if (score > best_active) {
-      best_active = score;
-      D->cl_C = C; D->cl_rows = rows; D->cl_threads = threads; D->cl_smem = smem;
-      D->cl_ppt = ppt;
+  double best = 1e300;
+  bool found = false;
+  for (int groups = 1; groups <= 2; ++groups) {
+    if (force_groups > 0 && groups != force_groups) continue;
+    if (MoAll % groups != 0) continue;
+    if (found && D->cl_active >= 8) break;  // one cluster per octant, all resident
+    const int Mo = MoAll / groups;
+    for (int C = 16; C >= 1; --C) {
+      if (force_C > 0 && C != force_C) continue;
+      const int rows = (g.nz + C - 1) / C;
+      if ((g.nz + rows - 1) / rows != C) continue;
+      const int pencils = rows * g.ny;
+      const int ppt = pencils <= CL_MAX_THREADS_1 ? 1 : (pencils <= 2 * CL_MAX_THREADS_2 ? 2 : 0);
+      if (ppt == 0) continue;
+      const int threads = ((pencils + ppt - 1) / ppt + 31) / 32 * 32;
+      const void* fn = octant_cl_ptr(D->fp32 != 0, Mo, ppt);
+      if (!fn) continue;
+      cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+      const size_t need = cl_layout(tsize, Mo, rows, g.ny, g.nz).total;
+      const size_t pad = (size_t)smem_sm / 2 + 1024;  // no two CTAs on one SM
+      const size_t smem = need > pad ? need : pad;
+      if (smem > (size_t)optin) continue;
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(8 * groups * C); cfg.blockDim = dim3(threads);
+      cfg.dynamicSmemBytes = smem; cfg.attrs = at; cfg.numAttrs = 1;
+      int active = 0;
+      if (cudaOccupancyMaxActiveClusters(&active, fn, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        active = 0;
+      }
+      if (active < 1) continue;
+      const int waves = (8 * groups + active - 1) / active;
+      const double cost = (double)waves * pencils * Mo;
+      if (cost < best) {
+        best = cost; found = true;
+        D->cl_C = C; D->cl_rows = rows; D->cl_threads = threads; D->cl_smem = smem;
+        D->cl_ppt = ppt; D->groups = groups;
+        D->cl_active = waves == 1 ? 8 : 0;  // 8: every cluster resident at once
+      }
     }
   }
-  D->cl_active = best_active;
-  return best_active > 0;
+  return found;
 }
 
 static void alloc_st_ring(DomCtx* D) {
@@ -2082,13 +2106,13 @@ static int dom_prepare(DomCtx* D) {
       return FS_EARG;
     }
     D->mode = kind;
-    D->groups = 1;
+    if (kind != 8) D->groups = 1;  // path 8 planned its own grouping
     D->Mo = D->M / 8;
     int slot = 0;
     for (int o = 0; o < 8; ++o) D->down_slot[o] = D->hoz[o * D->Mo] < 0.0 ? slot++ : -1;
     cudaMalloc(&D->kb32, sizeof(float2) * N);
-    cudaMalloc(&D->Goct32, sizeof(float) * 8 * N);
-    cudaMalloc(&D->Qoct32, sizeof(float) * 8 * n2);
+    cudaMalloc(&D->Goct32, sizeof(float) * 8 * D->groups * N);
+    cudaMalloc(&D->Qoct32, sizeof(float) * 8 * D->groups * n2);
     cudaMalloc(&D->wrap32, sizeof(float) * D->M * g.nz * g.nx);
     cudaMemset(D->wrap32, 0, sizeof(float) * D->M * g.nz * g.nx);
     if (D->mode == 7) alloc_st_ring(D);
@@ -2102,13 +2126,13 @@ static int dom_prepare(DomCtx* D) {
       (kind == 7 ? plan_st(D, D->force_C)
                  : (kind == 8 ? plan_cl(D, D->force_C) : plan_clusters(D, D->force_C, kind, groups)))) {
     D->mode = kind == 8 ? 8 : (want == 1 ? 1 : (want == 6 ? 6 : (want == 7 ? 7 : 4)));
-    D->groups = groups;
+    if (kind != 8) D->groups = groups;  // path 8 planned its own grouping
     D->Mo = D->M / 8;
     int slot = 0;
     for (int o = 0; o < 8; ++o) D->down_slot[o] = D->hoz[o * D->Mo] < 0.0 ? slot++ : -1;
     cudaMalloc(&D->kb, sizeof(double2) * N);
-    cudaMalloc(&D->Goct, sizeof(double) * 8 * groups * N);
-    cudaMalloc(&D->Qoct, sizeof(double) * 8 * groups * n2);
+    cudaMalloc(&D->Goct, sizeof(double) * 8 * D->groups * N);
+    cudaMalloc(&D->Qoct, sizeof(double) * 8 * D->groups * n2);
     cudaMalloc(&D->wrap, sizeof(double) * D->M * g.nz * g.nx);
     cudaMemset(D->wrap, 0, sizeof(double) * D->M * g.nz * g.nx);
     if (D->mode == 7) alloc_st_ring(D);
@@ -2153,6 +2177,17 @@ int dom_set_mode(void* h, int mode, int cluster_ctas) {
 }
 
 int dom_mode(void* h) { return ((DomCtx*)h)->mode; }
+
+int dom_set_groups(void* h, int groups) {
+  DomCtx* D = (DomCtx*)h;
+  if (groups < 0 || groups > 2) return FS_EARG;
+  if (D->mode != 0) {
+    fs_set_error("ordinate groups must be set before the first solve or intensity load");
+    return FS_EARG;
+  }
+  D->force_groups = groups;
+  return FS_OK;
+}
 
 int dom_set_precision(void* h, int fp32) {
   DomCtx* D = (DomCtx*)h;
@@ -2291,7 +2326,7 @@ static int launch_cl_sweep(DomCtx* D, const ClArgs& a, cudaStream_t st) {
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = D->cl_C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-  cfg.gridDim = dim3(8 * D->cl_C);
+  cfg.gridDim = dim3(8 * D->groups * D->cl_C);
   cfg.blockDim = dim3(D->cl_threads);
   cfg.dynamicSmemBytes = D->cl_smem;
   cfg.stream = st;
@@ -2300,11 +2335,13 @@ static int launch_cl_sweep(DomCtx* D, const ClArgs& a, cudaStream_t st) {
   cudaError_t e = cudaErrorInvalidValue;
   const bool f = D->fp32 != 0;
 #define CLL(T, M, P) e = cudaLaunchKernelEx(&cfg, k_dom_octant_cl<T, M, P>, D->g, a)
-  switch (D->Mo * 4 + D->cl_ppt) {
+  switch ((D->Mo / D->groups) * 4 + D->cl_ppt) {
     case 3 * 4 + 1: if (f) CLL(float, 3, 1); else CLL(double, 3, 1); break;
+    case 5 * 4 + 1: if (f) CLL(float, 5, 1); else CLL(double, 5, 1); break;
     case 6 * 4 + 1: if (f) CLL(float, 6, 1); else CLL(double, 6, 1); break;
     case 10 * 4 + 1: if (f) CLL(float, 10, 1); else CLL(double, 10, 1); break;
     case 3 * 4 + 2: if (f) CLL(float, 3, 2); else CLL(double, 3, 2); break;
+    case 5 * 4 + 2: if (f) CLL(float, 5, 2); else CLL(double, 5, 2); break;
     case 6 * 4 + 2: if (f) CLL(float, 6, 2); else CLL(double, 6, 2); break;
     case 10 * 4 + 2: if (f) CLL(float, 10, 2); else CLL(double, 10, 2); break;
   }
@@ -2425,6 +2462,7 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
       ca.I_amb = I_amb;
       ca.ox = D->ox; ca.oy = D->oy; ca.oz = D->oz; ca.w = D->w; ca.Ig = D->Ig_out;
       ca.C = D->cl_C; ca.rows = D->cl_rows; ca.periodic = 1; ca.down_slots = oa.down_slots;
+      ca.groups = D->groups;
       rc = launch_cl_sweep(D, ca, st);
       if (rc != FS_OK) return rc;
     } else if (D->mode == 7) {
@@ -2488,7 +2526,7 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
     unsigned nb = blocks_for(N, 256);
     if (nb > 1184) nb = 1184;
     if (D->fp32) {
-      k_dom_G_oct32<<<nb, 256, 0, st>>>(N, D->Goct32, D->G, D->Gp, D->keys);
+      k_dom_G_oct32<<<nb, 256, 0, st>>>(N, 8 * D->groups, D->Goct32, D->G, D->Gp, D->keys);
       fs_count_launch();
       k_dom_ground_oct32<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, nslots, D->Qoct32,
                                                               D->Isoil, refl, D->relax,

@@ -101,6 +101,7 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
 void dom_destroy(void* h);
 double* dom_intensity(void* h);
 int dom_set_mode(void* h, int mode, int cluster_ctas);
+int dom_set_groups(void* h, int groups);
 int dom_mode(void* h);
 int dom_set_precision(void* h, int fp32);
 int dom_load_intensity(void* h, const double* I_full, cudaStream_t st);

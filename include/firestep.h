@@ -253,6 +253,10 @@ double* fs_dom_intensity(void* handle);
  * the first solve or intensity load.  Paths 1 and 7 bound their waits: a
  * stalled hand-off returns FS_ETIMEOUT. */
 int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
+/* Path 8 only: clusters per octant, 1 (all ordinates of the octant in one
+ * cluster) or 2 (half each, the octant partials of G then summed per half);
+ * 0 (default) plans it.  Only before the first solve or intensity load. */
+int fs_dom_set_octant_groups(void* handle, int groups);
 /* The path in use (0 before the first solve or intensity load). */
 int fs_dom_sweep_mode(void* handle);
 /* fp32 = 1: the mixed-precision form of the sweep (path 4, 7 or 8 with kappa,

@@ -315,7 +315,7 @@ def test_dom_fp32_form(vectors, mode):
             lib().fs_dom_destroy(h)
 
 
-def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0):
+def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0, groups=0):
     """q_rad_solid, q_rad_gas, q_in_soil after each of ``calls`` solves of an
     S_order DOM on seeded random fields (the y-inflow rows persist between calls)."""
     from firewebapp_b200.quadrature import level_symmetric
@@ -331,6 +331,8 @@ def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0):
         if fp32:
             call("fs_dom_set_precision", h, 1)
         call("fs_dom_set_sweep_mode", h, mode, cluster_ctas)
+        if groups:
+            call("fs_dom_set_octant_groups", h, groups)
         shape = (nz, ny, nx)
         for it in range(calls):
             Ts = dev(300.0 + 900.0 * rng.random(shape) ** 4)
@@ -354,14 +356,14 @@ def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0):
 
 @pytest.mark.parametrize("mode", [7, 8])
 @pytest.mark.parametrize("fp32", [0, 1])
-@pytest.mark.parametrize("case", [((29, 40, 48), 8, 0), ((13, 7, 21), 8, 0),
-                                  ((60, 120, 24), 8, 0), ((64, 100, 16), 4, 8)])
+@pytest.mark.parametrize("case", [((29, 40, 48), 8, 10), ((13, 7, 21), 8, 7),
+                                  ((60, 120, 24), 8, 10), ((64, 100, 16), 4, 8)])
 def test_dom_octant_paths_equal_barrier_path(mode, fp32, case):
     """The self-timed octant pipeline (path 7) and the co-resident octant
-    clusters (path 8) reproduce the cluster-barrier sweep (path 4) bit for bit,
-    over two solves, in both precisions, on grids with full and partial last
-    CTAs; the last case makes path 8 take two pencils per thread (8 CTAs of
-    8 rows of 100 pencils)."""
+    clusters (path 8, at a cluster size where one cluster per octant is best)
+    reproduce the cluster-barrier sweep (path 4) bit for bit, over two solves,
+    in both precisions, on grids with full and partial last CTAs; the last case
+    makes path 8 take two pencils per thread (8 CTAs of 8 rows of 100 pencils)."""
     (nz, ny, nx), order, cc = case
     a = _dom_solves(4, fp32, nz, ny, nx, seed=5, order=order)
     b = _dom_solves(mode, fp32, nz, ny, nx, seed=5, order=order,
@@ -369,6 +371,25 @@ def test_dom_octant_paths_equal_barrier_path(mode, fp32, case):
     for (qa, ga, sa, ia), (qb, gb, sb, ib) in zip(a, b):
         assert ia == ib
         assert np.array_equal(qa, qb) and np.array_equal(ga, gb) and np.array_equal(sa, sb)
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_dom_two_clusters_per_octant(fp32):
+    """Path 8 with every octant's ordinates split over two clusters (on the
+    60 x 120 cross-section: sixteen 6-CTA clusters on 96 SMs).  The G partials
+    are then summed in ordinate-group order, as in path 6, which it reproduces
+    bit for bit in FP64; in FP32 it agrees with path 4 to FP32 rounding."""
+    nz, ny, nx = 60, 120, 24
+    b = _dom_solves(8, fp32, nz, ny, nx, seed=9, groups=2)
+    if not fp32:
+        a = _dom_solves(6, 0, nz, ny, nx, seed=9)
+        for (qa, ga, sa, ia), (qb, gb, sb, ib) in zip(a, b):
+            assert ia == ib
+            assert np.array_equal(qa, qb) and np.array_equal(ga, gb) and np.array_equal(sa, sb)
+    else:
+        a = _dom_solves(4, 1, nz, ny, nx, seed=9)
+        for (qa, ga, sa, ia), (qb, gb, sb, ib) in zip(a, b):
+            assert rel_l2(qb, qa) <= 1e-6 and rel_l2(gb, ga) <= 1e-6 and rel_l2(sb, sa) <= 1e-6
 
 
 def _segments(x, y, z, dx, dy, z_face, nz, ny, nx, alive):
