@@ -90,6 +90,8 @@ SIGNATURES = {
                           PP]),
     "fs_dom_destroy": (None, [P]),
     "fs_dom_solve": (I, [P, P, P, P, P, D, D, P, P, P, P, P, P, P, P]),
+    "fs_dom_begin": (I, [P, P, P, P, P, D, D, P, P, P, P, P]),
+    "fs_dom_end": (I, [P, P, P, P, P]),
     "fs_dom_intensity": (P, [P]),
     "fs_dom_iterations": (I, [P]),
     "fs_dom_set_sweep_mode": (I, [P, I, I]),

@@ -423,6 +423,21 @@ int fs_dom_solve(void* handle, const double* T_s, const double* T_g, const doubl
                "fs_dom_solve");
 }
 
+int fs_dom_begin(void* handle, const double* T_s, const double* T_g, const double* alpha_s,
+                 const double* omega, double sigma_sav, double T_amb, const double* T_soil0,
+                 const double* Y_H2O, const double* rho, const double* M_local, void* stream) {
+  if (!handle) return check(FS_EARG, "fs_dom_begin");
+  return check(dom_begin(handle, T_s, T_g, alpha_s, omega, sigma_sav, T_amb, T_soil0, Y_H2O, rho,
+                         M_local, ST(stream)),
+               "fs_dom_begin");
+}
+
+int fs_dom_end(void* handle, double* q_rad_solid, double* q_rad_gas, double* q_in_soil,
+               void* stream) {
+  if (!handle) return check(FS_EARG, "fs_dom_end");
+  return check(dom_end(handle, q_rad_solid, q_rad_gas, q_in_soil, ST(stream)), "fs_dom_end");
+}
+
 double* fs_dom_intensity(void* handle) { return handle ? dom_intensity(handle) : nullptr; }
 
 int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas) {

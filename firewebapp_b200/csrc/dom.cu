@@ -61,6 +61,8 @@ struct DomCtx {
   float *Goct32, *Qoct32, *wrap32;
   int Mo, cl_C, cl_rows, cl_threads, cl_lg_ring, cl_ppt, cl_active;
   int force_groups;            // path 8: ordinate groups per octant (0 automatic)
+  int begun;                  // dom_begin done, dom_end due
+  double pend_I_amb;          // ambient intensity of the begun solve
   void* st_ring;              // path 7 hand-off ring, then the read counters
   size_t st_ring_bytes;       // ring and counters (filled with 0xff before each sweep)
   size_t st_cnt_offset;
@@ -1860,7 +1862,7 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1;
   D->fp32 = 0; D->kb32 = nullptr; D->Goct32 = nullptr; D->Qoct32 = nullptr; D->wrap32 = nullptr;
   D->st_ring = nullptr; D->st_ring_bytes = 0; D->st_cnt_offset = 0;
-  D->cl_ppt = 1; D->cl_active = 0; D->force_groups = 0;
+  D->cl_ppt = 1; D->cl_active = 0; D->force_groups = 0; D->begun = 0; D->pend_I_amb = 0.0;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemset(D->G, 0, sizeof(double) * N);
   cudaMalloc(&D->ks, sizeof(double) * N); cudaMalloc(&D->kg, sizeof(double) * N);
@@ -2403,16 +2405,18 @@ static int launch_ord_sweep(DomCtx* D, double I_amb, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? FS_OK : FS_ECUDA;
 }
 
-int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, const double* om,
-              double sigma, double T_amb, const double* Tsoil0, const double* YH, const double* rho,
-              const double* Mloc, double* q_solid, double* q_gas, double* q_in_soil,
-              cudaStream_t st) {
+// The first half of a solve: absorption, emission and the ground's own
+// emission from the caller's fields.  Once this work has run on the stream,
+// the solve reads none of those fields again, so the caller may change them
+// while dom_end's sweeps run.
+int dom_begin(void* h, const double* Ts, const double* Tg, const double* as, const double* om,
+              double sigma, double T_amb, const double* Tsoil0, const double* YH,
+              const double* rho, const double* Mloc, cudaStream_t st) {
   DomCtx* D = (DomCtx*)h;
   int rc = dom_prepare(D);
   if (rc != FS_OK) return rc;
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
-  const int M = D->M;
   const bool octp = D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7 || D->mode == 8;
   const double Tamb4 = pow(T_amb, 4.0);
   k_dom_setup<<<blocks_for(N, 256), 256, 0, st>>>(g, Ts, Tg, as, om, YH, rho, Mloc, sigma, Tamb4,
@@ -2424,6 +2428,34 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
   k_dom_ground_init<<<blocks_for(n2, 128), 128, 0, st>>>((int)n2, Tsoil0, D->eps_w, I_amb, D->Isoil,
                                                         D->Ig_out);
   fs_count_launch();
+  D->pend_I_amb = I_amb;
+  D->begun = 1;
+  return cuda_status();
+}
+
+int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, const double* om,
+              double sigma, double T_amb, const double* Tsoil0, const double* YH, const double* rho,
+              const double* Mloc, double* q_solid, double* q_gas, double* q_in_soil,
+              cudaStream_t st) {
+  int rc = dom_begin(h, Ts, Tg, as, om, sigma, T_amb, Tsoil0, YH, rho, Mloc, st);
+  if (rc != FS_OK) return rc;
+  return dom_end(h, q_solid, q_gas, q_in_soil, st);
+}
+
+// The second half: the source iterations and the radiative sources.
+int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStream_t st) {
+  DomCtx* D = (DomCtx*)h;
+  if (!D->begun) {
+    fs_set_error("dom_end without a dom_begin");
+    return FS_EARG;
+  }
+  D->begun = 0;
+  int rc = FS_OK;
+  const GridDev& g = D->g;
+  const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
+  const int M = D->M;
+  const bool octp = D->mode == 1 || D->mode == 4 || D->mode == 6 || D->mode == 7 || D->mode == 8;
+  const double I_amb = D->pend_I_amb;
   SweepArgs a{};
   a.ox = D->ox; a.oy = D->oy; a.oz = D->oz; a.I = D->I; a.ksafe = D->ksafe; a.B = D->B;
   a.Ig = D->Ig_out; a.I_amb = I_amb; a.inv_dx = 1.0 / g.dx; a.inv_dy = 1.0 / g.dy; a.M = M;

@@ -101,6 +101,10 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
 void dom_destroy(void* h);
 double* dom_intensity(void* h);
 int dom_set_mode(void* h, int mode, int cluster_ctas);
+int dom_begin(void* h, const double* Ts, const double* Tg, const double* as, const double* om,
+              double sigma, double T_amb, const double* Tsoil0, const double* YH,
+              const double* rho, const double* Mloc, cudaStream_t st);
+int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStream_t st);
 int dom_set_groups(void* h, int groups);
 int dom_mode(void* h);
 int dom_set_precision(void* h, int fp32);

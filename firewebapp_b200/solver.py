@@ -409,6 +409,8 @@ class Tier3Solver:
             dom_args = (ptr(f["T_s"]), ptr(f["T_g"]), ptr(f["alpha_s"]), ptr(w["omega"]),
                         ptr(f["Y_H2O"]), ptr(f["rho"]), ptr(w["M_local"]), ptr(w["q_rad"]),
                         ptr(w["q_rad_gas"]))
+            from concurrent.futures import Future
+            self._dom_inputs = Future()
             dom_job = self._pool.submit(self._dom_job, ready, dom_args)
         # --- 3/4. drag + tentative momentum (spread_3d.py:2223-2276)
         self._phase("momentum")
@@ -465,7 +467,21 @@ class Tier3Solver:
         self._swap("nu_t", "tmp3")
         # --- 8. DOM (every dom_subcycle_every steps) + soil (spread_3d.py:2472-2514)
         self._phase("dom")
+        dt_sub = dt / N_SUB
+        drip = int(ign)
+        early = None
         if dom_job is not None:
+            # Once the DOM has read its input fields, the work that follows it
+            # but does not read its outputs (the flame mask, the gas advection
+            # and the chemistry and species half of the first sub-step) runs
+            # while the sweeps are still going; nothing it writes is read by
+            # the soil step or the ignition pulse, so the order of the values
+            # is that of the reference loop.
+            ev_in = self._dom_inputs.result()
+            torch.cuda.current_stream(self.dev).wait_event(ev_in)
+            self._flame_mask_and_gas_adv(dt)
+            early = self._substep_prep()
+            self._substep_chem(dt_sub, Sp, Sd, *early)
             done = dom_job.result()
             torch.cuda.current_stream(self.dev).wait_event(done)
             d.dom_iters = L.fs_dom_iterations(self.dom)
@@ -486,85 +502,19 @@ class Tier3Solver:
         if ign and g.n_z_bed > 0:
             sl = w["q_rad"][g.n_z_bed - 1, :, p["i_src_start"]:p["i_src_end"]]
             sl += 240_000.0 * p["ignition_q_mult"]
-        # --- 10. flame mask (only its emptiness is used downstream)
-        self.active_count.zero_()
-        check(L.fs_active_count(self.n, ptr(w["omega"]), ptr(f["T_g"]), ptr(f["Y_fuel"]),
-                                ptr(self.active_count), None, s), "active_count")
-        # --- 11. gas-temperature advection (:2648)
-        self._phase("gas_adv")
-        with self._ktime("gas_energy_adv"):
-            check(L.fs_gas_energy_adv(gp, ptr(f["T_g"]), ptr(f["u"]), ptr(f["v"]), ptr(f["w"]),
-                                      ptr(w["tmp1"]), dt, 2.0e-5, p["T_amb"], s), "gas_adv")
-        self._swap("T_g", "tmp1")
-        # --- 12. ten chemistry/transport sub-steps (:2678-3196)
-        self._phase("substeps")
-        dt_sub = dt / N_SUB
-        nu_in = self._maxes([f["nu_t"]], [2])[0]
-        n_sc, dts_sc = self._nsub_from(nu_in, SC_T, dt_sub)
-        n_pr, dts_pr = self._nsub_from(nu_in, PR_T, dt_sub)
+        if early is None:
+            # --- 10/11. flame mask, gas-temperature advection
+            self._flame_mask_and_gas_adv(dt)
+            early = self._substep_prep()
+            self._substep_chem(dt_sub, Sp, Sd, *early)
+        # --- 12. ten chemistry/transport sub-steps (:2678-3196); the first one's
+        # chemistry and species half ran above
+        n_sc, dts_sc, n_pr, dts_pr = early
         d.n_sub_sc, d.n_sub_pr = n_sc, n_pr
-        drip = int(ign)
         for _sub in range(N_SUB):
-            self._phase("edc")
-            with self._ktime("edc"):
-                check(L.fs_edc(self.n, ptr(f["rho"]), ptr(f["T_g"]), ptr(f["Y_fuel"]),
-                               ptr(f["Y_O2"]), ptr(f["k_turb"]), ptr(f["eps_turb"]),
-                               ptr(f["Y_H2O"]), ptr(w["omega"]), p["chi_rad"], 1100.0, dt_sub,
-                               1, 1.3, 17_000_000.0, int(p["edc_extinction_enable"]),
-                               ptr(self.edc_scratch), s), "edc")
-            self._phase("species")
-            check(L.fs_species_sources(self.n, ptr(Sp), ptr(Sd), ptr(f["Y_fuel"]),
-                                       ptr(f["Y_O2"]), ptr(f["Y_H2O"]), ptr(w["S_F"]),
-                                       ptr(w["S_O2"]), ptr(w["S_H2O"]), s), "sources")
-            Ys = [f["Y_fuel"], f["Y_O2"], f["Y_H2O"]]
-            Yo = [w["tmp1"], w["tmp2"], w["tmp3"]]
-            with self._ktime("species_transport"):
-                check(L.fs_species_transport(gp, 3, ptr_array(Ys), ptr_array(Yo),
-                                             ptr_array([w["S_F"], w["S_O2"], w["S_H2O"]]),
-                                             dbl_array([0.0, 0.232, 0.0]), ptr(f["rho"]),
-                                             ptr(f["u"]), ptr(f["v"]), ptr(f["w"]), dt_sub,
-                                             1.0e-5, s), "species")
-            self._swap("Y_fuel", "tmp1")
-            self._swap("Y_O2", "tmp2")
-            self._swap("Y_H2O", "tmp3")
-            self._phase("turb_diff_Y")
-            check(L.fs_clip(self.n, ptr(f["Y_O2"]), 0.0, 0.232, s), "clip_O2")
-            if n_sc > 0:
-                for q in range(n_sc):
-                    last = q == n_sc - 1
-                    Ys = [f["Y_fuel"], f["Y_O2"], f["Y_H2O"]]
-                    Yo = [w["tmp1"], w["tmp2"], w["tmp3"]]
-                    with self._ktime("turb_diffusion_Y"):
-                        check(L.fs_turb_diffusion_substep(
-                            gp, 3, ptr_array(Ys), ptr_array(Yo), ptr(f["nu_t"]), SC_T, dts_sc,
-                            int(last), dbl_array([0.0, 0.0, 0.0]),
-                            dbl_array([1.0, 0.232, 1.0]), s), "turb_diff_Y")
-                    self._swap("Y_fuel", "tmp1")
-                    self._swap("Y_O2", "tmp2")
-                    self._swap("Y_H2O", "tmp3")
-            self._phase("gas_update")
-            check(L.fs_gas_energy_update(gp, ptr(f["T_g"]), ptr(f["rho"]), ptr(f["Y_H2O"]),
-                                         ptr(f["T_s"]), ptr(Sp), ptr(Sd),
-                                         ptr(self.bed_out["Q_g_conv"]), ptr(w["q_rad_gas"]),
-                                         ptr(w["Q_comb"]), dt_sub, p["T_amb"], p["h_bed"],
-                                         drip, g.n_z_bed, p["i_src_start"], p["i_src_end"], s),
-                  "gas_update")
-            self._phase("solid_cond")
-            check(L.fs_solid_conduction(gp, ptr(f["T_s"]), ptr(f["alpha_s"]), ptr(w["tmp4"]),
-                                        0.20, 500.0, 1300.0, dt_sub, s), "solid_cond")
-            self._swap("T_s", "tmp4")
-            self._phase("turb_diff_T")
-            if n_pr > 0:
-                for q in range(n_pr):
-                    last = q == n_pr - 1
-                    check(L.fs_turb_diffusion_substep(
-                        gp, 1, ptr_array([f["T_g"]]), ptr_array([w["tmp4"]]), ptr(f["nu_t"]),
-                        PR_T, dts_pr, int(last), dbl_array([p["T_amb"]]), dbl_array([T_CAP]),
-                        s), "turb_diff_T")
-                    self._swap("T_g", "tmp4")
-            else:
-                check(L.fs_clip(self.n, ptr(f["T_g"]), p["T_amb"], T_CAP, s), "cap_Tg")
-            check(L.fs_clip(self.n, ptr(f["T_s"]), p["T_amb"], T_CAP, s), "cap_Ts")
+            if _sub > 0:
+                self._substep_chem(dt_sub, Sp, Sd, n_sc, dts_sc, n_pr, dts_pr)
+            self._substep_energy(dt_sub, Sp, Sd, drip, n_pr, dts_pr)
         # --- 13. level set (passive: v_n = 0, so evolve leaves phi; reinit every 10)
         self._phase("levelset")
         self.lset_step += 1
@@ -598,6 +548,104 @@ class Tier3Solver:
         self.diag = d
         return True
 
+    def _flame_mask_and_gas_adv(self, dt):
+        """Steps 10-11 of the loop: the flame-mask count and the gas
+        temperature advection (spread_3d.py:2648, flame_front_3d.py:756-813)."""
+        L, f, w, p, gp = self.lib, self.f, self.w, self.p, self.gp
+        s = self._s()
+        self.active_count.zero_()
+        check(L.fs_active_count(self.n, ptr(w["omega"]), ptr(f["T_g"]), ptr(f["Y_fuel"]),
+                                ptr(self.active_count), None, s), "active_count")
+        self._phase("gas_adv")
+        with self._ktime("gas_energy_adv"):
+            check(L.fs_gas_energy_adv(gp, ptr(f["T_g"]), ptr(f["u"]), ptr(f["v"]), ptr(f["w"]),
+                                      ptr(w["tmp1"]), dt, 2.0e-5, p["T_amb"], s), "gas_adv")
+        self._swap("T_g", "tmp1")
+
+    def _substep_prep(self):
+        """Sub-step counts of the turbulent diffusion from the interior maximum
+        of nu_t (turbulence_3d.py:880-915), for species and for temperature."""
+        self._phase("substeps")
+        dt_sub = self.dt / N_SUB
+        nu_in = self._maxes([self.f["nu_t"]], [2])[0]
+        n_sc, dts_sc = self._nsub_from(nu_in, SC_T, dt_sub)
+        n_pr, dts_pr = self._nsub_from(nu_in, PR_T, dt_sub)
+        return n_sc, dts_sc, n_pr, dts_pr
+
+    def _substep_chem(self, dt_sub, Sp, Sd, n_sc, dts_sc, n_pr, dts_pr):
+        """First half of a chemistry/transport sub-step: EDC, species sources
+        and transport, the O2 clip and the turbulent diffusion of the species
+        (spread_3d.py:2678-3060)."""
+        L, f, w, p, gp = self.lib, self.f, self.w, self.p, self.gp
+        s = self._s()
+        self._phase("edc")
+        with self._ktime("edc"):
+            check(L.fs_edc(self.n, ptr(f["rho"]), ptr(f["T_g"]), ptr(f["Y_fuel"]),
+                           ptr(f["Y_O2"]), ptr(f["k_turb"]), ptr(f["eps_turb"]),
+                           ptr(f["Y_H2O"]), ptr(w["omega"]), p["chi_rad"], 1100.0, dt_sub,
+                           1, 1.3, 17_000_000.0, int(p["edc_extinction_enable"]),
+                           ptr(self.edc_scratch), s), "edc")
+        self._phase("species")
+        check(L.fs_species_sources(self.n, ptr(Sp), ptr(Sd), ptr(f["Y_fuel"]),
+                                   ptr(f["Y_O2"]), ptr(f["Y_H2O"]), ptr(w["S_F"]),
+                                   ptr(w["S_O2"]), ptr(w["S_H2O"]), s), "sources")
+        Ys = [f["Y_fuel"], f["Y_O2"], f["Y_H2O"]]
+        Yo = [w["tmp1"], w["tmp2"], w["tmp3"]]
+        with self._ktime("species_transport"):
+            check(L.fs_species_transport(gp, 3, ptr_array(Ys), ptr_array(Yo),
+                                         ptr_array([w["S_F"], w["S_O2"], w["S_H2O"]]),
+                                         dbl_array([0.0, 0.232, 0.0]), ptr(f["rho"]),
+                                         ptr(f["u"]), ptr(f["v"]), ptr(f["w"]), dt_sub,
+                                         1.0e-5, s), "species")
+        self._swap("Y_fuel", "tmp1")
+        self._swap("Y_O2", "tmp2")
+        self._swap("Y_H2O", "tmp3")
+        self._phase("turb_diff_Y")
+        check(L.fs_clip(self.n, ptr(f["Y_O2"]), 0.0, 0.232, s), "clip_O2")
+        if n_sc > 0:
+            for q in range(n_sc):
+                last = q == n_sc - 1
+                Ys = [f["Y_fuel"], f["Y_O2"], f["Y_H2O"]]
+                Yo = [w["tmp1"], w["tmp2"], w["tmp3"]]
+                with self._ktime("turb_diffusion_Y"):
+                    check(L.fs_turb_diffusion_substep(
+                        gp, 3, ptr_array(Ys), ptr_array(Yo), ptr(f["nu_t"]), SC_T, dts_sc,
+                        int(last), dbl_array([0.0, 0.0, 0.0]),
+                        dbl_array([1.0, 0.232, 1.0]), s), "turb_diff_Y")
+                self._swap("Y_fuel", "tmp1")
+                self._swap("Y_O2", "tmp2")
+                self._swap("Y_H2O", "tmp3")
+
+    def _substep_energy(self, dt_sub, Sp, Sd, drip, n_pr, dts_pr):
+        """Second half of a sub-step: gas-energy update with the radiative
+        gas source, vertical solid conduction, turbulent diffusion of T_g and
+        the caps (spread_3d.py:3104-3196)."""
+        L, f, w, p, gp, g = self.lib, self.f, self.w, self.p, self.gp, self.grid
+        s = self._s()
+        self._phase("gas_update")
+        check(L.fs_gas_energy_update(gp, ptr(f["T_g"]), ptr(f["rho"]), ptr(f["Y_H2O"]),
+                                     ptr(f["T_s"]), ptr(Sp), ptr(Sd),
+                                     ptr(self.bed_out["Q_g_conv"]), ptr(w["q_rad_gas"]),
+                                     ptr(w["Q_comb"]), dt_sub, p["T_amb"], p["h_bed"],
+                                     drip, g.n_z_bed, p["i_src_start"], p["i_src_end"], s),
+              "gas_update")
+        self._phase("solid_cond")
+        check(L.fs_solid_conduction(gp, ptr(f["T_s"]), ptr(f["alpha_s"]), ptr(w["tmp4"]),
+                                    0.20, 500.0, 1300.0, dt_sub, s), "solid_cond")
+        self._swap("T_s", "tmp4")
+        self._phase("turb_diff_T")
+        if n_pr > 0:
+            for q in range(n_pr):
+                last = q == n_pr - 1
+                check(L.fs_turb_diffusion_substep(
+                    gp, 1, ptr_array([f["T_g"]]), ptr_array([w["tmp4"]]), ptr(f["nu_t"]),
+                    PR_T, dts_pr, int(last), dbl_array([p["T_amb"]]), dbl_array([T_CAP]),
+                    s), "turb_diff_T")
+                self._swap("T_g", "tmp4")
+        else:
+            check(L.fs_clip(self.n, ptr(f["T_g"]), p["T_amb"], T_CAP, s), "cap_Tg")
+        check(L.fs_clip(self.n, ptr(f["T_s"]), p["T_amb"], T_CAP, s), "cap_Ts")
+
     def _dom_job(self, ready, a):
         """M_local aggregation and the DOM solve on the second stream, after
         the bed work queued before ``ready``; returns the event that marks the
@@ -608,11 +656,18 @@ class Tier3Solver:
         sp = st.cuda_stream
         L, p = self.lib, self.p
         Ts, Tg, a_s, om, YH, rho, Ml, qr, qrg = a
-        check(L.fs_bed_aggregate(_ctypes_ref(self.fs_parts), _ctypes_ref(self.fs_segs), Ml, 1,
-                                 sp), "bed_aggregate_M")
-        check(L.fs_dom_solve(self.dom, Ts, Tg, a_s, om, p["sav"], p["T_amb"],
-                             ptr(self.T_soil[0]), YH, rho, Ml, qr, qrg, ptr(self.q_in_soil), sp),
-              "dom_solve")
+        try:
+            check(L.fs_bed_aggregate(_ctypes_ref(self.fs_parts), _ctypes_ref(self.fs_segs), Ml,
+                                     1, sp), "bed_aggregate_M")
+            check(L.fs_dom_begin(self.dom, Ts, Tg, a_s, om, p["sav"], p["T_amb"],
+                                 ptr(self.T_soil[0]), YH, rho, Ml, sp), "dom_begin")
+            inputs = torch.cuda.Event()
+            inputs.record(st)
+            self._dom_inputs.set_result(inputs)
+        except BaseException as e:
+            self._dom_inputs.set_exception(e)
+            raise
+        check(L.fs_dom_end(self.dom, qr, qrg, ptr(self.q_in_soil), sp), "dom_end")
         done = torch.cuda.Event()
         done.record(st)
         return done

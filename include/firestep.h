@@ -232,6 +232,17 @@ int fs_dom_solve(void* handle, const double* T_s, const double* T_g, const doubl
                  const double* omega, double sigma_sav, double T_amb, const double* T_soil0,
                  const double* Y_H2O, const double* rho, const double* M_local, double* q_rad_solid,
                  double* q_rad_gas, double* q_in_soil, void* stream);
+/* fs_dom_solve in two halves (no counterpart in the reference, which solves
+ * in one call): fs_dom_begin reads the fields (absorption, emission, ground
+ * emission) and fs_dom_end runs the source iterations and writes the
+ * radiative sources.  Once fs_dom_begin's work has run on its stream the
+ * solve reads none of its input fields again, so other streams may update
+ * them while fs_dom_end runs; the result is that of fs_dom_solve. */
+int fs_dom_begin(void* handle, const double* T_s, const double* T_g, const double* alpha_s,
+                 const double* omega, double sigma_sav, double T_amb, const double* T_soil0,
+                 const double* Y_H2O, const double* rho, const double* M_local, void* stream);
+int fs_dom_end(void* handle, double* q_rad_solid, double* q_rad_gas, double* q_in_soil,
+               void* stream);
 /* Full intensity field (M x Nz x Ny x Nx) for sweep paths 2 and 3; NULL for the
  * default octant-cluster path, which keeps only the y-periodic inflow rows
  * (the part of I_set that a later sweep reads, dom_3d.py:147-211). */
