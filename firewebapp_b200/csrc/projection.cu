@@ -14,7 +14,8 @@
 //   * coarse cells aggregate 2x2x2 fine cells (odd tails keep 1);
 //   * coarse operator = 1/2 (P^T S P) with piecewise-constant P, which keeps
 //     the face-conductance form (coarse face = sum of fine faces across it);
-//   * nu pre- and nu post-sweeps of damped Jacobi (default nu = 4, omega = 0.8);
+//   * nu pre- and nu post-sweeps of damped Jacobi (default nu = 4, omega = 0.9:
+//     fewer CG iterations than 0.8 at the same cost per iteration, measured);
 //   * the coarsest level (<= 64 cells) is solved with a dense inverse built
 //     at each rebuild.
 // The stopping test mirrors scipy's: ||b - A x||_2 < rtol ||b||_2 on the
@@ -26,7 +27,8 @@
 #include "kernels.h"
 
 #define PROJ_EPS 1.0e-6
-#define MG_OMEGA 0.8
+#define MG_OMEGA 0.8          // damping of the coarsest level's smoothing-only solve
+#define MG_OMEGA_DEFAULT 0.9  // damping of the V-cycle's smoothing sweeps
 #define MG_NU_DEFAULT 4
 #define MG_COARSE_MAX 48
 #define RED_BLOCKS 296
@@ -633,7 +635,7 @@ void* proj_create(const GridDev& g) {
   P->Ainv32 = nullptr; P->r32 = nullptr; P->z32 = nullptr;
   for (int l = 0; l < 16; ++l) P->lev32[l] = MGLevelT<float>{};
   for (int q = 0; q < 8; ++q) P->stats[q] = 0.0;
-  P->omega = MG_OMEGA;
+  P->omega = MG_OMEGA_DEFAULT;
   cudaStreamCreateWithFlags(&P->cs, cudaStreamNonBlocking);
   if (cudaGetLastError() != cudaSuccess || !P->p_prev) {
     proj_destroy(P);

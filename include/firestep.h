@@ -199,7 +199,7 @@ int fs_proj_project(void* handle, double* u, double* v, double* w, const double*
 double* fs_proj_pressure(void* handle);
 int fs_proj_apply(void* handle, const double* x, double* y, void* stream);
 /* Multigrid preconditioner: nu damped-Jacobi sweeps (weight omega) before and
- * after each coarse correction (default 4 and 0.8).  The reference's
+ * after each coarse correction (default 4 and 0.9).  The reference's
  * preconditioner (projection_3d.py:236-246, an FFT solve) has no such knob;
  * only the converged solution is shared. */
 int fs_proj_configure(void* handle, int nu, double omega);
