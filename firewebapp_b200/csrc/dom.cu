@@ -1568,7 +1568,7 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
   // per-pencil constants: pencil index, row and column, global row base, roles
   int pq[PPT], pjp[PPT], pkp[PPT], pk[PPT], pqi[PPT];
   int64_t prb[PPT];
-  unsigned prole[PPT];  // 1 has, 2 first row, 4 first column, 8 last column, 16 ground flux, 32 ground inflow
+  unsigned prole[PPT];  // 1 has, 2 first row, 16 ground flux, 32 ground inflow, 64 last row with a CTA above
 #pragma unroll
   for (int pp = 0; pp < PPT; ++pp) {
     const int q = threadIdx.x + pp * TT;
@@ -1581,9 +1581,9 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
     pq[pp] = q; pjp[pp] = jp; pkp[pp] = kp; pk[pp] = k;
     pqi[pp] = (kl + 1) * RS + jp + 1;
     prb[pp] = ((int64_t)k * ny + j) * nx;
-    prole[pp] = (has ? 1u : 0u) | (has && kl == 0 ? 2u : 0u) | (has && jp == 0 ? 4u : 0u) |
-                (has && jp == ny - 1 ? 8u : 0u) | (has && !fz && k == 0 && slot >= 0 ? 16u : 0u) |
-                (has && fz && kp == 0 ? 32u : 0u);
+    prole[pp] = (has ? 1u : 0u) | (has && kl == 0 ? 2u : 0u) |
+                (has && !fz && k == 0 && slot >= 0 ? 16u : 0u) | (has && fz && kp == 0 ? 32u : 0u) |
+                (has && kl == rows - 1 && rank < C - 1 ? 64u : 0u);
   }
   auto prefetch = [&](int d) {
 #pragma unroll
@@ -1599,28 +1599,61 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
         }
       }
     }
-    if (periodic && (d + 1) % CL_CHUNK == 0 && d + 1 < nplanes) load_inflow((d + 1) / CL_CHUNK);
+    // a chunk of inflow rows two hyperplanes before it starts: the first
+    // column's ghosts of hyperplane c*CL_CHUNK are written on the one before
+    if (periodic && (d + 2) % CL_CHUNK == 0 && d + 2 < nplanes) load_inflow((d + 2) / CL_CHUNK);
     cp_async_commit();
+  };
+  // Threads t < rows*MO move the y-wrap values between the staged chunks and
+  // the hyperplane buffers' first and last columns, one value each, so that no
+  // pencil carries that work: the ghost column of hyperplane dn (in the buffer
+  // that is then the previous one), and the last column of hyperplane dp.
+  const int nmove = rows * MO;
+  auto fill_ghost_col = [&](T* buf, int dn) {
+    const int t = threadIdx.x;
+    if (t < nmove) {
+      const int m = t / rows, kl = t - m * rows;
+      if (kl < nrows)
+        buf[(size_t)m * P + (kl + 1) * RS] =
+            periodic ? win[((size_t)(((dn / CL_CHUNK) & 1) * MO + m) * rows + kl) * CL_CHUNK +
+                           dn % CL_CHUNK]
+                     : I_amb;
+    }
+  };
+  auto copy_last_col = [&](const T* buf, int dp) {
+    const int t = threadIdx.x;
+    if (periodic && t < nmove) {
+      const int m = t / rows, kl = t - m * rows;
+      if (kl < nrows)
+        wout[((size_t)(((dp / CL_CHUNK) & 1) * MO + m) * rows + kl) * CL_CHUNK + dp % CL_CHUNK] =
+            buf[(size_t)m * P + (kl + 1) * RS + ny];
+    }
   };
   if (periodic) load_inflow(0);
   for (int d = 0; d < OCT_AHEAD - 1; ++d) prefetch(d);
   cp_async_wait<OCT_AHEAD - 2>();  // group 0, which holds chunk 0 of the inflow rows
+  __syncthreads();
+  fill_ghost_col(buf1, 0);  // hyperplane 0 reads buf1 as its previous one
   // the first cluster barrier also publishes the ambient-filled buffers
   cluster_arrive_release();
-  // the upstream CTA's shared memory, for the row below this CTA's first row
-  const T* up0 = rank > 0 ? cl.map_shared_rank(buf0, rank - 1) : nullptr;
-  const T* up1 = rank > 0 ? cl.map_shared_rank(buf1, rank - 1) : nullptr;
+  // the downstream CTA's buffers: this CTA's last row goes straight into their
+  // ghost row below the first row (a store before the barrier's release, not
+  // a load after its acquire, so its latency is not on the next hyperplane)
+  T* dn0 = rank < C - 1 ? cl.map_shared_rank(buf0, rank + 1) : nullptr;
+  T* dn1 = rank < C - 1 ? cl.map_shared_rank(buf1, rank + 1) : nullptr;
   for (int d = 0; d < nplanes; ++d) {
     prefetch(d + OCT_AHEAD - 1);  // an empty group past the last plane
     T* cur = (d & 1) ? buf1 : buf0;
     T* prev = (d & 1) ? buf0 : buf1;
-    const T* uprev = (d & 1) ? up0 : up1;
+    T* dcur = (d & 1) ? dn1 : dn0;
     cp_async_wait<OCT_AHEAD - 1>();  // this plane's group has landed
     cluster_wait_acquire();
-    // a finished chunk of outflow rows leaves for global memory
-    if (periodic && d > 0 && d % CL_CHUNK == 0) store_outflow(d / CL_CHUNK - 1);
+    // the last column of hyperplane d-1 into its chunk; a chunk whose last
+    // column arrived on the previous hyperplane leaves for global memory
+    if (d > 0) copy_last_col(prev, d - 1);
+    if (periodic && d > 1 && (d - 1) % CL_CHUNK == 0) store_outflow((d - 1) / CL_CHUNK - 1);
+    if (d + 1 < nplanes) fill_ghost_col(cur, d + 1);
     const int sl = d % OCT_AHEAD;
-    const int ch = (d / CL_CHUNK) & 1, tt = d % CL_CHUNK;
     T gsv[PPT], qsv[PPT];
 #pragma unroll
     for (int pp = 0; pp < PPT; ++pp) {
@@ -1629,22 +1662,12 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
       const bool act = (prole[pp] & 1u) && ip >= 0 && ip < nx;
       T gs = (T)0, qs = (T)0;
       if (act) {
-        // inflow ghosts of this cell: z below the first row, y left of the first column
-        if (prole[pp] & 2u) {
+        // the ground's (or the ambient) z-inflow below the first CTA's first row;
+        // the other CTAs' got it from the CTA below on the previous hyperplane
+        if ((prole[pp] & 2u) && kp == 0) {
+          const T z = fz ? (T)ig_ring[(size_t)sl * ny + jp] : I_amb;
 #pragma unroll
-          for (int m = 0; m < MO; ++m) {
-            T z;
-            if (kp > 0) z = uprev[(size_t)m * P + (size_t)rows * RS + jp + 1];
-            else z = fz ? (T)ig_ring[(size_t)sl * ny + jp] : I_amb;
-            prev[(size_t)m * P + jp + 1] = z;
-          }
-        }
-        if (prole[pp] & 4u) {
-          const int kl = kp - r0;
-#pragma unroll
-          for (int m = 0; m < MO; ++m)
-            prev[(size_t)m * P + (kl + 1) * RS] =
-                periodic ? win[((size_t)(ch * MO + m) * rows + kl) * CL_CHUNK + tt] : I_amb;
+          for (int m = 0; m < MO; ++m) prev[(size_t)m * P + jp + 1] = z;
         }
         const T2 kab = kab_ring[(size_t)sl * S + pq[pp]];
         const bool ground_out = (prole[pp] & 16u) != 0;
@@ -1658,14 +1681,9 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
           const T den = kab.x + ix + iy + iz;
           const T v = sweep_div(num, den);
           cur[(size_t)m * P + qi] = v;
+          if (prole[pp] & 64u) dcur[(size_t)m * P + jp + 1] = v;
           gs = gs + cw[m] * v;
           if (ground_out) qs = qs + cwm[m] * v;
-        }
-        if (periodic && (prole[pp] & 8u)) {
-          const int kl = kp - r0;
-#pragma unroll
-          for (int m = 0; m < MO; ++m)
-            wout[((size_t)(ch * MO + m) * rows + kl) * CL_CHUNK + tt] = cur[(size_t)m * P + qi];
         }
       } else if (prole[pp] & 1u) {
         // before its first cell a pencil's x-inflow is the ambient intensity
@@ -1690,7 +1708,13 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
     }
   }
   cluster_wait_acquire();
-  if (periodic) store_outflow((nplanes - 1) / CL_CHUNK);
+  // the last hyperplane's last column, then every chunk not yet flushed
+  copy_last_col(((nplanes - 1) & 1) ? buf1 : buf0, nplanes - 1);
+  __syncthreads();
+  if (periodic) {
+    for (int c = max(0, (nplanes - 1) / CL_CHUNK - 1); c <= (nplanes - 1) / CL_CHUNK; ++c)
+      if ((c + 1) * CL_CHUNK + 1 > nplanes - 1) store_outflow(c);
+  }
   cp_async_wait<0>();
 }
 
