@@ -278,9 +278,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--form", default="plain", choices=["plain", "mixed"],
+    ap.add_argument("--form", default="plain", choices=["plain", "mixed", "learned"],
                     help="plain: FP64 throughout; mixed: FP32 DOM sweep and multigrid "
-                         "preconditioner, pressure tolerance 1e-8")
+                         "preconditioner, pressure tolerance 1e-8; learned: mixed with the "
+                         "pressure solve in flexible CG preconditioned by the trained U-Net "
+                         "(bf16 tensor-core convolutions), V-cycle fallback on a stall")
     ap.add_argument("--no-clocks", action="store_true",
                     help="skip the clock sampler (diagnostics only; the line then has no clocks)")
     ap.add_argument("--nx", type=int, default=None,
@@ -365,7 +367,7 @@ def main():
         # octant sweeps (paths 1, 4, 6, 7, 8): read (kappa, kappa*B) once and write
         # the 8 octant partial G fields (FP32 in the mixed form; wrap rows and
         # ground partials < 1% more); per-ordinate paths write every intensity
-        "dom_sweep": (N * (8.0 + 4.0 * 8) if args.form == "mixed" else
+        "dom_sweep": (N * (8.0 + 4.0 * 8) if args.form != "plain" else
                       N * (16.0 + 8.0 * 8) if dom_mode in (1, 4, 6, 7, 8) else N * (8.0 * M + 16.0)),
         "species_transport": N * 8.0 * 12,
         "edc": N * 8.0 * 11,
@@ -409,11 +411,11 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.form == "plain" else "f64+f32",
+            "dtype": {"plain": "f64", "mixed": "f64+f32"}.get(args.form, "f64+f32+bf16"),
             "data": "synthetic",
             "config": {"workload": (WORKLOAD if not args.nx else
                                     f"tier3_step_{args.nx}x120x60_S8_fp64").replace(
-                                        "fp64", "fp64" if args.form == "plain" else "mixed"),
+                                        "fp64", "fp64" if args.form == "plain" else args.form),
                        "form": args.form, "cells": cells, "ordinates": M,
                        "parallelism": f"replicas{ws}", "l2": "inputs larger than L2",
                        "projection_rtol": solver.rtol},

@@ -85,6 +85,19 @@ SIGNATURES = {
     "fs_proj_set_coarse_tail": (I, [P, I]),
     "fs_proj_set_precision": (I, [P, I]),
     "fs_proj_stats": (I, [P, C.POINTER(D)]),
+    "fs_proj_set_learned": (I, [P, P, I, D]),
+    "fs_proj_set_log": (I, [P, P, P]),
+    "fs_proj_fcg_stats": (I, [P, C.POINTER(D)]),
+    "fs_unet_nparams": (I64, []),
+    "fs_unet_create": (I, [I, I, I, PP]),
+    "fs_unet_destroy": (None, [P]),
+    "fs_unet_set_params": (I, [P, P, I64, P]),
+    "fs_unet_get_params": (I, [P, P, I64, P]),
+    "fs_unet_get_grads": (I, [P, P, I64, P]),
+    "fs_unet_apply": (I, [P, P, P, P]),
+    "fs_unet_forward": (I, [P, P, P, P]),
+    "fs_unet_grad": (I, [P, P, P, C.POINTER(D), P]),
+    "fs_unet_train_step": (I, [P, P, P, C.c_float, C.POINTER(D), P]),
     "fs_divergence_max": (I, [_G, P, P, P, P, P, P, C.POINTER(D), P]),
     "fs_dom_create": (I, [_G, I, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(D), D,
                           PP]),

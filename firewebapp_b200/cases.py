@@ -113,3 +113,20 @@ def batch_cases(n: int = 32, seed0: int = 0, nx_range=(200, 600)) -> list[dict]:
             wind_speed_m_s=u10, jitter_seed=seed0 + k,
         ))
     return out
+
+
+def learned_cases(n: int = 4, seed0: int = 100, nx: int = 400) -> list[dict]:
+    """Cases for the learned preconditioner's training pairs and held-out
+    runs: the 400x120x60 workload (``nx`` x-cells) with U10 ~ U(2, 8) m/s and
+    moisture ~ U(0.02, 0.12) from a PCG64 stream seeded with ``seed0 + k``
+    (also the case's particle-jitter seed).  Grid: (60, 120, nx) cells."""
+    import numpy as np
+    out = []
+    for k in range(n):
+        rng = np.random.Generator(np.random.PCG64(seed0 + k))
+        c = scaled(CFG2, nx=nx) if nx != 400 else dict(CFG2)
+        c.update(wind_speed_m_s=float(rng.uniform(2.0, 8.0)),
+                 initial_moisture_frac=float(rng.uniform(0.02, 0.12)),
+                 jitter_seed=seed0 + k)
+        out.append(c)
+    return out

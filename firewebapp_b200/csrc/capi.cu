@@ -364,6 +364,57 @@ int fs_proj_stats(void* handle, double* out8) {
   return FS_OK;
 }
 
+int fs_proj_set_learned(void* handle, void* net, int max_learned, double stall) {
+  if (!handle) return check(FS_EARG, "fs_proj_set_learned");
+  return check(proj_set_learned(handle, net, max_learned, stall), "fs_proj_set_learned");
+}
+int fs_proj_set_log(void* handle, double* r0, double* x0) {
+  if (!handle) return check(FS_EARG, "fs_proj_set_log");
+  return check(proj_set_log(handle, r0, x0), "fs_proj_set_log");
+}
+int fs_proj_fcg_stats(void* handle, double* out4) {
+  if (!handle || !out4) return FS_EARG;
+  proj_fcg_stats(handle, out4);
+  return FS_OK;
+}
+
+int64_t fs_unet_nparams(void) { return unet_nparams(); }
+int fs_unet_create(int nz, int ny, int nx, void** handle) {
+  if (!handle) return check(FS_EARG, "fs_unet_create");
+  return check(unet_create(nz, ny, nx, handle), "fs_unet_create");
+}
+void fs_unet_destroy(void* handle) { unet_destroy(handle); }
+int fs_unet_set_params(void* handle, const float* host, int64_t n, void* stream) {
+  if (!handle || !host) return check(FS_EARG, "fs_unet_set_params");
+  return check(unet_set_params(handle, host, n, (cudaStream_t)stream), "fs_unet_set_params");
+}
+int fs_unet_get_params(void* handle, float* host, int64_t n, void* stream) {
+  if (!handle || !host) return check(FS_EARG, "fs_unet_get_params");
+  return check(unet_get(handle, 0, host, n, (cudaStream_t)stream), "fs_unet_get_params");
+}
+int fs_unet_get_grads(void* handle, float* host, int64_t n, void* stream) {
+  if (!handle || !host) return check(FS_EARG, "fs_unet_get_grads");
+  return check(unet_get(handle, 1, host, n, (cudaStream_t)stream), "fs_unet_get_grads");
+}
+int fs_unet_apply(void* handle, const double* r, double* z, void* stream) {
+  if (!handle || !r || !z) return check(FS_EARG, "fs_unet_apply");
+  return check(unet_apply(handle, r, z, (cudaStream_t)stream), "fs_unet_apply");
+}
+int fs_unet_forward(void* handle, const float* r, float* z, void* stream) {
+  if (!handle || !r || !z) return check(FS_EARG, "fs_unet_forward");
+  return check(unet_forward_f32(handle, r, z, (cudaStream_t)stream), "fs_unet_forward");
+}
+int fs_unet_grad(void* handle, const float* r, const float* tau, double* loss, void* stream) {
+  if (!handle || !r || !tau) return check(FS_EARG, "fs_unet_grad");
+  return check(unet_grad(handle, r, tau, loss, (cudaStream_t)stream), "fs_unet_grad");
+}
+int fs_unet_train_step(void* handle, const float* r, const float* tau, float lr, double* loss,
+                       void* stream) {
+  if (!handle || !r || !tau || !loss || !(lr > 0.f)) return check(FS_EARG, "fs_unet_train_step");
+  return check(unet_train_step(handle, r, tau, lr, loss, (cudaStream_t)stream),
+               "fs_unet_train_step");
+}
+
 int fs_proj_set_precision(void* handle, int fp32) {
   if (!handle) return FS_EARG;
   return check(proj_set_precision(handle, fp32), "fs_proj_set_precision");

@@ -92,6 +92,23 @@ int proj_configure(void* h, int nu, double omega);
 int proj_set_coarse_tail(void* h, int on);
 int proj_set_precision(void* h, int fp32);
 void proj_stats(void* h, double* out8);
+// learned preconditioner (flexible CG); net = NULL returns to the V-cycle
+int proj_set_learned(void* h, void* net, int max_learned, double stall);
+// copies of the residual and the iterate at the start of every solve (NULL: off)
+int proj_set_log(void* h, double* r0, double* x0);
+void proj_fcg_stats(void* h, double* out4);
+
+// U-Net (unet.cu)
+int64_t unet_nparams();
+int unet_create(int nz, int ny, int nx, void** out);
+void unet_destroy(void* h);
+int unet_set_params(void* h, const float* host, int64_t n, cudaStream_t st);
+int unet_get(void* h, int which, float* host, int64_t n, cudaStream_t st);
+int unet_apply(void* h, const double* r, double* z, cudaStream_t st);
+int unet_forward_f32(void* h, const float* r, float* z, cudaStream_t st);
+int unet_grad(void* h, const float* r, const float* tau, double* loss, cudaStream_t st);
+int unet_train_step(void* h, const float* r, const float* tau, float lr, double* loss,
+                    cudaStream_t st);
 int launch_div_resid_max(const GridDev& g, const double* u, const double* v, const double* w,
                          const double* u_in, const double* target, double* div_out,
                          unsigned long long* out_key, cudaStream_t st);

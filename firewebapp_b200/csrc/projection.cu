@@ -23,6 +23,7 @@
 #include <vector>
 #include <chrono>
 #include <cstdlib>
+#include <cmath>
 #include "common.cuh"
 #include "kernels.h"
 
@@ -84,6 +85,17 @@ struct ProjCtx {
   // host-side statistics of the last solve (ms): total, fetch waits (sum, max),
   // graph-launch calls (sum, max), fetches, iteration launches, iterations
   double stats[8];
+  // learned form: flexible CG preconditioned by a U-Net (unet.cu), falling
+  // back to V-cycle PCG from the current iterate when it stalls
+  void* net;
+  int max_learned;    // learned iterations before the fallback
+  double stall;       // fallback when the residual norm shrinks by less than
+                      // this factor per iteration (over the last 3)
+  double* log_r0;     // optional copies of the starting residual / iterate
+  double* log_x0;
+  // last solve: learned iterations, V-cycle iterations, fell back (0/1);
+  // then the number of fallbacks since creation
+  double fcg[4];
 };
 
 // ---------------------------------------------------------------------------
@@ -518,6 +530,35 @@ __global__ void k_zero_if_zero_rhs(int64_t n, const double* __restrict__ scal, d
   if (c < n) x[c] = 0.0;
 }
 
+// Flexible CG (truncated to one previous direction): p = z - (z.q_prev / p.q_prev) p,
+// first iteration p = z.  Slots: 10 z.q_prev, 11 p.q of the previous iteration.
+__global__ void k_fcg_dir(int64_t n, const double* __restrict__ scal, const double* __restrict__ z,
+                          double* p) {
+  PCG_SKIP(scal + SC_DONE);
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  if (scal[SC_IT] == 0.0) { p[c] = z[c]; return; }
+  const double beta = -scal[10] / scal[11];
+  p[c] = z[c] + beta * p[c];
+}
+
+// alpha = p.r / p.q into slot 0 (read by k_pcg_update); a zero direction
+// (p.q = 0, e.g. a network output of 0) gives alpha = 0, so the residual
+// stalls and the solve falls back instead of dividing by zero
+__global__ void k_fcg_alpha(double* scal) {
+  if (scal[SC_DONE] != 0.0) return;
+  const bool ok = scal[1] > 0.0;
+  scal[0] = ok ? scal[12] : 0.0;
+  if (!ok) scal[1] = 1.0;
+}
+
+// restart as V-cycle PCG from the current iterate (the residual was just
+// recomputed into slot 5)
+__global__ void k_fcg_restart(double* scal) {
+  scal[SC_IT] = 0.0;
+  scal[SC_DONE] = (scal[5] < scal[6]) ? 1.0 : 0.0;
+}
+
 // ---------------------------------------------------------------------------
 // velocity correction (projection_3d.py:818-842)
 // ---------------------------------------------------------------------------
@@ -636,6 +677,12 @@ void* proj_create(const GridDev& g) {
   for (int l = 0; l < 16; ++l) P->lev32[l] = MGLevelT<float>{};
   for (int q = 0; q < 8; ++q) P->stats[q] = 0.0;
   P->omega = MG_OMEGA_DEFAULT;
+  P->net = nullptr;
+  P->max_learned = 30;
+  P->stall = 0.9;
+  P->log_r0 = nullptr;
+  P->log_x0 = nullptr;
+  for (int q = 0; q < 4; ++q) P->fcg[q] = 0.0;
   cudaStreamCreateWithFlags(&P->cs, cudaStreamNonBlocking);
   if (cudaGetLastError() != cudaSuccess || !P->p_prev) {
     proj_destroy(P);
@@ -1107,6 +1154,96 @@ static int fetch(ProjCtx* P, int n, cudaStream_t st) {
   return rc;
 }
 
+// One flexible-CG iteration with the U-Net preconditioner (kernels as in
+// pcg_iteration; the host reads the scalars after every iteration).
+static int fcg_iteration(ProjCtx* P, double* x, int it, cudaStream_t st) {
+  MGLevel& l0 = P->lev[0];
+  const int64_t n = l0.n;
+  const double* done = P->scal + SC_DONE;
+  int rc = unet_apply(P->net, P->pc_r, P->pc_z, st);
+  if (rc) return rc;
+  if (it > 0) {
+    k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, P->pc_z, P->pc_q, P->partial, done);
+    k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 10, done);  // z.q_prev
+    fs_count_launch(); fs_count_launch();
+  }
+  k_fcg_dir<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, P->pc_z, P->pc_p);
+  k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.nx, l0.ny, l0.nz, l0.gx, l0.gy, l0.gz,
+                                                   l0.e, P->pc_p, P->pc_q, P->partial, done);
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 1, done);  // p.q
+  k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, P->pc_p, P->pc_r, P->partial, done);
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 12, done);  // p.r
+  k_fcg_alpha<<<1, 1, 0, st>>>(P->scal);  // alpha = p.r / p.q
+  k_pcg_update<<<RED_BLOCKS, RED_THREADS, 0, st>>>(P->g, P->scal, x, P->pc_r, P->pc_p, P->pc_q,
+                                                   P->partial);
+  k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5, done);  // ||r_A||^2
+  k_set_scal<<<1, 1, 0, st>>>(P->scal, 11, 1);
+  k_pcg_check<<<1, 1, 0, st>>>(P->scal);
+  for (int k = 0; k < 10; ++k) fs_count_launch();
+  return cuda_status();
+}
+
+// Learned iterations until convergence, a stall or max_learned; on a stall
+// the residual is recomputed and the scalars reset so that the V-cycle PCG
+// loop continues from the current iterate.
+static int fcg_solve(ProjCtx* P, double* x, int maxiter, int* learned, cudaStream_t st) {
+  const GridDev& g = P->g;
+  MGLevel& l0 = P->lev[0];
+  std::vector<double> rn;
+  int it = 0;
+  while (true) {
+    int stt = fetch(P, 9, st);
+    if (stt) return stt;
+    const double bn2 = P->h_scal[4], rn2 = P->h_scal[5];
+    if (!(bn2 == bn2) || !(rn2 == rn2)) return FS_ENONFINITE;
+    if (P->h_scal[SC_DONE] != 0.0) break;
+    rn.push_back(rn2);
+    bool fall = it >= P->max_learned || it >= maxiter;
+    if (!fall && it >= 3) {
+      const double f = std::pow(rn2 / rn[it - 3], 1.0 / 6.0);  // per-iteration norm factor
+      fall = !(f < P->stall);
+    }
+    if (fall) {
+      k_pcg_residual<<<RED_BLOCKS, RED_THREADS, 0, st>>>(g, l0.gx, l0.gy, l0.gz, l0.e, P->rhs, x,
+                                                         P->pc_r, P->partial);
+      k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5, nullptr);
+      k_fcg_restart<<<1, 1, 0, st>>>(P->scal);
+      fs_count_launch(); fs_count_launch(); fs_count_launch();
+      P->fcg[2] = 1.0;
+      P->fcg[3] += 1.0;
+      break;
+    }
+    stt = fcg_iteration(P, x, it, st);
+    if (stt) return stt;
+    ++it;
+  }
+  *learned = it;
+  P->fcg[0] = it;
+  return cuda_status();
+}
+
+int proj_set_learned(void* h, void* net, int max_learned, double stall) {
+  ProjCtx* P = (ProjCtx*)h;
+  if (max_learned < 0 || !(stall > 0.0 && stall <= 1.0)) return FS_EARG;
+  P->net = net;
+  P->max_learned = max_learned;
+  P->stall = stall;
+  return FS_OK;
+}
+
+int proj_set_log(void* h, double* r0, double* x0) {
+  ProjCtx* P = (ProjCtx*)h;
+  if ((r0 == nullptr) != (x0 == nullptr)) return FS_EARG;
+  P->log_r0 = r0;
+  P->log_x0 = x0;
+  return FS_OK;
+}
+
+void proj_fcg_stats(void* h, double* out4) {
+  ProjCtx* P = (ProjCtx*)h;
+  for (int q = 0; q < 4; ++q) out4[q] = P->fcg[q];
+}
+
 // Solve for the pressure and correct u, v, w in place.  The iterations run
 // as graph launches in batches (sized from the previous solve's count); the
 // host reads the converged flag once per batch.
@@ -1129,8 +1266,18 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
   k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 5, nullptr); fs_count_launch();
   k_pcg_init<<<1, 1, 0, st>>>(P->scal, rtol * rtol); fs_count_launch();
   k_zero_if_zero_rhs<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, x); fs_count_launch();
+  if (P->log_r0) {
+    cudaMemcpyAsync(P->log_r0, P->pc_r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(P->log_x0, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+  }
+  int learned = 0;
+  P->fcg[0] = P->fcg[1] = P->fcg[2] = 0.0;
+  if (P->net) {
+    int stt = fcg_solve(P, x, maxiter, &learned, st);
+    if (stt) return stt;
+  }
   if (!P->iter_exec && !P->graph_failed) capture_iteration(P);
-  int launched = 0;
+  int launched = learned;
   int batch = P->last_iters > 2 ? P->last_iters - 2 : 1;
   while (true) {
     int stt = fetch(P, 9, st);
@@ -1150,7 +1297,8 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
     P->stats[6] += batch;
     batch = 2;
   }
-  *iters = (int)P->h_scal[SC_IT];
+  if (P->net && P->fcg[2] != 0.0) P->fcg[1] = P->h_scal[SC_IT];
+  *iters = P->fcg[2] != 0.0 ? learned + (int)P->h_scal[SC_IT] : (int)P->h_scal[SC_IT];
   P->last_iters = *iters;
   P->stats[7] = *iters;
   P->stats[0] = ms_since(t_start);

@@ -89,15 +89,19 @@ class Tier3Solver:
     ``form="plain"`` is FP64 throughout.  ``form="mixed"`` runs the DOM sweep
     and the multigrid preconditioner in FP32; the state, every other kernel,
     the CG (operator, residuals, dot products), the divergence test and all
-    reductions stay FP64.  ``dom_sweep`` forces a DOM sweep path
-    (``fs_dom_set_sweep_mode``; 0 picks automatically)."""
+    reductions stay FP64.  ``form="learned"`` is the mixed form with the
+    pressure solve in flexible CG preconditioned by the U-Net of
+    ``learned.py`` (weights from ``learned_weights``, default the packaged
+    file), falling back to the V-cycle when it stalls.  ``dom_sweep`` forces a
+    DOM sweep path (``fs_dom_set_sweep_mode``; 0 picks automatically)."""
 
     FIELDS = ("rho", "u", "v", "w", "T_g", "Y_fuel", "Y_O2", "Y_H2O", "T_s", "alpha_s",
               "k_turb", "eps_turb", "nu_t", "phi")
 
     def __init__(self, case: dict, device="cuda", projection_cg_rtol: float | None = None,
                  proj_maxiter: int = 200, mg_sweeps: int | None = None, form: str = "plain",
-                 overlap_dom: bool = True, dom_sweep: int = 0):
+                 overlap_dom: bool = True, dom_sweep: int = 0, learned_weights=None,
+                 learned_max: int = 30, learned_stall: float = 0.9):
         self.lib = _lib.lib()
         self.dev = torch.device(device)
         if self.dev.type == "cuda" and self.dev.index is None:
@@ -108,9 +112,10 @@ class Tier3Solver:
         g = su.grid
         self.grid = g
         self.p = dict(su.params)
-        if form not in ("plain", "mixed"):
-            raise ValueError(f"unknown solver form {form!r} (plain or mixed)")
+        if form not in ("plain", "mixed", "learned"):
+            raise ValueError(f"unknown solver form {form!r} (plain, mixed or learned)")
         self.form = form
+        fp32 = form in ("mixed", "learned")
         if projection_cg_rtol is None:
             # the reference's production tolerance for the plain form; the
             # mixed form's pressure tolerance is 1e-8 relative
@@ -171,8 +176,17 @@ class Tier3Solver:
         self.proj = h
         if mg_sweeps is not None:
             check(self.lib.fs_proj_configure(self.proj, int(mg_sweeps), 0.8), "fs_proj_configure")
-        if form == "mixed":
+        if fp32:
             check(self.lib.fs_proj_set_precision(self.proj, 1), "fs_proj_set_precision")
+        self.net = None
+        if form == "learned":
+            from . import learned
+            path = learned.WEIGHTS if learned_weights is None else learned_weights
+            if isinstance(path, np.ndarray):
+                self.net = learned.UNetPreconditioner(*g.shape, params=path)
+            else:
+                self.net = learned.UNetPreconditioner.load(path, *g.shape)
+            learned.attach(self, self.net, learned_max, learned_stall)
         om, wq = level_symmetric(self.p["n_quadrature"])
         self.Omega, self.weights = om, wq
         h2 = _ctypes_void()
@@ -190,7 +204,7 @@ class Tier3Solver:
         if self.overlap_dom:
             from concurrent.futures import ThreadPoolExecutor
             self._pool = ThreadPoolExecutor(max_workers=1, thread_name_prefix="dom")
-        if form == "mixed":
+        if fp32:
             check(self.lib.fs_dom_set_precision(self.dom, 1), "fs_dom_set_precision")
         if dom_sweep:
             check(self.lib.fs_dom_set_sweep_mode(self.dom, int(dom_sweep), 0),
@@ -278,6 +292,9 @@ class Tier3Solver:
         if getattr(self, "proj", None):
             self.lib.fs_proj_destroy(self.proj)
             self.proj = None
+        if getattr(self, "net", None) is not None:
+            self.net.close()
+            self.net = None
         if getattr(self, "dom", None):
             self.lib.fs_dom_destroy(self.dom)
             self.dom = None

@@ -218,6 +218,49 @@ int fs_proj_set_precision(void* handle, int fp32);
  * (sum, max), iteration launch calls (sum, max), then the number of fetches,
  * queued iterations and CG iterations (diagnostics; no reference counterpart). */
 int fs_proj_stats(void* handle, double* out8);
+
+/* Learned form (no counterpart in the reference): with net != NULL (a
+ * fs_unet_create handle for the same grid) fs_proj_project runs flexible CG
+ * preconditioned by the U-Net, truncated to one previous direction:
+ *   z = N(r), p = z - (z.q_prev / p.q_prev) p_prev, q = S p,
+ *   alpha = p.r / p.q, x += alpha p, r -= alpha q,
+ * with the same stopping test.  When the residual norm shrinks by less than
+ * `stall` per iteration (geometric mean of the last three) or after
+ * `max_learned` iterations, the residual is recomputed and V-cycle PCG
+ * continues from the current iterate (the fallback).  net = NULL restores
+ * V-cycle PCG. */
+int fs_proj_set_learned(void* handle, void* net, int max_learned, double stall);
+/* Copy the residual and the iterate at the start of every solve into r0 and
+ * x0 (device arrays of Nx*Ny*Nz doubles; both NULL turns it off).  The pair
+ * (r0, x_solved - x0) solves S e = r0: the learned preconditioner's training
+ * data. */
+int fs_proj_set_log(void* handle, double* r0, double* x0);
+/* Last solve: learned iterations, V-cycle iterations after a fallback, fell
+ * back (0/1); then the number of fallbacks since creation. */
+int fs_proj_fcg_stats(void* handle, double* out4);
+
+/* The learned preconditioner: a 3-D conv U-Net (4 levels, 16/32/48/64
+ * channels, bfloat16 activations, fp32 master weights, mma.sync tensor-core
+ * convolutions), sized for one (nz, ny, nx) grid.  Parameters are a flat fp32
+ * vector of fs_unet_nparams() values: per conv layer W[27][cin][cout] then
+ * bias[cout], then the 1x1 head's w[16] and b. */
+int64_t fs_unet_nparams(void);
+int fs_unet_create(int nz, int ny, int nx, void** handle);
+void fs_unet_destroy(void* handle);
+/* host <-> device parameter copies (synchronous); set resets Adam's state */
+int fs_unet_set_params(void* handle, const float* host, int64_t n, void* stream);
+int fs_unet_get_params(void* handle, float* host, int64_t n, void* stream);
+/* gradient of the last fs_unet_grad / fs_unet_train_step (synchronous) */
+int fs_unet_get_grads(void* handle, float* host, int64_t n, void* stream);
+/* z = N(r / rms(r)), device doubles (the preconditioner) */
+int fs_unet_apply(void* handle, const double* r, double* z, void* stream);
+/* z = N(r), device floats, no scaling */
+int fs_unet_forward(void* handle, const float* r, float* z, void* stream);
+/* mean squared error of N(r) against tau and its gradient (synchronous) */
+int fs_unet_grad(void* handle, const float* r, const float* tau, double* loss, void* stream);
+/* fs_unet_grad, then one Adam step (lr; betas 0.9, 0.999; eps 1e-8) */
+int fs_unet_train_step(void* handle, const float* r, const float* tau, float lr, double* loss,
+                       void* stream);
 /* max |div(u) - target| to *result (synchronises); div_out optional. */
 int fs_divergence_max(const FsGrid* g, const double* u, const double* v, const double* w,
                       const double* u_inlet, const double* div_target, double* div_out,

@@ -1,0 +1,158 @@
+"""The learned preconditioner on the GPU: the U-Net's forward pass and
+parameter gradients against the float64 oracle (which rounds to bfloat16
+where the device stores bfloat16), training, and the learned form of the
+pressure solve (flexible CG with the V-cycle fallback)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from oracle import unet as U
+
+pytestmark = pytest.mark.gpu
+
+SHAPE = (9, 10, 11)   # odd sizes: every level has a ragged 2x2x2 edge
+# bf16 activations: the device and the oracle differ only where fp32
+# accumulation order flips a bf16 rounding (1 ulp = 2^-8 relative) of an
+# element; the forward output then differs by about 1e-3 relative
+FWD_TOL = 1e-2
+# A weight gradient is a sum over voxels of terms of both signs, so an error
+# of the terms is measured against the norm of the sum of their absolute
+# values (the oracle's ``scale``).  The device accumulates each mma in fp32
+# with a bias toward zero that the float64 oracle does not have (about 1e-5
+# relative over a 3x3x3 x 112-channel sum), so a few bf16 roundings per
+# thousand differ by one ulp (2^-8); along the ~20 layers between the loss and
+# the coarsest level these add up to 2-3 % of the terms there (0.2 % at the
+# finest level, 1e-4 at the head).  A wrong tap, channel or mask gives errors
+# of order 1 and a direction far from the oracle's (cosine < 0.99).
+GRAD_TOL = 4e-2
+
+
+def _params(seed=3):
+    rng = np.random.default_rng(seed)
+    p = U.init_params(seed)
+    lay, hw, hb, _n = U.param_layout()
+    for _name, _cin, cout, _w, b in lay:
+        p[b:b + cout] = rng.uniform(0.0, 0.1, cout)
+    return p.astype(np.float32)
+
+
+def _net(params):
+    from firewebapp_b200.learned import UNetPreconditioner
+    return UNetPreconditioner(*SHAPE, params=params)
+
+
+def test_unet_forward_matches_oracle():
+    p = _params()
+    rng = np.random.default_rng(5)
+    r = rng.standard_normal(SHAPE).astype(np.float32)
+    net = _net(p)
+    z = net.forward(torch.tensor(r.ravel(), device="cuda")).cpu().numpy().reshape(SHAPE)
+    zo, _A = U.forward(p.astype(np.float64), r.astype(np.float64), rnd=True)
+    err = rel_l2(z, zo)
+    print("forward rel-L2", err)
+    assert err > 0.0 or np.array_equal(z, zo)
+    assert err <= FWD_TOL
+    # fs_unet_apply scales the residual to unit RMS first
+    r64 = torch.tensor(r.ravel() * 7.5, dtype=torch.float64, device="cuda")
+    z64 = torch.empty_like(r64)
+    net.apply(r64, z64)
+    rs = r.astype(np.float64) * 7.5
+    zo2, _ = U.forward(p.astype(np.float64), rs / np.sqrt(np.mean(rs * rs)), rnd=True)
+    assert rel_l2(z64.cpu().numpy().reshape(SHAPE), zo2) <= FWD_TOL
+    net.close()
+
+
+def test_unet_gradients_match_oracle():
+    p = _params()
+    rng = np.random.default_rng(6)
+    r = rng.standard_normal(SHAPE).astype(np.float32)
+    tau = rng.standard_normal(SHAPE).astype(np.float32)
+    net = _net(p)
+    loss = net.grad(torch.tensor(r.ravel(), device="cuda"), torch.tensor(tau.ravel(), device="cuda"))
+    g = net.get_grads().astype(np.float64)
+    scale = {}
+    Lo, go, _ = U.loss_and_grad(p.astype(np.float64), r.astype(np.float64),
+                                tau.astype(np.float64), rnd=True, scale=scale)
+    assert abs(loss - Lo) <= 1e-3 * Lo
+    lay, hw, hb, n = U.param_layout()
+    errs, rel, cos = {}, {}, {}
+    for name, cin, cout, w, b in lay:
+        for key, sl in ((name + ".W", slice(w, w + 27 * cin * cout)), (name + ".b", slice(b, b + cout))):
+            d = np.linalg.norm(g[sl] - go[sl])
+            errs[key] = d / scale[key]
+            rel[key] = rel_l2(g[sl], go[sl])
+            cos[key] = float(g[sl] @ go[sl] / (np.linalg.norm(g[sl]) * np.linalg.norm(go[sl])))
+    errs["head"] = np.linalg.norm(g[hw:n] - go[hw:n]) / scale["head"]
+    print("error / scale", {k: f"{v:.1e}" for k, v in errs.items()})
+    print("rel-L2", {k: f"{v:.1e}" for k, v in rel.items()})
+    assert all(v <= GRAD_TOL for v in errs.values()), errs
+    assert all(c >= 0.999 for c in cos.values()), cos
+    net.close()
+
+
+def test_unet_training_reduces_loss():
+    p = _params()
+    rng = np.random.default_rng(7)
+    r = torch.tensor(rng.standard_normal(SHAPE).astype(np.float32).ravel(), device="cuda")
+    tau = torch.tensor(rng.standard_normal(SHAPE).astype(np.float32).ravel(), device="cuda")
+    net = _net(p)
+    losses = [net.train_step(r, tau, 1e-3) for _ in range(60)]
+    assert losses[-1] < 0.5 * losses[0], (losses[0], losses[-1])
+    assert not np.array_equal(net.get_params(), p)
+    net.close()
+
+
+def test_learned_form_matches_mixed_form():
+    """Flexible CG with an untrained network reaches the same tolerance, so the
+    state after five steps matches the V-cycle form within the mixed form's
+    own bound against FP64 (1e-4);
+    with max_learned = 0 it falls back at once and is bit-identical."""
+    from firewebapp_b200.cases import TINY
+    from firewebapp_b200.learned import fcg_stats, init_params
+    from firewebapp_b200.solver import Tier3Solver
+    a = Tier3Solver(TINY, form="mixed")
+    b = Tier3Solver(TINY, form="learned", learned_weights=init_params(1), learned_stall=1.0,
+                    learned_max=200)
+    c = Tier3Solver(TINY, form="learned", learned_weights=init_params(1), learned_max=0)
+    its_b = []
+    for _ in range(5):
+        a.step(); b.step(); c.step()
+        its_b.append(fcg_stats(b)["learned_iters"])
+        st = fcg_stats(c)
+        assert st["fell_back"] and st["learned_iters"] == 0
+    sa, sb, sc = a.state(), b.state(), c.state()
+    for k in ("u", "v", "w", "T_g", "Y_O2", "rho"):
+        # both forms stop at ||r|| < 1e-8 ||b||; v is nearly zero on this
+        # case, so its relative difference is the largest (about 5e-6)
+        assert rel_l2(sb[k], sa[k]) <= 1e-4, k
+        assert np.array_equal(sc[k], sa[k]), k
+    assert min(its_b) > 0
+    for s in (a, b, c):
+        s.close()
+
+
+def test_pair_logger_pairs_solve_the_pressure_system():
+    """The logged residual and start iterate satisfy S (x_solved - x0) = r0 to
+    the solver tolerance, and the float32 pair is their scaled copy."""
+    from firewebapp_b200.cases import TINY
+    from firewebapp_b200.learned import PairLogger
+    from firewebapp_b200.solver import Tier3Solver
+    from firewebapp_b200._lib import check, ptr
+    s = Tier3Solver(TINY, projection_cg_rtol=1e-10)
+    log = PairLogger(s)
+    for _ in range(3):
+        s.step()
+    r, e = log.take()
+    e64 = (s.pressure_view().reshape(-1) - log.x0).contiguous()
+    Se = torch.empty(s.n, dtype=torch.float64, device="cuda")
+    check(s.lib.fs_proj_apply(s.proj, ptr(e64), ptr(Se),
+                              torch.cuda.current_stream().cuda_stream), "apply")
+    torch.cuda.synchronize()
+    r0 = log.r0.cpu().numpy()
+    assert rel_l2(Se.cpu().numpy(), r0) <= 1e-6
+    rms = np.sqrt(np.mean(r0 * r0))
+    assert rel_l2(r.cpu().numpy(), r0 / rms) <= 1e-7
+    assert rel_l2(e.cpu().numpy(), e64.cpu().numpy() / rms) <= 1e-7
+    log.close()
+    s.close()
