@@ -88,6 +88,8 @@ SIGNATURES = {
     "fs_proj_set_learned": (I, [P, P, I, D]),
     "fs_proj_set_log": (I, [P, P, P]),
     "fs_proj_fcg_stats": (I, [P, C.POINTER(D)]),
+    "fs_proj_smooth_pair": (I, [P, P, P, P, P, P]),
+    "fs_unet_set_output_scale": (I, [P, C.c_float]),
     "fs_unet_nparams": (I64, []),
     "fs_unet_create": (I, [I, I, I, PP]),
     "fs_unet_destroy": (None, [P]),

@@ -378,6 +378,17 @@ int fs_proj_fcg_stats(void* handle, double* out4) {
   return FS_OK;
 }
 
+int fs_proj_smooth_pair(void* handle, const double* r0, const double* e0, float* r1, float* e1,
+                        void* stream) {
+  if (!handle || !r0 || !e0 || !r1 || !e1) return check(FS_EARG, "fs_proj_smooth_pair");
+  return check(proj_smooth_pair(handle, r0, e0, r1, e1, (cudaStream_t)stream),
+               "fs_proj_smooth_pair");
+}
+int fs_unet_set_output_scale(void* handle, float s) {
+  if (!handle) return check(FS_EARG, "fs_unet_set_output_scale");
+  return check(unet_set_output_scale(handle, s), "fs_unet_set_output_scale");
+}
+
 int64_t fs_unet_nparams(void) { return unet_nparams(); }
 int fs_unet_create(int nz, int ny, int nx, void** handle) {
   if (!handle) return check(FS_EARG, "fs_unet_create");

@@ -109,6 +109,11 @@ int unet_forward_f32(void* h, const float* r, float* z, cudaStream_t st);
 int unet_grad(void* h, const float* r, const float* tau, double* loss, cudaStream_t st);
 int unet_train_step(void* h, const float* r, const float* tau, float lr, double* loss,
                     cudaStream_t st);
+int unet_correct(void* h, const float* r, const float* base, float* out, cudaStream_t st);
+int unet_set_output_scale(void* h, float s);
+int64_t unet_cells(void* h);
+int proj_smooth_pair(void* h, const double* r0, const double* e0, float* r1, float* e1,
+                     cudaStream_t st);
 int launch_div_resid_max(const GridDev& g, const double* u, const double* v, const double* w,
                          const double* u_in, const double* target, double* div_out,
                          unsigned long long* out_key, cudaStream_t st);

@@ -552,6 +552,28 @@ __global__ void k_fcg_alpha(double* scal) {
   if (!ok) scal[1] = 1.0;
 }
 
+// out = b - S x (level operator, any precision)
+template <typename T>
+__global__ void k_lp_residual(int nx, int ny, int nz, const T* __restrict__ gx,
+                              const T* __restrict__ gy, const T* __restrict__ gz,
+                              const T* __restrict__ e, const T* __restrict__ b,
+                              const T* __restrict__ x, T* out) {
+  int64_t n = (int64_t)nx * ny * nz;
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  int i = (int)(c % nx);
+  int j = (int)((c / nx) % ny);
+  int k = (int)(c / ((int64_t)nx * ny));
+  out[c] = b[c] - mg_apply(nx, ny, nz, gx, gy, gz, e, x, c, i, j, k);
+}
+
+// e1 = float(e0) - t
+__global__ void k_lp_err(int64_t n, const double* __restrict__ e0, const float* __restrict__ t,
+                         float* e1) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c < n) e1[c] = (float)e0[c] - t[c];
+}
+
 // restart as V-cycle PCG from the current iterate (the residual was just
 // recomputed into slot 5)
 __global__ void k_fcg_restart(double* scal) {
@@ -1154,13 +1176,78 @@ static int fetch(ProjCtx* P, int n, cudaStream_t st) {
   return rc;
 }
 
-// One flexible-CG iteration with the U-Net preconditioner (kernels as in
+// Pre-smoothing of the learned preconditioner: nu damped-Jacobi sweeps on
+// the FP32 level-0 operator from x = 0 for S t = r32, ending in f.t (the
+// V-cycle's first half at level 0); then f.b = r32 - S t.
+static void lp_presmooth(ProjCtx* P, cudaStream_t st) {
+  MGLevelT<float>& f = P->lev32[0];
+  const unsigned nb = blocks_for(f.n, 256);
+  const float* src = nullptr;
+  for (int i = 0; i < P->nu; ++i) {
+    float* dst = ((P->nu - 1 - i) % 2 == 0) ? f.t : f.s;
+    k_mg_jacobi<float><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv,
+                                           P->r32, src, dst, P->omega, nullptr);
+    src = dst;
+    fs_count_launch();
+  }
+  k_lp_residual<float><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, P->r32, f.t,
+                                           f.b);
+  fs_count_launch();
+}
+
+// The learned preconditioner z = M(r), a two-level cycle whose coarse
+// correction is the network: pre-smoothing (lp_presmooth), s = t + N(r1)
+// (the network's estimate of S^-1 r1, scaled back), then nu post-smoothing
+// sweeps from s.  The sweeps remove the high-frequency part of the network's
+// error, which the residual norm would otherwise be dominated by.
+static int learned_precond(ProjCtx* P, cudaStream_t st) {
+  MGLevelT<float>& f = P->lev32[0];
+  const int64_t n = f.n;
+  const unsigned nb = blocks_for(n, 256);
+  k_cvt_d2f<<<nb, 256, 0, st>>>(n, P->pc_r, P->r32, nullptr);
+  fs_count_launch();
+  lp_presmooth(P, st);
+  int rc = unet_correct(P->net, f.b, f.t, f.s, st);
+  if (rc) return rc;
+  const float* src = f.s;
+  for (int i = 0; i < P->nu; ++i) {
+    float* dst = (i == P->nu - 1) ? P->z32 : ((i % 2 == 0) ? f.t : f.x);
+    k_mg_jacobi<float><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv,
+                                           P->r32, src, dst, P->omega, nullptr);
+    src = dst;
+    fs_count_launch();
+  }
+  k_cvt_f2d<<<nb, 256, 0, st>>>(n, P->z32, P->pc_z, nullptr);
+  fs_count_launch();
+  return cuda_status();
+}
+
+// Training pair for the network from a logged solve (r0, e0 with S e0 = r0):
+// the residual after pre-smoothing and the error left, r1 = r0 - S t and
+// e1 = e0 - t, in FP32 (the operator of the last rebuild).
+int proj_smooth_pair(void* h, const double* r0, const double* e0, float* r1, float* e1,
+                     cudaStream_t st) {
+  ProjCtx* P = (ProjCtx*)h;
+  if (!P->fp32) return FS_EARG;
+  MGLevelT<float>& f = P->lev32[0];
+  const int64_t n = f.n;
+  const unsigned nb = blocks_for(n, 256);
+  k_cvt_d2f<<<nb, 256, 0, st>>>(n, r0, P->r32, nullptr);
+  fs_count_launch();
+  lp_presmooth(P, st);
+  cudaMemcpyAsync(r1, f.b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+  k_lp_err<<<nb, 256, 0, st>>>(n, e0, f.t, e1);
+  fs_count_launch();
+  return cuda_status();
+}
+
+// One flexible-CG iteration with the learned preconditioner (kernels as in
 // pcg_iteration; the host reads the scalars after every iteration).
 static int fcg_iteration(ProjCtx* P, double* x, int it, cudaStream_t st) {
   MGLevel& l0 = P->lev[0];
   const int64_t n = l0.n;
   const double* done = P->scal + SC_DONE;
-  int rc = unet_apply(P->net, P->pc_r, P->pc_z, st);
+  int rc = learned_precond(P, st);
   if (rc) return rc;
   if (it > 0) {
     k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, P->pc_z, P->pc_q, P->partial, done);
@@ -1225,6 +1312,8 @@ static int fcg_solve(ProjCtx* P, double* x, int maxiter, int* learned, cudaStrea
 int proj_set_learned(void* h, void* net, int max_learned, double stall) {
   ProjCtx* P = (ProjCtx*)h;
   if (max_learned < 0 || !(stall > 0.0 && stall <= 1.0)) return FS_EARG;
+  // the learned cycle runs on the FP32 level-0 operator of the mixed form
+  if (net && (!P->fp32 || unet_cells(net) != P->lev[0].n)) return FS_EARG;
   P->net = net;
   P->max_learned = max_learned;
   P->stall = stall;

@@ -64,7 +64,10 @@ struct Dims { int nz, ny, nx; int64_t n; };
 //   out[p][co] = act( bias[co] + sum_tap sum_ci in[p + off(tap)][ci] * W[tap][ci][co] )
 // then out *= (mask[p][co] > 0) when mask is given.  W arrives packed as
 // mma B fragments: [(tap * cin/16 + kc) * NT + nt][lane] (uint2).  Each warp
-// owns MT x 16 consecutive voxels and all NT x 8 output channels.
+// owns MT x 16 consecutive voxels and all NT x 8 output channels.  (A
+// variant that staged each row's 3x3 neighbour rows in shared memory and read
+// the A fragments by ldmatrix measured 9 % slower for the whole network on the
+// 400x120x60 grid, so the fragments are loaded directly.)
 // ---------------------------------------------------------------------------
 struct ConvArgs {
   const bf16* in;
@@ -554,6 +557,16 @@ __global__ void k_un_adam(int64_t n, float* p, const float* __restrict__ g, floa
 // ---------------------------------------------------------------------------
 namespace {
 
+// out[p] = base[p] + zf[p] * out_scale / scale   (scale = 1 / rms of the input)
+__global__ void k_un_correct(int64_t n, const float* __restrict__ zf, const double* __restrict__ scale,
+                             float out_scale, const float* __restrict__ base, float* out) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double s = *scale;
+  const float f = s > 0.0 ? (float)((double)out_scale / s) : 0.f;
+  out[p] = (base ? base[p] : 0.f) + zf[p] * f;
+}
+
 __global__ void k_un_dsum(const double* __restrict__ partial, int nb, double* out) {
   double s = 0.0;
   for (int b = threadIdx.x; b < nb; b += 32) s += partial[b];
@@ -576,6 +589,7 @@ struct UNetCtx {
   int64_t wchunk[UN_NL];
   int nchunks[UN_NL];
   int step = 0;
+  float out_scale = 1.f;  // z = N(r / rms) * rms * out_scale in unet_correct
   bool failed = false;
   std::vector<void*> owned;
 };
@@ -862,6 +876,31 @@ int unet_apply(void* h, const double* r, double* z, cudaStream_t st) {
                                                             U->params + U->hb, nullptr, z)));
   return cuda_status();
 }
+
+// out = base + N(r / rms(r)) * rms(r) * out_scale  (fp32; the coarse
+// correction of the learned preconditioner; base may be NULL)
+int unet_correct(void* h, const float* r, const float* base, float* out, cudaStream_t st) {
+  UNetCtx* U = (UNetCtx*)h;
+  const int64_t n0 = U->lv[0].n;
+  UN_LAUNCH((k_un_sumsq<float><<<RB, 256, 0, st>>>(n0, r, U->dpart)));
+  UN_LAUNCH((k_un_scale<<<1, 32, 0, st>>>(U->dpart, RB, n0, U->scale)));
+  UN_LAUNCH((k_un_input<float><<<blocks_for(n0, 256), 256, 0, st>>>(n0, r, U->scale, U->x0)));
+  forward(U, st);
+  UN_LAUNCH((k_un_head<<<blocks_for(n0, 256), 256, 0, st>>>(n0, U->u0, U->params + U->hw,
+                                                            U->params + U->hb, U->zf, nullptr)));
+  UN_LAUNCH((k_un_correct<<<blocks_for(n0, 256), 256, 0, st>>>(n0, U->zf, U->scale, U->out_scale,
+                                                               base, out)));
+  return cuda_status();
+}
+
+int unet_set_output_scale(void* h, float s) {
+  UNetCtx* U = (UNetCtx*)h;
+  if (!(s >= 0.f) || !std::isfinite(s)) return FS_EARG;
+  U->out_scale = s;
+  return FS_OK;
+}
+
+int64_t unet_cells(void* h) { return ((UNetCtx*)h)->lv[0].n; }
 
 // z = N(r) for an already normalised fp32 input (training data, tests)
 int unet_forward_f32(void* h, const float* r, float* z, cudaStream_t st) {

@@ -7,13 +7,22 @@ Adam live in ``csrc/unet.cu``; ``fs_proj_set_learned`` makes
 the V-cycle PCG from the current iterate when the residual stalls.  The
 tolerance is unchanged, so the network's error only costs iterations.
 
+The preconditioner M is a two-level cycle whose coarse correction is the
+network: damped-Jacobi pre-smoothing t, r1 = r - S t, s = t + N(r1) (scaled
+back to the size of the error), post-smoothing from s.  The sweeps take the
+high-frequency error that a bf16 network leaves; the network replaces the
+V-cycle's coarse levels.
+
 Training data are the solver's own pressure solves: ``PairLogger`` records,
 for every step, the residual r0 at the start of the solve and the correction
-e = x_solved - x0 that the solve added (S e = r0), both divided by rms(r0).
+e0 = x_solved - x0 that the solve added (S e0 = r0), and turns them into the
+network's pair (r1, e1 = e0 - t) with the cycle's own pre-smoothing, both
+divided by rms(r1).
 """
 from __future__ import annotations
 
 import ctypes as C
+import json
 import math
 from pathlib import Path
 
@@ -68,7 +77,15 @@ class UNetPreconditioner:
     @classmethod
     def load(cls, path, nz, ny, nx):
         d = np.load(path)
-        return cls(nz, ny, nx, params=d["params"])
+        net = cls(nz, ny, nx, params=d["params"])
+        if "target_scale" in d.files:
+            net.set_output_scale(1.0 / float(d["target_scale"]))
+        return net
+
+    def set_output_scale(self, c: float):
+        """N's output times c is the error estimate (1 / the training target
+        scale); c = 0 turns the coarse correction off (smoothing only)."""
+        check(self.lib.fs_unet_set_output_scale(self.h, float(c)), "fs_unet_set_output_scale")
 
     def save(self, path, **meta):
         Path(path).parent.mkdir(parents=True, exist_ok=True)
@@ -156,9 +173,10 @@ def fcg_stats(solver) -> dict:
 
 
 class PairLogger:
-    """Records (r0, e) of every pressure solve of ``solver`` (the last solve of
-    a step when ``take`` is called after the step), normalised by rms(r0), as
-    float32 device tensors."""
+    """Records (r0, x0) of every pressure solve of ``solver``; ``take`` (after
+    a step) returns the network's training pair of the step's last solve:
+    (r1, e1) after the learned cycle's pre-smoothing, divided by rms(r1), as
+    float32 device tensors.  The solver must be in an FP32 form."""
 
     def __init__(self, solver):
         self.solver = solver
@@ -169,14 +187,18 @@ class PairLogger:
               "fs_proj_set_log")
 
     def take(self):
-        """(r_hat, e_hat) of the last solve, or None when its residual was 0."""
-        torch.cuda.synchronize(self.solver.dev)
-        rms = float(torch.sqrt(torch.mean(self.r0 * self.r0)))
+        """(r1_hat, e1_hat) of the last solve, or None when its residual was 0."""
+        s = self.solver
+        e0 = (s.pressure_view().reshape(-1) - self.x0).contiguous()
+        r1 = torch.empty(s.n, dtype=torch.float32, device=s.dev)
+        e1 = torch.empty_like(r1)
+        check(s.lib.fs_proj_smooth_pair(s.proj, ptr(self.r0), ptr(e0), ptr(r1), ptr(e1),
+                                        torch.cuda.current_stream(s.dev).cuda_stream),
+              "fs_proj_smooth_pair")
+        rms = float(torch.sqrt(torch.mean(r1.double() * r1.double())))
         if not rms > 0.0:
             return None
-        x = self.solver.pressure_view().reshape(-1)
-        e = (x - self.x0) / rms
-        return (self.r0 / rms).float(), e.float()
+        return r1 / rms, e1 / rms
 
     def close(self):
         check(self.solver.lib.fs_proj_set_log(self.solver.proj, None, None), "fs_proj_set_log")
@@ -184,13 +206,13 @@ class PairLogger:
 
 def collect_pairs(cases, steps: int, warmup: int = 5, every: int = 1, device="cuda",
                   on_pair=None):
-    """Run every case of ``cases`` (plain form) for ``warmup + steps`` outer
+    """Run every case of ``cases`` (mixed form) for ``warmup + steps`` outer
     steps and return the logged (r_hat, e_hat) pairs of the last ``steps``
     (every ``every``-th step) as float32 device tensors."""
     from .solver import Tier3Solver
     pairs = []
     for case in cases:
-        s = Tier3Solver(case, device=device, form="plain")
+        s = Tier3Solver(case, device=device, form="mixed")
         log = PairLogger(s)
         try:
             for k in range(warmup + steps):
@@ -229,14 +251,75 @@ def train(net: UNetPreconditioner, pairs, iters: int, lr: float = 1e-3, seed: in
     return losses, float(target_scale)
 
 
+def evaluate(cases, steps: int, weights=WEIGHTS, warmup: int = 3, device="cuda",
+             variants=None) -> list[dict]:
+    """Held-out comparison at the same tolerance (1e-8): every case stepped
+    ``warmup + steps`` times in the mixed form (V-cycle PCG) and in the
+    learned form; per case and variant the CG iterations per step (learned
+    plus V-cycle after a fallback), the fallback count and the wall time of the
+    timed steps.  ``variants``: (name, form, output scale or None,
+    learned_max, learned_stall) tuples; the default adds the learned form
+    with a looser fallback and the same cycle with the network switched off
+    (smoothing only); both stop the learned phase only on a stall (or after
+    100 iterations).  A variant that fails (e.g. no convergence within the
+    solver's iteration limit) records the error and its completed steps."""
+    import time
+    from .solver import Tier3Solver
+    if variants is None:
+        variants = (("vcycle", "mixed", None, 30, 0.9),
+                    ("learned", "learned", None, 30, 0.9),
+                    ("learned_stall_only", "learned", None, 100, 1.0),
+                    ("smoothing_only_stall_only", "learned", 0.0, 100, 1.0))
+    out = []
+    for ci, case in enumerate(cases):
+        for name, form, scale, lmax, stall in variants:
+            s = Tier3Solver(case, device=device, form=form, learned_weights=weights,
+                            learned_max=lmax, learned_stall=stall)
+            try:
+                if scale is not None:
+                    s.net.set_output_scale(scale)
+                for _ in range(warmup):
+                    s.step()
+                its, lits, fb = [], [], 0
+                err = None
+                torch.cuda.synchronize(s.dev)
+                t0 = time.perf_counter()
+                for _ in range(steps):
+                    try:
+                        if not s.step():
+                            break
+                    except _lib.FireStepError as e:  # e.g. no convergence in proj_maxiter
+                        err = str(e)
+                        break
+                    its.append(int(sum(s.diag.cg_iters)))
+                    if form == "learned":
+                        st = fcg_stats(s)
+                        lits.append(st["learned_iters"])
+                        fb += int(st["fell_back"])
+                torch.cuda.synchronize(s.dev)
+                wall = time.perf_counter() - t0
+            finally:
+                s.close()
+            out.append({"case": ci, "variant": name, "steps": len(its), "error": err,
+                        "cg_iters_mean": float(np.mean(its)), "cg_iters": its,
+                        "learned_iters": lits, "fallbacks": fb,
+                        "ms_per_step": 1e3 * wall / max(len(its), 1)})
+            print(json.dumps(out[-1]), flush=True)
+    return out
+
+
 def _main(argv=None):
-    """python -m firewebapp_b200.learned --cases 4 --steps 60 --iters 1500:
+    """python -m firewebapp_b200.learned [train] --cases 4 --steps 60 --iters 1500:
     collects training pairs from seeded cases of the 400x120x60 workload
-    (U10 in 2-8 m/s, moisture in 0.02-0.12), trains, writes the weights."""
+    (U10 in 2-8 m/s, moisture in 0.02-0.12), trains, writes the weights.
+    python -m firewebapp_b200.learned evaluate --seed 200 --cases 5 --steps 20:
+    the held-out comparison (``evaluate``) on fresh seeds."""
     import argparse
     import time
     from .cases import learned_cases
     ap = argparse.ArgumentParser()
+    ap.add_argument("mode", nargs="?", default="train", choices=["train", "evaluate"])
+    ap.add_argument("--weights", default=None)
     ap.add_argument("--cases", type=int, default=4)
     ap.add_argument("--seed", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=10)
@@ -248,6 +331,9 @@ def _main(argv=None):
     ap.add_argument("--out", default=str(WEIGHTS))
     a = ap.parse_args(argv)
     cases = learned_cases(a.cases, seed0=a.seed, nx=a.nx)
+    if a.mode == "evaluate":
+        evaluate(cases, a.steps, weights=a.weights or str(WEIGHTS), warmup=a.warmup)
+        return
     t0 = time.time()
     pairs = collect_pairs(cases, a.steps, warmup=a.warmup, every=a.every)
     t1 = time.time()

@@ -220,16 +220,26 @@ int fs_proj_set_precision(void* handle, int fp32);
 int fs_proj_stats(void* handle, double* out8);
 
 /* Learned form (no counterpart in the reference): with net != NULL (a
- * fs_unet_create handle for the same grid) fs_proj_project runs flexible CG
- * preconditioned by the U-Net, truncated to one previous direction:
- *   z = N(r), p = z - (z.q_prev / p.q_prev) p_prev, q = S p,
+ * fs_unet_create handle for the same grid; the context must be in the FP32
+ * preconditioner form, fs_proj_set_precision(h, 1)) fs_proj_project runs
+ * flexible CG truncated to one previous direction,
+ *   z = M(r), p = z - (z.q_prev / p.q_prev) p_prev, q = S p,
  *   alpha = p.r / p.q, x += alpha p, r -= alpha q,
- * with the same stopping test.  When the residual norm shrinks by less than
- * `stall` per iteration (geometric mean of the last three) or after
- * `max_learned` iterations, the residual is recomputed and V-cycle PCG
- * continues from the current iterate (the fallback).  net = NULL restores
- * V-cycle PCG. */
+ * with the same stopping test.  M is a two-level cycle on the FP32 level-0
+ * operator whose coarse correction is the network: nu damped-Jacobi sweeps
+ * from 0 give t, r1 = r - S t, s = t + N(r1 / rms(r1)) rms(r1) c (c from
+ * fs_unet_set_output_scale), then nu sweeps from s (nu and the damping of
+ * fs_proj_configure).  When the residual norm shrinks by less than `stall`
+ * per iteration (geometric mean of the last three) or after `max_learned`
+ * iterations, the residual is recomputed and V-cycle PCG continues from the
+ * current iterate (the fallback).  net = NULL restores V-cycle PCG. */
 int fs_proj_set_learned(void* handle, void* net, int max_learned, double stall);
+/* A training pair for the network from a logged solve (r0, e0 with
+ * S e0 = r0, device doubles): r1 = r0 - S t and e1 = e0 - t after M's
+ * pre-smoothing t, as device floats (FP32 form; the operator of the last
+ * rebuild). */
+int fs_proj_smooth_pair(void* handle, const double* r0, const double* e0, float* r1, float* e1,
+                        void* stream);
 /* Copy the residual and the iterate at the start of every solve into r0 and
  * x0 (device arrays of Nx*Ny*Nz doubles; both NULL turns it off).  The pair
  * (r0, x_solved - x0) solves S e = r0: the learned preconditioner's training
@@ -252,7 +262,10 @@ int fs_unet_set_params(void* handle, const float* host, int64_t n, void* stream)
 int fs_unet_get_params(void* handle, float* host, int64_t n, void* stream);
 /* gradient of the last fs_unet_grad / fs_unet_train_step (synchronous) */
 int fs_unet_get_grads(void* handle, float* host, int64_t n, void* stream);
-/* z = N(r / rms(r)), device doubles (the preconditioner) */
+/* c in the learned cycle's coarse correction N(r / rms(r)) rms(r) c (default
+ * 1; 0 leaves only the smoothing sweeps) */
+int fs_unet_set_output_scale(void* handle, float s);
+/* z = N(r / rms(r)), device doubles */
 int fs_unet_apply(void* handle, const double* r, double* z, void* stream);
 /* z = N(r), device floats, no scaling */
 int fs_unet_forward(void* handle, const float* r, float* z, void* stream);

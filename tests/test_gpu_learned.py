@@ -134,25 +134,54 @@ def test_learned_form_matches_mixed_form():
 
 def test_pair_logger_pairs_solve_the_pressure_system():
     """The logged residual and start iterate satisfy S (x_solved - x0) = r0 to
-    the solver tolerance, and the float32 pair is their scaled copy."""
+    the solver tolerance, and the training pair after the cycle's
+    pre-smoothing still solves S e1 = r1 (to FP32 operator accuracy)."""
     from firewebapp_b200.cases import TINY
     from firewebapp_b200.learned import PairLogger
     from firewebapp_b200.solver import Tier3Solver
     from firewebapp_b200._lib import check, ptr
-    s = Tier3Solver(TINY, projection_cg_rtol=1e-10)
+    s = Tier3Solver(TINY, projection_cg_rtol=1e-10, form="mixed")
     log = PairLogger(s)
     for _ in range(3):
         s.step()
-    r, e = log.take()
-    e64 = (s.pressure_view().reshape(-1) - log.x0).contiguous()
-    Se = torch.empty(s.n, dtype=torch.float64, device="cuda")
-    check(s.lib.fs_proj_apply(s.proj, ptr(e64), ptr(Se),
-                              torch.cuda.current_stream().cuda_stream), "apply")
-    torch.cuda.synchronize()
-    r0 = log.r0.cpu().numpy()
-    assert rel_l2(Se.cpu().numpy(), r0) <= 1e-6
-    rms = np.sqrt(np.mean(r0 * r0))
-    assert rel_l2(r.cpu().numpy(), r0 / rms) <= 1e-7
-    assert rel_l2(e.cpu().numpy(), e64.cpu().numpy() / rms) <= 1e-7
+    r1, e1 = log.take()
+    st = torch.cuda.current_stream().cuda_stream
+
+    def S(x):
+        y = torch.empty(s.n, dtype=torch.float64, device="cuda")
+        check(s.lib.fs_proj_apply(s.proj, ptr(x.double().contiguous()), ptr(y), st), "apply")
+        torch.cuda.synchronize()
+        return y.cpu().numpy()
+
+    e0 = s.pressure_view().reshape(-1) - log.x0
+    assert rel_l2(S(e0), log.r0.cpu().numpy()) <= 1e-6
+    assert rel_l2(S(e1), r1.double().cpu().numpy()) <= 1e-4
+    assert abs(float(torch.sqrt(torch.mean(r1.double() ** 2))) - 1.0) <= 1e-6
     log.close()
     s.close()
+
+
+def test_trained_network_gains_over_the_cycle_without_it():
+    """On a held-out case of the 400x120x60 workload (seed not used in
+    training), flexible CG with the trained network as the cycle's coarse
+    correction needs fewer iterations than the same cycle with the network
+    switched off (output scale 0: smoothing sweeps only), both stopping the
+    learned phase only on a stall, at the same 1e-8 tolerance."""
+    from firewebapp_b200.cases import learned_cases
+    from firewebapp_b200.learned import WEIGHTS
+    from firewebapp_b200.solver import Tier3Solver
+    case = learned_cases(1, seed0=300)[0]
+    its = {}
+    for name, scale in (("trained", None), ("off", 0.0)):
+        s = Tier3Solver(case, form="learned", learned_weights=WEIGHTS, learned_max=100,
+                        learned_stall=1.0)
+        if scale is not None:
+            s.net.set_output_scale(scale)
+        tot = 0
+        for _ in range(6):
+            s.step()
+            tot += sum(s.diag.cg_iters)
+        its[name] = tot
+        s.close()
+    print("CG iterations over 6 steps:", its)
+    assert its["trained"] < 0.85 * its["off"], its

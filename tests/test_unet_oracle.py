@@ -44,3 +44,10 @@ def test_bf16_rounding_is_nearest_even():
     assert y[2] == 1.0 + 2 ** -6                  # tie to even (up)
     assert y[3] == -2.5 and y[5] == 0.0
     assert abs(y[4] - 1e-3) <= 2 ** -9 * 1e-3
+
+
+def test_packaged_weights_have_the_layout():
+    from firewebapp_b200 import learned
+    d = np.load(learned.WEIGHTS)
+    assert d["params"].dtype == np.float32 and d["params"].size == learned.n_params()
+    assert np.all(np.isfinite(d["params"])) and float(d["target_scale"]) > 0.0
