@@ -308,6 +308,45 @@ def evaluate(cases, steps: int, weights=WEIGHTS, warmup: int = 3, device="cuda",
     return out
 
 
+def time_network(nz: int, ny: int, nx: int, reps: int = 20) -> dict:
+    """CUDA-event time of one preconditioner application (fs_unet_apply) and
+    one training step on a (nz, ny, nx) grid, after 3 warm-up calls, with the
+    network's multiply-add count."""
+    net = UNetPreconditioner(nz, ny, nx, seed=1)
+    try:
+        r = torch.randn(net.n, dtype=torch.float64, device="cuda")
+        z = torch.empty_like(r)
+        for _ in range(3):
+            net.apply(r, z)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            net.apply(r, z)
+        e1.record()
+        torch.cuda.synchronize()
+        apply_ms = e0.elapsed_time(e1) / reps
+        r32, tau = r.float(), torch.randn(net.n, device="cuda")
+        net.train_step(r32, tau, 1e-6)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(max(reps // 4, 1)):
+            net.train_step(r32, tau, 1e-6)
+        e1.record()
+        torch.cuda.synchronize()
+        train_ms = e0.elapsed_time(e1) / max(reps // 4, 1)
+    finally:
+        net.close()
+    dims = [(nz, ny, nx)]
+    for _ in range(3):
+        dims.append(tuple((v + 1) // 2 for v in dims[-1]))
+    level = (0, 0, 1, 1, 2, 2, 3, 3, 2, 1, 0)
+    macs = sum(27 * ci * co * math.prod(dims[lv]) for (ci, co), lv in zip(CONV_LAYERS, level))
+    return {"grid": [nz, ny, nx], "apply_ms": apply_ms, "train_step_ms": train_ms,
+            "conv_gflop": 2e-9 * macs, "apply_tflops": 2e-9 * macs / apply_ms}
+
+
 def _main(argv=None):
     """python -m firewebapp_b200.learned [train] --cases 4 --steps 60 --iters 1500:
     collects training pairs from seeded cases of the 400x120x60 workload
@@ -318,7 +357,8 @@ def _main(argv=None):
     import time
     from .cases import learned_cases
     ap = argparse.ArgumentParser()
-    ap.add_argument("mode", nargs="?", default="train", choices=["train", "evaluate"])
+    ap.add_argument("mode", nargs="?", default="train", choices=["train", "evaluate", "time"])
+    ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--weights", default=None)
     ap.add_argument("--cases", type=int, default=4)
     ap.add_argument("--seed", type=int, default=100)
@@ -330,6 +370,9 @@ def _main(argv=None):
     ap.add_argument("--nx", type=int, default=400)
     ap.add_argument("--out", default=str(WEIGHTS))
     a = ap.parse_args(argv)
+    if a.mode == "time":
+        print(json.dumps(time_network(60, 120, a.nx, a.reps)))
+        return
     cases = learned_cases(a.cases, seed0=a.seed, nx=a.nx)
     if a.mode == "evaluate":
         evaluate(cases, a.steps, weights=a.weights or str(WEIGHTS), warmup=a.warmup)
