@@ -237,7 +237,13 @@ def run_batch_bench(args):
     from firewebapp_b200.batch import time_concurrent
     from firewebapp_b200.cases import batch_cases
     cases = batch_cases(args.batch, seed0=rank * args.batch)
-    conc = time_concurrent(cases, args.steps, warmup=args.warmup, form=args.form)
+    tuned = None
+    kw = {}
+    if args.autotune:
+        from firewebapp_b200.autotune import tune_batch
+        tuned = tune_batch(cases, concurrency=len(cases), form=args.form, use_cache=False)
+        kw = tuned["solver_kw"]
+    conc = time_concurrent(cases, args.steps, warmup=args.warmup, form=args.form, solver_kw=kw)
     seq_work, seq_wall = 0.0, 0.0
     for c in cases:
         one = time_concurrent([c], args.steps, warmup=args.warmup, form=args.form)
@@ -264,6 +270,9 @@ def run_batch_bench(args):
                        "device-wide synchronisations"},
             "sequential_value": seq_work / seq_wall,
             "concurrency_gain": (work / wall) / (seq_work / seq_wall),
+            "autotune": ({"solver_kw": tuned["solver_kw"],
+                          "trials": [{"solver_kw": t["solver_kw"], "value": t["value"]}
+                                     for t in tuned["trials"]]} if tuned else None),
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -293,6 +302,9 @@ def main():
                     help="instead of the headline line: N cases of the batched sweep of uneven "
                          "domains (Nx 200-600) stepped concurrently, against the same cases "
                          "stepped one after another")
+    ap.add_argument("--autotune", action="store_true",
+                    help="with --batch: pick the DOM cluster shape for the concurrent cases "
+                         "by timing each candidate on them first (autotune.tune_batch)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -54,12 +54,13 @@ def shard(n_cases: int, rank: int, world: int, weights=None) -> list[int]:
 
 def run_batch(cases, steps: int, form: str = "plain", concurrency: int = 2,
               device="cuda", keep_state: bool = False, warmup: int = 0,
-              on_case_done=None) -> list[BatchCaseResult]:
+              on_case_done=None, solver_kw: dict | None = None) -> list[BatchCaseResult]:
     """Step every case of ``cases`` for ``steps`` outer steps (fewer if the
     case ends, as the reference loop ends), ``concurrency`` cases at a time.
     ``warmup`` untimed steps precede the timed ones of each case.  Returns one
     ``BatchCaseResult`` per case, in input order; ``keep_state`` adds the
-    final state (``Tier3Solver.state()``) to each."""
+    final state (``Tier3Solver.state()``) to each.  ``solver_kw`` goes to every
+    ``Tier3Solver`` (e.g. an ``autotune.tune_batch`` choice)."""
     if concurrency < 1:
         raise ValueError("concurrency must be >= 1")
     dev = torch.device(device)
@@ -81,7 +82,7 @@ def run_batch(cases, steps: int, form: str = "plain", concurrency: int = 2,
                             return
                         i = nxt[0]
                         nxt[0] += 1
-                    s = Tier3Solver(cases[i], device=dev, form=form)
+                    s = Tier3Solver(cases[i], device=dev, form=form, **(solver_kw or {}))
                     try:
                         for _ in range(warmup):
                             if not s.step():
@@ -120,7 +121,7 @@ def run_batch(cases, steps: int, form: str = "plain", concurrency: int = 2,
 
 
 def time_concurrent(cases, steps: int, warmup: int = 3, form: str = "plain",
-                    device="cuda") -> dict:
+                    device="cuda", solver_kw: dict | None = None) -> dict:
     """Aggregate cell-steps/s of all ``cases`` stepped at the same time, one
     host thread and stream per case: every solver is built and warmed up
     first, then the timed region runs ``steps`` steps of every case between
@@ -133,7 +134,7 @@ def time_concurrent(cases, steps: int, warmup: int = 3, form: str = "plain",
         for c in cases:
             st = torch.cuda.Stream(device=dev)
             with torch.cuda.stream(st):
-                s = Tier3Solver(c, device=dev, form=form)
+                s = Tier3Solver(c, device=dev, form=form, **(solver_kw or {}))
                 for _ in range(warmup):
                     s.step()
             solvers.append(s)

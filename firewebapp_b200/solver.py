@@ -93,7 +93,9 @@ class Tier3Solver:
     pressure solve in flexible CG preconditioned by the U-Net of
     ``learned.py`` (weights from ``learned_weights``, default the packaged
     file), falling back to the V-cycle when it stalls.  ``dom_sweep`` forces a
-    DOM sweep path (``fs_dom_set_sweep_mode``; 0 picks automatically)."""
+    DOM sweep path (``fs_dom_set_sweep_mode``; 0 picks automatically) and
+    ``dom_cluster_ctas`` its CTAs per octant (0: automatic; a nonzero value
+    alone selects path 8)."""
 
     FIELDS = ("rho", "u", "v", "w", "T_g", "Y_fuel", "Y_O2", "Y_H2O", "T_s", "alpha_s",
               "k_turb", "eps_turb", "nu_t", "phi")
@@ -101,7 +103,7 @@ class Tier3Solver:
     def __init__(self, case: dict, device="cuda", projection_cg_rtol: float | None = None,
                  proj_maxiter: int = 200, mg_sweeps: int | None = None, form: str = "plain",
                  overlap_dom: bool = True, dom_sweep: int = 0, learned_weights=None,
-                 learned_max: int = 30, learned_stall: float = 0.9):
+                 learned_max: int = 30, learned_stall: float = 0.9, dom_cluster_ctas: int = 0):
         self.lib = _lib.lib()
         self.dev = torch.device(device)
         if self.dev.type == "cuda" and self.dev.index is None:
@@ -206,8 +208,9 @@ class Tier3Solver:
             self._pool = ThreadPoolExecutor(max_workers=1, thread_name_prefix="dom")
         if fp32:
             check(self.lib.fs_dom_set_precision(self.dom, 1), "fs_dom_set_precision")
-        if dom_sweep:
-            check(self.lib.fs_dom_set_sweep_mode(self.dom, int(dom_sweep), 0),
+        if dom_sweep or dom_cluster_ctas:
+            check(self.lib.fs_dom_set_sweep_mode(self.dom, int(dom_sweep or 8),
+                                                 int(dom_cluster_ctas)),
                   "fs_dom_set_sweep_mode")
         # clock
         self.t = 0.0

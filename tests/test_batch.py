@@ -38,3 +38,33 @@ def test_concurrent_cases_match_single_runs():
         assert a.steps == b.steps == 6 and a.t == b.t
         for k, v in a.state.items():
             assert np.array_equal(v, b.state[k]), k
+
+
+def test_autotune_picks_the_fastest_candidate_and_caches(tmp_path, monkeypatch):
+    """The tuner times each candidate through batch.time_concurrent (faked
+    here: no GPU), keeps the fastest, skips shapes that fail, and answers the
+    same question from its cache."""
+    import firewebapp_b200.autotune as A
+    import firewebapp_b200.batch as B
+    from firewebapp_b200._lib import FireStepError
+    from firewebapp_b200.cases import batch_cases
+    monkeypatch.setenv("FIREWEBAPP_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    monkeypatch.setattr(A.torch.cuda, "get_device_name", lambda d=None: "fake")
+    calls = []
+
+    def fake(cases, steps, warmup=3, form="plain", device="cuda", solver_kw=None):
+        calls.append(dict(solver_kw))
+        c = solver_kw["dom_cluster_ctas"]
+        if c == 7:
+            raise FireStepError(1, "no such cluster shape")
+        return {"value": {0: 1.0e8, 8: 1.2e8, 6: 1.5e8}[c], "wall_s": 1.0}
+
+    monkeypatch.setattr(B, "time_concurrent", fake)
+    cases = batch_cases(2, seed0=0)
+    out = A.tune_batch(cases, concurrency=2)
+    assert out["solver_kw"] == {"dom_sweep": 8, "dom_cluster_ctas": 6} and not out["cached"]
+    assert len(calls) == len(A.CANDIDATES)
+    assert any("error" in t for t in out["trials"])
+    again = A.tune_batch(cases, concurrency=2)
+    assert again["cached"] and again["solver_kw"] == out["solver_kw"]
+    assert len(calls) == len(A.CANDIDATES)
