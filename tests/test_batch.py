@@ -54,10 +54,10 @@ def test_autotune_picks_the_fastest_candidate_and_caches(tmp_path, monkeypatch):
 
     def fake(cases, steps, warmup=3, form="plain", device="cuda", solver_kw=None):
         calls.append(dict(solver_kw))
-        c = solver_kw["dom_cluster_ctas"]
-        if c == 7:
-            raise FireStepError(1, "no such cluster shape")
-        return {"value": {0: 1.0e8, 8: 1.2e8, 6: 1.5e8}[c], "wall_s": 1.0}
+        key = (solver_kw["dom_sweep"], solver_kw["dom_cluster_ctas"])
+        if key == (4, 0):
+            raise FireStepError(1, "no such sweep shape")
+        return {"value": {(8, 0): 1.0e8, (8, 6): 1.5e8}[key], "wall_s": 1.0}
 
     monkeypatch.setattr(B, "time_concurrent", fake)
     cases = batch_cases(2, seed0=0)
@@ -68,3 +68,30 @@ def test_autotune_picks_the_fastest_candidate_and_caches(tmp_path, monkeypatch):
     again = A.tune_batch(cases, concurrency=2)
     assert again["cached"] and again["solver_kw"] == out["solver_kw"]
     assert len(calls) == len(A.CANDIDATES)
+
+
+@pytest.mark.gpu
+def test_tuned_sweep_shapes_agree():
+    """The autotuner's candidates compute the same state: paths 8 and 4 with
+    one cluster per octant bit for bit, the two-cluster shape to round-off
+    (the workload's 60 x 120 cross-section, cut to 40 x-cells)."""
+    import numpy as np
+    from firewebapp_b200.autotune import CANDIDATES
+    from firewebapp_b200.cases import CFG2, scaled
+    from firewebapp_b200.solver import Tier3Solver
+    case = scaled(CFG2, nx=40)
+    states = {}
+    for mode, ctas in CANDIDATES:
+        s = Tier3Solver(case, dom_sweep=mode, dom_cluster_ctas=ctas)
+        for _ in range(2):
+            s.step()
+        states[(mode, ctas)] = s.state()
+        s.close()
+    a = states[(8, 0)]
+    for key, st in states.items():
+        for k in ("T_g", "q_rad", "u", "T_s"):
+            if key[1] == 0:
+                assert np.array_equal(st[k], a[k]), (key, k)
+            else:
+                d = np.linalg.norm(st[k] - a[k]) / np.linalg.norm(a[k])
+                assert d <= 1e-12, (key, k, d)
