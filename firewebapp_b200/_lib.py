@@ -57,6 +57,7 @@ SIGNATURES = {
     "fs_launch_count": (C.c_ulonglong, []),
     "fs_species_transport": (I, [_G, I, PP, PP, PP, C.POINTER(D), P, P, P, P, D, D, P]),
     "fs_species_sources": (I, [I64, P, P, P, P, P, P, P, P, P]),
+    "fs_species_step": (I, [_G, PP, PP, P, P, C.POINTER(D), P, P, P, P, D, D, D, P]),
     "fs_advect_scalar_muscl": (I, [_G, P, P, P, P, P, D, P]),
     "fs_gas_energy_adv": (I, [_G, P, P, P, P, P, D, D, D, P]),
     "fs_turb_diffusion_nsub": (I, [_G, P, D, D, C.POINTER(I), C.POINTER(D), P]),

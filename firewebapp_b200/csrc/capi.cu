@@ -116,6 +116,20 @@ int fs_species_transport(const FsGrid* g, int nspec, const double* const* Y, dou
                "fs_species_transport");
 }
 
+int fs_species_step(const FsGrid* g, const double* const* Y, double* const* Y_out,
+                    const double* S_pyro, const double* S_drying, const double* Y_inlet,
+                    const double* rho, const double* u, const double* v, const double* w,
+                    double dt, double D, double o2_cap, void* stream) {
+  GRID("fs_species_step");
+  if (!Y || !Y_out || !S_pyro || !S_drying || !Y_inlet) {
+    fs_set_error("fs_species_step: bad species arguments");
+    return FS_EARG;
+  }
+  return check(launch_species_step(gd, Y, Y_out, S_pyro, S_drying, Y_inlet, rho, u, v, w, dt, D,
+                                   o2_cap, ST(stream)),
+               "fs_species_step");
+}
+
 int fs_species_sources(int64_t n, const double* S_pyro, const double* S_drying, const double* Y_F,
                        const double* Y_O2, const double* Y_H2O, double* S_F, double* S_O2,
                        double* S_H2O, void* stream) {

@@ -99,6 +99,10 @@ int proj_set_log(void* h, double* r0, double* x0);
 void proj_fcg_stats(void* h, double* out4);
 
 // U-Net (unet.cu)
+int launch_species_step(const GridDev& g, const double* const* Y, double* const* Yo,
+                        const double* Sp, const double* Sd, const double* Y_inlet,
+                        const double* rho, const double* u, const double* v, const double* w,
+                        double dt, double D, double o2_cap, cudaStream_t st);
 int64_t unet_nparams();
 int unet_create(int nz, int ny, int nx, void** out);
 void unet_destroy(void* h);

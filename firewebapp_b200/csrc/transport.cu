@@ -17,6 +17,12 @@ struct SpeciesArgs {
   const double* S[3];
   double Y_inlet[3];
   int nspec;
+  // fused form (fuel, O2, H2O in that order): the sources from S_pyro and
+  // S_drying as k_species_sources forms them, and O2 clipped to [0, o2_cap]
+  // after the update as k_clip does
+  const double* Sp;
+  const double* Sd;
+  double o2_cap;
 };
 
 // One thread per cell; a block is a 32 (x) by 8 (y) tile of one z-level, so
@@ -31,7 +37,7 @@ struct SpeciesArgs {
 // reciprocal per cell, shared by the three species.
 #define SP_TX 32
 #define SP_TY 8
-template <int NS>
+template <int NS, bool FUSED>
 __global__ void __launch_bounds__(SP_TX * SP_TY, 4)
 k_species(GridDev g, SpeciesArgs a, const double* __restrict__ rho,
           const double* __restrict__ u, const double* __restrict__ v,
@@ -60,6 +66,12 @@ k_species(GridDev g, SpeciesArgs a, const double* __restrict__ rho,
   const double ui = u[c], vi = v[c], wi = w[c];
   const double inv_rho = 1.0 / rho[c];
   const double inv_d_above = rk[0], inv_d_below = rk[1], inv_dz_k = rk[2], inv_hz = rk[3];
+  double sp = 0.0, sd = 0.0, stot = 0.0;
+  if (FUSED) {
+    sp = a.Sp[c];
+    sd = a.Sd[c];
+    stot = sp + sd;
+  }
   const bool mx = (i >= 2 && i <= nx - 3);
   const bool mz = (k >= 2 && k <= nz - 3);
 #pragma unroll
@@ -95,11 +107,18 @@ k_species(GridDev g, SpeciesArgs a, const double* __restrict__ rho,
     double d2y = (Yjp1 - 2.0 * Yi + Yjm1) * inv_dy2;
     double d2z = ((YR_z - Yi) * inv_d_above - (Yi - YL_z) * inv_d_below) * inv_dz_k;
     double diff = D * (d2x + d2y + d2z);
-    double src = a.S[s][c] * inv_rho;
+    double S;
+    if (FUSED) S = (s == 0) ? sp - Yi * stot : ((s == 1) ? -(Yi * stot) : sd - Yi * stot);
+    else S = a.S[s][c];
+    double src = S * inv_rho;
     double dY = (adv + diff + src) * dt;
     double nw = Yi + dY;
     if (nw < 0.0) nw = 0.0;
     else if (nw > 1.0) nw = 1.0;
+    if (FUSED && s == 1) {
+      if (nw > a.o2_cap) nw = a.o2_cap;
+      if (nw < 0.0) nw = 0.0;
+    }
     a.Yo[s][c] = nw;
   }
 }
@@ -118,13 +137,38 @@ int launch_species(const GridDev& g, int nspec, const double* const* Y, double* 
   const dim3 nb((g.nx + SP_TX - 1) / SP_TX, (g.ny + SP_TY - 1) / SP_TY, g.nz);
   const dim3 tb(SP_TX, SP_TY);
   switch (nspec) {
-    case 1: k_species<1><<<nb, tb, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
-                                            inv_dx * inv_dx, inv_dy * inv_dy); break;
-    case 2: k_species<2><<<nb, tb, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
-                                            inv_dx * inv_dx, inv_dy * inv_dy); break;
-    default: k_species<3><<<nb, tb, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
-                                             inv_dx * inv_dx, inv_dy * inv_dy); break;
+    case 1: k_species<1, false><<<nb, tb, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
+                                                   inv_dx * inv_dx, inv_dy * inv_dy); break;
+    case 2: k_species<2, false><<<nb, tb, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
+                                                   inv_dx * inv_dx, inv_dy * inv_dy); break;
+    default: k_species<3, false><<<nb, tb, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
+                                                    inv_dx * inv_dx, inv_dy * inv_dy); break;
   }
+  fs_count_launch();
+  return cuda_status();
+}
+
+// The sub-step's species work in one pass: the sources with dilution
+// (k_species_sources), the transport of fuel, O2 and H2O, and the O2 clip
+// that follows it (spread_3d.py:2996-3004, 3015-3038, 3059); the results equal
+// those three launches'.
+int launch_species_step(const GridDev& g, const double* const* Y, double* const* Yo,
+                        const double* Sp, const double* Sd, const double* Y_inlet,
+                        const double* rho, const double* u, const double* v, const double* w,
+                        double dt, double D, double o2_cap, cudaStream_t st) {
+  SpeciesArgs a{};
+  a.nspec = 3;
+  for (int s = 0; s < 3; ++s) {
+    a.Y[s] = Y[s]; a.Yo[s] = Yo[s]; a.S[s] = nullptr; a.Y_inlet[s] = Y_inlet[s];
+  }
+  a.Sp = Sp;
+  a.Sd = Sd;
+  a.o2_cap = o2_cap;
+  double inv_dx = 1.0 / g.dx, inv_dy = 1.0 / g.dy;
+  const dim3 nb((g.nx + SP_TX - 1) / SP_TX, (g.ny + SP_TY - 1) / SP_TY, g.nz);
+  const dim3 tb(SP_TX, SP_TY);
+  k_species<3, true><<<nb, tb, 0, st>>>(g, a, rho, u, v, w, dt, D, inv_dx, inv_dy,
+                                        inv_dx * inv_dx, inv_dy * inv_dy);
   fs_count_launch();
   return cuda_status();
 }

@@ -606,22 +606,19 @@ class Tier3Solver:
                            1, 1.3, 17_000_000.0, int(p["edc_extinction_enable"]),
                            ptr(self.edc_scratch), s), "edc")
         self._phase("species")
-        check(L.fs_species_sources(self.n, ptr(Sp), ptr(Sd), ptr(f["Y_fuel"]),
-                                   ptr(f["Y_O2"]), ptr(f["Y_H2O"]), ptr(w["S_F"]),
-                                   ptr(w["S_O2"]), ptr(w["S_H2O"]), s), "sources")
+        # sources with dilution, transport of the three species and the O2
+        # clip in one pass (fs_species_step; equal to the three calls)
         Ys = [f["Y_fuel"], f["Y_O2"], f["Y_H2O"]]
         Yo = [w["tmp1"], w["tmp2"], w["tmp3"]]
         with self._ktime("species_transport"):
-            check(L.fs_species_transport(gp, 3, ptr_array(Ys), ptr_array(Yo),
-                                         ptr_array([w["S_F"], w["S_O2"], w["S_H2O"]]),
-                                         dbl_array([0.0, 0.232, 0.0]), ptr(f["rho"]),
-                                         ptr(f["u"]), ptr(f["v"]), ptr(f["w"]), dt_sub,
-                                         1.0e-5, s), "species")
+            check(L.fs_species_step(gp, ptr_array(Ys), ptr_array(Yo), ptr(Sp), ptr(Sd),
+                                    dbl_array([0.0, 0.232, 0.0]), ptr(f["rho"]), ptr(f["u"]),
+                                    ptr(f["v"]), ptr(f["w"]), dt_sub, 1.0e-5, 0.232, s),
+                  "species")
         self._swap("Y_fuel", "tmp1")
         self._swap("Y_O2", "tmp2")
         self._swap("Y_H2O", "tmp3")
         self._phase("turb_diff_Y")
-        check(L.fs_clip(self.n, ptr(f["Y_O2"]), 0.0, 0.232, s), "clip_O2")
         if n_sc > 0:
             for q in range(n_sc):
                 last = q == n_sc - 1

@@ -89,6 +89,16 @@ int fs_species_sources(int64_t n, const double* S_pyro, const double* S_drying,
                        const double* Y_F, const double* Y_O2, const double* Y_H2O, double* S_F,
                        double* S_O2, double* S_H2O, void* stream);
 
+/* The sub-step's species work fused into one pass (no reference counterpart
+ * as a single call): fs_species_sources, then fs_species_transport of
+ * (Y_F, Y_O2, Y_H2O) with those sources, then fs_clip(Y_O2, 0, o2_cap)
+ * (spread_3d.py:2996-3004, 3015-3038, 3059); the same results as the three
+ * calls, without the source arrays. */
+int fs_species_step(const FsGrid* g, const double* const* Y, double* const* Y_out,
+                    const double* S_pyro, const double* S_drying, const double* Y_inlet,
+                    const double* rho, const double* u, const double* v, const double* w,
+                    double dt, double D, double o2_cap, void* stream);
+
 /* muscl_3d.py:68 advect_3d_scalar_muscl: rhs -= u . grad(phi). */
 int fs_advect_scalar_muscl(const FsGrid* g, const double* phi, const double* u, const double* v,
                            const double* w, double* rhs, double phi_inlet, void* stream);

@@ -80,6 +80,34 @@ def test_species_three_fused_equals_single(vectors):
         assert np.array_equal(host(o1), host(outs3[s]))
 
 
+def test_species_step_equals_sources_transport_clip(vectors):
+    """fs_species_step (sources, transport and O2 clip in one pass) gives the
+    same fields bit for bit as fs_species_sources, fs_species_transport and
+    fs_clip(Y_O2) in sequence, with O2 values pushed over the cap."""
+    c = vectors.case("species", "small3d")
+    g = grid_of(c)
+    rho, u, v, w = (dev(c[k]) for k in ("rho", "u", "v", "w"))
+    rng = np.random.default_rng(11)
+    shape = c["Y_in"].shape
+    Ys = [dev(c["Y_in"] * 0.5), dev(0.20 + 0.05 * rng.random(shape)), dev(0.3 * rng.random(shape))]
+    Sp, Sd = dev(0.02 * rng.random(shape)), dev(0.01 * rng.random(shape))
+    n = Ys[0].numel()
+    Ss = [torch.empty_like(Ys[0]) for _ in range(3)]
+    call("fs_species_sources", n, ptr(Sp), ptr(Sd), ptr(Ys[0]), ptr(Ys[1]), ptr(Ys[2]),
+         ptr(Ss[0]), ptr(Ss[1]), ptr(Ss[2]), stream())
+    ref = [torch.empty_like(Ys[0]) for _ in range(3)]
+    inlet = dbl_array([0.0, 0.232, 0.0])
+    call("fs_species_transport", g.ref, 3, ptr_array(Ys), ptr_array(ref), ptr_array(Ss), inlet,
+         ptr(rho), ptr(u), ptr(v), ptr(w), c["dt"], c["D"], stream())
+    call("fs_clip", n, ptr(ref[1]), 0.0, 0.232, stream())
+    out = [torch.empty_like(Ys[0]) for _ in range(3)]
+    call("fs_species_step", g.ref, ptr_array(Ys), ptr_array(out), ptr(Sp), ptr(Sd), inlet,
+         ptr(rho), ptr(u), ptr(v), ptr(w), c["dt"], c["D"], 0.232, stream())
+    assert float(host(ref[1]).max()) == 0.232  # the clip was exercised
+    for s in range(3):
+        assert np.array_equal(host(out[s]), host(ref[s])), s
+
+
 def test_momentum(vectors):
     for name in vectors.cases("momentum"):
         c = vectors.case("momentum", name)
