@@ -75,6 +75,7 @@ SIGNATURES = {
     "fs_eos": (I, [_G, P, P, P, P, D, P]),
     "fs_clip": (I, [I64, P, D, D, P]),
     "fs_solid_conduction": (I, [_G, P, P, P, D, D, D, D, P]),
+    "fs_solid_conduction_capped": (I, [_G, P, P, P, D, D, D, D, D, D, P]),
     "fs_soil_step": (I, [I, I, I, P, P, D, P, P, P, D, D, D, D, D, P]),
     "fs_proj_create": (I, [_G, PP]),
     "fs_proj_destroy": (None, [P]),

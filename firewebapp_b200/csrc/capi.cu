@@ -335,6 +335,15 @@ int fs_solid_conduction(const FsGrid* g, const double* T_s, const double* alpha_
                "fs_solid_conduction");
 }
 
+int fs_solid_conduction_capped(const FsGrid* g, const double* T_s, const double* alpha_s,
+                               double* T_out, double k_solid, double rho_solid, double cp_solid,
+                               double dt, double lo, double hi, void* stream) {
+  GRID("fs_solid_conduction_capped");
+  return check(launch_solid_cond(gd, T_s, alpha_s, T_out, k_solid, rho_solid, cp_solid, dt, gd.nz,
+                                 ST(stream), 1, lo, hi),
+               "fs_solid_conduction_capped");
+}
+
 int fs_soil_step(int nsoil, int ny, int nx, double* T_soil, const double* q_in, double dt,
                  const double* soil_dz, const double* d_above, const double* d_below, double k_s,
                  double rho_s, double cp_s, double eps_s, double T_amb, void* stream) {

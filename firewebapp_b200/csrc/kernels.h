@@ -55,7 +55,7 @@ int launch_keps(const GridDev& g, const double* k, const double* e, const double
                 double T_amb, double beta_p, double beta_d, cudaStream_t st);
 int launch_solid_cond(const GridDev& g, const double* Ts, const double* as, double* To,
                       double k_solid, double rho_s, double cp_s, double dt, int nz_active,
-                      cudaStream_t st);
+                      cudaStream_t st, int cap = 0, double lo = 0.0, double hi = 0.0);
 int launch_soil(int nsoil, int ny, int nx, double* T, const double* qin, double dt,
                 const double* sdz, const double* sda, const double* sdb, double k_s,
                 double rho_s, double cp_s, double eps_s, double T_amb, cudaStream_t st);

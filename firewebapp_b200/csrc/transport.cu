@@ -816,9 +816,12 @@ int launch_keps(const GridDev& g, const double* k, const double* e, const double
 // ---------------------------------------------------------------------------
 // Vertical solid conduction on the bed T_s grid (solid_conduction_3d.py:56-127)
 // ---------------------------------------------------------------------------
+// cap = 1: the result is then clipped to [lo, hi] as k_clip does (the T_s
+// cap that follows the conduction, spread_3d.py:3193-3196)
 __global__ void k_solid_cond(GridDev g, const double* __restrict__ Ts,
                              const double* __restrict__ as, double* __restrict__ To,
-                             double k_solid, double inv_rho_cp, double dt) {
+                             double k_solid, double inv_rho_cp, double dt, int cap, double lo,
+                             double hi) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   int k = blockIdx.z;
@@ -827,7 +830,15 @@ __global__ void k_solid_cond(GridDev g, const double* __restrict__ Ts,
   const int64_t c = cidx(g, k, j, i);
   const double asc = as[c];
   const double T0 = Ts[c];
-  if (asc <= 0.0) { To[c] = T0; return; }
+  if (asc <= 0.0) {
+    double x = T0;
+    if (cap) {
+      if (x > hi) x = hi;
+      if (x < lo) x = lo;
+    }
+    To[c] = x;
+    return;
+  }
   double fu = 0.0, fd = 0.0;
   if (k < g.nz - 1) {
     double aa = as[c + sz];
@@ -845,16 +856,22 @@ __global__ void k_solid_cond(GridDev g, const double* __restrict__ Ts,
   }
   double src = (fu + fd) / g.dz[k];
   double dT = dt * src * inv_rho_cp / asc;
-  To[c] = T0 + dT;
+  double x = T0 + dT;
+  if (cap) {
+    if (x > hi) x = hi;
+    if (x < lo) x = lo;
+  }
+  To[c] = x;
 }
 
 int launch_solid_cond(const GridDev& g, const double* Ts, const double* as, double* To,
                       double k_solid, double rho_s, double cp_s, double dt, int nz_active,
-                      cudaStream_t st) {
+                      cudaStream_t st, int cap, double lo, double hi) {
   GridDev gg = g;
   Launch3 L = launch_cells(g);
   (void)nz_active;
-  k_solid_cond<<<L.grid, L.block, 0, st>>>(gg, Ts, as, To, k_solid, 1.0 / (rho_s * cp_s), dt); fs_count_launch();
+  k_solid_cond<<<L.grid, L.block, 0, st>>>(gg, Ts, as, To, k_solid, 1.0 / (rho_s * cp_s), dt,
+                                           cap, lo, hi); fs_count_launch();
   return cuda_status();
 }
 

@@ -647,8 +647,11 @@ class Tier3Solver:
                                      drip, g.n_z_bed, p["i_src_start"], p["i_src_end"], s),
               "gas_update")
         self._phase("solid_cond")
-        check(L.fs_solid_conduction(gp, ptr(f["T_s"]), ptr(f["alpha_s"]), ptr(w["tmp4"]),
-                                    0.20, 500.0, 1300.0, dt_sub, s), "solid_cond")
+        # the conduction with the T_s cap of the sub-step's end fused in: nothing
+        # between them reads or writes T_s (spread_3d.py:3168-3196)
+        check(L.fs_solid_conduction_capped(gp, ptr(f["T_s"]), ptr(f["alpha_s"]), ptr(w["tmp4"]),
+                                           0.20, 500.0, 1300.0, dt_sub, p["T_amb"], T_CAP, s),
+              "solid_cond")
         self._swap("T_s", "tmp4")
         self._phase("turb_diff_T")
         if n_pr > 0:
@@ -661,7 +664,6 @@ class Tier3Solver:
                 self._swap("T_g", "tmp4")
         else:
             check(L.fs_clip(self.n, ptr(f["T_g"]), p["T_amb"], T_CAP, s), "cap_Tg")
-        check(L.fs_clip(self.n, ptr(f["T_s"]), p["T_amb"], T_CAP, s), "cap_Ts")
 
     def _dom_job(self, ready, a):
         """M_local aggregation and the DOM solve on the second stream, after

@@ -192,6 +192,12 @@ int fs_solid_conduction(const FsGrid* g, const double* T_s, const double* alpha_
                         double k_solid, double rho_solid, double cp_solid, double dt,
                         void* stream);
 
+/* fs_solid_conduction followed by fs_clip(T_out, lo, hi) in one pass (the
+ * T_s cap of spread_3d.py:3193-3196); the same results as the two calls. */
+int fs_solid_conduction_capped(const FsGrid* g, const double* T_s, const double* alpha_s,
+                               double* T_out, double k_solid, double rho_solid, double cp_solid,
+                               double dt, double lo, double hi, void* stream);
+
 /* soil_3d.py:106 step_soil_conduction, in place. */
 int fs_soil_step(int nsoil, int ny, int nx, double* T_soil, const double* q_in, double dt,
                  const double* soil_dz, const double* d_above, const double* d_below, double k_s,

@@ -108,6 +108,24 @@ def test_species_step_equals_sources_transport_clip(vectors):
         assert np.array_equal(host(out[s]), host(ref[s])), s
 
 
+def test_solid_conduction_capped_equals_conduction_then_clip():
+    rng = np.random.default_rng(12)
+    nz, ny, nx = 9, 7, 11
+    g = Grid(nz, ny, nx, 0.1, 0.1, np.linspace(0.02, 0.05, nz))
+    shape = (nz, ny, nx)
+    Ts = dev(250.0 + 2000.0 * rng.random(shape))
+    a_s = dev(np.where(rng.random(shape) < 0.6, 0.05 * rng.random(shape), 0.0))
+    ref, out = torch.empty_like(Ts), torch.empty_like(Ts)
+    call("fs_solid_conduction", g.ref, ptr(Ts), ptr(a_s), ptr(ref), 0.2, 500.0, 1300.0, 0.5,
+         stream())
+    call("fs_clip", Ts.numel(), ptr(ref), 300.0, 1800.0, stream())
+    call("fs_solid_conduction_capped", g.ref, ptr(Ts), ptr(a_s), ptr(out), 0.2, 500.0, 1300.0,
+         0.5, 300.0, 1800.0, stream())
+    r = host(ref)
+    assert r.min() == 300.0 and r.max() == 1800.0
+    assert np.array_equal(host(out), r)
+
+
 def test_momentum(vectors):
     for name in vectors.cases("momentum"):
         c = vectors.case("momentum", name)
