@@ -103,6 +103,9 @@ struct EdcArgs {
   double* omega;
   const signed char* carry;
   double chi_rad, cp_g, dt, s_stoich, HoC_eff, relax;
+  // reciprocals of the constant divisors (1/s_stoich, 1/dt); the divisions
+  // by them, by rho and by tau* are multiplications
+  double inv_s, inv_dt;
   int extinction, nsub;
 };
 
@@ -150,6 +153,11 @@ __global__ void k_edc_main(int64_t n, EdcArgs a) {
   double gamma_star = gx * (gx * gx);
   if (gamma_star > 1.0) gamma_star = 1.0;
   double tau_star = 0.4083 * sqrt(1.5e-5 / e_t);
+  // Division costs a Newton sequence here, so the constant and per-cell
+  // divisors become one reciprocal each: every quotient below is then within
+  // an ulp or two of the reference's (the kernel is instruction-bound).
+  const double inv_tau = 1.0 / tau_star;
+  const double inv_rho = 1.0 / rho_i;
   const double h = a.dt / (double)a.nsub;
   double acc = 0.0;
   for (int sub = 0; sub < a.nsub; ++sub) {
@@ -157,12 +165,12 @@ __global__ void k_edc_main(int64_t n, EdcArgs a) {
     if (Yf <= 1e-9 || YO2 <= 1e-9) {
       omega = 0.0;
     } else {
-      double lim = YO2 / a.s_stoich;
+      double lim = YO2 * a.inv_s;
       double Y_lim = Yf < lim ? Yf : lim;
-      double omega_fine = rho_i * Y_lim / tau_star;
+      double omega_fine = rho_i * Y_lim * inv_tau;
       omega = gamma_star * omega_fine;
       if (YH > 0.0) {
-        double fac = 1.0 - YH / 0.18;
+        double fac = 1.0 - YH * (1.0 / 0.18);
         if (fac < 0.0) fac = 0.0;
         omega = omega * fac;
       }
@@ -171,7 +179,7 @@ __global__ void k_edc_main(int64_t n, EdcArgs a) {
     if (a.extinction && omega > 0.0) {
       double Yib = 1.0 - Yf - YO2;
       if (Yib > 0.88) {
-        double rs = (1.0 - Yib) / (1.0 - 0.88);
+        double rs = (1.0 - Yib) * (1.0 / (1.0 - 0.88));
         if (rs < 0.0) rs = 0.0;
         omega = omega * rs;
         if (rs < 0.5) fired = true;
@@ -184,26 +192,26 @@ __global__ void k_edc_main(int64_t n, EdcArgs a) {
     }
     if ((fired || flag) && Tg > 373.15) {
       if (YH > 0.0) {
-        double wb = YH / 0.10;
+        double wb = YH * (1.0 / 0.10);
         if (wb > 1.0) wb = 1.0;
         double dT_wb = (Tg - 373.15) * a.relax * wb;
         Tg = Tg - dT_wb;
       }
     }
-    double dY = -omega * h / rho_i;
+    double dY = -omega * h * inv_rho;
     Yf = Yf + dY;
     if (Yf < 0.0) Yf = 0.0;
     YO2 = YO2 + a.s_stoich * dY;
     if (YO2 < 0.0) YO2 = 0.0;
     double cp_mix = (1.0 - YH) * a.cp_g + YH * 2000.0;
-    Tg = Tg + omega * a.HoC_eff * h / (rho_i * cp_mix);
+    Tg = Tg + omega * a.HoC_eff * h * inv_rho / cp_mix;
     if (Tg > 2400.0) Tg = 2400.0;
     acc += omega * h;
   }
   a.Yf[c] = Yf;
   a.YO[c] = YO2;
   a.Tg[c] = Tg;
-  a.omega[c] = a.dt > 0.0 ? acc / a.dt : 0.0;
+  a.omega[c] = a.dt > 0.0 ? acc * a.inv_dt : 0.0;
 }
 
 int edc_scratch_bytes(int64_t n) {
@@ -224,6 +232,8 @@ int launch_edc(int64_t n, const double* rho, double* Tg, double* Yf, double* YO,
   a.rho = rho; a.Tg = Tg; a.Yf = Yf; a.YO = YO; a.kt = kt; a.et = et; a.YH = YH;
   a.omega = omega; a.carry = carry;
   a.chi_rad = chi_rad; a.cp_g = cp_g; a.dt = dt; a.s_stoich = s_stoich;
+  a.inv_s = 1.0 / s_stoich;
+  a.inv_dt = dt > 0.0 ? 1.0 / dt : 0.0;
   a.HoC_eff = hoc_J * (1.0 - chi_rad);
   a.nsub = n_substeps > 1 ? n_substeps : 1;
   a.relax = 1.0 - exp(-(dt / (double)a.nsub) / 0.5);
