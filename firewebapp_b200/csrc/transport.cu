@@ -324,23 +324,31 @@ struct DiffArgs {
   int clip;
 };
 
+// One thread per cell in 32 x 8 (x, y) tiles of one z-level (y-neighbours
+// from L1); the level's reciprocal spacings are computed once per block.
 template <int NF>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(SP_TX * SP_TY, 4)
 k_turb_diff(GridDev g, DiffArgs a, const double* __restrict__ nu_t, double sc_t, double dt_sub,
             double inv_dx2, double inv_dy2) {
+  __shared__ double rk[3];  // 1/dz, 1/da, 1/db of the block's level
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int64_t sy = nx, sz = (int64_t)nx * ny;
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= sz * nz) return;
-  const int k = (int)(c / sz);
-  const int64_t rem = c - (int64_t)k * sz;
-  const int j = (int)(rem / nx);
-  const int i = (int)(rem - (int64_t)j * nx);
-  const int64_t crow = c - (int64_t)j * sy;
+  const int k = blockIdx.z;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    rk[0] = 1.0 / g.dz[k];
+    rk[1] = 1.0 / g.da[k];
+    rk[2] = 1.0 / g.db[k];
+  }
+  __syncthreads();
+  const int i = blockIdx.x * SP_TX + threadIdx.x;
+  const int j = blockIdx.y * SP_TY + threadIdx.y;
+  if (i >= nx || j >= ny) return;
+  const int64_t crow = (int64_t)k * sz + i;
+  const int64_t c = crow + (int64_t)j * sy;
   const int64_t cjp = crow + wrapj(j + 1, ny) * sy, cjm = crow + wrapj(j - 1, ny) * sy;
-  const double inv_dz_k = 1.0 / g.dz[k];
-  const double inv_d_above = 1.0 / g.da[k];
-  const double inv_d_below = 1.0 / g.db[k];
+  const double inv_dz_k = rk[0];
+  const double inv_d_above = rk[1];
+  const double inv_d_below = rk[2];
   const double D_t = nu_t[c] / sc_t;
 #pragma unroll
   for (int s = 0; s < NF; ++s) {
@@ -375,13 +383,14 @@ int launch_turb_diff(const GridDev& g, int nfield, const double* const* f, doubl
     a.lo[s] = clip ? lo[s] : 0.0;
     a.hi[s] = clip ? hi[s] : 0.0;
   }
-  const unsigned nb = blocks_for(ncells(g), 256);
+  const dim3 nb((g.nx + SP_TX - 1) / SP_TX, (g.ny + SP_TY - 1) / SP_TY, g.nz);
+  const dim3 tb(SP_TX, SP_TY);
   const double ix2 = 1.0 / (g.dx * g.dx), iy2 = 1.0 / (g.dy * g.dy);
   switch (nfield) {
-    case 1: k_turb_diff<1><<<nb, 256, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
-    case 2: k_turb_diff<2><<<nb, 256, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
-    case 3: k_turb_diff<3><<<nb, 256, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
-    default: k_turb_diff<4><<<nb, 256, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
+    case 1: k_turb_diff<1><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
+    case 2: k_turb_diff<2><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
+    case 3: k_turb_diff<3><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
+    default: k_turb_diff<4><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
   }
   fs_count_launch();
   return cuda_status();
