@@ -3,6 +3,7 @@
 #include <mutex>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
 #include "common.cuh"
 #include "kernels.h"
 
@@ -23,15 +24,33 @@ void fs_set_error(const char* fmt, ...) {
 // Host wait for a stream through a blocking-sync event: the calling thread
 // sleeps instead of spinning, so waits do not consume the process's CPU time
 // (spinning threads can get a CPU-quota-limited process throttled).
+// Wait for a stream: poll an event for up to FS_SPIN_US microseconds (the
+// step's host decisions wait on short queues, where a sleeping wait's wake-up
+// costs more than the work), then sleep on a blocking-sync event recorded at
+// the same point.
+#define FS_SPIN_US 300
 int fs_stream_wait(cudaStream_t st) {
-  static thread_local cudaEvent_t ev[64] = {};
+  static thread_local cudaEvent_t ev_poll[64] = {};
+  static thread_local cudaEvent_t ev_block[64] = {};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FS_ECUDA;
-  if (!ev[dev] && cudaEventCreateWithFlags(&ev[dev], cudaEventBlockingSync |
-                                                          cudaEventDisableTiming) != cudaSuccess)
+  if (!ev_poll[dev] &&
+      cudaEventCreateWithFlags(&ev_poll[dev], cudaEventDisableTiming) != cudaSuccess)
     return FS_ECUDA;
-  if (cudaEventRecord(ev[dev], st) != cudaSuccess) return FS_ECUDA;
-  return cudaEventSynchronize(ev[dev]) == cudaSuccess ? FS_OK : FS_ECUDA;
+  if (!ev_block[dev] && cudaEventCreateWithFlags(&ev_block[dev], cudaEventBlockingSync |
+                                                                     cudaEventDisableTiming) !=
+                            cudaSuccess)
+    return FS_ECUDA;
+  if (cudaEventRecord(ev_poll[dev], st) != cudaSuccess) return FS_ECUDA;
+  if (cudaEventRecord(ev_block[dev], st) != cudaSuccess) return FS_ECUDA;
+  const auto t0 = std::chrono::steady_clock::now();
+  while (true) {
+    const cudaError_t q = cudaEventQuery(ev_poll[dev]);
+    if (q == cudaSuccess) return FS_OK;
+    if (q != cudaErrorNotReady) return FS_ECUDA;
+    if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(FS_SPIN_US)) break;
+  }
+  return cudaEventSynchronize(ev_block[dev]) == cudaSuccess ? FS_OK : FS_ECUDA;
 }
 
 // Per-thread, per-device scratch for the synchronous reductions (a few device

@@ -161,6 +161,7 @@ class Tier3Solver:
         # pinned host mirrors for the per-step scalar reads
         self.h_count = torch.zeros(1, dtype=torch.int64).pin_memory()
         self.h_row = torch.zeros(g.Nx, dtype=torch.float64).pin_memory()
+        self.h_rows = torch.zeros((2, g.Nx), dtype=torch.float64).pin_memory()
         self.max_scratch = torch.zeros(64, dtype=torch.float64, device=dev)
         # soil
         so = su.soil
@@ -540,10 +541,16 @@ class Tier3Solver:
         self.lset_step += 1
         if self.lset_step % 10 == 0:
             self._reinit_levelset()
-        check(self.lib.fs_copy_to_host(self.h_count.data_ptr(), ptr(self.active_count), 8,
-                                       self._s()), "active_count")
+        # one wait for the exit tests and the front tracking: the active-cell
+        # count and the two phi rows they read (phi does not change again in
+        # this step, so the second row may be read before the closing EoS)
+        stream = torch.cuda.current_stream(self.dev)
+        self.h_count.copy_(self.active_count, non_blocking=True)
+        self.h_rows[0].copy_(f["phi"][1, g.Ny // 2, :], non_blocking=True)
+        self.h_rows[1].copy_(f["phi"][g.n_z_bed // 2, g.Ny // 2, :], non_blocking=True)
+        stream.synchronize()
         n_active = int(self.h_count[0])
-        front_lset = self._front_x(1, g.Ny // 2)
+        front_lset = self._front_from_row(self.h_rows[0].numpy())
         exit_now = False
         if n_active == 0 and t > p["ignition_duration_s"] + 2.0:
             self.extinct_count += 1
@@ -558,7 +565,7 @@ class Tier3Solver:
             return False
         # --- 14. closing EoS (:3440) and clock
         check(L.fs_eos(gp, ptr(f["rho"]), None, ptr(f["T_g"]), None, p["T_amb"], s), "eos2")
-        fx = self._front_x(g.n_z_bed // 2, g.Ny // 2)
+        fx = self._front_from_row(self.h_rows[1].numpy())
         if math.isfinite(fx) and fx > self.front_x[-1]:
             self.front_t.append(t)
             self.front_x.append(fx)
@@ -744,7 +751,10 @@ class Tier3Solver:
         src = self.f["phi"][k, j, :]
         check(self.lib.fs_copy_to_host(self.h_row.data_ptr(), src.data_ptr(),
                                        8 * self.grid.Nx, self._s()), "front_row")
-        row = self.h_row.numpy()
+        return self._front_from_row(self.h_row.numpy())
+
+    def _front_from_row(self, row):
+        """x of the first sign change of phi along a host row (spread_3d.py:3743)."""
         for i in range(row.size - 1):
             a, b = row[i], row[i + 1]
             if a < 0.0 < b or b < 0.0 < a:
