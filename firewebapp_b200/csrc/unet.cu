@@ -766,9 +766,23 @@ void unet_destroy(void* h) {
   delete U;
 }
 
+// The instantiated kernels: forward and adjoint convolutions for NT (output
+// channels / 8) in {2, 4, 6, 8, 10, 14}, weight gradients for cout / 8 in
+// {2, 4, 6, 8}; the layer table must stay within them (checked at creation,
+// so the launch switches never meet another value).
+static bool conv_nt_ok(int nt) {
+  return nt == 2 || nt == 4 || nt == 6 || nt == 8 || nt == 10 || nt == 14;
+}
+
 int unet_create(int nz, int ny, int nx, void** out) {
   *out = nullptr;
   if (nz < 1 || ny < 1 || nx < 1) return FS_EARG;
+  for (int li = 0; li < UN_NL; ++li) {
+    const LayerSpec& s = kSpec[li];
+    if (s.cin % 16 || s.cout % 16 || !conv_nt_ok(s.cout / 8) || !conv_nt_ok(s.cin / 8) ||
+        s.cout / 8 > 8)
+      return FS_EARG;
+  }
   UNetCtx* U = new UNetCtx();
   int z = nz, y = ny, x = nx;
   for (int l = 0; l < 4; ++l) {
