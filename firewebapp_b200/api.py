@@ -229,6 +229,21 @@ class HostStepper:
     PARTS = ("x", "y", "z", "alive", "m_solid", "m_water", "m_char", "T_s", "m_water_0",
              "sav", "m_char_max")
 
+    # Fields the step no longer changes from a phase on: their download starts
+    # there, on a copy stream, while the rest of the step runs.  At the DOM
+    # phase: velocities (after the projection and sponge), k-epsilon (after its
+    # update), particles (after the bed phase).  At the first gas-energy update:
+    # the radiative sources (after the ignition pulse) and the soil (after its
+    # step).
+    EARLY_AT = {"dom": ("u", "v", "w", "k_turb", "eps_turb", "nu_t")
+                       + tuple("p_" + k for k in PARTS),
+                "gas_update": ("q_rad", "q_rad_gas", "T_soil")}
+    EARLY = tuple(k for ks in EARLY_AT.values() for k in ks)
+    # Fields the step first reads at the outflow sponge or later (spread_3d.py
+    # order: dt, EoS, bed and the DOM's inputs, momentum and the projection come
+    # first): their upload runs on the copy stream while those phases compute.
+    LATE = ("Y_fuel", "k_turb", "eps_turb", "phi", "q_rad_gas")
+
     def __init__(self, case: dict, device="cuda", projection_cg_rtol: float | None = None,
                  form: str = "plain"):
         self.solver = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol,
@@ -242,6 +257,32 @@ class HostStepper:
         self.host["T_soil"] = s.T_soil.cpu().pin_memory()
         for k in self.PARTS:
             self.host["p_" + k] = s.part[k].cpu().pin_memory()
+        # device copies taken at the DOM phase (the solver swaps field buffers
+        # afterwards, so the copy stream reads these, not the live fields)
+        self.stage = {k: torch.empty_like(self._dev(k)) for k in self.EARLY}
+        self.copy_stream = torch.cuda.Stream(device=s.dev)
+        self._sent = set()
+        self._late_ev = None
+        s.phase_hook = self._on_phase
+
+    def _on_phase(self, label):
+        if label == "sponge" and self._late_ev is not None:
+            torch.cuda.current_stream(self.solver.dev).wait_event(self._late_ev)
+            self._late_ev = None
+            return
+        keys = self.EARLY_AT.get(label)
+        if keys is None or label in self._sent:
+            return
+        cur = torch.cuda.current_stream(self.solver.dev)
+        for k in keys:
+            self.stage[k].copy_(self._dev(k), non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(cur)
+        self.copy_stream.wait_event(ev)
+        with torch.cuda.stream(self.copy_stream):
+            for k in keys:
+                self.host[k].copy_(self.stage[k], non_blocking=True)
+        self._sent.add(label)
 
     def _dev(self, k):
         s = self.solver
@@ -259,11 +300,24 @@ class HostStepper:
     def step(self):
         """Upload the host state, advance one outer step, download it."""
         for k, h in self.host.items():
-            self._dev(k).copy_(h, non_blocking=True)
+            if k not in self.LATE:
+                self._dev(k).copy_(h, non_blocking=True)
+        with torch.cuda.stream(self.copy_stream):
+            for k in self.LATE:
+                self._dev(k).copy_(self.host[k], non_blocking=True)
+            self._late_ev = torch.cuda.Event()
+            self._late_ev.record(self.copy_stream)
+        self._sent = set()
         alive = self.solver.step()
+        if self._late_ev is not None:  # the step ended before the sponge
+            torch.cuda.current_stream(self.solver.dev).wait_event(self._late_ev)
+            self._late_ev = None
+        sent = {k for lab in self._sent for k in self.EARLY_AT[lab]}
         for k, h in self.host.items():
-            h.copy_(self._dev(k), non_blocking=True)
+            if k not in sent:
+                h.copy_(self._dev(k), non_blocking=True)
         torch.cuda.current_stream().synchronize()
+        self.copy_stream.synchronize()
         return alive
 
     def close(self):

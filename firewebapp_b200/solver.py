@@ -316,6 +316,9 @@ class Tier3Solver:
         self._mark = None
 
     def _phase(self, label):
+        hook = getattr(self, "phase_hook", None)
+        if hook is not None:
+            hook(label)  # e.g. HostStepper's early download (api.py)
         tm = getattr(self, "_timers", None)
         if tm is None:
             return

@@ -97,3 +97,32 @@ def test_smoke_case_matches_reference(ref_smoke):
                 _compare(s.state(), ref_smoke[f"s{n}"], f"smoke step {n}")
     finally:
         s.close()
+
+
+def test_host_stepper_state_equals_device_state():
+    """api.HostStepper (the e2e path: upload, step, download, with the early
+    fields downloaded on a copy stream from the DOM phase on) leaves in host
+    memory exactly the state that stepping the solver directly gives."""
+    import numpy as np
+    from firewebapp_b200.api import HostStepper
+    from firewebapp_b200.cases import TINY
+    from firewebapp_b200.solver import Tier3Solver
+    hs = HostStepper(TINY)
+    ref = Tier3Solver(TINY)
+    for n in range(3):
+        # the caller changes its host state between steps: every field must
+        # reach the device before the step reads it (the same change is made
+        # to the directly stepped solver)
+        for k in ("Y_fuel", "k_turb", "eps_turb", "phi", "T_g", "u"):
+            f = 1.0 + 1e-3 * (n + 1)
+            hs.host[k].mul_(f)
+            ref.f[k].mul_(f)
+        hs.step()
+        ref.step()
+    st = ref.state()
+    for k in HostStepper.FIELDS + ("omega", "q_rad", "q_rad_gas", "T_soil"):
+        assert np.array_equal(hs.host[k].numpy(), st[k]), k
+    for k in HostStepper.PARTS:
+        assert np.array_equal(hs.host["p_" + k].numpy(), ref.part[k].cpu().numpy()), k
+    hs.close()
+    ref.close()
