@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <chrono>
+#include <thread>
 #include "common.cuh"
 #include "kernels.h"
 
@@ -24,11 +25,12 @@ void fs_set_error(const char* fmt, ...) {
 // Host wait for a stream through a blocking-sync event: the calling thread
 // sleeps instead of spinning, so waits do not consume the process's CPU time
 // (spinning threads can get a CPU-quota-limited process throttled).
-// Wait for a stream: poll an event for up to FS_SPIN_US microseconds (the
-// step's host decisions wait on short queues, where a sleeping wait's wake-up
-// costs more than the work), then sleep on a blocking-sync event recorded at
-// the same point.
-#define FS_SPIN_US 300
+// Wait for a stream: poll an event (yielding the core between polls) for up
+// to FS_SPIN_US microseconds, then sleep on a blocking-sync event recorded at
+// the same point.  The step's host decisions wait on queues of 0.01-3 ms (a
+// reduction, a CG batch, a DOM sweep), where a sleeping wait's wake-up costs
+// as much as short work; longer waits (a stalled device) still sleep.
+#define FS_SPIN_US 10000
 int fs_stream_wait(cudaStream_t st) {
   static thread_local cudaEvent_t ev_poll[64] = {};
   static thread_local cudaEvent_t ev_block[64] = {};
@@ -49,6 +51,7 @@ int fs_stream_wait(cudaStream_t st) {
     if (q == cudaSuccess) return FS_OK;
     if (q != cudaErrorNotReady) return FS_ECUDA;
     if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(FS_SPIN_US)) break;
+    std::this_thread::yield();
   }
   return cudaEventSynchronize(ev_block[dev]) == cudaSuccess ? FS_OK : FS_ECUDA;
 }
