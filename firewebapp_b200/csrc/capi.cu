@@ -27,10 +27,11 @@ void fs_set_error(const char* fmt, ...) {
 // (spinning threads can get a CPU-quota-limited process throttled).
 // Wait for a stream: poll an event (yielding the core between polls) for up
 // to FS_SPIN_US microseconds, then sleep on a blocking-sync event recorded at
-// the same point.  The step's host decisions wait on queues of 0.01-3 ms (a
-// reduction, a CG batch, a DOM sweep), where a sleeping wait's wake-up costs
-// as much as short work; longer waits (a stalled device) still sleep.
-#define FS_SPIN_US 10000
+// the same point.  The step's host decisions wait on queues of 0.01-15 ms (a
+// reduction, a CG batch, the DOM's queued source iterations), and the work
+// queued after a wait starts only when the host wakes; longer waits (a
+// stalled device) still sleep.
+#define FS_SPIN_US 50000
 int fs_stream_wait(cudaStream_t st) {
   static thread_local cudaEvent_t ev_poll[64] = {};
   static thread_local cudaEvent_t ev_block[64] = {};

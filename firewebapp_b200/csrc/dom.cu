@@ -73,6 +73,8 @@ struct DomCtx {
   double *Ig_out, *Isoil, *qin;  // (Ny, Nx)
   unsigned long long* keys;      // reduction slots
   unsigned long long* h_keys;
+  int* dstate;                   // path 8's device-side test: done, iterations, error
+  int* h_dstate;
   double eps_w, tol, relax, kgmax;
   int max_iter;
   int last_iters;
@@ -762,7 +764,9 @@ static const void* octant_f32_ptr(int Mo) {
 
 // G (FP64) from FP32 octant partials; max G and max |G - G_prev|
 __global__ void k_dom_G_oct32(int64_t N, int nparts, const float* __restrict__ Goct, double* G,
-                              const double* __restrict__ Gp, unsigned long long* keys) {
+                              const double* __restrict__ Gp, unsigned long long* keys,
+                              const int* done = nullptr) {
+  if (done && *done) return;
   unsigned long long bg = 0, bd = 0;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < N;
        c += (int64_t)gridDim.x * blockDim.x) {
@@ -791,7 +795,8 @@ __global__ void k_dom_G_oct32(int64_t N, int nparts, const float* __restrict__ G
 
 __global__ void k_dom_ground_oct32(int n2, int nslots, const float* __restrict__ Qoct,
                                    const double* __restrict__ Isoil, double refl, double relax,
-                                   double* Ig, double* qin) {
+                                   double* Ig, double* qin, const int* done = nullptr) {
+  if (done && *done) return;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n2) return;
   double s = 0.0;
@@ -1442,6 +1447,7 @@ struct ClArgs {
   int C, rows, periodic;
   int groups;  // clusters (ordinate groups of MO) per octant
   unsigned down_slots;
+  const int* done;  // device flag: nonzero = the source iteration has converged, do nothing
 };
 // The hyperplane buffers carry a ghost row below the CTA's first row and a
 // ghost column left of every row (rows+1 by ny+1 per ordinate): the first
@@ -1480,6 +1486,9 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
     k_dom_octant_cl(GridDev g, ClArgs a) {
   using T2 = typename Vec2Of<T>::type;
   extern __shared__ __align__(16) unsigned char shraw[];
+  // an iteration queued past convergence: every CTA leaves before any
+  // cluster barrier or shared-memory traffic
+  if (a.done && *(volatile const int*)a.done) return;
   cg::cluster_group cl = cg::this_cluster();
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int C = a.C;
@@ -1778,7 +1787,9 @@ static const void* octant_kernel_ptr(int Mo, bool pipe, int groups = 1) {
 
 // G = sum over octants of the octant partials (octant order); max G and max |G - G_prev|
 __global__ void k_dom_G_oct(int64_t N, int nparts, const double* __restrict__ Goct, double* G,
-                            const double* __restrict__ Gp, unsigned long long* keys) {
+                            const double* __restrict__ Gp, unsigned long long* keys,
+                            const int* done = nullptr) {
+  if (done && *done) return;
   unsigned long long bg = 0, bd = 0;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < N;
        c += (int64_t)gridDim.x * blockDim.x) {
@@ -1808,7 +1819,8 @@ __global__ void k_dom_G_oct(int64_t N, int nparts, const double* __restrict__ Go
 // q_in at the ground from the downward octants' partial fluxes; ground intensity relaxation
 __global__ void k_dom_ground_oct(int n2, int nslots, const double* __restrict__ Qoct,
                                  const double* __restrict__ Isoil, double refl, double relax,
-                                 double* Ig, double* qin) {
+                                 double* Ig, double* qin, const int* done = nullptr) {
+  if (done && *done) return;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n2) return;
   double s = 0.0;
@@ -1895,6 +1907,8 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   cudaMalloc(&D->qin, sizeof(double) * n2);
   cudaMalloc(&D->keys, sizeof(unsigned long long) * 4);
   cudaMallocHost(&D->h_keys, sizeof(unsigned long long) * 4);
+  cudaMalloc(&D->dstate, sizeof(int) * 4);
+  cudaMallocHost(&D->h_dstate, sizeof(int) * 4);
   D->eps_w = 0.85; D->tol = 1.0e-3; D->relax = 0.7; D->kgmax = kgmax; D->max_iter = 30;
   D->last_iters = 0;
   D->timing = 0; D->sweep_ms = 0.0; D->sweep_count = 0;
@@ -1919,6 +1933,8 @@ void dom_destroy(void* h) {
   cudaFree(D->G); cudaFree(D->Gp); cudaFree(D->ks); cudaFree(D->kg); cudaFree(D->ksafe);
   cudaFree(D->B); cudaFree(D->Ig_out); cudaFree(D->Isoil); cudaFree(D->qin); cudaFree(D->keys);
   cudaFreeHost(D->h_keys);
+  cudaFree(D->dstate);
+  cudaFreeHost(D->h_dstate);
   for (int q = 0; q < 32; ++q) {
     cudaEventDestroy(D->ev0[q]);
     cudaEventDestroy(D->ev1[q]);
@@ -2467,6 +2483,78 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
 }
 
 // The second half: the source iterations and the radiative sources.
+// End of queued source iteration q: the host loop's test (dom_end) on the
+// device.  st: [0] done, [1] iterations run, [2] error (1 stalled hand-off,
+// 2 non-finite G).
+__global__ void k_dom_check(const unsigned long long* __restrict__ keys, double tol, int q,
+                            int* st) {
+  if (st[0]) return;
+  if (q == 0) return;
+  if (keys[2] != 0) { st[2] = 1; st[1] = q + 1; st[0] = 1; return; }
+  double Gmax = __longlong_as_double((long long)keys[0]);
+  const double dmax = __longlong_as_double((long long)keys[1]);
+  if (Gmax != Gmax || dmax != dmax) { st[2] = 2; st[1] = q + 1; st[0] = 1; return; }
+  if (Gmax < 1e-12) Gmax = 1e-12;
+  if (dmax / Gmax < tol) { st[1] = q + 1; st[0] = 1; }
+}
+
+// Path 8's source iterations without a host round trip between sweeps: the
+// iterations are queued in batches (the first as long as the previous solve),
+// every kernel of an iteration queued past convergence returns at once (the
+// flag k_dom_check sets), and the host reads the flag once per batch.  The
+// iterations that run, their order and their results are the host loop's.
+static int dom_iterate_dev(DomCtx* D, const ClArgs& base, int nslots, double refl,
+                           cudaStream_t st, int* iters_out) {
+  const GridDev& g = D->g;
+  const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
+  unsigned nb = blocks_for(N, 256);
+  if (nb > 1184) nb = 1184;
+  cudaMemsetAsync(D->dstate, 0, sizeof(int) * 4, st);
+  int queued = 0;
+  int batch = D->last_iters > 2 ? D->last_iters : 2;
+  int it = 0;
+  while (true) {
+    for (int q = 0; q < batch && queued < D->max_iter; ++q, ++queued) {
+      std::swap(D->G, D->Gp);
+      if (D->timing) cudaEventRecord(D->ev0[queued], st);
+      ClArgs ca = base;
+      ca.done = D->dstate;
+      int rc = launch_cl_sweep(D, ca, st);
+      if (rc != FS_OK) return rc;
+      if (D->timing) cudaEventRecord(D->ev1[queued], st);
+      cudaMemsetAsync(D->keys, 0, sizeof(unsigned long long) * 2, st);
+      if (D->fp32) {
+        k_dom_G_oct32<<<nb, 256, 0, st>>>(N, 8 * D->groups, D->Goct32, D->G, D->Gp, D->keys,
+                                          D->dstate);
+        k_dom_ground_oct32<<<blocks_for(n2, 128), 128, 0, st>>>(
+            (int)n2, nslots, D->Qoct32, D->Isoil, refl, D->relax, D->Ig_out, D->qin, D->dstate);
+      } else {
+        k_dom_G_oct<<<nb, 256, 0, st>>>(N, 8 * D->groups, D->Goct, D->G, D->Gp, D->keys,
+                                        D->dstate);
+        k_dom_ground_oct<<<blocks_for(n2, 128), 128, 0, st>>>(
+            (int)n2, nslots, D->Qoct, D->Isoil, refl, D->relax, D->Ig_out, D->qin, D->dstate);
+      }
+      k_dom_check<<<1, 1, 0, st>>>(D->keys, D->tol, queued, D->dstate);
+      fs_count_launch(); fs_count_launch(); fs_count_launch();
+    }
+    cudaMemcpyAsync(D->h_dstate, D->dstate, sizeof(int) * 4, cudaMemcpyDeviceToHost, st);
+    if (fs_stream_wait(st) != FS_OK) return FS_ECUDA;
+    if (D->h_dstate[2] == 1) {
+      fs_set_error("fs_dom_solve: pipelined sweep wait gave up (hand-off between CTAs stalled)");
+      return FS_ETIMEOUT;
+    }
+    if (D->h_dstate[2] == 2) return FS_ENONFINITE;
+    if (D->h_dstate[0]) { it = D->h_dstate[1]; break; }
+    if (queued >= D->max_iter) { it = queued; break; }
+    batch = 1;
+  }
+  // the host swapped G and Gp once per queued iteration; undo the swaps of
+  // the iterations that returned at once
+  if ((queued - it) & 1) std::swap(D->G, D->Gp);
+  *iters_out = it;
+  return FS_OK;
+}
+
 int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStream_t st) {
   DomCtx* D = (DomCtx*)h;
   if (!D->begun) {
@@ -2505,7 +2593,20 @@ int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStre
     cudaFuncSetAttribute(k_dom_sweep_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
   cudaMemsetAsync(D->keys + 2, 0, sizeof(unsigned long long), st);
-  int it;
+  int it = 0;
+  if (D->mode == 8) {
+    ClArgs ca{};
+    ca.kb = D->fp32 ? (const void*)D->kb32 : (const void*)D->kb;
+    ca.Goct = D->fp32 ? (void*)D->Goct32 : (void*)D->Goct;
+    ca.Qoct = D->fp32 ? (void*)D->Qoct32 : (void*)D->Qoct;
+    ca.wrap = D->fp32 ? (void*)D->wrap32 : (void*)D->wrap;
+    ca.I_amb = I_amb;
+    ca.ox = D->ox; ca.oy = D->oy; ca.oz = D->oz; ca.w = D->w; ca.Ig = D->Ig_out;
+    ca.C = D->cl_C; ca.rows = D->cl_rows; ca.periodic = 1; ca.down_slots = oa.down_slots;
+    ca.groups = D->groups;
+    rc = dom_iterate_dev(D, ca, nslots, refl, st, &it);
+    if (rc != FS_OK) return rc;
+  } else
   for (it = 0; it < D->max_iter; ++it) {
     std::swap(D->G, D->Gp);
     if (D->timing) cudaEventRecord(D->ev0[it], st);

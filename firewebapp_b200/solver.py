@@ -202,7 +202,11 @@ class Tier3Solver:
         # M_local) and writes only fields they do not read, so it runs on a
         # second stream from a worker thread, concurrently with them.
         self.overlap_dom = bool(overlap_dom)
-        self.s_dom = torch.cuda.Stream(device=dev) if self.overlap_dom else None
+        # high priority: the DOM is the longer branch, so when SMs free up the
+        # block scheduler starts its kernels (each sweep CTA needs a whole SM)
+        # before the main stream's
+        self.s_dom = (torch.cuda.Stream(device=dev, priority=-1) if self.overlap_dom
+                      else None)
         self._pool = None
         if self.overlap_dom:
             from concurrent.futures import ThreadPoolExecutor
