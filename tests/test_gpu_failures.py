@@ -1,0 +1,87 @@
+"""Failure detection mirrored as status codes, driven from host-side inputs
+(no GPU fault): non-finite fields, a pressure solve that cannot converge in
+its iteration budget, and the learned solve's forced fallback."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from firewebapp_b200._lib import FireStepError
+
+pytestmark = pytest.mark.gpu
+
+
+def test_nan_gas_temperature_raises_like_the_reference():
+    """spread_3d.py:1927-1932: NaN/Inf in T_g raises RuntimeError at the dt check."""
+    from firewebapp_b200.cases import TINY
+    from firewebapp_b200.solver import Tier3Solver
+    s = Tier3Solver(TINY)
+    s.step()
+    s.f["T_g"][3, 2, 5] = float("nan")
+    with pytest.raises(RuntimeError, match="NaN/Inf"):
+        s.step()
+    s.close()
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_dom_non_finite_input_returns_status_2(fp32):
+    """NaN temperatures make G non-finite; the path-8 source iteration's
+    device-side test reports it as FS_ENONFINITE, and the context stays usable."""
+    from test_gpu_kernels import _dom_solves
+    import test_gpu_kernels as K
+    orig = K.dev
+    calls = {"n": 0}
+
+    def poisoned(a, dtype=torch.float64):
+        t = orig(a, dtype)
+        calls["n"] += 1
+        if calls["n"] in (1, 2):  # T_s and T_g of the first solve, every 97th cell
+            t.view(-1)[::97] = float("nan")
+        return t
+
+    K.dev = poisoned
+    try:
+        with pytest.raises(FireStepError) as ei:
+            _dom_solves(8, fp32, 29, 40, 48, seed=5, calls=1)
+    finally:
+        K.dev = orig
+    assert ei.value.status == 2
+    # a clean solve on the same device afterwards works
+    out = _dom_solves(8, fp32, 29, 40, 48, seed=5, calls=1)
+    assert np.all(np.isfinite(out[0][0]))
+
+
+def test_projection_iteration_cap_returns_status_3():
+    """projection_3d.py:785-790 raises on BiCGSTAB failure; here a solve that
+    cannot meet its tolerance within maxiter returns FS_ENOCONV (3)."""
+    from firewebapp_b200.cases import TINY
+    from firewebapp_b200.solver import Tier3Solver
+    s = Tier3Solver(TINY)
+    for _ in range(3):
+        s.step()
+    s.rtol, s.proj_maxiter = 1e-14, 1
+    with pytest.raises(FireStepError) as ei:
+        s.step()
+    assert ei.value.status == 3
+    s.close()
+
+
+def test_learned_stall_falls_back_and_converges():
+    """A network switched off (output scale 0) with a strict stall test falls
+    back to the V-cycle within the solve and still reaches the tolerance."""
+    from firewebapp_b200.cases import TINY
+    from firewebapp_b200.learned import fcg_stats, init_params
+    from firewebapp_b200.solver import Tier3Solver
+    s = Tier3Solver(TINY, form="learned", learned_weights=init_params(2), learned_stall=0.5,
+                    learned_max=50)
+    s.net.set_output_scale(0.0)
+    fell = 0
+    for _ in range(5):
+        assert s.step()
+        st = fcg_stats(s)
+        fell += int(st["fell_back"])
+        if st["fell_back"]:
+            assert st["learned_iters"] >= 3 and st["vcycle_iters"] >= 1
+    assert fell >= 1 and fcg_stats(s)["fallbacks_total"] == fell
+    s.close()
