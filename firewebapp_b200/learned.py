@@ -359,6 +359,8 @@ def _main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("mode", nargs="?", default="train", choices=["train", "evaluate", "time"])
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--pair-only", action="store_true",
+                    help="evaluate: only the V-cycle and the learned form (many seeds)")
     ap.add_argument("--weights", default=None)
     ap.add_argument("--cases", type=int, default=4)
     ap.add_argument("--seed", type=int, default=100)
@@ -375,7 +377,10 @@ def _main(argv=None):
         return
     cases = learned_cases(a.cases, seed0=a.seed, nx=a.nx)
     if a.mode == "evaluate":
-        evaluate(cases, a.steps, weights=a.weights or str(WEIGHTS), warmup=a.warmup)
+        var = ((("vcycle", "mixed", None, 30, 0.9), ("learned", "learned", None, 30, 0.9))
+               if a.pair_only else None)
+        evaluate(cases, a.steps, weights=a.weights or str(WEIGHTS), warmup=a.warmup,
+                 variants=var)
         return
     t0 = time.time()
     pairs = collect_pairs(cases, a.steps, warmup=a.warmup, every=a.every)
