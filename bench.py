@@ -16,6 +16,13 @@ independent replica of the case ("replicas only": the single-case step does
 not shard); value = cell-steps/s summed over ranks, time = max over ranks.
 ``--impl reference`` times the CPU restatement of the reference algorithm
 (oracle/) on the host on a bounded slice of the same workload.
+
+At N = 1 the line also carries a ``forms`` block: the mixed-precision and the
+learned-preconditioner forms timed the same way on the same case (value, e2e,
+CG and DOM iterations per step, fallbacks of the learned solve) and their
+ratio to the plain form, and a ``step_roofline``: the per-cell-step
+algorithmic bytes of the whole step (distinct fields read and written per
+operator, with the measured CG and DOM iteration counts) over the step time.
 """
 from __future__ import annotations
 
@@ -287,6 +294,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the mixed and learned forms block of the N = 1 line")
     ap.add_argument("--form", default="plain", choices=["plain", "mixed", "learned"],
                     help="plain: FP64 throughout; mixed: FP32 DOM sweep and multigrid "
                          "preconditioner, pressure tolerance 1e-8; learned: mixed with the "
@@ -322,7 +331,6 @@ def main():
     if ws > 1:
         dist.init_process_group("nccl", init_method="env://",
                                 timeout=__import__("datetime").timedelta(seconds=600))
-    from firewebapp_b200 import _lib
     from firewebapp_b200.cases import CFG2
     from firewebapp_b200.solver import Tier3Solver
 
@@ -332,78 +340,16 @@ def main():
         case = dict(scaled(CFG2, nx=args.nx), jitter_seed=rank)
     solver = Tier3Solver(case, form=args.form, dom_sweep=args.dom_sweep)
     cells = solver.n
-    for _ in range(args.warmup):
-        solver.step()
-    torch.cuda.synchronize()
-
-    def barrier():
-        if ws > 1:
-            dist.barrier()
-
-    # ---- timed region: device-resident state, CUDA events on the stream
-    # Objects alive now (torch, numpy, the solver) move to the permanent GC
-    # generation, so a full collection during the steps scans only new ones.
-    gc.collect()
-    gc.freeze()
-    solver.enable_kernel_timers(True)
-    lib = _lib.lib()
+    M = solver.Omega.shape[0]
     clocks = ClockSampler(local) if not args.no_clocks else None
-    if clocks:
-        clocks.start()
-    barrier()
-    torch.cuda.synchronize()
-    n0 = lib.fs_launch_count()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        solver.step()
-    e1.record()
-    torch.cuda.synchronize()
-    launches = int(lib.fs_launch_count() - n0)
-    barrier()
-    clk = clocks.stop() if clocks else {"sm_mhz": None, "reasons": ["not sampled"]}
-    ms = e0.elapsed_time(e1) / args.steps
-    kt = solver.kernel_times()
-    solver.enable_kernel_timers(False)
-    work, sec = job_totals(cells * args.steps, ms * 1e-3 * args.steps, device="cuda")
-    ms = 1e3 * sec / args.steps
-    value = work / sec
+    tm = time_steps(solver, args.steps, args.warmup, ws, clocks=clocks, kernel_timers=True)
+    clk = tm["clocks"] or {"sm_mhz": None, "reasons": ["not sampled"]}
+    ms, value, launches, kt = tm["ms"], tm["value"], tm["launches"], tm["kernel_times"]
 
     # ---- roofline of the dominant bracketed kernel
     peak, peak_src = _peaks()
-    N = cells
-    M = solver.Omega.shape[0]
-    dom_mode = lib.fs_dom_sweep_mode(solver.dom)
-    alg = {  # algorithmic bytes per launch (distinct fields read + written, 8 B each)
-        # octant sweeps (paths 1, 4, 6, 7, 8): read (kappa, kappa*B) once and write
-        # the 8 octant partial G fields (FP32 in the mixed form; wrap rows and
-        # ground partials < 1% more); per-ordinate paths write every intensity
-        "dom_sweep": (N * (8.0 + 4.0 * 8) if args.form != "plain" else
-                      N * (16.0 + 8.0 * 8) if dom_mode in (1, 4, 6, 7, 8) else N * (8.0 * M + 16.0)),
-        "species_transport": N * 8.0 * 12,
-        "edc": N * 8.0 * 11,
-        "turb_diffusion_Y": N * 8.0 * 7,
-        "momentum_drag": N * 8.0 * 10,
-        "k_epsilon": N * 8.0 * 14,
-        "gas_energy_adv": N * 8.0 * 5,
-    }
-    dom_k = max((k for k in kt if k in alg), key=lambda k: kt[k][0])
-    tot_ms, nl = kt[dom_k]
-    avg_ms = tot_ms / max(nl, 1)
-    achieved = alg[dom_k] / (avg_ms * 1e-3) / 1e9
-    # DRAM bytes per launch of the dominant kernel from an ncu capture of the
-    # 100x120x60 slice of this workload (dram__bytes_read.sum + write.sum) with
-    # the default sweep (path 8), scaled by the cell count to a full launch
-    traffic = (TRAFFIC_PER_CELL.get(dom_k)
-               if args.form == "plain" and (dom_k != "dom_sweep" or dom_mode == 8) else None)
-    if traffic is not None:
-        traffic *= N
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "kernel": dom_k,
-                "peak_source": peak_src, "launches": nl, "avg_launch_ms": avg_ms,
-                "algorithmic_bytes_per_launch": alg[dom_k], "dom_sweep_path": dom_mode,
-                "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()}}
+    roofline = kernel_roofline(solver, kt, args.steps, args.form, peak, peak_src)
+    step_roof = step_roofline(solver, tm, peak, peak_src, args.form)
 
     # ---- end to end through the public API: host state in, result out
     e2e = None
@@ -418,6 +364,10 @@ def main():
                          f"({c} cells, {el:.1f} s), numpy oracle port, projection "
                          f"BiCGSTAB rtol 1e-6"}
 
+    forms = None
+    if ws == 1 and not args.nx and args.form == "plain" and not args.no_forms:
+        forms = time_forms(case, args, value, e2e)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
@@ -431,13 +381,179 @@ def main():
                        "form": args.form, "cells": cells, "ordinates": M,
                        "parallelism": f"replicas{ws}", "l2": "inputs larger than L2",
                        "projection_rtol": solver.rtol},
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,
-            "gpu_launches": launches,
+            "roofline": roofline, "step_roofline": step_roof, "cpu_baseline": cpu,
+            "clocks": clk, "e2e": e2e, "gpu_launches": launches,
+            "iterations_per_step": {"cg": tm["cg_per_step"], "dom_source": tm["dom_per_step"],
+                                    "pressure": tm["proj_per_step"]},
+            "forms": forms,
         }
         print(json.dumps(line), flush=True)
     solver.close()
     if ws > 1:
         dist.destroy_process_group()
+
+
+def time_steps(solver, steps, warmup, ws, clocks=None, kernel_timers=False):
+    """Warm up, then time ``steps`` outer steps with CUDA events on the
+    solver's stream (barrier and synchronize on both sides, max over ranks).
+    Also counts this library's kernel launches and the CG, pressure and DOM
+    source iterations of the timed steps, and the learned solve's fallbacks."""
+    import torch
+    import torch.distributed as dist
+    from firewebapp_b200 import _lib
+    lib = _lib.lib()
+    for _ in range(warmup):
+        solver.step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    # Objects alive now (torch, numpy, the solver) move to the permanent GC
+    # generation, so a full collection during the steps scans only new ones.
+    gc.collect()
+    gc.freeze()
+    if kernel_timers:
+        solver.enable_kernel_timers(True)
+    fb0 = None
+    if solver.form == "learned":
+        from firewebapp_b200.learned import fcg_stats
+        fb0 = fcg_stats(solver)["fallbacks_total"]
+    if clocks:
+        clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    n0 = lib.fs_launch_count()
+    cg = proj = dom = 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        solver.step()
+        d = solver.diag
+        cg += sum(d.cg_iters)
+        proj += d.proj_iters
+        dom += d.dom_iters
+    e1.record()
+    torch.cuda.synchronize()
+    launches = int(lib.fs_launch_count() - n0)
+    barrier()
+    clk = clocks.stop() if clocks else None
+    ms = e0.elapsed_time(e1) / steps
+    kt = solver.kernel_times() if kernel_timers else {}
+    if kernel_timers:
+        solver.enable_kernel_timers(False)
+    work, sec = job_totals(solver.n * steps, ms * 1e-3 * steps, device="cuda")
+    out = {"ms": 1e3 * sec / steps, "value": work / sec, "launches": launches,
+           "kernel_times": kt, "clocks": clk, "cg_per_step": cg / steps,
+           "proj_per_step": proj / steps, "dom_per_step": dom / steps}
+    if fb0 is not None:
+        from firewebapp_b200.learned import fcg_stats
+        out["fallbacks"] = fcg_stats(solver)["fallbacks_total"] - fb0
+    return out
+
+
+def kernel_roofline(solver, kt, steps, form, peak, peak_src):
+    """Roofline of the dominant bracketed kernel.  Algorithmic bytes per
+    launch follow the step's per-operator count (each distinct field read or
+    written once per launch, at its storage width).  For the DOM sweep that
+    count is the reference's: every one of the M ordinates reads and writes
+    its intensity field, plus G read and written, 16 M + 16 bytes per cell
+    and source iteration at FP64 (8 M + 8 at FP32); the fused sweep here never
+    stores intensities, and its own field traffic (kappa, kappa*B in, eight
+    octant partial G fields out) is given beside it."""
+    from firewebapp_b200 import _lib
+    lib = _lib.lib()
+    N = solver.n
+    M = solver.Omega.shape[0]
+    dom_mode = lib.fs_dom_sweep_mode(solver.dom)
+    w = 8.0 if form == "plain" else 4.0
+    alg = {
+        "dom_sweep": N * (2.0 * w * M + 16.0),
+        "species_transport": N * 8.0 * 12,
+        "edc": N * 8.0 * 11,
+        "turb_diffusion_Y": N * 8.0 * 7,
+        "momentum_drag": N * 8.0 * 10,
+        "k_epsilon": N * 8.0 * 14,
+        "gas_energy_adv": N * 8.0 * 5,
+    }
+    fused_dom = N * (2.0 * w + 8.0 * w) if dom_mode in (4, 8) else N * (8.0 * M + 16.0)
+    dom_k = max((k for k in kt if k in alg), key=lambda k: kt[k][0])
+    tot_ms, nl = kt[dom_k]
+    avg_ms = tot_ms / max(nl, 1)
+    achieved = alg[dom_k] / (avg_ms * 1e-3) / 1e9
+    # DRAM bytes per launch of the dominant kernel from an ncu capture of the
+    # 100x120x60 slice of this workload (dram__bytes_read.sum + write.sum) with
+    # the default sweep (path 8), scaled by the cell count to a full launch
+    traffic = (TRAFFIC_PER_CELL.get(dom_k)
+               if form == "plain" and (dom_k != "dom_sweep" or dom_mode == 8) else None)
+    if traffic is not None:
+        traffic *= N
+    out = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "traffic": traffic, "kernel": dom_k,
+           "peak_source": peak_src, "launches": nl, "avg_launch_ms": avg_ms,
+           "algorithmic_bytes_per_launch": alg[dom_k], "dom_sweep_path": dom_mode,
+           "kernels_ms_per_step": {k: v[0] / steps for k, v in kt.items()}}
+    if dom_k == "dom_sweep":
+        out["fused_sweep_bytes_per_launch"] = fused_dom
+        out["fused_sweep_achieved"] = fused_dom / (avg_ms * 1e-3) / 1e9
+    return out
+
+
+def step_roofline(solver, tm, peak, peak_src, form):
+    """Whole-step roofline: algorithmic bytes per cell and outer step
+    B = B_step + N_SUB B_sub + 128 n_pc f_b + n_cg B_cg + n_src (16 M + 16)
+    + 96 (per-operator field counts of the reference loop; n_cg and n_src the
+    measured CG and DOM source iterations per step, f_b the bed fraction of
+    the cells, n_pc the particles per bed cell), FP64 widths; times cells over
+    the step time."""
+    g = solver.grid
+    M = solver.Omega.shape[0]
+    f_b = g.n_z_bed / g.Nz
+    n_pc = float(solver.p["n_per_cell"])
+    B_step, B_sub, B_cg = 688.0, 328.0 + 24.0 * f_b, 280.0
+    n_cg, n_src = tm["cg_per_step"], tm["dom_per_step"]
+    terms = {"B_step": B_step, "N_SUB*B_sub": 10 * B_sub, "bed": 128.0 * n_pc * f_b,
+             "n_cg*B_cg": n_cg * B_cg, "dom": 96.0 + n_src * (16.0 * M + 16.0)}
+    per_cell = sum(terms.values())
+    achieved = per_cell * solver.n / (tm["ms"] * 1e-3) / 1e9
+    return {"bound": "hbm", "bytes_per_cell_step": per_cell, "terms": terms,
+            "bytes_per_step": per_cell * solver.n, "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+            "widths": "fp64 field widths for every form"}
+
+
+def time_forms(case, args, plain_value, plain_e2e):
+    """The mixed-precision and learned-preconditioner forms on the same case,
+    timed like the headline (device-resident) and end to end."""
+    import torch
+    from firewebapp_b200.solver import Tier3Solver
+    out = {}
+    for form in ("mixed", "learned"):
+        s = Tier3Solver(case, form=form)
+        try:
+            tm = time_steps(s, args.steps, args.warmup, 1)
+            rec = {"value": tm["value"], "ms_per_step": tm["ms"], "gpu_launches": tm["launches"],
+                   "projection_rtol": s.rtol, "cg_per_step": tm["cg_per_step"],
+                   "pressure_iterations_per_step": tm["proj_per_step"],
+                   "dom_source_per_step": tm["dom_per_step"],
+                   "over_plain": tm["value"] / plain_value}
+            if "fallbacks" in tm:
+                rec["fallbacks"] = tm["fallbacks"]
+                rec["pressure_solves"] = int(round(tm["proj_per_step"] * args.steps))
+        finally:
+            s.close()
+            del s
+            torch.cuda.empty_cache()
+        if not args.no_e2e:
+            rec["e2e"] = measure_e2e(case, args.steps, 1, form)
+            if plain_e2e:
+                rec["e2e_over_plain"] = rec["e2e"]["value"] / plain_e2e["value"]
+        out[form] = rec
+    out["learned_mixed_over_plain"] = out["learned"]["over_plain"]
+    out["mixed_over_plain"] = out["mixed"]["over_plain"]
+    return out
 
 
 def measure_e2e(case, steps, ws, form="plain"):

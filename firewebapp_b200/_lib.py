@@ -48,6 +48,10 @@ class FsBedParams(C.Structure):
                 ("i_src1", I)]
 
 
+class FsColumnDiag(C.Structure):
+    _fields_ = [("n_ign", I64), ("lead_i", I), ("S_pyro_max", D), ("hrr_max", D)]
+
+
 _G = C.POINTER(FsGrid)
 
 # name -> (restype, argtypes)
@@ -74,6 +78,10 @@ SIGNATURES = {
     "fs_gas_energy_update": (I, [_G, P, P, P, P, P, P, P, P, P, D, D, D, I, I, I, I, P]),
     "fs_eos": (I, [_G, P, P, P, P, D, P]),
     "fs_clip": (I, [I64, P, D, D, P]),
+    "fs_div_target": (I, [I64, P, P, P, P, D, P, P]),
+    "fs_column_diag_scratch_bytes": (I64, [_G]),
+    "fs_column_diag": (I, [_G, P, P, P, P, D, D, D, P, P, C.POINTER(FsColumnDiag), P]),
+    "fs_ignition_pulse": (I, [_G, P, I, I, I, D, P]),
     "fs_solid_conduction": (I, [_G, P, P, P, D, D, D, D, P]),
     "fs_solid_conduction_capped": (I, [_G, P, P, P, D, D, D, D, D, D, P]),
     "fs_soil_step": (I, [I, I, I, P, P, D, P, P, P, D, D, D, D, D, P]),

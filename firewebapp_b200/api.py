@@ -17,6 +17,7 @@ warm-start pressure, DOM intensities) stay on the device, as the reference's
 """
 from __future__ import annotations
 
+import ctypes as _C
 import gc
 import json
 import math
@@ -26,7 +27,7 @@ from pathlib import Path
 import numpy as np
 import torch
 
-from ._lib import check, ptr, ptr_array
+from ._lib import FsColumnDiag, check, ptr, ptr_array
 from .solver import Tier3Solver, _ctypes_double
 
 HOC_J = 1.7e7            # heat of combustion, _constants.py:36
@@ -57,6 +58,8 @@ class Spread3DResultGPU:
     nu_t_final: np.ndarray | None = None
     ros_Ts: float | None = None
     hrrpua_peak: float | None = None
+    snap_t: list = field(default_factory=list)
+    snap_lead_x: list = field(default_factory=list)
 
     def save(self, path, metadata=None):
         """Write the ``Spread3DResult.save`` key set (``spread_3d.py:460-511``).
@@ -107,66 +110,95 @@ def compute_steady_ros(front_t, front_x, t_end, source_x, domain_m):
 
 
 def ros_from_snapshots(times, x_lead):
-    """ROS_Ts: least-squares slope of the leading x with T_s >= 600 K over
-    the snapshots with t >= 1 s (``_cheney_phase16_worker.py:208-231``)."""
+    """ROS_Ts [m/s] as the snapshot worker computes it
+    (``_cheney_phase16_worker.py:208-231``): over the snapshots in which some
+    column holds T_s >= 600 K (``x_lead`` finite there), at least three, a
+    least-squares line through (t, x_lead) of those with t >= 1 s, at least
+    three; NaN otherwise.  The worker reports the slope in m/min."""
     t = np.asarray(times, dtype=np.float64)
     x = np.asarray(x_lead, dtype=np.float64)
-    ok = (t >= 1.0) & np.isfinite(x)
-    if ok.sum() < 2:
+    burned = np.isfinite(x)
+    t, x = t[burned], x[burned]
+    if t.size < 3:
         return float("nan")
-    return float(np.polyfit(t[ok], x[ok], 1)[0])
+    late = t >= 1.0
+    if int(late.sum()) < 3:
+        return float("nan")
+    return float(np.polyfit(t[late], x[late], 1)[0])
 
 
 class _Diag:
-    """Per-step maxima of ``spread_3d.py:3503-3512`` on the device."""
+    """Per-step diagnostics of ``spread_3d.py:3503-3512`` and the front and
+    heat-release columns, on the device (``fs_field_max_multi`` and
+    ``fs_column_diag``); one host read per call."""
 
     def __init__(self, solver: Tier3Solver):
-        self.s = solver
-        self.sp = torch.empty_like(solver.f["rho"])
-        self.col = torch.empty(solver.shape, dtype=torch.float64, device=solver.dev)
+        s = solver
+        self.s = s
+        g = s.grid
+        self.scratch = torch.empty(int(s.lib.fs_column_diag_scratch_bytes(s.gp)),
+                                   dtype=torch.uint8, device=s.dev)
+        self.hrr = torch.empty(g.Nx, dtype=torch.float64, device=s.dev)
+        self.scale = HOC_J * g.dy / g.Ly
+        # cell-centre x as the snapshot files hold it (float32, spread_3d.py:3662)
+        self.x_mid32 = np.asarray(g.x_mid, dtype=np.float32)
+        self.last = None
 
-    def record(self, res: Spread3DResultGPU):
+    def columns(self) -> FsColumnDiag:
+        """Ignited cells, max S_pyro, HRRPUA(x) (kept in ``self.hrr``), its
+        maximum and the leading column with T_s >= 600 K, from the current state."""
         s = self.s
-        torch.add(s.bed_out["S_pyro"], s.bed_out["S_drying"], out=self.sp)
-        m = s._maxes([s.f["T_g"], s.f["T_s"], self.sp, s.w["Q_comb"], s.w["omega"],
-                      s.f["Y_fuel"]], [1, 1, 1, 1, 1, 1])
-        n_ign = int((s.f["T_s"] >= s.p["T_ign"]).sum().item())
+        out = FsColumnDiag()
+        check(s.lib.fs_column_diag(s.gp, ptr(s.f["T_s"]), ptr(s.w["omega"]),
+                                   ptr(s.bed_out["S_pyro"]), ptr(s.bed_out["S_drying"]),
+                                   float(s.p["T_ign"]), T_IGN_ROS, self.scale, ptr(self.hrr),
+                                   ptr(self.scratch), _C.byref(out), s._s()), "fs_column_diag")
+        self.last = out
+        return out
+
+    def record(self, res: "Spread3DResultGPU"):
+        s = self.s
+        m = s._maxes([s.f["T_g"], s.f["T_s"], s.w["Q_comb"], s.w["omega"], s.f["Y_fuel"]],
+                     [1, 1, 1, 1, 1])
+        c = self.columns()
         res.diag_t.append(s.t)
         res.diag_Tg_max.append(m[0])
         res.diag_Ts_max.append(m[1])
-        res.diag_Sp_max.append(m[2])
-        res.diag_Qc_max.append(m[3])
-        res.diag_omega_max.append(m[4])
-        res.diag_Y_max.append(m[5])
-        res.diag_n_ign.append(n_ign)
+        res.diag_Sp_max.append(c.S_pyro_max)
+        res.diag_Qc_max.append(m[2])
+        res.diag_omega_max.append(m[3])
+        res.diag_Y_max.append(m[4])
+        res.diag_n_ign.append(int(c.n_ign))
         res.diag_proj_div_max.append(s.diag.proj_div_max)
-        res.diag_proj_n_iter.append(len(s.diag.proj_iters))
+        res.diag_proj_n_iter.append(int(s.diag.proj_iters))
+        return c
 
     def lead_x_Ts(self):
-        """Largest cell-centre x with any T_s >= 600 K, or NaN."""
-        s = self.s
-        hot = (s.f["T_s"] >= T_IGN_ROS).any(dim=0).any(dim=0)
-        idx = torch.nonzero(hot)
-        if idx.numel() == 0:
-            return float("nan")
-        return (float(idx.max().item()) + 0.5) * s.grid.dx
+        """x (float32 cell centre) of the last column with T_s >= 600 K, or NaN."""
+        c = self.last if self.last is not None else self.columns()
+        return float(self.x_mid32[c.lead_i]) if c.lead_i >= 0 else float("nan")
 
     def hrrpua_x(self):
         """HRRPUA(x) = (1/Ly) sum_{j,k} omega * HOC_J * dz_k * dy  [W/m^2]."""
-        s = self.s
-        w = s.w["omega"] * s.dz_t.view(-1, 1, 1)
-        return (w.sum(dim=(0, 1)) * HOC_J * s.grid.dy / s.grid.Ly)
+        if self.last is None:
+            self.columns()
+        return self.hrr
 
 
 def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | None = None,
-                      snapshot_every_s: float = 1.0, device="cuda",
-                      projection_cg_rtol: float | None = None, snapshot_dir=None,
-                      snapshot_interval_s: float = 1.0, form: str = "plain") -> Spread3DResultGPU:
+                      device="cuda", projection_cg_rtol: float | None = None,
+                      snapshot_dir=None, snapshot_interval_s: float = 1.0,
+                      form: str = "plain") -> Spread3DResultGPU:
     """Device-resident ``run_3d_spread`` for a case; stops at ``n_steps``
     outer steps, at ``t_end`` simulated seconds or at the reference's own
-    exit tests, whichever comes first.  With ``snapshot_dir`` it writes
-    ``snap_NNNN.npz`` files every ``snapshot_interval_s`` of simulated time,
-    as the reference does (spread_3d.py:3537-3669)."""
+    exit tests, whichever comes first.
+
+    Snapshot instants follow the reference (``spread_3d.py:3537``): after the
+    first step and then whenever ``snapshot_interval_s`` of simulated time has
+    passed since the last one.  With ``snapshot_dir`` a ``snap_NNNN.npz`` file
+    with the reference's key set is written at each instant; either way the
+    leading column with T_s >= 600 K is recorded there, and ``ros_Ts`` is the
+    snapshot worker's fit over those instants (``ros_from_snapshots``)."""
     if n_steps is None and t_end is None:
         raise ValueError("run_3d_spread_gpu needs n_steps or t_end")
     s = Tier3Solver(case, device=device, projection_cg_rtol=projection_cg_rtol, form=form)
@@ -184,7 +216,6 @@ def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | 
         if snapshot_dir is not None:
             snapshot_dir = Path(snapshot_dir)
             snapshot_dir.mkdir(parents=True, exist_ok=True)
-        next_snap = snapshot_every_s
         hrr_peak = 0.0
         k = 0
         while True:
@@ -195,16 +226,15 @@ def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | 
             if not s.step():
                 break
             k += 1
-            dg.record(res)
-            hrr_peak = max(hrr_peak, float(dg.hrrpua_x().max().item()))
-            if s.t >= next_snap:
+            c = dg.record(res)
+            hrr_peak = max(hrr_peak, c.hrr_max)
+            if s.t - last_snap_t >= snapshot_interval_s:
+                last_snap_t = s.t
                 snap_t.append(s.t)
                 snap_x.append(dg.lead_x_Ts())
-                next_snap += snapshot_every_s
-            if snapshot_dir is not None and s.t - last_snap_t >= snapshot_interval_s:
-                last_snap_t = s.t
-                write_snapshot(s, snapshot_dir / f"snap_{snap_idx:04d}.npz",
-                               float(case.get("wind_speed_m_s", 0.0)))
+                if snapshot_dir is not None:
+                    write_snapshot(s, snapshot_dir / f"snap_{snap_idx:04d}.npz",
+                                   float(case.get("wind_speed_m_s", 0.0)))
                 snap_idx += 1
         st = s.state()
         res.state_final = st
@@ -215,6 +245,7 @@ def run_3d_spread_gpu(case: dict, *, n_steps: int | None = None, t_end: float | 
         res.ros_m_s = compute_steady_ros(s.front_t, s.front_x, s.t,
                                          source_x=s.p["i_src_end"] * g.dx, domain_m=g.Lx)
         res.ros_Ts = ros_from_snapshots(snap_t, snap_x)
+        res.snap_t, res.snap_lead_x = snap_t, snap_x
         res.hrrpua_peak = hrr_peak
         return res
     finally:

@@ -69,7 +69,16 @@ SMOKE = dict(
     Lx=2.4, Ly=0.8, Lz=1.0, bed_x_start=0.3, bed_x_end=2.4,
 )
 
-CASES = {"cfg1": CFG1, "cfg2": CFG2, "tiny": TINY, "smoke": SMOKE}
+# The 400 x 120 x 60 workload's geometry and physics (dz = 0.0625 m, n_z_bed 4,
+# 16 bed particles per surface cell, S8, U10 6 m/s, moisture 0.06, bulk
+# density 0.35) on a 40 x 16 x 60 cell slice, whose reference states are
+# committed as fixtures.
+CFG2_SLICE = dict(
+    CFG2,
+    Lx=4.0, Ly=1.6, bed_x_start=1.0, bed_x_end=4.0,
+)
+
+CASES = {"cfg1": CFG1, "cfg2": CFG2, "tiny": TINY, "smoke": SMOKE, "cfg2_slice": CFG2_SLICE}
 
 
 def scaled(case: dict, nx: int | None = None, ny: int | None = None,

@@ -320,6 +320,7 @@ int fs_edc(int64_t n, const double* rho, double* T_g, double* Y_F, double* Y_O2,
     fs_set_error("fs_edc: bad argument");
     return FS_EARG;
   }
+  if (n == 0) return FS_OK;
   return check(launch_edc(n, rho, T_g, Y_F, Y_O2, k, eps, Y_H2O, omega, chi_rad, cp_g, dt,
                           n_substeps, s_stoich, hoc_J, extinction, scratch, ST(stream)),
                "fs_edc");
@@ -343,6 +344,60 @@ int fs_eos(const FsGrid* g, double* rho, double* rho_prev, const double* T_g, do
   const double R_air = 8.314 / 0.029;
   return check(launch_eos(gd, rho, rho_prev, T_g, Y_O2, 101325.0, R_air, T_amb, ST(stream)),
                "fs_eos");
+}
+
+int fs_div_target(int64_t n, const double* rho, const double* rho_prev, const double* S_pyro,
+                  const double* S_drying, double dt, double* div_target, void* stream) {
+  if (n < 0 || !(dt > 0.0) || (n > 0 && (!rho || !rho_prev || !S_pyro || !S_drying ||
+                                         !div_target))) {
+    fs_set_error("fs_div_target: bad argument");
+    return FS_EARG;
+  }
+  return check(launch_div_target(n, rho, rho_prev, S_pyro, S_drying, dt, div_target, ST(stream)),
+               "fs_div_target");
+}
+
+int fs_ignition_pulse(const FsGrid* g, double* q_rad, int k, int i0, int i1, double q_add,
+                      void* stream) {
+  GRID("fs_ignition_pulse");
+  if (!q_rad || k < 0 || k >= gd.nz || i0 < 0 || i1 > gd.nx || i0 > i1) {
+    fs_set_error("fs_ignition_pulse: bad argument (k=%d, i0=%d, i1=%d)", k, i0, i1);
+    return FS_EARG;
+  }
+  return check(launch_ignition_pulse(gd, q_rad, k, i0, i1, q_add, ST(stream)),
+               "fs_ignition_pulse");
+}
+
+int64_t fs_column_diag_scratch_bytes(const FsGrid* g) {
+  GridDev gd;
+  if (!to_grid(g, gd, "fs_column_diag_scratch_bytes")) return -1;
+  return coldiag_scratch_bytes(gd);
+}
+
+int fs_column_diag(const FsGrid* g, const double* T_s, const double* omega, const double* S_pyro,
+                   const double* S_drying, double T_ign, double T_front, double hrr_scale,
+                   double* hrr_x, void* scratch, FsColumnDiag* out, void* stream) {
+  GRID("fs_column_diag");
+  if (!T_s || !omega || !S_pyro || !S_drying || !scratch || !out) {
+    fs_set_error("fs_column_diag: bad argument");
+    return FS_EARG;
+  }
+  SmallScratch* sc = small_scratch();
+  if (!sc) {
+    fs_set_error("fs_column_diag: scratch allocation failed");
+    return FS_ECUDA;
+  }
+  int rc = launch_coldiag(gd, T_s, omega, S_pyro, S_drying, T_ign, T_front, hrr_scale, hrr_x,
+                          scratch, ST(stream));
+  if (rc != FS_OK) return check(rc, "fs_column_diag");
+  launch_coldiag_keys(scratch, sc->dres, ST(stream));
+  cudaMemcpyAsync(sc->hpin, sc->dres, 4 * sizeof(double), cudaMemcpyDeviceToHost, ST(stream));
+  if (fs_stream_wait(ST(stream)) != FS_OK) return check(FS_ECUDA, "fs_column_diag");
+  out->n_ign = (int64_t)sc->hpin[0];
+  out->S_pyro_max = sc->hpin[1];
+  out->hrr_max = sc->hpin[2];
+  out->lead_i = (int)sc->hpin[3];
+  return check(cuda_status(), "fs_column_diag");
 }
 
 int fs_clip(int64_t n, double* f, double lo, double hi, void* stream) {

@@ -2489,11 +2489,13 @@ int dom_solve(void* h, const double* Ts, const double* Tg, const double* as, con
 __global__ void k_dom_check(const unsigned long long* __restrict__ keys, double tol, int q,
                             int* st) {
   if (st[0]) return;
-  if (q == 0) return;
+  // a stalled hand-off or a non-finite G ends the solve on every iteration,
+  // the first included; only the convergence ratio waits for a second one
   if (keys[2] != 0) { st[2] = 1; st[1] = q + 1; st[0] = 1; return; }
   double Gmax = __longlong_as_double((long long)keys[0]);
   const double dmax = __longlong_as_double((long long)keys[1]);
   if (Gmax != Gmax || dmax != dmax) { st[2] = 2; st[1] = q + 1; st[0] = 1; return; }
+  if (q == 0) return;
   if (Gmax < 1e-12) Gmax = 1e-12;
   if (dmax / Gmax < tol) { st[1] = q + 1; st[0] = 1; }
 }
@@ -2703,7 +2705,9 @@ int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStre
                                                         D->qin);
       fs_count_launch();
     }
-    if (it > 0) {
+    // the error checks run on every iteration (a single-iteration solve
+    // included); the convergence test, as the reference's, from the second
+    {
       cudaMemcpyAsync(D->h_keys, D->keys, sizeof(unsigned long long) * 3, cudaMemcpyDeviceToHost,
                       st);
       if (fs_stream_wait(st) != FS_OK) return FS_ECUDA;
@@ -2715,7 +2719,7 @@ int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStre
       double dmax = key_to_double(D->h_keys[1]);
       if (Gmax != Gmax || dmax != dmax) return FS_ENONFINITE;
       if (Gmax < 1e-12) Gmax = 1e-12;
-      if (dmax / Gmax < D->tol) { ++it; break; }
+      if (it > 0 && dmax / Gmax < D->tol) { ++it; break; }
     }
   }
   D->last_iters = it;

@@ -160,3 +160,13 @@ int launch_levelset(const GridDev& g, const double* phi, const double* aux, doub
                     double coef, int mode, cudaStream_t st);
 int launch_active_count(int64_t n, const double* om, const double* Tg, const double* YF,
                         unsigned long long* count, unsigned char* mask, cudaStream_t st);
+int launch_div_target(int64_t n, const double* rho, const double* rho_prev, const double* Sp,
+                      const double* Sd, double dt, double* out, cudaStream_t st);
+int launch_ignition_pulse(const GridDev& g, double* q, int k, int i0, int i1, double q_add,
+                          cudaStream_t st);
+int coldiag_slices(const GridDev& g);
+int64_t coldiag_scratch_bytes(const GridDev& g);
+int launch_coldiag(const GridDev& g, const double* Ts, const double* om, const double* Sp,
+                   const double* Sd, double T_ign, double T_front, double scale, double* hrr_x,
+                   void* scratch, cudaStream_t st);
+int launch_coldiag_keys(const void* scratch, double* out4, cudaStream_t st);

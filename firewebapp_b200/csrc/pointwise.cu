@@ -338,6 +338,178 @@ int launch_eos(const GridDev& g, double* rho, double* rho_prev, const double* Tg
   return cuda_status();
 }
 
+// Divergence target of the pressure projection (spread_3d.py:2300-2317, the
+// unweighted form): ((S_pyro + S_drying) - (rho - rho_prev)/dt) / max(rho, 0.1),
+// with S_pyro = copy of the bed's pyrolysis source plus its drying source
+// (spread_3d.py:2147-2148).  np.maximum keeps a NaN rho.
+__global__ void k_div_target(int64_t n, const double* __restrict__ rho,
+                             const double* __restrict__ rho_prev, const double* __restrict__ Sp,
+                             const double* __restrict__ Sd, double dt, double* __restrict__ out) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const double r = rho[c];
+  const double s = Sp[c] + Sd[c];
+  const double drho = (r - rho_prev[c]) / dt;
+  const double rs = (r != r) ? r : (r > 0.1 ? r : 0.1);
+  out[c] = (s - drho) / rs;
+}
+
+int launch_div_target(int64_t n, const double* rho, const double* rho_prev, const double* Sp,
+                      const double* Sd, double dt, double* out, cudaStream_t st) {
+  if (n == 0) return FS_OK;
+  k_div_target<<<blocks_for(n, 256), 256, 0, st>>>(n, rho, rho_prev, Sp, Sd, dt, out);
+  fs_count_launch();
+  return cuda_status();
+}
+
+// External ignition pulse (spread_3d.py:2528-2532): q_rad[k, :, i0:i1] += q_add.
+__global__ void k_ignition_pulse(GridDev g, double* q, int k, int i0, int w, double q_add) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= w * g.ny) return;
+  const int j = t / w, i = i0 + (t - j * w);
+  q[cidx(g, k, j, i)] += q_add;
+}
+
+int launch_ignition_pulse(const GridDev& g, double* q, int k, int i0, int i1, double q_add,
+                          cudaStream_t st) {
+  const int w = i1 - i0;
+  if (w <= 0 || g.ny <= 0) return FS_OK;
+  k_ignition_pulse<<<blocks_for((int64_t)w * g.ny, 128), 128, 0, st>>>(g, q, k, i0, w, q_add);
+  fs_count_launch();
+  return cuda_status();
+}
+
+// ---------------------------------------------------------------------------
+// Per-step front and heat-release diagnostics over x columns, in two passes:
+//   hrr_x[i] = scale * sum_{k,j} omega[k,j,i] * dz[k]   (HRRPUA(x) with
+//              scale = HOC * dy / Ly)
+//   lead     = largest i whose column holds a T_s >= T_front, T_s rounded to
+//              float32 first (the snapshot worker's ROS_Ts test,
+//              _cheney_phase16_worker.py:208-231, reads float32 snapshots)
+//   n_ign    = number of cells with T_s >= T_ign (spread_3d.py:3509)
+//   sp_max   = max(S_pyro + S_drying) (spread_3d.py:3506)
+//   hrr_max  = max_i hrr_x[i]
+// Pass 1: a block holds 32 columns and one of S slices of the (k, j) rows;
+// partial column sums are added per slice in a fixed order, so the result
+// does not depend on scheduling.  Pass 2 adds the slices in slice order.
+// ---------------------------------------------------------------------------
+#define COLDIAG_X 32
+#define COLDIAG_Y 8
+
+__global__ void __launch_bounds__(COLDIAG_X * COLDIAG_Y)
+    k_coldiag_partial(GridDev g, const double* __restrict__ Ts, const double* __restrict__ om,
+                      const double* __restrict__ Sp, const double* __restrict__ Sd, double T_ign,
+                      float T_front, int S, double* __restrict__ part, int* __restrict__ hot,
+                      unsigned long long* keys) {
+  __shared__ double s_sum[COLDIAG_Y][COLDIAG_X];
+  __shared__ int s_hot[COLDIAG_Y][COLDIAG_X];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.x * COLDIAG_X + tx;
+  const int rows = g.nz * g.ny;
+  double acc = 0.0;
+  int h = 0;
+  unsigned long long cnt = 0, spk = 0;
+  if (i < g.nx) {
+    for (int r = blockIdx.y * COLDIAG_Y + ty; r < rows; r += COLDIAG_Y * S) {
+      const int k = r / g.ny;
+      const int64_t c = (int64_t)r * g.nx + i;
+      const double t = Ts[c];
+      acc += om[c] * g.dz[k];
+      h |= ((float)t >= T_front) ? 1 : 0;
+      cnt += (t >= T_ign) ? 1ull : 0ull;
+      const unsigned long long kk = dkey(Sp[c] + Sd[c]);
+      spk = kk > spk ? kk : spk;
+    }
+  }
+  s_sum[ty][tx] = acc;
+  s_hot[ty][tx] = h;
+  for (int o = 16; o > 0; o >>= 1) {
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    const unsigned long long y = __shfl_xor_sync(0xffffffffu, spk, o);
+    spk = y > spk ? y : spk;
+  }
+  if (tx == 0) {
+    if (cnt) atomicAdd(keys + 0, cnt);
+    if (spk) atomicMax(keys + 1, spk);
+  }
+  __syncthreads();
+  if (ty == 0 && i < g.nx) {
+    double sum = s_sum[0][tx];
+    int hh = s_hot[0][tx];
+    for (int y = 1; y < COLDIAG_Y; ++y) {
+      sum += s_sum[y][tx];
+      hh |= s_hot[y][tx];
+    }
+    part[(int64_t)blockIdx.y * g.nx + i] = sum;
+    hot[(int64_t)blockIdx.y * g.nx + i] = hh;
+  }
+}
+
+__global__ void k_coldiag_final(int nx, int S, const double* __restrict__ part,
+                                const int* __restrict__ hot, double scale, double* hrr_x,
+                                unsigned long long* keys) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    int h = 0;
+    for (int b = 0; b < S; ++b) {
+      s += part[(int64_t)b * nx + i];
+      h |= hot[(int64_t)b * nx + i];
+    }
+    const double v = s * scale;
+    if (hrr_x) hrr_x[i] = v;
+    atomicMax(keys + 2, dkey(v));
+    if (h) atomicMax(keys + 3, (unsigned long long)(i + 1));
+  }
+}
+
+int coldiag_slices(const GridDev& g) {
+  const int bx = (g.nx + COLDIAG_X - 1) / COLDIAG_X;
+  int S = (2 * 148 + bx - 1) / bx;
+  const int rows = g.nz * g.ny;
+  const int smax = (rows + COLDIAG_Y - 1) / COLDIAG_Y;
+  if (S > smax) S = smax;
+  if (S > 64) S = 64;
+  return S < 1 ? 1 : S;
+}
+
+int64_t coldiag_scratch_bytes(const GridDev& g) {
+  const int S = coldiag_slices(g);
+  return 32 + (int64_t)S * g.nx * (int64_t)(sizeof(double) + sizeof(int)) + 256;
+}
+
+int launch_coldiag(const GridDev& g, const double* Ts, const double* om, const double* Sp,
+                   const double* Sd, double T_ign, double T_front, double scale, double* hrr_x,
+                   void* scratch, cudaStream_t st) {
+  const int S = coldiag_slices(g);
+  unsigned long long* keys = (unsigned long long*)scratch;
+  double* part = (double*)((char*)scratch + 32);
+  int* hot = (int*)(part + (int64_t)S * g.nx);
+  cudaMemsetAsync(keys, 0, 32, st);
+  dim3 grid((g.nx + COLDIAG_X - 1) / COLDIAG_X, S);
+  k_coldiag_partial<<<grid, dim3(COLDIAG_X, COLDIAG_Y), 0, st>>>(
+      g, Ts, om, Sp, Sd, T_ign, (float)T_front, S, part, hot, keys);
+  fs_count_launch();
+  k_coldiag_final<<<blocks_for(g.nx, 128), 128, 0, st>>>(g.nx, S, part, hot, scale, hrr_x,
+                                                         keys);
+  fs_count_launch();
+  return cuda_status();
+}
+
+__global__ void k_coldiag_keys(const unsigned long long* keys, double* out) {
+  if (threadIdx.x == 0) {
+    out[0] = (double)keys[0];
+    out[1] = keys[1] ? dkey_inv(keys[1]) : 0.0;
+    out[2] = keys[2] ? dkey_inv(keys[2]) : 0.0;
+    out[3] = (double)keys[3] - 1.0;
+  }
+}
+
+int launch_coldiag_keys(const void* scratch, double* out4, cudaStream_t st) {
+  k_coldiag_keys<<<1, 32, 0, st>>>((const unsigned long long*)scratch, out4);
+  fs_count_launch();
+  return cuda_status();
+}
+
 // clip a field to [lo, hi] (numpy minimum/maximum semantics: NaN stays NaN)
 __global__ void k_clip(int64_t n, double* f, double lo, double hi) {
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;

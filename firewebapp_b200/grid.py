@@ -188,7 +188,18 @@ class CaseSetup:
     soil: dict = field(default_factory=dict)
 
 
+# Grid3D.build options that select the boundary-layer or segmented mesh
+# kernels (spread_3d.py:190-302) instead of the legacy uniform bed.
+_MESH_BRANCH_KEYS = ("dz_first", "dz_first_above", "bed_top_inner_bl_N", "bed_top_outer_bl_N")
+
+
 def build_grid_from_case(case):
+    for key in _MESH_BRANCH_KEYS:
+        v = _pick(case, key, None)
+        if v is not None and not (isinstance(v, bool) and not v) and float(v) > 0.0:
+            raise NotImplementedError(
+                f"{key}={v!r} selects the boundary-layer mesh, which the GPU Tier-3 step does "
+                "not provide (uniform bed layers only)")
     Lx = float(_pick(case, "Lx", 10.0)); Ly = float(_pick(case, "Ly", 2.0))
     Lz = float(_pick(case, "Lz", 1.5)); dx = float(_pick(case, "dx", 0.05))
     dy = float(_pick(case, "dy", dx))

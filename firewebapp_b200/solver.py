@@ -75,7 +75,7 @@ def build_segments(cell):
 class StepDiag:
     t: float = 0.0
     dt: float = 0.0
-    proj_iters: list = field(default_factory=list)
+    proj_iters: int = 0
     cg_iters: list = field(default_factory=list)
     proj_div_max: float = 0.0
     dom_iters: int = 0
@@ -528,8 +528,10 @@ class Tier3Solver:
         # --- 9. ignition pulse on the top bed layer of the source strip (:2528-2532)
         self._phase("misc")
         if ign and g.n_z_bed > 0:
-            sl = w["q_rad"][g.n_z_bed - 1, :, p["i_src_start"]:p["i_src_end"]]
-            sl += 240_000.0 * p["ignition_q_mult"]
+            check(L.fs_ignition_pulse(gp, ptr(w["q_rad"]), int(g.n_z_bed - 1),
+                                      int(p["i_src_start"]), int(p["i_src_end"]),
+                                      240_000.0 * float(p["ignition_q_mult"]), s),
+                  "ignition_pulse")
         if early is None:
             # --- 10/11. flame mask, gas-temperature advection
             self._flame_mask_and_gas_adv(dt)
@@ -708,9 +710,9 @@ class Tier3Solver:
     def _div_target(self, dt):
         # (S_pyro - (rho - rho_prev)/dt) / max(rho, 0.1), S_pyro = Sp + Sd (:2147, :2317)
         f, w = self.f, self.w
-        Sp, Sd = self.bed_out["S_pyro"], self.bed_out["S_drying"]
-        drho = (f["rho"] - w["rho_prev"]) / dt
-        torch.div((Sp + Sd) - drho, torch.clamp(f["rho"], min=0.1), out=w["div_target"])
+        check(self.lib.fs_div_target(self.n, ptr(f["rho"]), ptr(w["rho_prev"]),
+                                     ptr(self.bed_out["S_pyro"]), ptr(self.bed_out["S_drying"]),
+                                     dt, ptr(w["div_target"]), self._s()), "div_target")
 
     def _maxes(self, tensors, modes):
         res = (_C.c_double * len(tensors))()

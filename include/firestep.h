@@ -164,7 +164,10 @@ int fs_edc(int64_t n, const double* rho, double* T_g, double* Y_F, double* Y_O2,
  * FS_EDC_NOALLOC_MAX_CELLS cells (larger n is rejected with FS_EARG).  The
  * first call on a device looks the array up (make it before any stream
  * capture); all calls share the array, so calls whose kernels overlap on the
- * GPU race.  It calls no allocation routine. */
+ * GPU race.  It calls no allocation routine.  The looked-up address is kept
+ * for the life of the process: it is valid in the device's primary context
+ * (the one the CUDA runtime and torch use) and not after cudaDeviceReset or
+ * in another context made on the same device. */
 #define FS_EDC_NOALLOC_MAX_CELLS (1LL << 27)
 int fs_edc_noalloc(int64_t n, const double* rho, double* T_g, double* Y_F, double* Y_O2,
                    const double* k, const double* eps, const double* Y_H2O, double* omega,
@@ -178,6 +181,37 @@ int fs_gas_energy_update(const FsGrid* g, double* T_g, const double* rho, const 
                          const double* Q_g_conv, const double* q_rad_gas, double* Q_comb_out,
                          double dt_sub, double T_amb, double h_bed, int drip_on, int n_z_bed,
                          int i_src0, int i_src1, void* stream);
+
+/* spread_3d.py:2300-2317 (with S_pyro = S_pyro_bed + S_drying_bed,
+ * :2147-2148): div_target = (S_pyro - (rho - rho_prev)/dt) / max(rho, 0.1),
+ * the right-hand side of the pressure iterations; overwrites div_target. */
+int fs_div_target(int64_t n, const double* rho, const double* rho_prev, const double* S_pyro,
+                  const double* S_drying, double dt, double* div_target, void* stream);
+
+/* spread_3d.py:2528-2532: the external ignition pulse, q_rad[k, :, i0:i1] +=
+ * q_add (k = n_z_bed - 1, q_add = 240 kW/m2 x ignition_q_mult), in place. */
+int fs_ignition_pulse(const FsGrid* g, double* q_rad, int k, int i0, int i1, double q_add,
+                      void* stream);
+
+/* Per-step diagnostics over x columns, one pass over T_s, omega and the bed
+ * sources (spread_3d.py:3503-3512 maxima and ignited-cell count; ROS_Ts front
+ * test of _cheney_phase16_worker.py:208-231; HRRPUA(x)):
+ *   hrr_x[i] = hrr_scale * sum_{k,j} omega * dz_k  (device, Nx; may be NULL),
+ *   lead_i   = largest column i with any float32(T_s) >= T_front, or -1,
+ *   n_ign    = count of T_s >= T_ign,  S_pyro_max = max(S_pyro + S_drying),
+ *   hrr_max  = max_i hrr_x[i].
+ * Column sums are added in a fixed order (reproducible).  scratch: device,
+ * fs_column_diag_scratch_bytes(g) bytes.  Waits for the stream (host result). */
+typedef struct {
+  int64_t n_ign;
+  int lead_i;
+  double S_pyro_max;
+  double hrr_max;
+} FsColumnDiag;
+int64_t fs_column_diag_scratch_bytes(const FsGrid* g);
+int fs_column_diag(const FsGrid* g, const double* T_s, const double* omega, const double* S_pyro,
+                   const double* S_drying, double T_ign, double T_front, double hrr_scale,
+                   double* hrr_x, void* scratch, FsColumnDiag* out, void* stream);
 
 /* spread_3d.py:2042 / :3440 EoS; with rho_prev != NULL also copies the old
  * rho (:1984) and with Y_O2 != NULL sets the inlet column to 0.232 (:2050). */

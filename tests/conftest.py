@@ -75,3 +75,24 @@ def rel_l2(a, b):
     if den == 0.0:
         return num
     return num / den
+
+
+def dom_s8_cases():
+    """Cases of tests/golden/dom_s8.npz (reference DOM solves at S8, made by
+    tests/golden/make_dom_s8.py): {case: (inputs, [outputs of solve 0, solve 1])}."""
+    d = np.load(GOLDEN / "dom_s8.npz")
+    out = {}
+    for k in d.files:
+        parts = k.split("/")
+        case = out.setdefault(parts[0], ({}, [{}, {}]))
+        v = d[k]
+        v = v.item() if v.ndim == 0 else v
+        if len(parts) == 2:
+            case[0][parts[1]] = v
+        else:
+            case[1][int(parts[1][4:])][parts[2]] = v
+    for inp, _ in out.values():
+        for key in ("nz", "ny", "nx"):
+            inp[key] = int(inp[key])
+    return out
+

@@ -22,6 +22,14 @@ Outputs
 ``ref_smoke.npz``
     Same for the 24 x 8 x 10 ``SMOKE`` case after steps 1 and 3 (used by the
     GPU smoke check).
+``ref_cfg2_slice.npz``
+    The 40 x 16 x 60 ``CFG2_SLICE`` case (the 400 x 120 x 60 workload's
+    dz = 0.0625 m, four bed layers, 16 particles per surface cell, S8
+    quadrature injected into the reference) after steps 1, 2 and 10, without
+    the DOM intensities (80 ordinates would dominate the file).
+``ref_cfg1_10.npz``
+    The 64 x 24 x 20 ``CFG1`` case after steps 1 and 10, without the DOM
+    intensities.
 """
 from __future__ import annotations
 
@@ -68,7 +76,7 @@ def pack_vectors():
     print("kernel_vectors.npz:", len(out), "arrays")
 
 
-def ref_run(case_name, n_steps, steps, out_name):
+def ref_run(case_name, n_steps, steps, out_name, intensities=True):
     from refharness import run_reference
     from firewebapp_b200.cases import CASES
     case = CASES[case_name]
@@ -78,6 +86,8 @@ def ref_run(case_name, n_steps, steps, out_name):
         out[f"init/{k}"] = np.asarray(v)
     for n, snap in snaps.items():
         for k, v in snap.items():
+            if k == "I_set" and not intensities:
+                continue
             out[f"s{n}/{k}"] = np.asarray(v)
     for k, v in trace.items():
         out[f"trace/{k}"] = np.asarray(v, dtype=np.float64)
@@ -93,3 +103,7 @@ if __name__ == "__main__":
         ref_run("tiny", 10, [1, 2, 9, 10], "ref_tiny.npz")
     if "smoke" in what:
         ref_run("smoke", 3, [1, 3], "ref_smoke.npz")
+    if "cfg2_slice" in what:
+        ref_run("cfg2_slice", 10, [1, 2, 10], "ref_cfg2_slice.npz", intensities=False)
+    if "cfg1_10" in what:
+        ref_run("cfg1", 10, [1, 10], "ref_cfg1_10.npz", intensities=False)

@@ -126,7 +126,8 @@ PART_FIELDS = ("x", "y", "z", "alive", "m_solid", "m_water", "m_char", "T_s",
 
 
 def run_reference(case: dict, n_steps: int, capture_steps=None,
-                  projection_cg_rtol: float = 1e-12, verbose=False, step_hook=None):
+                  projection_cg_rtol: float = 1e-12, verbose=False, step_hook=None,
+                  snapshot_dir=None):
     """Run the reference for ``n_steps`` outer steps; return per-step snapshots.
 
     Returns ``(init, snaps, trace)``: ``init`` is the state right after the
@@ -134,7 +135,9 @@ def run_reference(case: dict, n_steps: int, capture_steps=None,
     ``n`` for every ``n`` in ``capture_steps`` and ``trace`` per-step scalars
     (dt, projection iterations, DOM source iterations).  ``step_hook(n,
     state, extras)``, if given, is called after every step with the
-    reference's state object and the captured extra fields.
+    reference's state object and the captured extra fields.  With
+    ``snapshot_dir`` the reference writes its own ``snap_NNNN.npz`` files
+    there (``spread_3d.py:3536-3670``).
     """
     R = load_reference()
     S, T, D, P, L, soil, F, C = (R[k] for k in "S T D P L soil F C".split())
@@ -318,7 +321,8 @@ def run_reference(case: dict, n_steps: int, capture_steps=None,
             ctx = contextlib.nullcontext() if verbose else contextlib.redirect_stdout(sink)
             with ctx:
                 S.run_3d_spread(deck, wind_speed_m_s=float(case["wind_speed_m_s"]),
-                                projection_cg_rtol=projection_cg_rtol)
+                                projection_cg_rtol=projection_cg_rtol,
+                                snapshot_dir=snapshot_dir)
         except _Stop:
             pass
         finally:

@@ -361,6 +361,50 @@ def test_dom_fp32_form(vectors, mode):
             lib().fs_dom_destroy(h)
 
 
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_dom_s8_matches_reference(fp32):
+    """The S8 sweep the 400 x 120 x 60 workload runs (80 ordinates, automatic
+    path: the co-resident octant clusters) against the reference's own DOM
+    solver with S8 injected (tests/golden/dom_s8.npz): two solves in a row,
+    the second from the intensities the first left, on every golden-vector
+    geometry and on a 40 x 16 x 60 slice of the workload's grid (dz = 0.0625
+    m).  FP64: same source iterations, outputs to 1e-11 (the sweep sums G per
+    octant, then over octants).  FP32 sweep (mixed form): outputs to 2e-5."""
+    from conftest import dom_s8_cases
+    from firewebapp_b200.quadrature import level_symmetric
+    om, wq = level_symmetric(8)
+    for name, (c, calls) in dom_s8_cases().items():
+        nz, ny, nx = c["nz"], c["ny"], c["nx"]
+        g = Grid(nz, ny, nx, c["dx"], c["dy"], c["dz_arr"])
+        h = C.c_void_p()
+        call("fs_dom_create", g.ref, om.shape[0], dbl_array(om[:, 0]), dbl_array(om[:, 1]),
+             dbl_array(om[:, 2]), dbl_array(wq), 0.5, C.byref(h))
+        try:
+            if fp32:
+                call("fs_dom_set_precision", h, 1)
+            a, omg, M = (dev(c[x]) for x in ("alpha_s", "omega_comb", "bed_moisture"))
+            YH = dev(c["Y_H2O"]) if "Y_H2O" in c else None
+            rho = dev(c["rho"]) if "rho" in c else None
+            Tsoil = dev(c["T_soil"])
+            for n, want in enumerate(calls):
+                Ts, Tg = dev(want["T_s"]), dev(want["T_g"])
+                qs, qg = torch.zeros_like(Ts), torch.zeros_like(Ts)
+                qsoil = torch.zeros((ny, nx), dtype=torch.float64, device="cuda")
+                call("fs_dom_solve", h, ptr(Ts), ptr(Tg), ptr(a), ptr(omg), c["sigma_sav"],
+                     c["T_amb"], ptr(Tsoil), ptr(YH), ptr(rho), ptr(M), ptr(qs), ptr(qg),
+                     ptr(qsoil), stream())
+                tol = 2e-5 if fp32 else 1e-11
+                if not fp32:
+                    assert lib().fs_dom_iterations(h) == want["iterations"], (name, n)
+                for got, key in ((qs, "q_rad_solid"), (qg, "q_rad_gas"),
+                                 (qsoil, "q_in_soil")):
+                    assert rel_l2(host(got), want[key]) <= tol, (name, n, key)
+            if name == "slice":
+                assert lib().fs_dom_sweep_mode(h) == 8
+        finally:
+            lib().fs_dom_destroy(h)
+
+
 def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0, groups=0):
     """q_rad_solid, q_rad_gas, q_in_soil after each of ``calls`` solves of an
     S_order DOM on seeded random fields (the y-inflow rows persist between calls)."""

@@ -99,6 +99,40 @@ def test_smoke_case_matches_reference(ref_smoke):
         s.close()
 
 
+@pytest.mark.parametrize("fixture,case_name,steps", [
+    ("ref_cfg2_slice.npz", "cfg2_slice", (1, 2, 10)),
+    ("ref_cfg1_10.npz", "cfg1", (1, 10)),
+])
+def test_workload_geometry_matches_reference(fixture, case_name, steps):
+    """Ten steps on the benchmarked geometry and physics against the
+    reference's own run: the 400 x 120 x 60 workload's vertical grid, bed and
+    S8 quadrature on a 40 x 16 x 60 slice (dz = 0.0625 m, four bed layers, 16
+    particles per surface cell, U10 6 m/s, moisture 0.06), and the 64 x 24 x 20
+    case itself (S4).  Every field within 1e-9 relative L2 after each captured
+    step, and the same dt sequence."""
+    from conftest import load_ref
+    from firewebapp_b200.cases import CASES
+    ref = load_ref(fixture)
+    s = _solver(CASES[case_name])
+    try:
+        got0 = s.state()
+        for k in ("rho", "T_g", "alpha_s", "T_s"):
+            assert np.array_equal(got0[k], ref["init"][k]), k
+        for k in ("x", "y", "z", "m_solid", "m_water"):
+            assert np.array_equal(got0["p_" + k], ref["init"]["p_" + k]), k
+        dts = []
+        for n in range(1, max(steps) + 1):
+            assert s.step()
+            dts.append(s.diag.dt)
+            if n in steps:
+                _compare(s.state(), ref[f"s{n}"], f"{case_name} step {n}")
+        assert np.allclose(dts, ref["trace"]["dt"][:len(dts)], rtol=1e-12, atol=0.0)
+        if case_name == "cfg2_slice":
+            assert s.lib.fs_dom_sweep_mode(s.dom) == 8
+    finally:
+        s.close()
+
+
 def test_host_stepper_state_equals_device_state():
     """api.HostStepper (the e2e path: upload, step, download, with the early
     fields downloaded on a copy stream from the DOM phase on) leaves in host

@@ -119,6 +119,29 @@ def test_dom(vectors):
         assert rel_l2(qsoil, c["q_in_soil"]) <= 1e-11, name
 
 
+def test_dom_s8_matches_reference():
+    """The oracle's DOM at S8 (80 ordinates) against the reference's own
+    DOMRadiationSolver with the S8 set injected (tests/golden/dom_s8.npz):
+    two solves in a row on every golden-vector geometry and on a slice of the
+    400 x 120 x 60 grid; same iteration counts, outputs to 1e-11."""
+    from conftest import dom_s8_cases
+    from firewebapp_b200.quadrature import level_symmetric
+    om, wq = level_symmetric(8)
+    for name, (c, calls) in dom_s8_cases().items():
+        shp = (c["nz"], c["ny"], c["nx"])
+        I = np.zeros((om.shape[0],) + shp)
+        for n, want in enumerate(calls):
+            qs, qg, qsoil, it = K.dom_solve(
+                I, om, wq, want["T_s"], want["T_g"], c["alpha_s"], c["omega_comb"],
+                c["sigma_sav"], c["T_amb"], c["dx"], c["dy"], c["dz_arr"],
+                T_soil0=c["T_soil"], Y_H2O=c.get("Y_H2O"), rho=c.get("rho"),
+                M_local=c["bed_moisture"])
+            assert it == want["iterations"], (name, n)
+            assert rel_l2(qs, want["q_rad_solid"]) <= 1e-11, (name, n)
+            assert rel_l2(qg, want["q_rad_gas"]) <= 1e-11, (name, n)
+            assert rel_l2(qsoil, want["q_in_soil"]) <= 1e-11, (name, n)
+
+
 def test_lagrangian_bed(vectors):
     for name in vectors.cases("lagrangian_bed"):
         c = vectors.case("lagrangian_bed", name)

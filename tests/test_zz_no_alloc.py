@@ -72,3 +72,18 @@ def test_noalloc_rejects_sizes_beyond_the_limit():
     assert st == 1
     msg = L.fs_last_error().decode()
     assert "static scratch limit" in msg and str(MAX_CELLS) in msg
+
+
+def test_zero_cells_is_a_no_op_for_both_entries():
+    """n == 0 returns FS_OK from both EDC entry points and touches nothing."""
+    L = _lib.lib()
+    t = torch.full((8,), 7.0, dtype=torch.float64, device="cuda")
+    p = ptr(t)
+    s = torch.cuda.current_stream().cuda_stream
+    scratch = torch.zeros(64, dtype=torch.uint8, device="cuda")
+    assert L.fs_edc(0, p, p, p, p, p, p, p, p, 0.34, 1100.0, 1e-3, 1, 1.3, 17e6, 0,
+                    ptr(scratch), s) == 0
+    assert L.fs_edc_noalloc(0, p, p, p, p, p, p, p, p, 0.34, 1100.0, 1e-3, 1, 1.3, 17e6, 0,
+                            s) == 0
+    torch.cuda.synchronize()
+    assert torch.all(t == 7.0)
