@@ -1916,7 +1916,9 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
     cudaEventCreate(&D->ev0[q]);
     cudaEventCreate(&D->ev1[q]);
   }
-  if (cudaGetLastError() != cudaSuccess) {
+  // the copies and the clearing above run on the legacy default stream; wait
+  // for them here, since the solves run on streams that do not order after it
+  if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     dom_destroy(D);
     return nullptr;
   }
@@ -2132,7 +2134,12 @@ static void alloc_st_ring(DomCtx* D) {
   cudaMalloc(&D->st_ring, D->st_ring_bytes);
 }
 
-static int dom_prepare(DomCtx* D) {
+// The first call (at the first solve or intensity access) allocates the
+// sweep's buffers and clears the y-inflow rows on the caller's stream, so the
+// clearing is ordered before that stream's first sweep (a plain cudaMemset
+// runs on the legacy default stream, which does not order work on streams
+// created non-blocking, such as torch's side streams).
+static int dom_prepare(DomCtx* D, cudaStream_t st) {
   if (D->mode != 0) return FS_OK;
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
@@ -2156,7 +2163,7 @@ static int dom_prepare(DomCtx* D) {
     cudaMalloc(&D->Goct32, sizeof(float) * 8 * D->groups * N);
     cudaMalloc(&D->Qoct32, sizeof(float) * 8 * D->groups * n2);
     cudaMalloc(&D->wrap32, sizeof(float) * D->M * g.nz * g.nx);
-    cudaMemset(D->wrap32, 0, sizeof(float) * D->M * g.nz * g.nx);
+    cudaMemsetAsync(D->wrap32, 0, sizeof(float) * D->M * g.nz * g.nx, st);
     if (D->mode == 7) alloc_st_ring(D);
     return cuda_status();
   }
@@ -2176,7 +2183,7 @@ static int dom_prepare(DomCtx* D) {
     cudaMalloc(&D->Goct, sizeof(double) * 8 * D->groups * N);
     cudaMalloc(&D->Qoct, sizeof(double) * 8 * D->groups * n2);
     cudaMalloc(&D->wrap, sizeof(double) * D->M * g.nz * g.nx);
-    cudaMemset(D->wrap, 0, sizeof(double) * D->M * g.nz * g.nx);
+    cudaMemsetAsync(D->wrap, 0, sizeof(double) * D->M * g.nz * g.nx, st);
     if (D->mode == 7) alloc_st_ring(D);
     return cuda_status();
   }
@@ -2201,7 +2208,7 @@ static int dom_prepare(DomCtx* D) {
     D->mode = (want == 3 || smem > (size_t)max_smem) ? 3 : 2;
   }
   cudaMalloc(&D->I, sizeof(double) * N * D->M);
-  cudaMemset(D->I, 0, sizeof(double) * N * D->M);
+  cudaMemsetAsync(D->I, 0, sizeof(double) * N * D->M, st);
   return cuda_status();
 }
 
@@ -2243,7 +2250,7 @@ int dom_set_precision(void* h, int fp32) {
 
 int dom_load_intensity(void* h, const double* I_full, cudaStream_t st) {
   DomCtx* D = (DomCtx*)h;
-  int rc = dom_prepare(D);
+  int rc = dom_prepare(D, st);
   if (rc != FS_OK) return rc;
   const GridDev& g = D->g;
   if (D->fp32) {
@@ -2272,7 +2279,7 @@ int64_t dom_wrap_size(void* h) {
 // reads), M x Nz x Nx, out of or into whichever storage the sweep path uses.
 int dom_get_wrap(void* h, double* dst, cudaStream_t st) {
   DomCtx* D = (DomCtx*)h;
-  int rc = dom_prepare(D);
+  int rc = dom_prepare(D, st);
   if (rc != FS_OK) return rc;
   const int64_t tot = dom_wrap_size(h);
   if (D->fp32) {
@@ -2290,7 +2297,7 @@ int dom_get_wrap(void* h, double* dst, cudaStream_t st) {
 
 int dom_set_wrap(void* h, const double* src, cudaStream_t st) {
   DomCtx* D = (DomCtx*)h;
-  int rc = dom_prepare(D);
+  int rc = dom_prepare(D, st);
   if (rc != FS_OK) return rc;
   const int64_t tot = dom_wrap_size(h);
   if (D->fp32) {
@@ -2453,7 +2460,7 @@ int dom_begin(void* h, const double* Ts, const double* Tg, const double* as, con
               double sigma, double T_amb, const double* Tsoil0, const double* YH,
               const double* rho, const double* Mloc, cudaStream_t st) {
   DomCtx* D = (DomCtx*)h;
-  int rc = dom_prepare(D);
+  int rc = dom_prepare(D, st);
   if (rc != FS_OK) return rc;
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;

@@ -687,6 +687,9 @@ void* proj_create(const GridDev& g) {
   P->ir = dalloc(n0);
   cudaMemset(P->p_prev, 0, sizeof(double) * n0);
   cudaMemset(P->scal, 0, sizeof(double) * 16);
+  // the clearing runs on the legacy default stream; solves may run on streams
+  // that do not order after it
+  cudaDeviceSynchronize();
   P->have_prev = 0;
   P->last_iters = 0;
   P->iter_exec = nullptr;

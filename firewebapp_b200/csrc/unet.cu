@@ -853,6 +853,9 @@ int unet_create(int nz, int ny, int nx, void** out) {
   cudaMemset(U->params, 0, sizeof(float) * np);
   cudaMemset(U->am, 0, sizeof(float) * np);
   cudaMemset(U->av, 0, sizeof(float) * np);
+  // the clearing runs on the legacy default stream; later work may run on
+  // streams that do not order after it
+  cudaDeviceSynchronize();
   *out = U;
   return cuda_status();
 }
