@@ -5,16 +5,15 @@ A single case's default sweep (path 8) takes 8 octant clusters of 10 CTAs, 80
 of the 148 SMs, one CTA per SM, so two cases' sweeps cannot be resident at
 once.  The other shapes trade differently: 6-CTA clusters take two clusters
 per octant (an S8 octant's intensities for 10 rows of 120 pencils do not fit
-one CTA's shared memory), 16 clusters on 96 SMs; path 4 runs 15-CTA clusters
-in two waves on 120 SMs.  Which is fastest next to the other cases' kernels
-depends on the cases, the concurrency and the form, so ``tune_batch`` times
-every candidate on the cases themselves (``batch.time_concurrent``: fresh
-solvers, warm-up steps, then timed steps of all cases at once) and keeps the
-fastest.  Results are cached in a JSON file keyed by device, form,
-concurrency and the cases' grids.  Paths 4 and 8 with one cluster per octant
-give bit-identical results; the two-cluster shape sums each octant's G in two
-halves, which changes the last bits (about 2e-15 relative in the radiative
-sources).
+one CTA's shared memory), 16 clusters on 96 SMs; 15-CTA clusters run in two
+waves on 120 SMs.  Which is fastest next to the other cases' kernels depends
+on the cases, the concurrency and the form, so ``tune_batch`` times every
+candidate on the cases themselves (``batch.time_concurrent``: fresh solvers,
+warm-up steps, then timed steps of all cases at once) and keeps the fastest.
+Results are cached in a JSON file keyed by device, form, concurrency and the
+cases' grids.  Shapes with one cluster per octant give bit-identical results;
+the two-cluster shape sums each octant's G in two halves, which changes the
+last bits (about 2e-15 relative in the radiative sources).
 """
 from __future__ import annotations
 
@@ -25,8 +24,8 @@ from pathlib import Path
 import torch
 
 # (sweep path, CTAs per octant): path 8 automatic (10 CTAs per octant on the
-# 60 x 120 cross-section), path 8 with 6-CTA clusters, path 4
-CANDIDATES = ((8, 0), (8, 6), (4, 0))
+# 60 x 120 cross-section), 6-CTA clusters (two per octant), 15-CTA clusters
+CANDIDATES = ((8, 0), (8, 6), (8, 15))
 
 
 def cache_path() -> Path:

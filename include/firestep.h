@@ -27,7 +27,7 @@ extern "C" {
 #define FS_EARG 1
 #define FS_ENONFINITE 2
 #define FS_ENOCONV 3
-#define FS_ETIMEOUT 4
+#define FS_ETIMEOUT 4 /* reserved: a bounded device wait gave up */
 #define FS_ECUDA 5
 
 /* Grid3D geometry (spread_3d.py:158-188): dz, d_above, d_below are device
@@ -349,26 +349,21 @@ int fs_dom_begin(void* handle, const double* T_s, const double* T_g, const doubl
                  const double* Y_H2O, const double* rho, const double* M_local, void* stream);
 int fs_dom_end(void* handle, double* q_rad_solid, double* q_rad_gas, double* q_in_soil,
                void* stream);
-/* Full intensity field (M x Nz x Ny x Nx) for sweep paths 2 and 3; NULL for the
+/* Full intensity field (M x Nz x Ny x Nx) for sweep path 3; NULL for the
  * default octant-cluster path, which keeps only the y-periodic inflow rows
  * (the part of I_set that a later sweep reads, dom_3d.py:147-211). */
 double* fs_dom_intensity(void* handle);
-/* Sweep path: 0 auto (path 8 when the quadrature is octant-major and eight
- * octant clusters can be resident at once, else path 4 when the grid fits,
- * else one CTA per ordinate, else one launch per hyperplane),
- * 1 octant clusters with point-to-point hand-off between CTAs,
- * 2 one CTA per ordinate, 3 hyperplane launches, 4 octant clusters with a
- * cluster barrier per hyperplane, 5 one CTA per ordinate with per-thread
- * pencils and batched loads, 6 as 4 with two clusters per octant (half the
- * ordinates each, two CTAs per SM), 7 as 4 without clusters: a cooperative
- * launch of self-timed CTAs that hand their last row on through a ring in
- * global memory (needs all 8*C CTAs resident at once, one per SM; no other
- * path-7 sweep may run on the device at the same time), 8 as 4 with clusters
- * small enough that all eight octants run at once (up to two pencils per
- * thread); cluster_ctas 0 = automatic, else CTAs per octant (1..16; up to 64
- * for path 7).  Only before
- * the first solve or intensity load.  Paths 1 and 7 bound their waits: a
- * stalled hand-off returns FS_ETIMEOUT. */
+/* Sweep path: 0 auto (path 8 when the quadrature is octant-major and a
+ * cluster shape fits the grid, else path 3), 3 one launch per hyperplane
+ * over all ordinates with the full intensity field stored (any quadrature,
+ * FP64 only), 8 octant clusters: one thread-block cluster per octant (or per
+ * half of its ordinates), the cluster's CTAs splitting the k' rows, a cluster
+ * barrier per hyperplane, one or two pencils per thread, planned so that all
+ * clusters are resident at once where the part allows it; cluster_ctas 0 =
+ * automatic, else CTAs per octant (1..16).  Only before the first solve or
+ * intensity load.  Path 8 computes the numerator with fused multiply-adds
+ * and the quotient from a Newton-Raphson reciprocal (within about one ulp),
+ * so its FP64 results differ from path 3's by rounding only. */
 int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
 /* Path 8 only: clusters per octant, 1 (all ordinates of the octant in one
  * cluster) or 2 (half each, the octant partials of G then summed per half);
@@ -376,7 +371,7 @@ int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
 int fs_dom_set_octant_groups(void* handle, int groups);
 /* The path in use (0 before the first solve or intensity load). */
 int fs_dom_sweep_mode(void* handle);
-/* fp32 = 1: the mixed-precision form of the sweep (path 4, 7 or 8 with kappa,
+/* fp32 = 1: the mixed-precision form of the sweep (path 8 with kappa,
  * kappa*B, intensities and octant partials in FP32 and the quotient of
  * __fdividef, about 2 ulp; G, the ground exchange and all outputs in FP64).
  * No counterpart in the reference, which is FP64 throughout.  Only before the

@@ -55,7 +55,7 @@ def test_autotune_picks_the_fastest_candidate_and_caches(tmp_path, monkeypatch):
     def fake(cases, steps, warmup=3, form="plain", device="cuda", solver_kw=None):
         calls.append(dict(solver_kw))
         key = (solver_kw["dom_sweep"], solver_kw["dom_cluster_ctas"])
-        if key == (4, 0):
+        if key == (8, 15):
             raise FireStepError(1, "no such sweep shape")
         return {"value": {(8, 0): 1.0e8, (8, 6): 1.5e8}[key], "wall_s": 1.0}
 
@@ -72,9 +72,9 @@ def test_autotune_picks_the_fastest_candidate_and_caches(tmp_path, monkeypatch):
 
 @pytest.mark.gpu
 def test_tuned_sweep_shapes_agree():
-    """The autotuner's candidates compute the same state: paths 8 and 4 with
-    one cluster per octant bit for bit, the two-cluster shape to round-off
-    (the workload's 60 x 120 cross-section, cut to 40 x-cells)."""
+    """The autotuner's candidates compute the same state: the shapes with one
+    cluster per octant bit for bit, the two-cluster shape to round-off (the
+    workload's 60 x 120 cross-section, cut to 40 x-cells)."""
     import numpy as np
     from firewebapp_b200.autotune import CANDIDATES
     from firewebapp_b200.cases import CFG2, scaled
@@ -90,7 +90,7 @@ def test_tuned_sweep_shapes_agree():
     a = states[(8, 0)]
     for key, st in states.items():
         for k in ("T_g", "q_rad", "u", "T_s"):
-            if key[1] == 0:
+            if key[1] != 6:
                 assert np.array_equal(st[k], a[k]), (key, k)
             else:
                 d = np.linalg.norm(st[k] - a[k]) / np.linalg.norm(a[k])
