@@ -52,6 +52,38 @@ class FsColumnDiag(C.Structure):
     _fields_ = [("n_ign", I64), ("lead_i", I), ("S_pyro_max", D), ("hrr_max", D)]
 
 
+class FsCaseDesc(C.Structure):
+    _fields_ = ([("nx", I), ("ny", I), ("nz", I), ("n_z_bed", I), ("dx", D), ("dy", D),
+                 ("dz", P), ("d_above", P), ("d_below", P)]
+                + [(n, D) for n in ("T_amb", "h_bed", "sav", "cfl", "dz_min", "U_mf", "min_dt_s",
+                                    "dt0", "ignition_duration_s", "ignition_q_mult",
+                                    "canopy_C_d", "canopy_beta_p", "canopy_beta_d", "h_conv",
+                                    "rho_solid_true", "cp_solid", "eps_solid", "view_factor",
+                                    "kappa_bed_eff", "char_ox_flux_cap", "char_ox_ash_exp",
+                                    "chi_rad", "T_ign", "proj_div_tol", "x_front0",
+                                    "bed_x_end")]
+                + [(n, I) for n in ("drying_mode", "view_factor_geometric", "n_per_cell",
+                                    "i_src_start", "i_src_end", "proj_max_iter",
+                                    "dom_subcycle_every", "edc_extinction_enable")]
+                + [("M", I), ("ox", P), ("oy", P), ("oz", P), ("w", P), ("n_soil", I),
+                   ("soil_dz", P), ("soil_d_above", P), ("soil_d_below", P), ("form", I),
+                   ("projection_rtol", D), ("proj_maxiter", I), ("overlap_dom", I)])
+
+
+class FsInitState(C.Structure):
+    _fields_ = ([(n, P) for n in ("rho", "u", "v", "w", "T_g", "Y_fuel", "Y_O2", "Y_H2O", "T_s",
+                                  "alpha_s", "k_turb", "eps_turb", "nu_t", "phi", "u_inlet",
+                                  "sigma_x", "T_soil")]
+                + [("n_particles", I64)]
+                + [(n, P) for n in ("px", "py", "pz", "m_solid", "m_water", "m_char", "pT_s",
+                                    "m_water_0", "psav", "m_char_max", "alive")])
+
+
+class FsStepOut(C.Structure):
+    _fields_ = [("steps", I), ("finished", I), ("step_count", I64), ("t", D), ("dt", D),
+                ("cg_iters", I), ("proj_iters", I), ("dom_iters", I), ("div_max", D)]
+
+
 _G = C.POINTER(FsGrid)
 
 # name -> (restype, argtypes)
@@ -79,6 +111,16 @@ SIGNATURES = {
     "fs_eos": (I, [_G, P, P, P, P, D, P]),
     "fs_clip": (I, [I64, P, D, D, P]),
     "fs_div_target": (I, [I64, P, P, P, P, D, P, P]),
+    "fs_ctx_create": (I, [C.POINTER(FsCaseDesc), C.POINTER(FsInitState), C.POINTER(P)]),
+    "fs_ctx_destroy": (None, [P]),
+    "fs_ctx_last_error": (C.c_char_p, [P]),
+    "fs_step": (I, [P, I, C.POINTER(FsStepOut)]),
+    "fs_batch_run": (I, [C.POINTER(P), I, I, C.POINTER(FsStepOut)]),
+    "fs_ctx_field_size": (I64, [P, I]),
+    "fs_ctx_field": (P, [P, I]),
+    "fs_ctx_read": (I, [P, I, P]),
+    "fs_ctx_write": (I, [P, I, P]),
+    "fs_ctx_stream": (P, [P]),
     "fs_column_diag_scratch_bytes": (I64, [_G]),
     "fs_column_diag": (I, [_G, P, P, P, P, D, D, D, P, P, C.POINTER(FsColumnDiag), P]),
     "fs_ignition_pulse": (I, [_G, P, I, I, I, D, P]),

@@ -78,6 +78,15 @@ CFG2_SLICE = dict(
     Lx=4.0, Ly=1.6, bed_x_start=1.0, bed_x_end=4.0,
 )
 
+# Variants of the 32 x 8 x 12 case that reach the loop's exit tests
+# (spread_3d.py:3413-3437): no ignition at all (the flame body stays empty),
+# and a bed that ends one cell after the ignition strip (the front is at the
+# bed's end from the start).
+EXIT_CASES = {
+    "extinct": dict(TINY, solid_phase_ignition_enable=False, ignition_duration_s=0.0),
+    "front": dict(TINY, bed_x_end=0.75),
+}
+
 CASES = {"cfg1": CFG1, "cfg2": CFG2, "tiny": TINY, "smoke": SMOKE, "cfg2_slice": CFG2_SLICE}
 
 

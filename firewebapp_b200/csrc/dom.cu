@@ -500,14 +500,14 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
     if (periodic && (d + 2) % CL_CHUNK == 0 && d + 2 < nplanes) load_inflow((d + 2) / CL_CHUNK);
     cp_async_commit();
   };
-  // Threads t < rows*MO move the y-wrap values between the staged chunks and
-  // the hyperplane buffers' first and last columns, one value each, so that no
-  // pencil carries that work: the ghost column of hyperplane dn (in the buffer
-  // that is then the previous one), and the last column of hyperplane dp.
+  // The y-wrap values move between the staged chunks and the hyperplane
+  // buffers' first and last columns, one value per thread (rows*MO values;
+  // with fewer threads than that, a thread moves several), so that no pencil
+  // carries that work: the ghost column of hyperplane dn (in the buffer that
+  // is then the previous one), and the last column of hyperplane dp.
   const int nmove = rows * MO;
   auto fill_ghost_col = [&](T* buf, int dn) {
-    const int t = threadIdx.x;
-    if (t < nmove) {
+    for (int t = threadIdx.x; t < nmove; t += TT) {
       const int m = t / rows, kl = t - m * rows;
       if (kl < nrows)
         buf[(size_t)m * P + (kl + 1) * RS] =
@@ -517,8 +517,8 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
     }
   };
   auto copy_last_col = [&](const T* buf, int dp) {
-    const int t = threadIdx.x;
-    if (periodic && t < nmove) {
+    if (!periodic) return;
+    for (int t = threadIdx.x; t < nmove; t += TT) {
       const int m = t / rows, kl = t - m * rows;
       if (kl < nrows)
         wout[((size_t)(((dp / CL_CHUNK) & 1) * MO + m) * rows + kl) * CL_CHUNK + dp % CL_CHUNK] =

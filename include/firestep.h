@@ -434,6 +434,104 @@ int fs_field_max(const FsGrid* g, const double* f, int mode, double* result, voi
 int fs_field_max_multi(const FsGrid* g, int nf, const double* const* f, const int* modes,
                        double* results, void* scratch, void* stream);
 
+/* ---- Whole steps ----------------------------------------------------------
+ * The outer loop of run_3d_spread (spread_3d.py:1897-3512) in the
+ * production configuration (Lagrangian bed, k-epsilon, EDC, DOM, passive
+ * level set, periodic y, log-law inlet), operator by operator in the
+ * reference's order, device-resident and driven from C++: the host only
+ * reads back the scalars the loop branches on (dt, the pressure-iteration
+ * test, the DOM source-iteration test, the turbulent-diffusion sub-step
+ * count, the exit tests).  The context owns every buffer (state, workspaces,
+ * the projection's and the DOM's solver objects) and frees them in
+ * fs_ctx_destroy.  One context is driven by one host thread at a time; the
+ * DOM solve runs on a second stream from a worker thread of the context.
+ * No counterpart in the reference as a C call. */
+typedef struct FsCaseDesc {
+  /* grid (Grid3D, spread_3d.py:158-188); dz, d_above, d_below: host arrays of nz */
+  int nx, ny, nz, n_z_bed;
+  double dx, dy;
+  const double *dz, *d_above, *d_below;
+  /* constants of the case (spread_3d.py:563-1500), as resolved from its deck */
+  double T_amb, h_bed, sav, cfl, dz_min, U_mf, min_dt_s, dt0;
+  double ignition_duration_s, ignition_q_mult, canopy_C_d, canopy_beta_p, canopy_beta_d;
+  double h_conv, rho_solid_true, cp_solid, eps_solid, view_factor, kappa_bed_eff;
+  double char_ox_flux_cap, char_ox_ash_exp, chi_rad, T_ign, proj_div_tol, x_front0, bed_x_end;
+  int drying_mode, view_factor_geometric, n_per_cell, i_src_start, i_src_end;
+  int proj_max_iter, dom_subcycle_every, edc_extinction_enable;
+  /* DOM quadrature: M ordinates (host arrays) */
+  int M;
+  const double *ox, *oy, *oz, *w;
+  /* soil column (soil_3d.py:73-103): host arrays of n_soil */
+  int n_soil;
+  const double *soil_dz, *soil_d_above, *soil_d_below;
+  /* solver options: form 0 plain FP64, 1 mixed (FP32 DOM sweep and V-cycle);
+   * the CG tolerance and iteration cap of each pressure solve; overlap_dom 1
+   * runs the DOM solve on a second stream concurrently with momentum, the
+   * projection and k-epsilon (results identical either way) */
+  int form;
+  double projection_rtol;
+  int proj_maxiter;
+  int overlap_dom;
+} FsCaseDesc;
+
+/* Initial state, host arrays (C-order (nz, ny, nx) unless noted). */
+typedef struct FsInitState {
+  const double *rho, *u, *v, *w, *T_g, *Y_fuel, *Y_O2, *Y_H2O, *T_s, *alpha_s, *k_turb,
+      *eps_turb, *nu_t, *phi;
+  const double* u_inlet; /* (nz, ny) */
+  const double* sigma_x; /* (nx) outflow sponge */
+  const double* T_soil;  /* (n_soil, ny, nx) */
+  int64_t n_particles;
+  const double *px, *py, *pz, *m_solid, *m_water, *m_char, *pT_s, *m_water_0, *psav,
+      *m_char_max;
+  const signed char* alive;
+} FsInitState;
+
+typedef struct FsStepOut {
+  int steps;          /* outer steps taken by this call */
+  int finished;       /* 1 once the loop's exit tests fired (spread_3d.py:3413-3437) */
+  int64_t step_count; /* steps since creation */
+  double t, dt;       /* clock after the last step and that step's dt */
+  int cg_iters;       /* CG iterations of the last step (all its pressure solves) */
+  int proj_iters;     /* pressure iterations of the last step */
+  int dom_iters;      /* DOM source iterations of the last step */
+  double div_max;     /* last max |div u - div_target| */
+} FsStepOut;
+
+/* State and work fields of a context, for fs_ctx_field / fs_ctx_read /
+ * fs_ctx_write.  Cell fields hold nx*ny*nz doubles, FS_F_T_SOIL
+ * n_soil*ny*nx, particle fields n_particles doubles (FS_P_ALIVE bytes). */
+enum {
+  FS_F_RHO = 0, FS_F_U, FS_F_V, FS_F_W, FS_F_T_G, FS_F_Y_FUEL, FS_F_Y_O2, FS_F_Y_H2O,
+  FS_F_T_S, FS_F_ALPHA_S, FS_F_K_TURB, FS_F_EPS_TURB, FS_F_NU_T, FS_F_PHI,
+  FS_F_OMEGA, FS_F_Q_RAD, FS_F_Q_RAD_GAS, FS_F_M_LOCAL, FS_F_S_PYRO, FS_F_S_DRYING,
+  FS_F_Q_G_CONV, FS_F_Q_COMB, FS_F_PRESSURE, FS_F_T_SOIL,
+  FS_P_X, FS_P_Y, FS_P_Z, FS_P_M_SOLID, FS_P_M_WATER, FS_P_M_CHAR, FS_P_T_S, FS_P_M_WATER_0,
+  FS_P_SAV, FS_P_M_CHAR_MAX, FS_P_ALIVE,
+  FS_FIELD_COUNT
+};
+
+typedef struct FsCtx FsCtx;
+int fs_ctx_create(const FsCaseDesc* desc, const FsInitState* init, FsCtx** out);
+void fs_ctx_destroy(FsCtx* ctx);
+/* the context's last error message (the thread's fs_last_error() as well) */
+const char* fs_ctx_last_error(FsCtx* ctx);
+/* n_steps outer steps, fewer if the exit tests fire; out may be NULL */
+int fs_step(FsCtx* ctx, int n_steps, FsStepOut* out);
+/* n_steps outer steps of every context, each on its own host thread and
+ * streams at the same time (cases share nothing); outs[i] (may be NULL)
+ * receives context i's summary.  Returns the first failing status. */
+int fs_batch_run(FsCtx* const* ctxs, int n, int n_steps, FsStepOut* outs);
+/* number of elements of a field (-1 for an unknown id) */
+int64_t fs_ctx_field_size(FsCtx* ctx, int id);
+/* current device buffer of a field (valid until the next fs_step) */
+void* fs_ctx_field(FsCtx* ctx, int id);
+/* copy a field to / from host memory (synchronous) */
+int fs_ctx_read(FsCtx* ctx, int id, void* host_dst);
+int fs_ctx_write(FsCtx* ctx, int id, const void* host_src);
+/* the context's main stream (every fs_step launch is ordered on it) */
+void* fs_ctx_stream(FsCtx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,3 +39,17 @@ def test_bindings_resolve():
     L = _lib.lib()
     assert L.fs_version() == 1
     assert L.fs_edc_scratch_bytes(1 << 20) > 0
+
+
+def test_ctx_create_rejects_an_invalid_case_without_a_gpu():
+    """fs_ctx_create checks the case description before touching the device:
+    a grid of zero cells is refused with FS_EARG (1) and a message."""
+    import ctypes
+    from firewebapp_b200 import _lib
+    L = _lib.lib()
+    desc = _lib.FsCaseDesc(nx=0, ny=0, nz=0)
+    init = _lib.FsInitState()
+    h = ctypes.c_void_p()
+    assert L.fs_ctx_create(ctypes.byref(desc), ctypes.byref(init), ctypes.byref(h)) == 1
+    assert h.value is None
+    assert b"invalid case description" in L.fs_last_error()
