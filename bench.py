@@ -305,6 +305,9 @@ def main():
                     help="skip the clock sampler (diagnostics only; the line then has no clocks)")
     ap.add_argument("--nx", type=int, default=None,
                     help="run the workload cut to its first NX x-cells (profiling)")
+    ap.add_argument("--mg-fine-sweeps", type=int, default=None,
+                    help="Jacobi sweeps before and after the coarse correction on the finest "
+                         "multigrid level (fs_proj_set_fine_sweeps; default: the library's)")
     ap.add_argument("--dom-sweep", type=int, default=0,
                     help="force a DOM sweep path (fs_dom_set_sweep_mode); 0 picks automatically")
     ap.add_argument("--batch", type=int, default=0,
@@ -338,7 +341,8 @@ def main():
     if args.nx:
         from firewebapp_b200.cases import scaled
         case = dict(scaled(CFG2, nx=args.nx), jitter_seed=rank)
-    solver = Tier3Solver(case, form=args.form, dom_sweep=args.dom_sweep)
+    solver = Tier3Solver(case, form=args.form, dom_sweep=args.dom_sweep,
+                         mg_fine_sweeps=args.mg_fine_sweeps)
     cells = solver.n
     M = solver.Omega.shape[0]
     clocks = ClockSampler(local) if not args.no_clocks else None

@@ -134,6 +134,7 @@ SIGNATURES = {
     "fs_proj_pressure": (P, [P]),
     "fs_proj_apply": (I, [P, P, P, P]),
     "fs_proj_configure": (I, [P, I, D]),
+    "fs_proj_set_fine_sweeps": (I, [P, I]),
     "fs_proj_set_coarse_tail": (I, [P, I]),
     "fs_proj_set_precision": (I, [P, I]),
     "fs_proj_stats": (I, [P, C.POINTER(D)]),

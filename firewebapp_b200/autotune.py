@@ -11,9 +11,9 @@ on the cases, the concurrency and the form, so ``tune_batch`` times every
 candidate on the cases themselves (``batch.time_concurrent``: fresh solvers,
 warm-up steps, then timed steps of all cases at once) and keeps the fastest.
 Results are cached in a JSON file keyed by device, form, concurrency and the
-cases' grids.  Shapes with one cluster per octant give bit-identical results;
-the two-cluster shape sums each octant's G in two halves, which changes the
-last bits (about 2e-15 relative in the radiative sources).
+cases' grids.  The shapes agree to rounding (about 1e-15 relative in the
+radiative sources; the two-cluster shape also sums each octant's G in two
+halves).
 """
 from __future__ import annotations
 

@@ -536,6 +536,11 @@ int fs_proj_configure(void* handle, int nu, double omega) {
   if (!handle) return FS_EARG;
   return check(proj_configure(handle, nu, omega), "fs_proj_configure");
 }
+int fs_proj_set_fine_sweeps(void* handle, int nu0) {
+  if (!handle) return check(FS_EARG, "fs_proj_set_fine_sweeps");
+  return check(proj_set_fine_sweeps(handle, nu0), "fs_proj_set_fine_sweeps");
+}
+
 int fs_proj_set_coarse_tail(void* handle, int on) {
   if (!handle) return check(FS_EARG, "fs_proj_set_coarse_tail");
   return check(proj_set_coarse_tail(handle, on), "fs_proj_set_coarse_tail");

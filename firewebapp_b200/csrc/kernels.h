@@ -90,6 +90,7 @@ int proj_project(void* h, double* u, double* v, double* w, const double* u_in,
 int proj_apply(void* h, const double* x, double* y, cudaStream_t st);
 int proj_configure(void* h, int nu, double omega);
 int proj_set_coarse_tail(void* h, int on);
+int proj_set_fine_sweeps(void* h, int nu0);
 int proj_set_precision(void* h, int fp32);
 void proj_stats(void* h, double* out8);
 // learned preconditioner (flexible CG); net = NULL returns to the V-cycle

@@ -32,7 +32,9 @@
 #define MG_OMEGA_DEFAULT 0.9  // damping of the V-cycle's smoothing sweeps
 #define MG_NU_DEFAULT 4
 #define MG_COARSE_MAX 48
-#define RED_BLOCKS 296
+// blocks of the reducing CG kernels (8 per SM of the 148: enough loads in
+// flight to stream HBM); their partials are added in block order
+#define RED_BLOCKS 1184
 #define RED_THREADS 256
 // Device scalar slots: 0 rz, 1 pq, 2 rz_new, 4 ||b_A||^2, 5 ||r_A||^2,
 // 6 (rtol ||b_A||)^2, 7 converged flag, 8 iterations done.
@@ -74,6 +76,7 @@ struct ProjCtx {
   int iter_kernels;   // kernels in that graph
   int graph_failed;
   int nu;             // Jacobi sweeps before and after the coarse correction
+  int nu0;            // the same on the finest level (0: nu)
   double omega;       // Jacobi damping
   int tail_on;        // coarse levels in one launch (k_mg_vcycle_tail)
   // mixed-precision form: the V-cycle in FP32 (levels, coarse inverse, the
@@ -696,6 +699,7 @@ void* proj_create(const GridDev& g) {
   P->iter_kernels = 0;
   P->graph_failed = 0;
   P->nu = MG_NU_DEFAULT;
+  P->nu0 = 0;
   P->tail_on = 1;
   P->fp32 = 0;
   P->Ainv32 = nullptr; P->r32 = nullptr; P->z32 = nullptr;
@@ -1040,7 +1044,7 @@ static int vcycle(ProjCtx* P, MGLevelT<T>* lev, const T* Ainv, int l, const T* b
   }
   MGLevelT<T>& cl = lev[l + 1];
   unsigned nb = blocks_for(f.n, 256);
-  const int nu = P->nu;
+  const int nu = (l == 0 && P->nu0 > 0) ? P->nu0 : P->nu;
   const double om = P->omega;
   // pre-smoothing from x = 0, ending in t:  sweep i writes t when (nu-1-i) is even, else s
   const T* src = nullptr;
@@ -1081,6 +1085,18 @@ int proj_configure(void* h, int nu, double omega) {
   if (nu != P->nu || omega != P->omega) {
     P->nu = nu;
     P->omega = omega;
+    if (P->iter_exec) cudaGraphExecDestroy(P->iter_exec);
+    P->iter_exec = nullptr;
+    P->graph_failed = 0;
+  }
+  return FS_OK;
+}
+
+int proj_set_fine_sweeps(void* h, int nu0) {
+  ProjCtx* P = (ProjCtx*)h;
+  if (nu0 < 0 || nu0 > 16) return FS_EARG;
+  if (nu0 != P->nu0) {
+    P->nu0 = nu0;
     if (P->iter_exec) cudaGraphExecDestroy(P->iter_exec);
     P->iter_exec = nullptr;
     P->graph_failed = 0;

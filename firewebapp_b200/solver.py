@@ -103,7 +103,8 @@ class Tier3Solver:
     def __init__(self, case: dict, device="cuda", projection_cg_rtol: float | None = None,
                  proj_maxiter: int = 200, mg_sweeps: int | None = None, form: str = "plain",
                  overlap_dom: bool = True, dom_sweep: int = 0, learned_weights=None,
-                 learned_max: int = 30, learned_stall: float = 0.9, dom_cluster_ctas: int = 0):
+                 learned_max: int = 30, learned_stall: float = 0.9, dom_cluster_ctas: int = 0,
+                 mg_fine_sweeps: int | None = None):
         self.lib = _lib.lib()
         self.dev = torch.device(device)
         if self.dev.type == "cuda" and self.dev.index is None:
@@ -179,6 +180,9 @@ class Tier3Solver:
         self.proj = h
         if mg_sweeps is not None:
             check(self.lib.fs_proj_configure(self.proj, int(mg_sweeps), 0.8), "fs_proj_configure")
+        if mg_fine_sweeps is not None:
+            check(self.lib.fs_proj_set_fine_sweeps(self.proj, int(mg_fine_sweeps)),
+                  "fs_proj_set_fine_sweeps")
         if fp32:
             check(self.lib.fs_proj_set_precision(self.proj, 1), "fs_proj_set_precision")
         self.net = None

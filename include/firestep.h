@@ -253,6 +253,9 @@ int fs_proj_apply(void* handle, const double* x, double* y, void* stream);
  * preconditioner (projection_3d.py:236-246, an FFT solve) has no such knob;
  * only the converged solution is shared. */
 int fs_proj_configure(void* handle, int nu, double omega);
+/* Jacobi sweeps before and after the coarse correction on the finest level
+ * only (nu0 = 0: the same as the coarser levels, fs_proj_configure's nu). */
+int fs_proj_set_fine_sweeps(void* handle, int nu0);
 /* on = 1 (default): the coarse end of the V-cycle (the levels whose operators
  * and vectors fit in one CTA's shared memory) runs in one single-CTA launch;
  * 0: one launch per sweep.  The correction, and so the solve, is

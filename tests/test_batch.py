@@ -72,8 +72,7 @@ def test_autotune_picks_the_fastest_candidate_and_caches(tmp_path, monkeypatch):
 
 @pytest.mark.gpu
 def test_tuned_sweep_shapes_agree():
-    """The autotuner's candidates compute the same state: the shapes with one
-    cluster per octant bit for bit, the two-cluster shape to round-off (the
+    """The autotuner's candidates compute the same state to round-off (the
     workload's 60 x 120 cross-section, cut to 40 x-cells)."""
     import numpy as np
     from firewebapp_b200.autotune import CANDIDATES
@@ -90,8 +89,5 @@ def test_tuned_sweep_shapes_agree():
     a = states[(8, 0)]
     for key, st in states.items():
         for k in ("T_g", "q_rad", "u", "T_s"):
-            if key[1] != 6:
-                assert np.array_equal(st[k], a[k]), (key, k)
-            else:
-                d = np.linalg.norm(st[k] - a[k]) / np.linalg.norm(a[k])
-                assert d <= 1e-12, (key, k, d)
+            d = np.linalg.norm(st[k] - a[k]) / np.linalg.norm(a[k])
+            assert d <= 1e-12, (key, k, d)
