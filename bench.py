@@ -308,9 +308,6 @@ def main():
     ap.add_argument("--mg-fine-sweeps", type=int, default=None,
                     help="Jacobi sweeps before and after the coarse correction on the finest "
                          "multigrid level (fs_proj_set_fine_sweeps; default: the library's)")
-    ap.add_argument("--dom-shape", default=None,
-                    help="path-8 sweep shape 'groups,ctas,ppt,ctas_per_sm' (0 = automatic; "
-                         "fs_dom_set_octant_groups, fs_dom_set_sweep_mode, fs_dom_set_packing)")
     ap.add_argument("--dom-sweep", type=int, default=0,
                     help="force a DOM sweep path (fs_dom_set_sweep_mode); 0 picks automatically")
     ap.add_argument("--batch", type=int, default=0,
@@ -344,12 +341,8 @@ def main():
     if args.nx:
         from firewebapp_b200.cases import scaled
         case = dict(scaled(CFG2, nx=args.nx), jitter_seed=rank)
-    shape = {}
-    if args.dom_shape:
-        grp, ctas, ppt, per_sm = (int(v) for v in args.dom_shape.split(","))
-        shape = dict(dom_groups=grp, dom_cluster_ctas=ctas, dom_packing=(ppt, per_sm))
     solver = Tier3Solver(case, form=args.form, dom_sweep=args.dom_sweep,
-                         mg_fine_sweeps=args.mg_fine_sweeps, **shape)
+                         mg_fine_sweeps=args.mg_fine_sweeps)
     cells = solver.n
     M = solver.Omega.shape[0]
     clocks = ClockSampler(local) if not args.no_clocks else None

@@ -165,7 +165,6 @@ SIGNATURES = {
     "fs_dom_set_sweep_mode": (I, [P, I, I]),
     "fs_dom_sweep_mode": (I, [P]),
     "fs_dom_set_octant_groups": (I, [P, I]),
-    "fs_dom_set_packing": (I, [P, I, I]),
     "fs_dom_set_precision": (I, [P, I]),
     "fs_dom_load_intensity": (I, [P, P, P]),
     "fs_dom_wrap_size": (I64, [P]),

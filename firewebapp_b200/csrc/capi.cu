@@ -617,10 +617,6 @@ int fs_dom_set_octant_groups(void* handle, int groups) {
   if (!handle) return check(FS_EARG, "fs_dom_set_octant_groups");
   return check(dom_set_groups(handle, groups), "fs_dom_set_octant_groups");
 }
-int fs_dom_set_packing(void* handle, int ppt, int ctas_per_sm) {
-  if (!handle) return check(FS_EARG, "fs_dom_set_packing");
-  return check(dom_set_packing(handle, ppt, ctas_per_sm), "fs_dom_set_packing");
-}
 int fs_dom_sweep_mode(void* handle) { return handle ? dom_mode(handle) : -1; }
 
 int fs_dom_set_precision(void* handle, int fp32) {

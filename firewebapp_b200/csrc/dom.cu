@@ -48,8 +48,6 @@ struct DomCtx {
   int mode_req, force_C;      // requested path (0 auto) and cluster size (0 auto)
   int groups;                 // ordinate groups per octant (clusters per octant)
   int force_groups;           // requested groups (0 automatic)
-  int force_ppt;              // requested pencils per thread (0 automatic)
-  int ctas_per_sm;            // path 8 CTAs sharing an SM (1 default, or 2)
   int fp32;                   // single-precision sweep (path 8)
   // path 8 buffers (FP64 or FP32, by fp32): (kappa, kappa*B) per cell, octant
   // partial G (8*groups x N), octant partial ground flux (8*groups x Ny*Nx),
@@ -757,7 +755,6 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   cudaMemcpy(D->w, w, sizeof(double) * M, cudaMemcpyHostToDevice);
   D->I = nullptr; D->kb = nullptr; D->Goct = nullptr; D->Qoct = nullptr; D->wrap = nullptr;
   D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1; D->force_groups = 0;
-  D->force_ppt = 0; D->ctas_per_sm = 1;
   D->fp32 = 0; D->cl_ppt = 1; D->cl_waves = 0; D->begun = 0; D->pend_I_amb = 0.0;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemset(D->G, 0, sizeof(double) * N);
@@ -853,8 +850,7 @@ static bool plan_cl(DomCtx* D, int force_C) {
       const int rows = (g.nz + C - 1) / C;
       if ((g.nz + rows - 1) / rows != C) continue;
       const int pencils = rows * g.ny;
-      int ppt = pencils <= CL_MAX_THREADS_1 ? 1 : (pencils <= 2 * CL_MAX_THREADS_2 ? 2 : 0);
-      if (D->force_ppt == 2 && ppt == 1 && pencils <= 2 * CL_MAX_THREADS_2) ppt = 2;
+      const int ppt = pencils <= CL_MAX_THREADS_1 ? 1 : (pencils <= 2 * CL_MAX_THREADS_2 ? 2 : 0);
       if (ppt == 0) continue;
       const int threads = ((pencils + ppt - 1) / ppt + 31) / 32 * 32;
       const void* fn = octant_cl_ptr(D->fp32 != 0, Mo, ppt);
@@ -862,9 +858,7 @@ static bool plan_cl(DomCtx* D, int force_C) {
       cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
       const size_t need = cl_layout(tsize, Mo, rows, g.ny, g.nz).total;
-      // one CTA per SM unless two are asked for (then each may take up to
-      // half of the SM's shared memory)
-      const size_t pad = D->ctas_per_sm == 2 ? 0 : (size_t)smem_sm / 2 + 1024;
+      const size_t pad = (size_t)smem_sm / 2 + 1024;  // no two CTAs on one SM
       const size_t smem = need > pad ? need : pad;
       if (smem > (size_t)optin) continue;
       cudaLaunchConfig_t cfg = {};
@@ -956,18 +950,6 @@ int dom_set_groups(void* h, int groups) {
     return FS_EARG;
   }
   D->force_groups = groups;
-  return FS_OK;
-}
-
-int dom_set_packing(void* h, int ppt, int ctas_per_sm) {
-  DomCtx* D = (DomCtx*)h;
-  if (ppt < 0 || ppt > 2 || ctas_per_sm < 1 || ctas_per_sm > 2) return FS_EARG;
-  if (D->mode != 0) {
-    fs_set_error("packing must be set before the first solve or intensity load");
-    return FS_EARG;
-  }
-  D->force_ppt = ppt;
-  D->ctas_per_sm = ctas_per_sm;
   return FS_OK;
 }
 

@@ -133,7 +133,6 @@ int dom_begin(void* h, const double* Ts, const double* Tg, const double* as, con
               const double* rho, const double* Mloc, cudaStream_t st);
 int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStream_t st);
 int dom_set_groups(void* h, int groups);
-int dom_set_packing(void* h, int ppt, int ctas_per_sm);
 int dom_mode(void* h);
 int dom_set_precision(void* h, int fp32);
 int dom_load_intensity(void* h, const double* I_full, cudaStream_t st);

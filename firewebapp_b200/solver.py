@@ -104,8 +104,7 @@ class Tier3Solver:
                  proj_maxiter: int = 200, mg_sweeps: int | None = None, form: str = "plain",
                  overlap_dom: bool = True, dom_sweep: int = 0, learned_weights=None,
                  learned_max: int = 30, learned_stall: float = 0.9, dom_cluster_ctas: int = 0,
-                 mg_fine_sweeps: int | None = None, dom_groups: int = 0,
-                 dom_packing: tuple | None = None):
+                 mg_fine_sweeps: int | None = None):
         self.lib = _lib.lib()
         self.dev = torch.device(device)
         if self.dev.type == "cuda" and self.dev.index is None:
@@ -218,12 +217,6 @@ class Tier3Solver:
             self._pool = ThreadPoolExecutor(max_workers=1, thread_name_prefix="dom")
         if fp32:
             check(self.lib.fs_dom_set_precision(self.dom, 1), "fs_dom_set_precision")
-        if dom_groups:
-            check(self.lib.fs_dom_set_octant_groups(self.dom, int(dom_groups)),
-                  "fs_dom_set_octant_groups")
-        if dom_packing:
-            check(self.lib.fs_dom_set_packing(self.dom, int(dom_packing[0]), int(dom_packing[1])),
-                  "fs_dom_set_packing")
         if dom_sweep or dom_cluster_ctas:
             check(self.lib.fs_dom_set_sweep_mode(self.dom, int(dom_sweep or 8),
                                                  int(dom_cluster_ctas)),

@@ -372,12 +372,6 @@ int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
  * cluster) or 2 (half each, the octant partials of G then summed per half);
  * 0 (default) plans it.  Only before the first solve or intensity load. */
 int fs_dom_set_octant_groups(void* handle, int groups);
-/* Path 8 only: pencils per thread (0 automatic: one while a CTA's pencils fit
- * its threads, else two; 2 forces two) and CTAs per SM (1, the default, pads
- * each CTA's shared memory so that no two share an SM; 2 lets two CTAs of
- * different clusters share one, so that one computes while the other waits at
- * its cluster barrier).  Only before the first solve or intensity load. */
-int fs_dom_set_packing(void* handle, int ppt, int ctas_per_sm);
 /* The path in use (0 before the first solve or intensity load). */
 int fs_dom_sweep_mode(void* handle);
 /* fp32 = 1: the mixed-precision form of the sweep (path 8 with kappa,
