@@ -121,6 +121,8 @@ SIGNATURES = {
     "fs_ctx_read": (I, [P, I, P]),
     "fs_ctx_write": (I, [P, I, P]),
     "fs_ctx_stream": (P, [P]),
+    "fs_stencil_status": (I, [I]),
+    "fs_set_tma": (I, [I]),
     "fs_column_diag_scratch_bytes": (I64, [_G]),
     "fs_column_diag": (I, [_G, P, P, P, P, D, D, D, P, P, C.POINTER(FsColumnDiag), P]),
     "fs_ignition_pulse": (I, [_G, P, I, I, I, D, P]),

@@ -368,6 +368,13 @@ int fs_ignition_pulse(const FsGrid* g, double* q_rad, int k, int i0, int i1, dou
                "fs_ignition_pulse");
 }
 
+int fs_stencil_status(int clear) { return stencil_status(clear); }
+
+int fs_set_tma(int on) {
+  set_tma(on);
+  return FS_OK;
+}
+
 int64_t fs_column_diag_scratch_bytes(const FsGrid* g) {
   GridDev gd;
   if (!to_grid(g, gd, "fs_column_diag_scratch_bytes")) return -1;

@@ -171,3 +171,7 @@ int launch_coldiag(const GridDev& g, const double* Ts, const double* om, const d
                    const double* Sd, double T_ign, double T_front, double scale, double* hrr_x,
                    void* scratch, cudaStream_t st);
 int launch_coldiag_keys(const void* scratch, double* out4, cudaStream_t st);
+// stencil kernels with TMA-staged inputs: the bounded-wait failure flag
+// (read, optionally cleared; -1 on a CUDA error) and the on/off switch
+int stencil_status(int clear);
+void set_tma(int on);

@@ -826,6 +826,12 @@ static int one_step(FsCtx* C, int* alive) {
           cudaSuccess)
     return ctx_fail(C, FS_ECUDA, "exit readback");
   CK(fs_stream_wait(s), "exit readback");
+  if (fs_stencil_status(1) != 0) {
+    snprintf(C->err, sizeof(C->err),
+             "a stencil kernel's bounded shared-memory staging wait gave up");
+    fs_set_error("%s", C->err);
+    return FS_ETIMEOUT;
+  }
   const unsigned long long n_active = *C->h_count;
   const double front_lset = front_from_row(C->h_rows, c.nx, c.dx);
   bool exit_now = false;

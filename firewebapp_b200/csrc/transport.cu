@@ -4,8 +4,10 @@
 // the reference function and lines.  All kernels are out-of-place (read the
 // old field, write a new one), which is what the reference's double buffers
 // (dY, du/dv/dw, k_turb_new, T_s_new) amount to.
+#include <mutex>
 #include "common.cuh"
 #include "kernels.h"
+#include "tma.cuh"
 
 // ---------------------------------------------------------------------------
 // Species transport, up to 3 species in one pass
@@ -152,6 +154,11 @@ int launch_species(const GridDev& g, int nspec, const double* const* Y, double* 
 // (k_species_sources), the transport of fuel, O2 and H2O, and the O2 clip
 // that follows it (spread_3d.py:2996-3004, 3015-3038, 3059); the results equal
 // those three launches'.
+struct SpeciesArgs;
+static bool launch_species_step_tma(const GridDev& g, const SpeciesArgs& a, const double* rho,
+                                    const double* u, const double* v, const double* w, double dt,
+                                    double D, cudaStream_t st);
+
 int launch_species_step(const GridDev& g, const double* const* Y, double* const* Yo,
                         const double* Sp, const double* Sd, const double* Y_inlet,
                         const double* rho, const double* u, const double* v, const double* w,
@@ -164,6 +171,7 @@ int launch_species_step(const GridDev& g, const double* const* Y, double* const*
   a.Sp = Sp;
   a.Sd = Sd;
   a.o2_cap = o2_cap;
+  if (launch_species_step_tma(g, a, rho, u, v, w, dt, D, st)) return cuda_status();
   double inv_dx = 1.0 / g.dx, inv_dy = 1.0 / g.dy;
   const dim3 nb((g.nx + SP_TX - 1) / SP_TX, (g.ny + SP_TY - 1) / SP_TY, g.nz);
   const dim3 tb(SP_TX, SP_TY);
@@ -172,6 +180,257 @@ int launch_species_step(const GridDev& g, const double* const* Y, double* const*
   fs_count_launch();
   return cuda_status();
 }
+
+// ---------------------------------------------------------------------------
+// The fused species step with its stencil inputs staged by TMA.
+//
+// A block owns a 32 (x) by 8 (y) tile and marches up a chunk of z-levels.
+// Each z-plane of the three mass fractions arrives as one TMA box of
+// 36 x 12 doubles (the tile with the two-cell x and y halos the MUSCL faces
+// read) in a ring of six shared-memory slots: the five planes k-2..k+2 the
+// stencil reads and one in flight, so every value is fetched from L2/HBM once
+// per block instead of once per neighbour.  Tiles whose halo crosses the
+// periodic y boundary have those rows replaced by the wrapped rows after the
+// box lands (TMA fills rows outside the tensor with zeros).  Cell-centred
+// inputs (u, v, w, rho, the bed sources) are read directly.  The arithmetic
+// is k_species<3, true>'s, expression for expression (same results).
+// ---------------------------------------------------------------------------
+#define TS_HX (SP_TX + 4)
+#define TS_HY (SP_TY + 4)
+#define TS_PLANE (TS_HX * TS_HY)
+#define TS_SLOTS 6
+#define TS_MAXKZ 64
+
+struct SpeciesMaps {
+  CUtensorMap Y[3];
+};
+
+__device__ int g_stencil_err;  // set when a bounded TMA wait gave up
+
+__host__ __device__ inline size_t species_tma_smem() {
+  return (size_t)TS_SLOTS * 3 * TS_PLANE * sizeof(double) + TS_SLOTS * sizeof(uint64_t) +
+         4 * TS_MAXKZ * sizeof(double);
+}
+
+__global__ void __launch_bounds__(SP_TX * SP_TY, 3)
+k_species_tma(GridDev g, SpeciesArgs a, const __grid_constant__ SpeciesMaps tm,
+              const double* __restrict__ rho, const double* __restrict__ u,
+              const double* __restrict__ v, const double* __restrict__ w, double dt, double D,
+              double inv_dx, double inv_dy, double inv_dx2, double inv_dy2, int kz) {
+  extern __shared__ __align__(128) unsigned char ts_raw[];
+  double* ring = (double*)ts_raw;
+  uint64_t* bars = (uint64_t*)(ts_raw + (size_t)TS_SLOTS * 3 * TS_PLANE * sizeof(double));
+  double* rkz = (double*)(bars + TS_SLOTS);  // per level: 1/da, 1/db, 1/dz, 1/hz
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int64_t sy = nx, sz = (int64_t)nx * ny;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SP_TX + tx;
+  const int i0 = blockIdx.x * SP_TX, j0 = blockIdx.y * SP_TY;
+  const int k0 = blockIdx.z * kz;
+  const int k1 = min(nz, k0 + kz);
+  const int pfirst = k0 - 2, plast = k1 + 1;  // planes the chunk's stencil reads
+  const bool ywrap = (j0 - 2 < 0) || (j0 + SP_TY + 2 > ny);
+  if (tid == 0) {
+    for (int q = 0; q < TS_SLOTS; ++q) tma_mbar_init(&bars[q], 1);
+    tma_fence_init();
+  }
+  for (int q = tid; q < k1 - k0; q += SP_TX * SP_TY) {
+    const int k = k0 + q;
+    const double da = g.da[k], db = g.db[k];
+    rkz[4 * q + 0] = 1.0 / da;
+    rkz[4 * q + 1] = 1.0 / db;
+    rkz[4 * q + 2] = 1.0 / g.dz[k];
+    rkz[4 * q + 3] = 1.0 / (0.5 * (da + db));
+  }
+  __syncthreads();
+  auto slot_of = [&](int p) { return (p - pfirst) % TS_SLOTS; };
+  auto issue = [&](int p) {
+    const int sl = slot_of(p);
+    tma_arrive_expect(&bars[sl], 3 * TS_PLANE * sizeof(double));
+#pragma unroll
+    for (int s = 0; s < 3; ++s)
+      tma_load_3d(ring + ((size_t)sl * 3 + s) * TS_PLANE, &tm.Y[s], i0 - 2, j0 - 2, p, &bars[sl]);
+  };
+  if (tid == 0) {
+    tma_fence_proxy();
+    for (int p = pfirst; p <= min(pfirst + TS_SLOTS - 1, plast); ++p) issue(p);
+  }
+  const int i = i0 + tx, j = j0 + ty;
+  const bool inside = i < nx && j < ny;
+  const int ii = tx + 2, jj = ty + 2;
+  const int cix = jj * TS_HX + ii;
+  int waited = pfirst - 1;  // planes up to here have landed (and been patched)
+  for (int k = k0; k < k1; ++k) {
+    // the planes this level reads that have not been waited for yet
+    const int need = min(k + 2, plast);
+    for (int p = waited + 1; p <= need; ++p) {
+      const int sl = slot_of(p);
+      tma_wait(&bars[sl], (uint32_t)(((p - pfirst) / TS_SLOTS) & 1), &g_stencil_err);
+      if (ywrap && p >= 0 && p < nz) {
+        // rows of the box outside [0, ny) hold zeros: put the periodic rows there
+        for (int e = tid; e < 3 * TS_PLANE; e += SP_TX * SP_TY) {
+          const int s = e / TS_PLANE, r = (e % TS_PLANE) / TS_HX, col = e % TS_HX;
+          const int jg = j0 - 2 + r, ig = i0 - 2 + col;
+          if ((jg < 0 || jg >= ny) && ig >= 0 && ig < nx) {
+            const double* Ys = s == 0 ? a.Y[0] : (s == 1 ? a.Y[1] : a.Y[2]);
+            ring[((size_t)sl * 3 + s) * TS_PLANE + r * TS_HX + col] =
+                Ys[(int64_t)p * sz + (int64_t)wrapj(jg, ny) * sy + ig];
+          }
+        }
+      }
+    }
+    if (ywrap && need > waited) __syncthreads();
+    waited = need > waited ? need : waited;
+    if (inside) {
+      const double* const pl0 = ring + (size_t)slot_of(k) * 3 * TS_PLANE;
+      const double* const plm1 = ring + (size_t)slot_of(k - 1) * 3 * TS_PLANE;
+      const double* const plp1 = ring + (size_t)slot_of(k + 1) * 3 * TS_PLANE;
+      const double* const plm2 = ring + (size_t)slot_of(k - 2) * 3 * TS_PLANE;
+      const double* const plp2 = ring + (size_t)slot_of(k + 2) * 3 * TS_PLANE;
+      const int64_t c = (int64_t)k * sz + (int64_t)j * sy + i;
+      const double ui = u[c], vi = v[c], wi = w[c];
+      const double inv_rho = 1.0 / rho[c];
+      const double* rk = rkz + 4 * (k - k0);
+      const double inv_d_above = rk[0], inv_d_below = rk[1], inv_dz_k = rk[2], inv_hz = rk[3];
+      const double sp = a.Sp[c], sd = a.Sd[c];
+      const double stot = sp + sd;
+      const bool mx = (i >= 2 && i <= nx - 3);
+      const bool mz = (k >= 2 && k <= nz - 3);
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const double* P0 = pl0 + s * TS_PLANE;
+        const double Yi = P0[cix];
+        const double Yxm1 = P0[cix - 1], Yxp1 = P0[cix + 1];
+        const double YL_x = (i == 0) ? a.Y_inlet[s] : Yxm1;
+        const double YR_x = (i == nx - 1) ? Yi : Yxp1;
+        const double Yzm1 = plm1[s * TS_PLANE + cix], Yzp1 = plp1[s * TS_PLANE + cix];
+        const double YL_z = (k == 0) ? Yi : Yzm1;
+        const double YR_z = (k == nz - 1) ? Yi : Yzp1;
+        double flux_x, flux_z;
+        if (mx) {
+          double fxp = muscl_face(Yxm1, Yi, Yxp1, P0[cix + 2], ui);
+          double fxm = muscl_face(P0[cix - 2], Yxm1, Yi, Yxp1, ui);
+          flux_x = ui * (fxp - fxm) * inv_dx;
+        } else {
+          flux_x = (ui >= 0.0) ? ui * (Yi - YL_x) * inv_dx : ui * (YR_x - Yi) * inv_dx;
+        }
+        const double Yjm2 = P0[cix - 2 * TS_HX], Yjm1 = P0[cix - TS_HX];
+        const double Yjp1 = P0[cix + TS_HX], Yjp2 = P0[cix + 2 * TS_HX];
+        double fyp = muscl_face(Yjm1, Yi, Yjp1, Yjp2, vi);
+        double fym = muscl_face(Yjm2, Yjm1, Yi, Yjp1, vi);
+        double flux_y = vi * (fyp - fym) * inv_dy;
+        if (mz) {
+          double fzp = muscl_face(Yzm1, Yi, Yzp1, plp2[s * TS_PLANE + cix], wi);
+          double fzm = muscl_face(plm2[s * TS_PLANE + cix], Yzm1, Yi, Yzp1, wi);
+          flux_z = wi * (fzp - fzm) * inv_hz;
+        } else {
+          flux_z = (wi >= 0.0) ? wi * (Yi - YL_z) * inv_d_below : wi * (YR_z - Yi) * inv_d_above;
+        }
+        double adv = -(flux_x + flux_y + flux_z);
+        double d2x = (YR_x - 2.0 * Yi + YL_x) * inv_dx2;
+        double d2y = (Yjp1 - 2.0 * Yi + Yjm1) * inv_dy2;
+        double d2z = ((YR_z - Yi) * inv_d_above - (Yi - YL_z) * inv_d_below) * inv_dz_k;
+        double diff = D * (d2x + d2y + d2z);
+        double S = (s == 0) ? sp - Yi * stot : ((s == 1) ? -(Yi * stot) : sd - Yi * stot);
+        double src = S * inv_rho;
+        double dY = (adv + diff + src) * dt;
+        double nw = Yi + dY;
+        if (nw < 0.0) nw = 0.0;
+        else if (nw > 1.0) nw = 1.0;
+        if (s == 1) {
+          if (nw > a.o2_cap) nw = a.o2_cap;
+          if (nw < 0.0) nw = 0.0;
+        }
+        a.Yo[s][c] = nw;
+      }
+    }
+    // every thread is done with plane k-2's slot: plane k+4 may land there
+    if (ywrap) tma_fence_proxy();
+    __syncthreads();
+    if (tid == 0 && k + 4 <= plast && k + 4 > pfirst + TS_SLOTS - 1) {
+      tma_fence_proxy();
+      issue(k + 4);
+    }
+  }
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static std::once_flag g_encode_once;
+static bool g_tma_on = true;
+
+bool tma_enabled() { return g_tma_on; }
+
+bool tma_map_field(CUtensorMap* map, const double* base, int nx, int ny, int nz, int bx, int by) {
+  std::call_once(g_encode_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    else
+      cudaGetLastError();
+  });
+  if (!g_encode || !base || (nx & 1) || ((uintptr_t)base & 15) || bx > 256 || by > 256 ||
+      (bx * (int)sizeof(double)) % 16)
+    return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * sizeof(double),
+                                 (cuuint64_t)nx * ny * sizeof(double)};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the TMA form of the fused species step; false when it cannot run here
+static bool launch_species_step_tma(const GridDev& g, const SpeciesArgs& a, const double* rho,
+                                    const double* u, const double* v, const double* w, double dt,
+                                    double D, cudaStream_t st) {
+  if (!tma_enabled()) return false;
+  SpeciesMaps tm;
+  for (int s = 0; s < 3; ++s)
+    if (!tma_map_field(&tm.Y[s], a.Y[s], g.nx, g.ny, g.nz, TS_HX, TS_HY)) return false;
+  const int tiles = ((g.nx + SP_TX - 1) / SP_TX) * ((g.ny + SP_TY - 1) / SP_TY);
+  // enough blocks for about six per SM of the 148, in z-chunks of at most
+  // TS_MAXKZ levels
+  int chunks = (6 * 148 + tiles - 1) / tiles;
+  if (chunks > g.nz) chunks = g.nz;
+  if (chunks < 1) chunks = 1;
+  int kz = (g.nz + chunks - 1) / chunks;
+  if (kz > TS_MAXKZ) kz = TS_MAXKZ;
+  chunks = (g.nz + kz - 1) / kz;
+  static bool attr = false;
+  const size_t smem = species_tma_smem();
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_species_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    attr = true;
+  }
+  const dim3 nb((g.nx + SP_TX - 1) / SP_TX, (g.ny + SP_TY - 1) / SP_TY, chunks);
+  const dim3 tb(SP_TX, SP_TY);
+  const double inv_dx = 1.0 / g.dx, inv_dy = 1.0 / g.dy;
+  k_species_tma<<<nb, tb, smem, st>>>(g, a, tm, rho, u, v, w, dt, D, inv_dx, inv_dy,
+                                      inv_dx * inv_dx, inv_dy * inv_dy, kz);
+  fs_count_launch();
+  return true;
+}
+
+int stencil_status(int clear) {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_stencil_err, sizeof(int)) != cudaSuccess) return -1;
+  if (clear && v) {
+    const int z = 0;
+    cudaMemcpyToSymbol(g_stencil_err, &z, sizeof(int));
+  }
+  return v;
+}
+
+void set_tma(int on) { g_tma_on = on != 0; }
 
 // ---------------------------------------------------------------------------
 // Species source terms with dilution (spread_3d.py:2996-3004, Lagrangian branch)

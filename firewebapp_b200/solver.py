@@ -562,6 +562,9 @@ class Tier3Solver:
         self.h_rows[0].copy_(f["phi"][1, g.Ny // 2, :], non_blocking=True)
         self.h_rows[1].copy_(f["phi"][g.n_z_bed // 2, g.Ny // 2, :], non_blocking=True)
         stream.synchronize()
+        if self.lib.fs_stencil_status(1) != 0:
+            raise _lib.FireStepError(4, "a stencil kernel's bounded shared-memory staging wait "
+                                        "gave up (or the flag could not be read)")
         n_active = int(self.h_count[0])
         front_lset = self._front_from_row(self.h_rows[0].numpy())
         exit_now = False

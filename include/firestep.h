@@ -193,6 +193,17 @@ int fs_div_target(int64_t n, const double* rho, const double* rho_prev, const do
 int fs_ignition_pulse(const FsGrid* g, double* q_rad, int k, int i0, int i1, double q_add,
                       void* stream);
 
+/* The stencil kernels whose inputs are staged in shared memory by the
+ * tensor memory accelerator (the fused species step; see fs_species_step)
+ * wait on mbarriers with a bound.  fs_stencil_status returns 1 if such a wait
+ * gave up since the flag was last cleared (the kernel's results are then not
+ * to be trusted: the caller reports FS_ETIMEOUT), 0 if not, -1 on a CUDA
+ * error; clear = 1 clears it.  Synchronous.  fs_set_tma(0) makes those
+ * kernels read their inputs directly instead (the same results); 1, the
+ * default, stages them where the grid allows (even nx). */
+int fs_stencil_status(int clear);
+int fs_set_tma(int on);
+
 /* Per-step diagnostics over x columns, one pass over T_s, omega and the bed
  * sources (spread_3d.py:3503-3512 maxima and ignited-cell count; ROS_Ts front
  * test of _cheney_phase16_worker.py:208-231; HRRPUA(x)):
