@@ -399,6 +399,7 @@ static bool launch_species_step_tma(const GridDev& g, const SpeciesArgs& a, cons
   if (chunks > g.nz) chunks = g.nz;
   if (chunks < 1) chunks = 1;
   int kz = (g.nz + chunks - 1) / chunks;
+  if (kz < 4) kz = g.nz < 4 ? g.nz : 4;  // at least four levels per chunk (halo overhead)
   if (kz > TS_MAXKZ) kz = TS_MAXKZ;
   chunks = (g.nz + kz - 1) / kz;
   static bool attr = false;
