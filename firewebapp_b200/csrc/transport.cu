@@ -258,8 +258,20 @@ k_species_tma(GridDev g, SpeciesArgs a, const __grid_constant__ SpeciesMaps tm,
   const bool inside = i < nx && j < ny;
   const int ii = tx + 2, jj = ty + 2;
   const int cix = jj * TS_HX + ii;
+  // the cell-centred inputs of the next level are loaded while this level
+  // computes (registers, one level ahead)
+  double nu_ = 0.0, nv_ = 0.0, nw_ = 0.0, nr_ = 1.0, nsp = 0.0, nsd = 0.0;
+  auto load_centre = [&](int k) {
+    if (inside && k < k1) {
+      const int64_t c = (int64_t)k * sz + (int64_t)j * sy + i;
+      nu_ = u[c]; nv_ = v[c]; nw_ = w[c]; nr_ = rho[c]; nsp = a.Sp[c]; nsd = a.Sd[c];
+    }
+  };
+  load_centre(k0);
   int waited = pfirst - 1;  // planes up to here have landed (and been patched)
   for (int k = k0; k < k1; ++k) {
+    const double ui = nu_, vi = nv_, wi = nw_, rho_c = nr_, sp = nsp, sd = nsd;
+    load_centre(k + 1);
     // the planes this level reads that have not been waited for yet
     const int need = min(k + 2, plast);
     for (int p = waited + 1; p <= need; ++p) {
@@ -287,11 +299,9 @@ k_species_tma(GridDev g, SpeciesArgs a, const __grid_constant__ SpeciesMaps tm,
       const double* const plm2 = ring + (size_t)slot_of(k - 2) * 3 * TS_PLANE;
       const double* const plp2 = ring + (size_t)slot_of(k + 2) * 3 * TS_PLANE;
       const int64_t c = (int64_t)k * sz + (int64_t)j * sy + i;
-      const double ui = u[c], vi = v[c], wi = w[c];
-      const double inv_rho = 1.0 / rho[c];
+      const double inv_rho = 1.0 / rho_c;
       const double* rk = rkz + 4 * (k - k0);
       const double inv_d_above = rk[0], inv_d_below = rk[1], inv_dz_k = rk[2], inv_hz = rk[3];
-      const double sp = a.Sp[c], sd = a.Sd[c];
       const double stot = sp + sd;
       const bool mx = (i >= 2 && i <= nx - 3);
       const bool mz = (k >= 2 && k <= nz - 3);
