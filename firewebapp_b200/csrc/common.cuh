@@ -35,23 +35,26 @@ __device__ __forceinline__ int wrapj(int j, int ny) {
   return r < 0 ? r + ny : r;
 }
 
-// minmod limiter (muscl_3d.py:37-44)
+// minmod limiter (muscl_3d.py:37-44), as selects (no divergent branches):
+// 0 when a*b <= 0, else the argument of smaller magnitude
 __device__ __forceinline__ double minmod(double a, double b) {
-  if (a * b <= 0.0) return 0.0;
-  if (a > 0.0) return a < b ? a : b;
-  return a > b ? a : b;
+  const double lo = a < b ? a : b, hi = a > b ? a : b;
+  const double m = a > 0.0 ? lo : hi;
+  return (a * b <= 0.0) ? 0.0 : m;
 }
 
-// upwind-biased MUSCL face value at i+1/2 from cells i-1..i+2 (muscl_3d.py:47-64)
+// upwind-biased MUSCL face value at i+1/2 from cells i-1..i+2 (muscl_3d.py:47-64):
+// uf >= 0: pi + 0.5 minmod(pi - pim1, pip1 - pi); else pip1 - 0.5 minmod(pip1 - pi,
+// pip2 - pip1).  Both sides are formed by selects; x + (-0.5 s) equals x - 0.5 s
+// exactly, so the values are the branchy form's bit for bit.
 __device__ __forceinline__ double muscl_face(double pim1, double pi, double pip1,
                                              double pip2, double uf) {
-  if (uf >= 0.0) {
-    double s = minmod(pi - pim1, pip1 - pi);
-    return pi + 0.5 * s;
-  } else {
-    double s = minmod(pip1 - pi, pip2 - pip1);
-    return pip1 - 0.5 * s;
-  }
+  const bool up = uf >= 0.0;
+  const double a = up ? pi - pim1 : pip1 - pi;
+  const double b = up ? pip1 - pi : pip2 - pip1;
+  const double base = up ? pi : pip1;
+  const double half = up ? 0.5 : -0.5;
+  return base + half * minmod(a, b);
 }
 
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
