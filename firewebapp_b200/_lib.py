@@ -121,6 +121,14 @@ SIGNATURES = {
     "fs_ctx_read": (I, [P, I, P]),
     "fs_ctx_write": (I, [P, I, P]),
     "fs_ctx_stream": (P, [P]),
+    "fs_convert": (I, [I64, I, PP, PP, I, P]),
+    "fs_edc_f32_scratch_bytes": (I64, [I64]),
+    "fs_edc_f32": (I, [I64, P, P, P, P, P, P, P, P, D, D, D, I, D, D, I, P, P]),
+    "fs_species_step_f32": (I, [_G, PP, PP, P, P, C.POINTER(D), P, P, P, P, D, D, D, P]),
+    "fs_turb_diffusion_substep_f32": (I, [_G, I, PP, PP, P, D, D, I, C.POINTER(D),
+                                          C.POINTER(D), P]),
+    "fs_gas_energy_update_f32": (I, [_G, P, P, P, P, P, P, P, P, P, D, D, D, I, I, I, I, P]),
+    "fs_clip_f32": (I, [I64, P, D, D, P]),
     "fs_stencil_status": (I, [I]),
     "fs_set_tma": (I, [I]),
     "fs_column_diag_scratch_bytes": (I64, [_G]),

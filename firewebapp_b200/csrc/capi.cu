@@ -375,6 +375,76 @@ int fs_set_tma(int on) {
   return FS_OK;
 }
 
+// ---- single-precision sub-step kernels (mixed-precision form) ----
+int fs_convert(int64_t n, int nf, const void* const* src, void* const* dst, int to_f32,
+               void* stream) {
+  if (!src || !dst || n < 0 || nf < 1 || nf > 16) {
+    fs_set_error("fs_convert: bad argument");
+    return FS_EARG;
+  }
+  return check(launch_convert(n, nf, src, dst, to_f32, ST(stream)), "fs_convert");
+}
+
+int64_t fs_edc_f32_scratch_bytes(int64_t n) { return n < 0 ? -1 : edc32_scratch_bytes(n); }
+
+int fs_edc_f32(int64_t n, const float* rho, float* T_g, float* Y_F, float* Y_O2, const float* k,
+               const float* eps, const float* Y_H2O, float* omega, double chi_rad, double cp_g,
+               double dt, int n_substeps, double s_stoich, double hoc_J, int extinction,
+               void* scratch, void* stream) {
+  if (n < 0 || !scratch) {
+    fs_set_error("fs_edc_f32: bad argument");
+    return FS_EARG;
+  }
+  return check(launch_edc32(n, rho, T_g, Y_F, Y_O2, k, eps, Y_H2O, omega, chi_rad, cp_g, dt,
+                            n_substeps, s_stoich, hoc_J, extinction, scratch, ST(stream)),
+               "fs_edc_f32");
+}
+
+int fs_species_step_f32(const FsGrid* g, const float* const* Y, float* const* Y_out,
+                        const float* S_pyro, const float* S_drying, const double* Y_inlet,
+                        const float* rho, const float* u, const float* v, const float* w,
+                        double dt, double D, double o2_cap, void* stream) {
+  GRID("fs_species_step_f32");
+  if (!Y || !Y_out || !S_pyro || !S_drying || !Y_inlet) {
+    fs_set_error("fs_species_step_f32: bad species arguments");
+    return FS_EARG;
+  }
+  return check(launch_species_step32(gd, Y, Y_out, S_pyro, S_drying, Y_inlet, rho, u, v, w, dt,
+                                     D, o2_cap, ST(stream)),
+               "fs_species_step_f32");
+}
+
+int fs_turb_diffusion_substep_f32(const FsGrid* g, int nfield, const float* const* f,
+                                  float* const* f_out, const float* nu_t, double sc_t,
+                                  double dt_sub, int clip, const double* lo, const double* hi,
+                                  void* stream) {
+  GRID("fs_turb_diffusion_substep_f32");
+  if (!f || !f_out || (clip && (!lo || !hi))) {
+    fs_set_error("fs_turb_diffusion_substep_f32: bad argument");
+    return FS_EARG;
+  }
+  return check(launch_turb_diff32(gd, nfield, f, f_out, nu_t, sc_t, dt_sub, clip, lo, hi,
+                                  ST(stream)),
+               "fs_turb_diffusion_substep_f32");
+}
+
+int fs_gas_energy_update_f32(const FsGrid* g, float* T_g, const float* rho, const float* Y_H2O,
+                             const double* T_s, const float* S_pyro, const float* S_drying,
+                             const float* Q_g_conv, const double* q_rad_gas, float* Q_comb_out,
+                             double dt_sub, double T_amb, double h_bed, int drip_on, int n_z_bed,
+                             int i_src0, int i_src1, void* stream) {
+  GRID("fs_gas_energy_update_f32");
+  return check(launch_gas_update32(gd, T_g, rho, Y_H2O, T_s, S_pyro, S_drying, Q_g_conv,
+                                   q_rad_gas, Q_comb_out, dt_sub, T_amb, h_bed, drip_on, n_z_bed,
+                                   i_src0, i_src1, ST(stream)),
+               "fs_gas_energy_update_f32");
+}
+
+int fs_clip_f32(int64_t n, float* f, double lo, double hi, void* stream) {
+  if (n < 0) return FS_EARG;
+  return check(launch_clip32(n, f, lo, hi, ST(stream)), "fs_clip_f32");
+}
+
 int64_t fs_column_diag_scratch_bytes(const FsGrid* g) {
   GridDev gd;
   if (!to_grid(g, gd, "fs_column_diag_scratch_bytes")) return -1;

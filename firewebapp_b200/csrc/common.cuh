@@ -5,10 +5,10 @@
 // the reference kernels mutate in place (spread_3d.py:88-155).
 //
 // Arithmetic is transcribed operation by operation from the reference
-// expressions and the library is compiled with --fmad=false, so each cell
-// rounds the way the numba (no fast-math) build does; remaining differences
-// come only from libm transcendental functions (exp/pow/tanh), which are
-// within a few ulp of glibc.
+// expressions; the library is built with FMA contraction, so a multiply-add
+// rounds once where numba rounds twice, and libm transcendental functions
+// (exp/pow/tanh) are within a few ulp of glibc: results agree with the
+// reference to round-off.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>

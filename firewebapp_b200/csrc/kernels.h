@@ -175,3 +175,26 @@ int launch_coldiag_keys(const void* scratch, double* out4, cudaStream_t st);
 // (read, optionally cleared; -1 on a CUDA error) and the on/off switch
 int stencil_status(int clear);
 void set_tma(int on);
+int launch_edc_carry(int nb, const signed char* agg, signed char* carry, cudaStream_t st);
+// single-precision sub-step kernels (substep32.cu)
+int launch_convert(int64_t n, int nf, const void* const* src, void* const* dst, int to_f32,
+                   cudaStream_t st);
+int64_t edc32_scratch_bytes(int64_t n);
+int launch_edc32(int64_t n, const float* rho, float* Tg, float* Yf, float* YO, const float* kt,
+                 const float* et, const float* YH, float* omega, double chi_rad, double cp_g,
+                 double dt, int n_substeps, double s_stoich, double hoc_J, int extinction,
+                 void* scratch, cudaStream_t st);
+int launch_species_step32(const GridDev& g, const float* const* Y, float* const* Yo,
+                          const float* Sp, const float* Sd, const double* Y_inlet,
+                          const float* rho, const float* u, const float* v, const float* w,
+                          double dt, double D, double o2_cap, cudaStream_t st);
+int launch_turb_diff32(const GridDev& g, int nfield, const float* const* f, float* const* fo,
+                       const float* nu_t, double sc_t, double dt_sub, int clip, const double* lo,
+                       const double* hi, cudaStream_t st);
+int launch_gas_update32(const GridDev& g, float* Tg, const float* rho, const float* YH,
+                        const double* Ts, const float* Sp, const float* Sd, const float* Qgc,
+                        const double* qrg, float* Qcomb_out, double dt_sub, double T_amb,
+                        double h_bed, int drip_on, int n_z_bed, int i_src0, int i_src1,
+                        cudaStream_t st);
+int launch_clip32(int64_t n, float* f, double lo, double hi, cudaStream_t st);
+

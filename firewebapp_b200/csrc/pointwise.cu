@@ -96,6 +96,12 @@ k_edc_carry(int nb, const signed char* agg, signed char* carry, const signed cha
   }
 }
 
+int launch_edc_carry(int nb, const signed char* agg, signed char* carry, cudaStream_t st) {
+  k_edc_carry<<<1, EDC_CARRY_THREADS, 0, st>>>(nb, agg, carry, nullptr);
+  fs_count_launch();
+  return cuda_status();
+}
+
 struct EdcArgs {
   const double* rho;
   double *Tg, *Yf, *YO;

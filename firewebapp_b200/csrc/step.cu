@@ -64,6 +64,13 @@ enum {
   NSLOT
 };
 
+// FP32 copies of the mixed form's sub-steps: the fields they update (and
+// their work buffers) and the fields they only read
+enum {
+  F32_TG = 0, F32_YF, F32_YO, F32_YH, F32_T1, F32_T2, F32_T3, F32_T4, F32_RHO, F32_U, F32_V,
+  F32_W, F32_K, F32_EPS, F32_NU, F32_SP, F32_SD, F32_QGC, F32_OMEGA, F32_QCOMB, F32_N
+};
+
 struct FsCtx {
   FsCaseDesc c;
   std::vector<double> hdz, hda, hdb, hox, hoy, hoz, hw, hsdz, hsda, hsdb;
@@ -81,6 +88,9 @@ struct FsCtx {
   unsigned long long* active_count = nullptr;
   double *T_soil = nullptr, *q_in_soil = nullptr, *soil_dz = nullptr, *soil_da = nullptr,
          *soil_db = nullptr;
+  // FP32 sub-step copies of the mixed form (slots as F32_*), NULL in the plain form
+  float* h32[20] = {};
+  void* edc32_scratch = nullptr;
   // particles and their per-cell segments
   int64_t np = 0;
   double* pd[10] = {};  // x y z m_solid m_water m_char T_s m_water_0 sav m_char_max
@@ -269,6 +279,8 @@ static void ctx_free(FsCtx* C) {
   if (C->dom) fs_dom_destroy(C->dom);
   for (int q = 0; q < NSLOT; ++q) cudaFree(C->f[q]);
   for (int q = 0; q < 10; ++q) cudaFree(C->pd[q]);
+  for (int q = 0; q < F32_N; ++q) cudaFree(C->h32[q]);
+  cudaFree(C->edc32_scratch);
   cudaFree(C->dz); cudaFree(C->da); cudaFree(C->db);
   cudaFree(C->u_inlet); cudaFree(C->sigma_x); cudaFree(C->k_wall); cudaFree(C->eps_wall);
   cudaFree(C->zero2); cudaFree(C->hcond_scratch); cudaFree(C->max_scratch);
@@ -357,6 +369,12 @@ int fs_ctx_create(const FsCaseDesc* desc, const FsInitState* init, FsCtx** out) 
   C->max_scratch = dev_alloc(64, ok);
   if (cudaMalloc(&C->edc_scratch, (size_t)fs_edc_scratch_bytes(n) + 64) != cudaSuccess) ok = false;
   if (cudaMalloc(&C->active_count, sizeof(unsigned long long)) != cudaSuccess) ok = false;
+  if (c.form == 1) {
+    for (int q = 0; q < F32_N; ++q)
+      if (cudaMalloc(&C->h32[q], sizeof(float) * (size_t)n) != cudaSuccess) ok = false;
+    if (cudaMalloc(&C->edc32_scratch, (size_t)fs_edc_f32_scratch_bytes(n) + 64) != cudaSuccess)
+      ok = false;
+  }
   C->T_soil = dev_alloc((int64_t)c.n_soil * n2, ok);
   C->q_in_soil = dev_alloc(n2, ok);
   C->soil_dz = dev_alloc(c.n_soil, ok); C->soil_da = dev_alloc(c.n_soil, ok);
@@ -579,7 +597,94 @@ static int substep_prep(FsCtx* C, double dt, SubCounts* sc) {
   return FS_OK;
 }
 
+// the mixed form's FP32 copies of the fields the sub-steps read
+static int to32(FsCtx* C) {
+  if (C->c.form != 1) return FS_OK;
+  double** f = C->f;
+  float** h = C->h32;
+  const void* src[14] = {f[S_TG], f[S_YF], f[S_YO], f[S_YH], f[S_RHO], f[S_U], f[S_V],
+                         f[S_W], f[S_K], f[S_EPS], f[S_NU], f[B_SP], f[B_SD], f[B_QGC]};
+  void* dst[14] = {h[F32_TG], h[F32_YF], h[F32_YO], h[F32_YH], h[F32_RHO], h[F32_U], h[F32_V],
+                   h[F32_W], h[F32_K], h[F32_EPS], h[F32_NU], h[F32_SP], h[F32_SD], h[F32_QGC]};
+  CK(fs_convert(C->n, 14, src, dst, 1, C->s_main), "to_f32");
+  return FS_OK;
+}
+
+// the sub-steps' results back into the FP64 state
+static int from32(FsCtx* C) {
+  if (C->c.form != 1) return FS_OK;
+  double** f = C->f;
+  float** h = C->h32;
+  const void* src[6] = {h[F32_TG], h[F32_YF], h[F32_YO], h[F32_YH], h[F32_OMEGA], h[F32_QCOMB]};
+  void* dst[6] = {f[S_TG], f[S_YF], f[S_YO], f[S_YH], f[W_OMEGA], f[W_QCOMB]};
+  CK(fs_convert(C->n, 6, src, dst, 0, C->s_main), "to_f64");
+  return FS_OK;
+}
+
+static int substep_chem32(FsCtx* C, double dt_sub, const SubCounts& sc) {
+  const FsCaseDesc& c = C->c;
+  cudaStream_t s = C->s_main;
+  float** h = C->h32;
+  CK(fs_edc_f32(C->n, h[F32_RHO], h[F32_TG], h[F32_YF], h[F32_YO], h[F32_K], h[F32_EPS],
+                h[F32_YH], h[F32_OMEGA], c.chi_rad, 1100.0, dt_sub, 1, 1.3, 17000000.0,
+                c.edc_extinction_enable, C->edc32_scratch, s),
+     "edc_f32");
+  {
+    const float* Ys[3] = {h[F32_YF], h[F32_YO], h[F32_YH]};
+    float* Yo[3] = {h[F32_T1], h[F32_T2], h[F32_T3]};
+    const double Yin[3] = {0.0, 0.232, 0.0};
+    CK(fs_species_step_f32(&C->g, Ys, Yo, h[F32_SP], h[F32_SD], Yin, h[F32_RHO], h[F32_U],
+                           h[F32_V], h[F32_W], dt_sub, 1.0e-5, 0.232, s),
+       "species_f32");
+    std::swap(h[F32_YF], h[F32_T1]);
+    std::swap(h[F32_YO], h[F32_T2]);
+    std::swap(h[F32_YH], h[F32_T3]);
+  }
+  const double lo[3] = {0.0, 0.0, 0.0}, hi[3] = {1.0, 0.232, 1.0};
+  for (int q = 0; q < sc.n_sc; ++q) {
+    const float* Ys[3] = {h[F32_YF], h[F32_YO], h[F32_YH]};
+    float* Yo[3] = {h[F32_T1], h[F32_T2], h[F32_T3]};
+    CK(fs_turb_diffusion_substep_f32(&C->g, 3, Ys, Yo, h[F32_NU], SC_T, sc.dts_sc,
+                                     q == sc.n_sc - 1 ? 1 : 0, lo, hi, s),
+       "turb_diff_Y_f32");
+    std::swap(h[F32_YF], h[F32_T1]);
+    std::swap(h[F32_YO], h[F32_T2]);
+    std::swap(h[F32_YH], h[F32_T3]);
+  }
+  return FS_OK;
+}
+
+static int substep_energy32(FsCtx* C, double dt_sub, int drip, const SubCounts& sc) {
+  const FsCaseDesc& c = C->c;
+  cudaStream_t s = C->s_main;
+  double** f = C->f;
+  float** h = C->h32;
+  CK(fs_gas_energy_update_f32(&C->g, h[F32_TG], h[F32_RHO], h[F32_YH], f[S_TS], h[F32_SP],
+                              h[F32_SD], h[F32_QGC], f[W_QRADG], h[F32_QCOMB], dt_sub, c.T_amb,
+                              c.h_bed, drip, c.n_z_bed, c.i_src_start, c.i_src_end, s),
+     "gas_update_f32");
+  CK(fs_solid_conduction_capped(&C->g, f[S_TS], f[S_AS], f[W_T4], 0.20, 500.0, 1300.0, dt_sub,
+                                c.T_amb, T_CAP, s),
+     "solid_cond");
+  std::swap(f[S_TS], f[W_T4]);
+  if (sc.n_pr > 0) {
+    const double lo[1] = {c.T_amb}, hi[1] = {T_CAP};
+    for (int q = 0; q < sc.n_pr; ++q) {
+      const float* in[1] = {h[F32_TG]};
+      float* o[1] = {h[F32_T4]};
+      CK(fs_turb_diffusion_substep_f32(&C->g, 1, in, o, h[F32_NU], PR_T, sc.dts_pr,
+                                       q == sc.n_pr - 1 ? 1 : 0, lo, hi, s),
+         "turb_diff_T_f32");
+      std::swap(h[F32_TG], h[F32_T4]);
+    }
+  } else {
+    CK(fs_clip_f32(C->n, h[F32_TG], c.T_amb, T_CAP, s), "cap_Tg_f32");
+  }
+  return FS_OK;
+}
+
 static int substep_chem(FsCtx* C, double dt_sub, const SubCounts& sc) {
+  if (C->c.form == 1) return substep_chem32(C, dt_sub, sc);
   const FsCaseDesc& c = C->c;
   cudaStream_t s = C->s_main;
   double** f = C->f;
@@ -613,6 +718,7 @@ static int substep_chem(FsCtx* C, double dt_sub, const SubCounts& sc) {
 }
 
 static int substep_energy(FsCtx* C, double dt_sub, int drip, const SubCounts& sc) {
+  if (C->c.form == 1) return substep_energy32(C, dt_sub, drip, sc);
   const FsCaseDesc& c = C->c;
   cudaStream_t s = C->s_main;
   double** f = C->f;
@@ -767,6 +873,7 @@ static int one_step(FsCtx* C, int* alive) {
       return ctx_fail(C, FS_ECUDA, "wait inputs");
     rc = flame_mask_and_gas_adv(C, dt);
     if (rc == FS_OK) rc = substep_prep(C, dt, &sc);
+    if (rc == FS_OK) rc = to32(C);
     if (rc == FS_OK) rc = substep_chem(C, dt_sub, sc);
     const int rd = wait_state(C, &C->done_rc);
     if (rc != FS_OK) return rc;
@@ -794,6 +901,7 @@ static int one_step(FsCtx* C, int* alive) {
     // --- 10/11. flame mask, gas-temperature advection
     int rc = flame_mask_and_gas_adv(C, dt);
     if (rc == FS_OK) rc = substep_prep(C, dt, &sc);
+    if (rc == FS_OK) rc = to32(C);
     if (rc == FS_OK) rc = substep_chem(C, dt_sub, sc);
     if (rc != FS_OK) return rc;
   }
@@ -805,6 +913,10 @@ static int one_step(FsCtx* C, int* alive) {
       if (rc != FS_OK) return rc;
     }
     int rc = substep_energy(C, dt_sub, ign, sc);
+    if (rc != FS_OK) return rc;
+  }
+  {
+    int rc = from32(C);
     if (rc != FS_OK) return rc;
   }
   // --- 13. level set (passive: v_n = 0, so evolve leaves phi; reinit every 10)

@@ -159,6 +159,18 @@ class Tier3Solver:
         self.edc_scratch = torch.zeros(int(self.lib.fs_edc_scratch_bytes(self.n)) + 64,
                                        dtype=torch.uint8, device=dev)
         self.active_count = torch.zeros(1, dtype=torch.int64, device=dev)
+        # the FP32 forms run the ten chemistry/transport sub-steps on float
+        # copies (updated: T_g and the mass fractions; read-only: rho, u, v, w,
+        # k, eps, nu_t and the bed sources), made once per step
+        self.sub32 = None
+        if fp32:
+            f32 = dict(dtype=torch.float32, device=dev)
+            self.sub32 = {name: torch.zeros(shp, **f32) for name in (
+                "T_g", "Y_fuel", "Y_O2", "Y_H2O", "t1", "t2", "t3", "t4", "rho", "u", "v",
+                "w", "k_turb", "eps_turb", "nu_t", "S_pyro", "S_drying", "Q_g_conv", "omega",
+                "Q_comb")}
+            self.edc32_scratch = torch.zeros(int(self.lib.fs_edc_f32_scratch_bytes(self.n)) + 64,
+                                             dtype=torch.uint8, device=dev)
         # pinned host mirrors for the per-step scalar reads
         self.h_count = torch.zeros(1, dtype=torch.int64).pin_memory()
         self.h_row = torch.zeros(g.Nx, dtype=torch.float64).pin_memory()
@@ -513,6 +525,7 @@ class Tier3Solver:
             torch.cuda.current_stream(self.dev).wait_event(ev_in)
             self._flame_mask_and_gas_adv(dt)
             early = self._substep_prep()
+            self._to32()
             self._substep_chem(dt_sub, Sp, Sd, *early)
             done = dom_job.result()
             torch.cuda.current_stream(self.dev).wait_event(done)
@@ -540,6 +553,7 @@ class Tier3Solver:
             # --- 10/11. flame mask, gas-temperature advection
             self._flame_mask_and_gas_adv(dt)
             early = self._substep_prep()
+            self._to32()
             self._substep_chem(dt_sub, Sp, Sd, *early)
         # --- 12. ten chemistry/transport sub-steps (:2678-3196); the first one's
         # chemistry and species half ran above
@@ -549,6 +563,7 @@ class Tier3Solver:
             if _sub > 0:
                 self._substep_chem(dt_sub, Sp, Sd, n_sc, dts_sc, n_pr, dts_pr)
             self._substep_energy(dt_sub, Sp, Sd, drip, n_pr, dts_pr)
+        self._from32()
         # --- 13. level set (passive: v_n = 0, so evolve leaves phi; reinit every 10)
         self._phase("levelset")
         self.lset_step += 1
@@ -615,10 +630,103 @@ class Tier3Solver:
         n_pr, dts_pr = self._nsub_from(nu_in, PR_T, dt_sub)
         return n_sc, dts_sc, n_pr, dts_pr
 
+    _TO32 = (("T_g", "f"), ("Y_fuel", "f"), ("Y_O2", "f"), ("Y_H2O", "f"), ("rho", "f"),
+             ("u", "f"), ("v", "f"), ("w", "f"), ("k_turb", "f"), ("eps_turb", "f"),
+             ("nu_t", "f"), ("S_pyro", "b"), ("S_drying", "b"), ("Q_g_conv", "b"))
+    _FROM32 = (("T_g", "f"), ("Y_fuel", "f"), ("Y_O2", "f"), ("Y_H2O", "f"), ("omega", "w"),
+               ("Q_comb", "w"))
+
+    def _to32(self):
+        """FP32 copies of the fields the sub-steps read (FP32 forms only)."""
+        if self.sub32 is None:
+            return
+        src = [(self.f if kind == "f" else self.bed_out)[name] for name, kind in self._TO32]
+        dst = [self.sub32[name] for name, _ in self._TO32]
+        check(self.lib.fs_convert(self.n, len(src), ptr_array(src), ptr_array(dst), 1,
+                                  self._s()), "to_f32")
+
+    def _from32(self):
+        """The sub-steps' results back into the FP64 state (FP32 forms only)."""
+        if self.sub32 is None:
+            return
+        src = [self.sub32[name] for name, _ in self._FROM32]
+        dst = [(self.f if kind == "f" else self.w)[name] for name, kind in self._FROM32]
+        check(self.lib.fs_convert(self.n, len(src), ptr_array(src), ptr_array(dst), 0,
+                                  self._s()), "to_f64")
+
+    def _swap32(self, name, buf):
+        t = self.sub32
+        t[name], t[buf] = t[buf], t[name]
+
+    def _substep_chem32(self, dt_sub, n_sc, dts_sc):
+        """The FP32 form of _substep_chem (fs_edc_f32, fs_species_step_f32,
+        fs_turb_diffusion_substep_f32 on the float copies)."""
+        L, p, gp, t = self.lib, self.p, self.gp, self.sub32
+        s = self._s()
+        self._phase("edc")
+        with self._ktime("edc"):
+            check(L.fs_edc_f32(self.n, ptr(t["rho"]), ptr(t["T_g"]), ptr(t["Y_fuel"]),
+                               ptr(t["Y_O2"]), ptr(t["k_turb"]), ptr(t["eps_turb"]),
+                               ptr(t["Y_H2O"]), ptr(t["omega"]), p["chi_rad"], 1100.0, dt_sub,
+                               1, 1.3, 17_000_000.0, int(p["edc_extinction_enable"]),
+                               ptr(self.edc32_scratch), s), "edc_f32")
+        self._phase("species")
+        Ys = [t["Y_fuel"], t["Y_O2"], t["Y_H2O"]]
+        Yo = [t["t1"], t["t2"], t["t3"]]
+        with self._ktime("species_transport"):
+            check(L.fs_species_step_f32(gp, ptr_array(Ys), ptr_array(Yo), ptr(t["S_pyro"]),
+                                        ptr(t["S_drying"]), dbl_array([0.0, 0.232, 0.0]),
+                                        ptr(t["rho"]), ptr(t["u"]), ptr(t["v"]), ptr(t["w"]),
+                                        dt_sub, 1.0e-5, 0.232, s), "species_f32")
+        self._swap32("Y_fuel", "t1")
+        self._swap32("Y_O2", "t2")
+        self._swap32("Y_H2O", "t3")
+        self._phase("turb_diff_Y")
+        for q in range(n_sc):
+            Ys = [t["Y_fuel"], t["Y_O2"], t["Y_H2O"]]
+            Yo = [t["t1"], t["t2"], t["t3"]]
+            with self._ktime("turb_diffusion_Y"):
+                check(L.fs_turb_diffusion_substep_f32(
+                    gp, 3, ptr_array(Ys), ptr_array(Yo), ptr(t["nu_t"]), SC_T, dts_sc,
+                    int(q == n_sc - 1), dbl_array([0.0, 0.0, 0.0]),
+                    dbl_array([1.0, 0.232, 1.0]), s), "turb_diff_Y_f32")
+            self._swap32("Y_fuel", "t1")
+            self._swap32("Y_O2", "t2")
+            self._swap32("Y_H2O", "t3")
+
+    def _substep_energy32(self, dt_sub, drip, n_pr, dts_pr):
+        """The FP32 form of _substep_energy (the solid conduction stays FP64)."""
+        L, f, w, p, gp, g, t = self.lib, self.f, self.w, self.p, self.gp, self.grid, self.sub32
+        s = self._s()
+        self._phase("gas_update")
+        check(L.fs_gas_energy_update_f32(gp, ptr(t["T_g"]), ptr(t["rho"]), ptr(t["Y_H2O"]),
+                                         ptr(f["T_s"]), ptr(t["S_pyro"]), ptr(t["S_drying"]),
+                                         ptr(t["Q_g_conv"]), ptr(w["q_rad_gas"]),
+                                         ptr(t["Q_comb"]), dt_sub, p["T_amb"], p["h_bed"], drip,
+                                         g.n_z_bed, p["i_src_start"], p["i_src_end"], s),
+              "gas_update_f32")
+        self._phase("solid_cond")
+        check(L.fs_solid_conduction_capped(gp, ptr(f["T_s"]), ptr(f["alpha_s"]), ptr(w["tmp4"]),
+                                           0.20, 500.0, 1300.0, dt_sub, p["T_amb"], T_CAP, s),
+              "solid_cond")
+        self._swap("T_s", "tmp4")
+        self._phase("turb_diff_T")
+        if n_pr > 0:
+            for q in range(n_pr):
+                check(L.fs_turb_diffusion_substep_f32(
+                    gp, 1, ptr_array([t["T_g"]]), ptr_array([t["t4"]]), ptr(t["nu_t"]), PR_T,
+                    dts_pr, int(q == n_pr - 1), dbl_array([p["T_amb"]]), dbl_array([T_CAP]),
+                    s), "turb_diff_T_f32")
+                self._swap32("T_g", "t4")
+        else:
+            check(L.fs_clip_f32(self.n, ptr(t["T_g"]), p["T_amb"], T_CAP, s), "cap_Tg_f32")
+
     def _substep_chem(self, dt_sub, Sp, Sd, n_sc, dts_sc, n_pr, dts_pr):
         """First half of a chemistry/transport sub-step: EDC, species sources
         and transport, the O2 clip and the turbulent diffusion of the species
         (spread_3d.py:2678-3060)."""
+        if self.sub32 is not None:
+            return self._substep_chem32(dt_sub, n_sc, dts_sc)
         L, f, w, p, gp = self.lib, self.f, self.w, self.p, self.gp
         s = self._s()
         self._phase("edc")
@@ -660,6 +768,8 @@ class Tier3Solver:
         """Second half of a sub-step: gas-energy update with the radiative
         gas source, vertical solid conduction, turbulent diffusion of T_g and
         the caps (spread_3d.py:3104-3196)."""
+        if self.sub32 is not None:
+            return self._substep_energy32(dt_sub, drip, n_pr, dts_pr)
         L, f, w, p, gp, g = self.lib, self.f, self.w, self.p, self.gp, self.grid
         s = self._s()
         self._phase("gas_update")

@@ -204,6 +204,42 @@ int fs_ignition_pulse(const FsGrid* g, double* q_rad, int k, int i0, int i1, dou
 int fs_stencil_status(int clear);
 int fs_set_tma(int on);
 
+/* ---- Single-precision sub-step kernels (mixed-precision form; no
+ * counterpart in the reference, which is FP64 throughout).  The ten
+ * chemistry/transport sub-steps of an outer step (spread_3d.py:2678-3196) run
+ * on FP32 copies: fs_convert widens or narrows nf device arrays of n elements
+ * (to_f32 = 1: double -> float, 0: float -> double).  Each kernel restates its
+ * FP64 entry point in float arithmetic with the same arguments, float arrays
+ * in place of double ones:
+ *   fs_edc_f32                    = fs_edc (same flat-order flag scan; scratch
+ *                                   of fs_edc_f32_scratch_bytes(n) bytes)
+ *   fs_species_step_f32           = fs_species_step
+ *   fs_turb_diffusion_substep_f32 = fs_turb_diffusion_substep (1 or 3 fields)
+ *   fs_gas_energy_update_f32      = fs_gas_energy_update (T_s and q_rad_gas
+ *                                   stay FP64 inputs)
+ *   fs_clip_f32                   = fs_clip */
+int fs_convert(int64_t n, int nf, const void* const* src, void* const* dst, int to_f32,
+               void* stream);
+int64_t fs_edc_f32_scratch_bytes(int64_t n);
+int fs_edc_f32(int64_t n, const float* rho, float* T_g, float* Y_F, float* Y_O2, const float* k,
+               const float* eps, const float* Y_H2O, float* omega, double chi_rad, double cp_g,
+               double dt, int n_substeps, double s_stoich, double hoc_J, int extinction,
+               void* scratch, void* stream);
+int fs_species_step_f32(const FsGrid* g, const float* const* Y, float* const* Y_out,
+                        const float* S_pyro, const float* S_drying, const double* Y_inlet,
+                        const float* rho, const float* u, const float* v, const float* w,
+                        double dt, double D, double o2_cap, void* stream);
+int fs_turb_diffusion_substep_f32(const FsGrid* g, int nfield, const float* const* f,
+                                  float* const* f_out, const float* nu_t, double sc_t,
+                                  double dt_sub, int clip, const double* lo, const double* hi,
+                                  void* stream);
+int fs_gas_energy_update_f32(const FsGrid* g, float* T_g, const float* rho, const float* Y_H2O,
+                             const double* T_s, const float* S_pyro, const float* S_drying,
+                             const float* Q_g_conv, const double* q_rad_gas, float* Q_comb_out,
+                             double dt_sub, double T_amb, double h_bed, int drip_on, int n_z_bed,
+                             int i_src0, int i_src1, void* stream);
+int fs_clip_f32(int64_t n, float* f, double lo, double hi, void* stream);
+
 /* Per-step diagnostics over x columns, one pass over T_s, omega and the bed
  * sources (spread_3d.py:3503-3512 maxima and ignited-cell count; ROS_Ts front
  * test of _cheney_phase16_worker.py:208-231; HRRPUA(x)):
