@@ -499,6 +499,12 @@ def kernel_roofline(solver, kt, steps, form, peak, peak_src):
            "peak_source": peak_src, "launches": nl, "avg_launch_ms": avg_ms,
            "algorithmic_bytes_per_launch": alg[dom_k], "dom_sweep_path": dom_mode,
            "kernels_ms_per_step": {k: v[0] / steps for k, v in kt.items()}}
+    if dom_mode == 8:
+        import ctypes
+        shape = (ctypes.c_int * 5)()
+        if lib.fs_dom_launch_shape(solver.dom, shape) == 0:
+            out["dom_cluster"] = dict(zip(("ctas", "rows", "threads", "smem_bytes", "groups"),
+                                          list(shape)))
     if dom_k == "dom_sweep":
         out["fused_sweep_bytes_per_launch"] = fused_dom
         out["fused_sweep_achieved"] = fused_dom / (avg_ms * 1e-3) / 1e9

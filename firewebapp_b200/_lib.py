@@ -174,6 +174,7 @@ SIGNATURES = {
     "fs_dom_iterations": (I, [P]),
     "fs_dom_set_sweep_mode": (I, [P, I, I]),
     "fs_dom_sweep_mode": (I, [P]),
+    "fs_dom_launch_shape": (I, [P, P]),
     "fs_dom_set_octant_groups": (I, [P, I]),
     "fs_dom_set_precision": (I, [P, I]),
     "fs_dom_load_intensity": (I, [P, P, P]),

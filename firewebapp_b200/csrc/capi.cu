@@ -695,6 +695,13 @@ int fs_dom_set_octant_groups(void* handle, int groups) {
   return check(dom_set_groups(handle, groups), "fs_dom_set_octant_groups");
 }
 int fs_dom_sweep_mode(void* handle) { return handle ? dom_mode(handle) : -1; }
+int fs_dom_launch_shape(void* handle, int* out5) {
+  if (!handle || !out5) {
+    fs_set_error("fs_dom_launch_shape: null argument");
+    return FS_EARG;
+  }
+  return dom_launch_shape(handle, out5);
+}
 
 int fs_dom_set_precision(void* handle, int fp32) {
   if (!handle) return FS_EARG;

@@ -15,12 +15,18 @@
 //     the cluster's CTAs split the k' rows and every thread owns one or two
 //     pencils (j',k') and advances all the group's ordinates of its cell on
 //     each hyperplane, reading the previous hyperplane from shared memory.
-//     One cluster barrier per hyperplane; each CTA's last row is pushed into
-//     the downstream CTA's ghost row (distributed shared memory) before the
-//     barrier, so every read after it is local.  Inputs arrive by cp.async a
-//     few hyperplanes ahead; the sweep emits the octant's partial G and ground
-//     flux and never stores intensities.  The cluster shape is planned so
-//     that all clusters are resident at once where the part allows it.
+//     The CTAs form a pipeline, not a lock-step: each stores its last row of
+//     every hyperplane into a ring in the next CTA's shared memory
+//     (distributed shared memory) and signals the slot's "full" mbarrier; the
+//     next CTA's helper warp waits for it, and after the hyperplane that
+//     read it signals the slot's "empty" mbarrier back, so a CTA waits only
+//     for its neighbours, and only when it runs ahead of them by more than
+//     the ring's slack.  Within a CTA one __syncthreads per hyperplane.  All
+//     waits are bounded (an error flag, then FS_ETIMEOUT on the host).  Inputs
+//     arrive by cp.async a few hyperplanes ahead; the sweep emits the
+//     octant's partial G and ground flux and never stores intensities.  The
+//     cluster shape is planned so that all clusters are resident at once
+//     where the part allows it.
 //   3 (any quadrature) one launch per hyperplane over all ordinates, with the
 //     full intensity field stored; G summed over ordinates in ordinate order.
 // Path 8 sums G within each octant in ordinate order and then over octants in
@@ -29,6 +35,7 @@
 #include <vector>
 #include <cstring>
 #include <utility>
+#include <type_traits>
 #include <cooperative_groups.h>
 #include "common.cuh"
 #include "kernels.h"
@@ -138,10 +145,12 @@ __device__ __forceinline__ double clip01(double x) {
 // multiply-adds and the constant part of the denominator, ax + ay + az,
 // tabulated per ordinate and level.
 // FP64: the quotient from the hardware's approximate reciprocal refined by
-// two Newton-Raphson iterations (r <- r + r (1 - den r)), then one Markstein
-// correction of the quotient (q <- q + r (num - den q), Markstein 1990); the
-// result is within about one ulp of the correctly rounded quotient (den > 0
-// always: kappa >= 1e-3).  FP32 (mixed form): __fdividef (about 2 ulp).
+// one Newton-Raphson iteration (r <- r + r (1 - den r), which squares its
+// relative error), then one Markstein correction of the quotient
+// (q <- q + r (num - den q), Markstein 1990), whose error is the square of
+// the reciprocal's plus the final rounding: within about one ulp of the
+// correctly rounded quotient (den > 0 always: kappa >= 1e-3).  FP32 (mixed
+// form): __fdividef (about 2 ulp).
 __device__ __forceinline__ double rcp_approx(double x) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
@@ -151,11 +160,9 @@ __device__ __forceinline__ double sweep_quot(double num, double den) {
   const double r0 = rcp_approx(den);
   const double e = __fma_rn(-den, r0, 1.0);
   const double r1 = __fma_rn(r0, e, r0);
-  const double e2 = __fma_rn(-den, r1, 1.0);
-  const double r2 = __fma_rn(r1, e2, r1);
-  const double q0 = num * r2;
+  const double q0 = num * r1;
   const double res = __fma_rn(-den, q0, num);
-  return __fma_rn(r2, res, q0);
+  return __fma_rn(r1, res, q0);
 }
 __device__ __forceinline__ float sweep_quot(float num, float den) { return __fdividef(num, den); }
 __device__ __forceinline__ double fmat(double a, double b, double c) { return __fma_rn(a, b, c); }
@@ -323,49 +330,150 @@ struct ClArgs {
   int groups;  // clusters (ordinate groups of MO) per octant
   unsigned down_slots;  // 4 bits per octant: ground-flux slot, 15 = upward octant
   const int* done;  // device flag: nonzero = the source iteration has converged, do nothing
+  int* err;         // device flag: set when a bounded hand-off wait gave up
 };
-// Inputs (kappa, kappa*B and the ground intensity) arrive this many
-// hyperplanes ahead through cp.async commit groups.
+// Inputs (kappa, kappa*B, the ground intensity and the y-inflow of a row's
+// first pencil) arrive this many hyperplanes ahead through cp.async commit
+// groups.
 #define CL_AHEAD 4
-// The y-inflow and y-outflow rows move between global memory and shared
-// memory in chunks of this many hyperplanes (two chunks staged each way).
-#define CL_CHUNK 16
-// one pencil per thread up to this many pencils per CTA (80 registers a thread),
-// else two pencils per thread up to twice this many (at most 96 registers)
+// Slots of the ring through which a CTA hands the last row of each
+// hyperplane to the next CTA of the cluster: the upstream CTA runs up to
+// CL_RING - 2 hyperplanes ahead of the downstream one.
+#define CL_RING 4
+// Threads per CTA (the helper warp included): one pencil per thread up to
+// CL_MAX_THREADS_1 (80 registers a thread), else two pencils per thread up to
+// CL_MAX_THREADS_2 (96 registers).
 #define CL_MAX_THREADS_1 768
 #define CL_MAX_THREADS_2 640
-// The hyperplane buffers carry a ghost row below the CTA's first row and a
-// ghost column left of every row (rows+1 by ny+1 per ordinate): the first
-// row's threads put the z-inflow (upstream CTA, ground or ambient) into the
-// ghost row and the first column's threads the y-inflow into the ghost
-// column, and a pencil's own slot holds the ambient intensity until its
-// first cell, so every cell reads its three upwind neighbours the same way.
+// bounded hand-off waits: try_wait rounds before a thread gives up
+#define CL_WAIT_LIMIT (1 << 20)
+// Shared memory of a CTA: the hyperplane buffers (current and previous,
+// [pencil][ordinate]), the ring of the upstream CTA's last rows
+// ([slot][pencil][ordinate]), the prefetched inputs and the per-ordinate
+// tables.  A pencil's ordinates are contiguous and padded to an odd count
+// (cl_mpad), so that the per-ordinate offsets of the cell update are
+// immediates and a warp's 32 pencils fall in distinct shared-memory banks.  A pencil's own slot holds the ambient intensity until its first
+// cell; the z-inflow of the first row comes from the ring or, in the first
+// CTA, from the ground (or the ambient intensity); the y-inflow of a row's
+// first pencil is the value the previous sweep left at the other end of the
+// row, prefetched from the y-wrap array.
 struct ClLayout {
-  size_t kab, ig, win, wout, buf0, buf1, izt, cst, cix, total;
+  size_t bars, kab, ig, yin, buf0, buf1, ring, kz, cxy, cwq, total;
 };
+__host__ __device__ constexpr int cl_mpad(int Mo) { return Mo | 1; }
 __host__ __device__ inline ClLayout cl_layout(int tsize, int Mo, int rows, int ny, int nz) {
   ClLayout L;
   const size_t S = (size_t)rows * ny;
-  const size_t P = (size_t)(rows + 1) * (ny + 1);
-  const size_t chunk = (size_t)2 * Mo * rows * CL_CHUNK * tsize;
+  const size_t Mp = (size_t)cl_mpad(Mo);
   size_t o = 0;
+  L.bars = o; o = up16(o + 2 * CL_RING * sizeof(unsigned long long));
   L.kab = o; o = up16(o + (size_t)CL_AHEAD * S * 2 * tsize);
   L.ig = o; o = up16(o + (size_t)CL_AHEAD * ny * sizeof(double));
-  L.win = o; o = up16(o + chunk);
-  L.wout = o; o = up16(o + chunk);
-  L.buf0 = o; o = up16(o + (size_t)Mo * P * tsize);
-  L.buf1 = o; o = up16(o + (size_t)Mo * P * tsize);
-  L.izt = o; o = up16(o + (size_t)Mo * nz * tsize);
-  L.cst = o; o = up16(o + (size_t)Mo * nz * tsize);
-  L.cix = o; o = up16(o + 4 * (size_t)Mo * tsize);
+  L.yin = o; o = up16(o + (size_t)CL_AHEAD * rows * Mo * tsize);
+  L.buf0 = o; o = up16(o + Mp * S * tsize);
+  L.buf1 = o; o = up16(o + Mp * S * tsize);
+  L.ring = o; o = up16(o + (size_t)CL_RING * Mp * ny * tsize);
+  L.kz = o; o = up16(o + (size_t)nz * Mo * 2 * tsize);
+  L.cxy = o; o = up16(o + (size_t)Mo * 2 * tsize);
+  L.cwq = o; o = up16(o + (size_t)Mo * 2 * tsize);
   L.total = o;
   return L;
+}
+
+// mbarriers of the row hand-off (cluster scope)
+__device__ __forceinline__ void cl_mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+// this CTA's arrival on its own barrier, announcing the bytes the phase awaits
+__device__ __forceinline__ void cl_arrive_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+// the shared::cluster address of the same location in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cl_mapa(uint32_t addr, unsigned rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+// arrive on another CTA's mbarrier, releasing this thread's earlier writes
+__device__ __forceinline__ void cl_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+               : "memory");
+}
+// a value into another CTA's shared memory; its bytes count towards the
+// transaction count of that CTA's mbarrier (no fence or arrival needed)
+__device__ __forceinline__ void cl_st_async(uint32_t a, double v, uint32_t bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];" ::"r"(a),
+               "d"(v), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void cl_st_async(uint32_t a, float v, uint32_t bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f32 [%0], %1, [%2];" ::"r"(a),
+               "f"(v), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ bool cl_try_wait(uint32_t addr, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(addr), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of the given parity; a thread whose wait gave up
+// records it in *err and waits no more (the sweep's results are then not to
+// be trusted, and the host reports FS_ETIMEOUT).
+__device__ __forceinline__ void cl_wait(uint32_t addr, uint32_t parity, bool& failed, int* err) {
+  if (failed) return;
+  for (int it = 0; it < CL_WAIT_LIMIT; ++it)
+    if (cl_try_wait(addr, parity)) return;
+  failed = true;
+  if (err) atomicExch(err, 1);
+}
+
+// Shared-memory loads and stores of the sweep's hot loop by 32-bit address;
+// volatile, so they stay in program order (a batch's loads before its stores).
+template <typename T> __device__ __forceinline__ T sh_ld(uint32_t a);
+template <> __device__ __forceinline__ double sh_ld<double>(uint32_t a) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a) : "memory");
+  return v;
+}
+template <> __device__ __forceinline__ float sh_ld<float>(uint32_t a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a) : "memory");
+  return v;
+}
+template <typename T2> __device__ __forceinline__ T2 sh_ld2(uint32_t a);
+template <> __device__ __forceinline__ double2 sh_ld2<double2>(uint32_t a) {
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a) : "memory");
+  return v;
+}
+template <> __device__ __forceinline__ float2 sh_ld2<float2>(uint32_t a) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ void sh_st(uint32_t a, double v) {
+  asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void sh_st(uint32_t a, float v) {
+  asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
 }
 
 template <typename T, int MO, int PPT>
 __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2, 1)
     k_dom_octant_cl(GridDev g, ClArgs a) {
   using T2 = typename Vec2Of<T>::type;
+  // ordinates per batch of the cell update (the FP64 ten-ordinate groups in
+  // two batches of five, to stay within the register budget)
+  constexpr int CB = (sizeof(T) == 4 || MO <= 6) ? MO : (MO % 5 == 0 ? 5 : MO);
+  constexpr int MP = cl_mpad(MO);  // a pencil's padded ordinate stride
   extern __shared__ __align__(16) unsigned char shraw[];
   // an iteration queued past convergence: every CTA leaves before any
   // cluster barrier or shared-memory traffic
@@ -379,44 +487,65 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
   const int grp = part - oct * a.groups;
   const int n0 = part * MO;
   const int rows = a.rows;
-  const int S = rows * ny;
-  const int RS = ny + 1;           // padded row stride
-  const int P = (rows + 1) * RS;   // padded plane per ordinate
+  const int S = rows * ny;  // pencils per CTA; also the plane per ordinate
   const ClLayout L = cl_layout((int)sizeof(T), MO, rows, ny, nz);
+  unsigned long long* full = (unsigned long long*)(shraw + L.bars);
+  unsigned long long* empty = full + CL_RING;
   T2* kab_ring = (T2*)(shraw + L.kab);
   double* ig_ring = (double*)(shraw + L.ig);
-  T* win = (T*)(shraw + L.win);
-  T* wout = (T*)(shraw + L.wout);
+  T* yin = (T*)(shraw + L.yin);
   T* buf0 = (T*)(shraw + L.buf0);
   T* buf1 = (T*)(shraw + L.buf1);
-  T* izt = (T*)(shraw + L.izt);
-  T* cst = (T*)(shraw + L.cst);
-  T* cix = (T*)(shraw + L.cix);
-  T* ciy = cix + MO;
-  T* cw = ciy + MO;
-  T* cwm = cw + MO;
+  T* ring = (T*)(shraw + L.ring);
+  T2* kz = (T2*)(shraw + L.kz);
+  T2* cxy = (T2*)(shraw + L.cxy);
+  T2* cwq = (T2*)(shraw + L.cwq);
   const T2* kb = (const T2*)a.kb;
   T* Goct = (T*)a.Goct;
   T* Qoct = (T*)a.Qoct;
   T* wrap = (T*)a.wrap;
   const T I_amb = (T)a.I_amb;
   const int nplanes = nx + ny + nz - 2;
+  // the last warp is the helper: the hand-off signals only
+  const int TT = (int)blockDim.x - 32;
+  const bool helper = (int)threadIdx.x >= TT;
+  const int hl = (int)threadIdx.x - TT;
+  // per level and ordinate: (az, ax + ay + az); per ordinate (ax, ay) and
+  // (weight, weight * |mu|)
   for (int t = threadIdx.x; t < MO * nz; t += blockDim.x) {
-    const int m = t / nz, k = t - m * nz;
+    const int k = t / MO, m = t - k * MO;
     const double ax = fabs(a.ox[n0 + m]) / g.dx, ay = fabs(a.oy[n0 + m]) / g.dy;
     const double az = fabs(a.oz[n0 + m]) / g.dz[k];
-    izt[t] = (T)az;
-    cst[t] = (T)(ax + ay + az);
+    T2 v;
+    v.x = (T)az;
+    v.y = (T)(ax + ay + az);
+    kz[t] = v;
   }
   for (int m = threadIdx.x; m < MO; m += blockDim.x) {
-    cix[m] = (T)(fabs(a.ox[n0 + m]) / g.dx);
-    ciy[m] = (T)(fabs(a.oy[n0 + m]) / g.dy);
-    cw[m] = (T)a.w[n0 + m];
-    cwm[m] = (T)(a.w[n0 + m] * fabs(a.oz[n0 + m]));
+    T2 xy, wq;
+    xy.x = (T)(fabs(a.ox[n0 + m]) / g.dx);
+    xy.y = (T)(fabs(a.oy[n0 + m]) / g.dy);
+    wq.x = (T)a.w[n0 + m];
+    wq.y = (T)(a.w[n0 + m] * fabs(a.oz[n0 + m]));
+    cxy[m] = xy;
+    cwq[m] = wq;
   }
-  for (int t = threadIdx.x; t < MO * P; t += blockDim.x) {
+  for (int t = threadIdx.x; t < MP * S; t += blockDim.x) {
     buf0[t] = I_amb;
     buf1[t] = I_amb;
+  }
+  for (int t = threadIdx.x; t < CL_RING * MP * ny; t += blockDim.x) ring[t] = I_amb;
+  // a full slot: the ring slot's bytes (ny pencils x MO ordinates) have
+  // arrived from the upstream CTA and this CTA's helper has announced them; an
+  // empty slot: the helper of the downstream CTA has seen the hyperplane that
+  // read it complete
+  const uint32_t fill_bytes = (uint32_t)(ny * MO * sizeof(T));
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < CL_RING; ++s) {
+      cl_mbar_init(&full[s], 1u);
+      cl_mbar_init(&empty[s], 1u);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   const bool fx = a.ox[n0] >= 0.0, fy = a.oy[n0] >= 0.0, fz = a.oz[n0] >= 0.0;
   const int r0 = rank * rows;
@@ -430,54 +559,26 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
   const int64_t wstride = (int64_t)nz * nx;
   T* wrap0 = wrap + (int64_t)n0 * wstride;
   const bool periodic = a.periodic != 0;
-  const int TT = blockDim.x;
   const uint64_t keep = l2_policy_evict_last();
-  const int chunk_elems = MO * rows * CL_CHUNK;
-  // the y-inflow rows of chunk c, from global memory by the whole CTA
-  auto load_inflow = [&](int c) {
-    T* dst = win + (size_t)(c & 1) * chunk_elems;
-    for (int e = threadIdx.x; e < chunk_elems; e += TT) {
-      const int t = e % CL_CHUNK, rm = e / CL_CHUNK;
-      const int rl = rm % rows, m = rm / rows;
-      const int ip = c * CL_CHUNK + t - (r0 + rl);
-      if (rl < nrows && ip >= 0 && ip < nx) {
-        const int kk = fz ? r0 + rl : nz - 1 - (r0 + rl);
-        const int i = fx ? ip : nx - 1 - ip;
-        cp_async_val(&dst[e], &wrap0[m * wstride + (int64_t)kk * nx + i]);
-      }
-    }
-  };
-  // the y-outflow rows of chunk c, to global memory by the whole CTA
-  auto store_outflow = [&](int c) {
-    const T* src = wout + (size_t)(c & 1) * chunk_elems;
-    for (int e = threadIdx.x; e < chunk_elems; e += TT) {
-      const int t = e % CL_CHUNK, rm = e / CL_CHUNK;
-      const int rl = rm % rows, m = rm / rows;
-      const int ip = c * CL_CHUNK + t - (ny - 1) - (r0 + rl);
-      if (rl < nrows && ip >= 0 && ip < nx) {
-        const int kk = fz ? r0 + rl : nz - 1 - (r0 + rl);
-        const int i = fx ? ip : nx - 1 - ip;
-        wrap0[m * wstride + (int64_t)kk * nx + i] = src[e];
-      }
-    }
-  };
   // per-pencil constants: pencil index, row and column, global row base, roles
-  int pq[PPT], pjp[PPT], pkp[PPT], pk[PPT], pqi[PPT];
+  int pq[PPT], pjp[PPT], pkp[PPT], pk[PPT];
   int64_t prb[PPT];
-  unsigned prole[PPT];  // 1 has, 2 first row, 16 ground flux, 32 ground inflow, 64 last row with a CTA above
+  // 1 has, 2 first row, 4 first column (y-inflow), 8 last column (y-outflow),
+  // 16 ground flux, 32 ground inflow, 64 last row with a CTA below it
+  unsigned prole[PPT];
 #pragma unroll
   for (int pp = 0; pp < PPT; ++pp) {
     const int q = threadIdx.x + pp * TT;
-    const bool has = q < npen;
+    const bool has = !helper && q < npen;
     const int kl = has ? q / ny : 0;
     const int jp = has ? q - kl * ny : 0;
     const int kp = r0 + kl;
     const int k = fz ? kp : nz - 1 - kp;
     const int j = fy ? jp : ny - 1 - jp;
     pq[pp] = q; pjp[pp] = jp; pkp[pp] = kp; pk[pp] = k;
-    pqi[pp] = (kl + 1) * RS + jp + 1;
     prb[pp] = ((int64_t)k * ny + j) * nx;
-    prole[pp] = (has ? 1u : 0u) | (has && kl == 0 ? 2u : 0u) |
+    prole[pp] = (has ? 1u : 0u) | (has && kl == 0 ? 2u : 0u) | (has && jp == 0 ? 4u : 0u) |
+                (has && jp == ny - 1 && periodic ? 8u : 0u) |
                 (has && !fz && k == 0 && slot >= 0 ? 16u : 0u) | (has && fz && kp == 0 ? 32u : 0u) |
                 (has && kl == rows - 1 && rank < C - 1 ? 64u : 0u);
   }
@@ -493,101 +594,166 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
           const int j = fy ? pjp[pp] : ny - 1 - pjp[pp];
           cp_async8(&ig_ring[(size_t)sl * ny + pjp[pp]], &a.Ig[(int64_t)j * nx + i]);
         }
+        if (prole[pp] & 4u) {
+          // the y-inflow of this row's first pencil, ordinate by ordinate
+          T* dst = yin + ((size_t)sl * rows + (pkp[pp] - r0)) * MO;
+          const T* src = wrap0 + (int64_t)pk[pp] * nx + i;
+#pragma unroll
+          for (int m = 0; m < MO; ++m) {
+            if (periodic)
+              cp_async_val(&dst[m], src + m * wstride);
+            else
+              dst[m] = I_amb;
+          }
+        }
       }
     }
-    // a chunk of inflow rows two hyperplanes before it starts: the first
-    // column's ghosts of hyperplane c*CL_CHUNK are written on the one before
-    if (periodic && (d + 2) % CL_CHUNK == 0 && d + 2 < nplanes) load_inflow((d + 2) / CL_CHUNK);
     cp_async_commit();
   };
-  // The y-wrap values move between the staged chunks and the hyperplane
-  // buffers' first and last columns, one value per thread (rows*MO values;
-  // with fewer threads than that, a thread moves several), so that no pencil
-  // carries that work: the ghost column of hyperplane dn (in the buffer that
-  // is then the previous one), and the last column of hyperplane dp.
-  const int nmove = rows * MO;
-  auto fill_ghost_col = [&](T* buf, int dn) {
-    for (int t = threadIdx.x; t < nmove; t += TT) {
-      const int m = t / rows, kl = t - m * rows;
-      if (kl < nrows)
-        buf[(size_t)m * P + (kl + 1) * RS] =
-            periodic ? win[((size_t)(((dn / CL_CHUNK) & 1) * MO + m) * rows + kl) * CL_CHUNK +
-                           dn % CL_CHUNK]
-                     : I_amb;
-    }
-  };
-  auto copy_last_col = [&](const T* buf, int dp) {
-    if (!periodic) return;
-    for (int t = threadIdx.x; t < nmove; t += TT) {
-      const int m = t / rows, kl = t - m * rows;
-      if (kl < nrows)
-        wout[((size_t)(((dp / CL_CHUNK) & 1) * MO + m) * rows + kl) * CL_CHUNK + dp % CL_CHUNK] =
-            buf[(size_t)m * P + (kl + 1) * RS + ny];
-    }
-  };
-  if (periodic) load_inflow(0);
   for (int d = 0; d < CL_AHEAD - 1; ++d) prefetch(d);
-  cp_async_wait<CL_AHEAD - 2>();  // group 0, which holds chunk 0 of the inflow rows
   __syncthreads();
-  fill_ghost_col(buf1, 0);  // hyperplane 0 reads buf1 as its previous one
-  // the first cluster barrier also publishes the ambient-filled buffers
+  // the barriers' initialisation, the filled buffers and the first CL_RING
+  // fills announced, cluster-wide
+  if (helper && hl == 0 && rank > 0)
+    for (int s = 0; s < CL_RING; ++s) cl_arrive_expect(smem_u32(&full[s]), fill_bytes);
   cluster_arrive_release();
-  // the downstream CTA's buffers: this CTA's last row goes straight into their
-  // ghost row below the first row (a store before the barrier's release, not
-  // a load after its acquire, so its latency is not on the next hyperplane)
-  T* dn0 = rank < C - 1 ? cl.map_shared_rank(buf0, rank + 1) : nullptr;
-  T* dn1 = rank < C - 1 ? cl.map_shared_rank(buf1, rank + 1) : nullptr;
+  cluster_wait_acquire();
+  // shared-memory addresses (32-bit) of the hot loop's arrays; the
+  // downstream CTA's ring and full barriers, the upstream CTA's empty barriers
+  constexpr uint32_t TS = (uint32_t)sizeof(T);
+  constexpr uint32_t PS = (uint32_t)MP * TS;  // bytes per pencil
+  const uint32_t a_buf0 = smem_u32(buf0), a_buf1 = smem_u32(buf1), a_ring = smem_u32(ring);
+  const uint32_t a_yin = smem_u32(yin);
+  const uint32_t a_kz = smem_u32(kz), a_cxy = smem_u32(cxy), a_cwq = smem_u32(cwq);
+  const uint32_t a_dring = rank < C - 1 ? cl_mapa(a_ring, (unsigned)(rank + 1)) : 0u;
+  const uint32_t full_dn = rank < C - 1 ? cl_mapa(smem_u32(full), (unsigned)(rank + 1)) : 0u;
+  const uint32_t empty_up = rank > 0 ? cl_mapa(smem_u32(empty), (unsigned)(rank - 1)) : 0u;
+  bool failed = false;
   for (int d = 0; d < nplanes; ++d) {
     prefetch(d + CL_AHEAD - 1);  // an empty group past the last plane
-    T* cur = (d & 1) ? buf1 : buf0;
-    T* prev = (d & 1) ? buf0 : buf1;
-    T* dcur = (d & 1) ? dn1 : dn0;
     cp_async_wait<CL_AHEAD - 1>();  // this plane's group has landed
-    cluster_wait_acquire();
-    // the last column of hyperplane d-1 into its chunk; a chunk whose last
-    // column arrived on the previous hyperplane leaves for global memory
-    if (d > 0) copy_last_col(prev, d - 1);
-    if (periodic && d > 1 && (d - 1) % CL_CHUNK == 0) store_outflow((d - 1) / CL_CHUNK - 1);
-    if (d + 1 < nplanes) fill_ghost_col(cur, d + 1);
+    // the upstream CTA's last row of hyperplane d-1 is in the ring
+    if (helper && hl == 0 && rank > 0 && d > 0)
+      cl_wait(smem_u32(&full[(d - 1) % CL_RING]), (uint32_t)(((d - 1) / CL_RING) & 1), failed,
+              a.err);
+    __syncthreads();  // hyperplane d-1 complete in this CTA
+    if (helper) {
+      // the slot read on hyperplane d-1 awaits its next fill, and the
+      // upstream CTA may write it
+      if (hl == 0 && rank > 0 && d >= 2) {
+        cl_arrive_expect(smem_u32(&full[(d - 2) % CL_RING]), fill_bytes);
+        cl_arrive_remote(empty_up + 8u * ((d - 2) % CL_RING));
+      }
+      continue;
+    }
     const int sl = d % CL_AHEAD;
+    const int zslot = (d + CL_RING - 1) % CL_RING;
+    const int pslot = d % CL_RING;
+    const uint32_t a_prev = (d & 1) ? a_buf0 : a_buf1;
+    const uint32_t a_cur = (d & 1) ? a_buf1 : a_buf0;
     T gsv[PPT], qsv[PPT];
 #pragma unroll
     for (int pp = 0; pp < PPT; ++pp) {
-      const int jp = pjp[pp], kp = pkp[pp], qi = pqi[pp];
+      const int jp = pjp[pp], kp = pkp[pp];
+      const uint32_t qo = (uint32_t)pq[pp] * PS;
       const int ip = d - jp - kp;
       const bool act = (prole[pp] & 1u) && ip >= 0 && ip < nx;
+      const bool push = (prole[pp] & 64u) != 0;
+      // the downstream CTA has finished with what this slot held
+      if (push && d >= CL_RING)
+        cl_wait(smem_u32(&empty[pslot]), (uint32_t)((d / CL_RING - 1) & 1), failed, a.err);
+      const uint32_t apush = a_dring + (uint32_t)(pslot * ny + jp) * PS;
+      const uint32_t pbar = full_dn + 8u * pslot;
       T gs = (T)0, qs = (T)0;
       if (act) {
-        // the ground's (or the ambient) z-inflow below the first CTA's first row;
-        // the other CTAs' got it from the CTA below on the previous hyperplane
-        if ((prole[pp] & 2u) && kp == 0) {
-          const T z = fz ? (T)ig_ring[(size_t)sl * ny + jp] : I_amb;
+        const uint32_t ap = a_prev + qo;  // Ix at ap + m*TS
+        const uint32_t ac = a_cur + qo;
+        // y-inflow: the pencil to the left, or the prefetched wrap values
+        uint32_t ay = ap - PS;
+        if (prole[pp] & 4u) ay = a_yin + (uint32_t)((sl * rows + (kp - r0)) * MO) * TS;
+        // z-inflow: the row below in this CTA, else the ring; in the first
+        // CTA the ground's (or the ambient) intensity, put in the ring slot
+        uint32_t az = ap - (uint32_t)ny * PS;
+        if (prole[pp] & 2u) {
+          az = a_ring + (uint32_t)(zslot * ny + jp) * PS;
+          if (rank == 0) {
+            const T z = fz ? (T)ig_ring[(size_t)sl * ny + jp] : I_amb;
 #pragma unroll
-          for (int m = 0; m < MO; ++m) prev[(size_t)m * P + jp + 1] = z;
+            for (int m = 0; m < MO; ++m) sh_st(az + (uint32_t)m * TS, z);
+          } else {
+            // this thread's own acquire of the slot the helper waited for
+            cl_wait(smem_u32(&full[zslot]), (uint32_t)(((d - 1) / CL_RING) & 1), failed, a.err);
+          }
         }
         const T2 kab = kab_ring[(size_t)sl * S + pq[pp]];
-        const bool ground_out = (prole[pp] & 16u) != 0;
-        const int k = pk[pp];
+        const uint32_t akz = a_kz + (uint32_t)(pk[pp] * MO) * (2 * TS);
+        // The cell update of the group's ordinates, in batches of CB: every
+        // shared-memory load of a batch is issued before its stores, so the
+        // batch's updates overlap instead of waiting on one another's stores.
+        // Every per-ordinate offset is an immediate; a last-row pencil also
+        // stores its values into the downstream CTA's ring (one instance of
+        // the loop each way, so neither has a branch inside).
+        auto update = [&](auto push_tag) {
+          constexpr bool PUSH = decltype(push_tag)::value;
 #pragma unroll
-        for (int m = 0; m < MO; ++m) {
-          const T* pm = prev + (size_t)m * P + qi;
-          const T Ix = pm[0], Iy = pm[-1], Iz = pm[-RS];
-          const T num = fmat(izt[m * nz + k], Iz, fmat(ciy[m], Iy, fmat(cix[m], Ix, kab.y)));
-          const T v = sweep_quot(num, kab.x + cst[m * nz + k]);
-          cur[(size_t)m * P + qi] = v;
-          if (prole[pp] & 64u) dcur[(size_t)m * P + jp + 1] = v;
-          gs = fmat(cw[m], v, gs);
-          if (ground_out) qs = fmat(cwm[m], v, qs);
+          for (int m0 = 0; m0 < MO; m0 += CB) {
+            T Ix[CB], Iy[CB], Iz[CB], v[CB];
+#pragma unroll
+            for (int b = 0; b < CB; ++b) {
+              const uint32_t mo = (uint32_t)(m0 + b) * TS;
+              Ix[b] = sh_ld<T>(ap + mo);
+              Iy[b] = sh_ld<T>(ay + mo);
+              Iz[b] = sh_ld<T>(az + mo);
+            }
+#pragma unroll
+            for (int b = 0; b < CB; ++b) {
+              const uint32_t mo = (uint32_t)(m0 + b) * (2 * TS);
+              const T2 zc = sh_ld2<T2>(akz + mo);
+              const T2 xy = sh_ld2<T2>(a_cxy + mo);
+              const T num = fmat(zc.x, Iz[b], fmat(xy.y, Iy[b], fmat(xy.x, Ix[b], kab.y)));
+              v[b] = sweep_quot(num, kab.x + zc.y);
+            }
+#pragma unroll
+            for (int b = 0; b < CB; ++b) {
+              const T2 wq = sh_ld2<T2>(a_cwq + (uint32_t)(m0 + b) * (2 * TS));
+              gs = fmat(wq.x, v[b], gs);
+              qs = fmat(wq.y, v[b], qs);
+            }
+#pragma unroll
+            for (int b = 0; b < CB; ++b) {
+              const uint32_t mo = (uint32_t)(m0 + b) * TS;
+              sh_st(ac + mo, v[b]);
+              if (PUSH) cl_st_async(apush + mo, v[b], pbar);
+            }
+          }
+        };
+        if (push)
+          update(std::true_type{});
+        else
+          update(std::false_type{});
+        if (prole[pp] & 8u) {
+          // the y-outflow, read by the next sweep at the row's other end
+          T* wo = wrap0 + (int64_t)pk[pp] * nx + (fx ? ip : nx - 1 - ip);
+#pragma unroll
+          for (int m = 0; m < MO; ++m) wo[m * wstride] = sh_ld<T>(ac + (uint32_t)m * TS);
         }
-      } else if (prole[pp] & 1u) {
-        // before its first cell a pencil's x-inflow is the ambient intensity
+      } else {
+        if ((prole[pp] & 1u) && ip == -1) {
+          // the hyperplane before a pencil's first cell: its x-inflow there
+          // is the ambient intensity
+          const uint32_t ac = a_cur + qo;
 #pragma unroll
-        for (int m = 0; m < MO; ++m) cur[(size_t)m * P + qi] = I_amb;
+          for (int m = 0; m < MO; ++m) sh_st(ac + (uint32_t)m * TS, I_amb);
+        }
+        // an idle last-row pencil still delivers its share of the fill's bytes
+        if (push) {
+#pragma unroll
+          for (int m = 0; m < MO; ++m) cl_st_async(apush + (uint32_t)m * TS, I_amb, pbar);
+        }
       }
       gsv[pp] = gs;
       qsv[pp] = qs;
     }
-    cluster_arrive_release();
 #pragma unroll
     for (int pp = 0; pp < PPT; ++pp) {
       const int ip = d - pjp[pp] - pkp[pp];
@@ -601,15 +767,15 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
       }
     }
   }
-  cluster_wait_acquire();
-  // the last hyperplane's last column, then every chunk not yet flushed
-  copy_last_col(((nplanes - 1) & 1) ? buf1 : buf0, nplanes - 1);
-  __syncthreads();
-  if (periodic) {
-    for (int c = max(0, (nplanes - 1) / CL_CHUNK - 1); c <= (nplanes - 1) / CL_CHUNK; ++c)
-      if ((c + 1) * CL_CHUNK + 1 > nplanes - 1) store_outflow(c);
-  }
   cp_async_wait<0>();
+  // the last hyperplane's fill (read by no one) has landed too: no store of
+  // the upstream CTA is in flight to this CTA when it leaves
+  if (helper && hl == 0 && rank > 0)
+    cl_wait(smem_u32(&full[(nplanes - 1) % CL_RING]), (uint32_t)(((nplanes - 1) / CL_RING) & 1),
+            failed, a.err);
+  // no CTA leaves while another may still signal its barriers
+  cluster_arrive_release();
+  cluster_wait_acquire();
 }
 
 static const void* octant_cl_ptr(bool fp32, int Mo, int ppt) {
@@ -850,9 +1016,12 @@ static bool plan_cl(DomCtx* D, int force_C) {
       const int rows = (g.nz + C - 1) / C;
       if ((g.nz + rows - 1) / rows != C) continue;
       const int pencils = rows * g.ny;
-      const int ppt = pencils <= CL_MAX_THREADS_1 ? 1 : (pencils <= 2 * CL_MAX_THREADS_2 ? 2 : 0);
+      // pencil threads in whole warps, then the helper warp
+      const int t1 = (pencils + 31) / 32 * 32 + 32;
+      const int t2 = ((pencils + 1) / 2 + 31) / 32 * 32 + 32;
+      const int ppt = t1 <= CL_MAX_THREADS_1 ? 1 : (t2 <= CL_MAX_THREADS_2 ? 2 : 0);
       if (ppt == 0) continue;
-      const int threads = ((pencils + ppt - 1) / ppt + 31) / 32 * 32;
+      const int threads = ppt == 1 ? t1 : t2;
       const void* fn = octant_cl_ptr(D->fp32 != 0, Mo, ppt);
       if (!fn) continue;
       cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -941,6 +1110,19 @@ int dom_set_mode(void* h, int mode, int cluster_ctas) {
 }
 
 int dom_mode(void* h) { return ((DomCtx*)h)->mode; }
+int dom_launch_shape(void* h, int* out5) {
+  const DomCtx* D = (const DomCtx*)h;
+  if (D->mode != 8) {
+    fs_set_error("fs_dom_launch_shape: path 8 is not in use (path %d)", D->mode);
+    return FS_EARG;
+  }
+  out5[0] = D->cl_C;
+  out5[1] = D->cl_rows;
+  out5[2] = D->cl_threads;
+  out5[3] = (int)D->cl_smem;
+  out5[4] = D->groups;
+  return FS_OK;
+}
 
 int dom_set_groups(void* h, int groups) {
   DomCtx* D = (DomCtx*)h;
@@ -1149,6 +1331,7 @@ static int dom_iterate_dev(DomCtx* D, const ClArgs& base, int nslots, double ref
       if (D->timing) cudaEventRecord(D->ev0[queued], st);
       ClArgs ca = base;
       ca.done = D->dstate;
+      ca.err = D->dstate + 3;
       int rc = launch_cl_sweep(D, ca, st);
       if (rc != FS_OK) return rc;
       if (D->timing) cudaEventRecord(D->ev1[queued], st);
@@ -1171,6 +1354,11 @@ static int dom_iterate_dev(DomCtx* D, const ClArgs& base, int nslots, double ref
     }
     cudaMemcpyAsync(D->h_dstate, D->dstate, sizeof(int) * 4, cudaMemcpyDeviceToHost, st);
     if (fs_stream_wait(st) != FS_OK) return FS_ECUDA;
+    if (D->h_dstate[3]) {
+      fs_set_error("DOM sweep: a bounded wait for the row hand-off between the cluster's CTAs "
+                   "gave up");
+      return FS_ETIMEOUT;
+    }
     if (D->h_dstate[2] == 2) return FS_ENONFINITE;
     if (D->h_dstate[0]) { it = D->h_dstate[1]; break; }
     if (queued >= D->max_iter) { it = queued; break; }

@@ -134,6 +134,7 @@ int dom_begin(void* h, const double* Ts, const double* Tg, const double* as, con
 int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStream_t st);
 int dom_set_groups(void* h, int groups);
 int dom_mode(void* h);
+int dom_launch_shape(void* h, int* out5);
 int dom_set_precision(void* h, int fp32);
 int dom_load_intensity(void* h, const double* I_full, cudaStream_t st);
 int64_t dom_wrap_size(void* h);

@@ -421,6 +421,11 @@ int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
 int fs_dom_set_octant_groups(void* handle, int groups);
 /* The path in use (0 before the first solve or intensity load). */
 int fs_dom_sweep_mode(void* handle);
+/* Path 8's launch shape, once the path is resolved: out[0] CTAs per cluster,
+ * out[1] k' rows per CTA, out[2] threads per CTA, out[3] dynamic shared
+ * memory per CTA in bytes, out[4] clusters (ordinate groups) per octant.
+ * FS_EARG before the first solve or when another path is in use. */
+int fs_dom_launch_shape(void* handle, int* out5);
 /* fp32 = 1: the mixed-precision form of the sweep (path 8 with kappa,
  * kappa*B, intensities and octant partials in FP32 and the quotient of
  * __fdividef, about 2 ulp; G, the ground exchange and all outputs in FP64).
