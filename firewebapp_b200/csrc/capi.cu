@@ -110,8 +110,15 @@ static bool to_grid(const FsGrid* g, GridDev& d, const char* where) {
     fs_set_error("%s: invalid grid", where);
     return false;
   }
+  if ((long long)g->nx * g->ny * g->nz >= (1ll << 31)) {
+    fs_set_error("%s: grid of %lld cells (at most 2^31 - 1)", where,
+                 (long long)g->nx * g->ny * g->nz);
+    return false;
+  }
   d.nx = g->nx; d.ny = g->ny; d.nz = g->nz; d.dx = g->dx; d.dy = g->dy;
   d.dz = g->dz; d.da = g->d_above; d.db = g->d_below;
+  d.fnx = fastdiv_make((uint32_t)g->nx);
+  d.fny = fastdiv_make((uint32_t)g->ny);
   return true;
 }
 
@@ -695,6 +702,16 @@ int fs_dom_set_octant_groups(void* handle, int groups) {
   return check(dom_set_groups(handle, groups), "fs_dom_set_octant_groups");
 }
 int fs_dom_sweep_mode(void* handle) { return handle ? dom_mode(handle) : -1; }
+int fs_index_divide(uint32_t d, int64_t n, const uint32_t* x, uint32_t* q) {
+  if (d == 0 || n < 0 || (n > 0 && (!x || !q))) {
+    fs_set_error("fs_index_divide: divisor %u, count %lld", d, (long long)n);
+    return FS_EARG;
+  }
+  const FastDiv f = fastdiv_make(d);
+  for (int64_t t = 0; t < n; ++t) q[t] = fdiv(x[t], f);
+  return FS_OK;
+}
+
 int fs_dom_launch_shape(void* handle, int* out5) {
   if (!handle || !out5) {
     fs_set_error("fs_dom_launch_shape: null argument");

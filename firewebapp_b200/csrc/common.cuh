@@ -16,15 +16,54 @@
 
 #include "../../include/firestep.h"
 
+// Division by a run-time invariant divisor d >= 1 as a multiply-high, an
+// add and two shifts (Granlund and Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994, unsigned case with
+// l = ceil(log2 d)): exact for every 32-bit dividend.  Replaces the 64-bit
+// divisions a flat cell index would otherwise need to recover (i, j, k).
+struct FastDiv {
+  uint32_t d, m, s1, s2;
+};
+inline FastDiv fastdiv_make(uint32_t d) {
+  FastDiv f;
+  f.d = d;
+  uint32_t l = 0;
+  while (l < 32 && (1ull << l) < (unsigned long long)d) ++l;
+  f.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+  f.s1 = l < 1 ? l : 1;
+  f.s2 = l > 1 ? l - 1 : 0;
+  return f;
+}
+__host__ __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+#ifdef __CUDA_ARCH__
+  const uint32_t t = __umulhi(f.m, n);
+#else
+  const uint32_t t = (uint32_t)(((unsigned long long)f.m * n) >> 32);
+#endif
+  return (t + ((n - t) >> f.s1)) >> f.s2;
+}
+
 // Grid geometry as the kernels see it.  dz/da/db are device arrays of length nz
-// (dz_arr, d_face_above, d_face_below of Grid3D, spread_3d.py:180-188).
+// (dz_arr, d_face_above, d_face_below of Grid3D, spread_3d.py:180-188);
+// fnx/fny divide by nx and ny (grids hold fewer than 2^31 cells).
 struct GridDev {
   int nx, ny, nz;
   double dx, dy;
   const double* dz;
   const double* da;
   const double* db;
+  FastDiv fnx, fny;
 };
+
+// (i, j, k) of flat cell index c = (k*ny + j)*nx + i
+__device__ __forceinline__ void split_cell(uint32_t c, const FastDiv& fnx, const FastDiv& fny,
+                                           int& i, int& j, int& k) {
+  const uint32_t r = fdiv(c, fnx);
+  i = (int)(c - r * fnx.d);
+  const uint32_t kk = fdiv(r, fny);
+  j = (int)(r - kk * fny.d);
+  k = (int)kk;
+}
 
 __host__ __device__ inline int64_t cidx(const GridDev& g, int k, int j, int i) {
   return ((int64_t)k * g.ny + j) * (int64_t)g.nx + i;

@@ -339,7 +339,7 @@ struct ClArgs {
 // Slots of the ring through which a CTA hands the last row of each
 // hyperplane to the next CTA of the cluster: the upstream CTA runs up to
 // CL_RING - 2 hyperplanes ahead of the downstream one.
-#define CL_RING 4
+#define CL_RING 3
 // Threads per CTA (the helper warp included): one pencil per thread up to
 // CL_MAX_THREADS_1 (80 registers a thread), else two pencils per thread up to
 // CL_MAX_THREADS_2 (96 registers).

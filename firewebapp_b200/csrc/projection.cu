@@ -45,9 +45,23 @@
 #define PCG_SKIP(done) \
   if ((done) && *(done) != 0.0) return;
 
+// a level's extents with the divisions that recover (i, j, k) from a flat index
+struct Dims {
+  int nx, ny, nz;
+  FastDiv fnx, fny;
+};
+inline Dims dims_make(int nx, int ny, int nz) {
+  Dims D;
+  D.nx = nx; D.ny = ny; D.nz = nz;
+  D.fnx = fastdiv_make((uint32_t)nx);
+  D.fny = fastdiv_make((uint32_t)ny);
+  return D;
+}
+
 template <typename T>
 struct MGLevelT {
   int nx, ny, nz;
+  Dims dims;
   int64_t n;
   T *gx, *gy, *gz, *e, *dinv;  // conductances, per-cell term, 1/diag
   T *x, *b, *t, *s;            // correction, rhs, temps
@@ -147,15 +161,15 @@ __global__ void k_proj_level0(GridDev g, const double* __restrict__ rho, double*
 
 // diagonal of a face-conductance operator -> 1/diag
 template <typename T>
-__global__ void k_mg_diag(int nx, int ny, int nz, const T* __restrict__ gx,
+__global__ void k_mg_diag(Dims D, const T* __restrict__ gx,
                           const T* __restrict__ gy, const T* __restrict__ gz,
                           const T* __restrict__ e, T* dinv) {
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
   int64_t n = (int64_t)nx * ny * nz;
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
-  int i = (int)(c % nx);
-  int j = (int)((c / nx) % ny);
-  int k = (int)(c / ((int64_t)nx * ny));
+  int i, j, k;
+  split_cell((uint32_t)c, D.fnx, D.fny, i, j, k);
   int64_t sy = nx, sz = (int64_t)nx * ny;
   T d = e[c] + gx[c] + gy[c] + gz[c];
   if (i > 0) d += gx[c - 1];
@@ -197,14 +211,14 @@ __device__ __forceinline__ T mg_apply(int nx, int ny, int nz, const T* __restric
 template <typename T>
 __global__ void k_mg_coarsen(int fx, int fy, int fz, const T* __restrict__ gxf,
                              const T* __restrict__ gyf, const T* __restrict__ gzf,
-                             const T* __restrict__ ef, int cx, int cy, int cz, T* gxc,
+                             const T* __restrict__ ef, Dims DC, T* gxc,
                              T* gyc, T* gzc, T* ec, double scale_) {
+  const int cx = DC.nx, cy = DC.ny, cz = DC.nz;
   int64_t n = (int64_t)cx * cy * cz;
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= n) return;
-  int I = (int)(q % cx);
-  int J = (int)((q / cx) % cy);
-  int K = (int)(q / ((int64_t)cx * cy));
+  int I, J, K;
+  split_cell((uint32_t)q, DC.fnx, DC.fny, I, J, K);
   const int64_t fsy = fx, fsz = (int64_t)fx * fy;
   int i0 = 2 * I, i1 = min(2 * I + 1, fx - 1);
   int j0 = 2 * J, j1 = min(2 * J + 1, fy - 1);
@@ -293,12 +307,13 @@ __global__ void k_mg_coarse_solve(int n, const T* __restrict__ Ainv,
 
 // damped Jacobi sweep: xo = x + w (b - S x) / d ; x == null means x = 0
 template <typename T>
-__global__ void k_mg_jacobi(int nx, int ny, int nz, const T* __restrict__ gx,
+__global__ void k_mg_jacobi(Dims D, const T* __restrict__ gx,
                             const T* __restrict__ gy, const T* __restrict__ gz,
                             const T* __restrict__ e, const T* __restrict__ dinv,
                             const T* __restrict__ b, const T* __restrict__ x, T* xo,
                             double w_, const double* done) {
   PCG_SKIP(done);
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
   const T w = (T)w_;
   int64_t n = (int64_t)nx * ny * nz;
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -307,28 +322,28 @@ __global__ void k_mg_jacobi(int nx, int ny, int nz, const T* __restrict__ gx,
     xo[c] = w * b[c] * dinv[c];
     return;
   }
-  int i = (int)(c % nx);
-  int j = (int)((c / nx) % ny);
-  int k = (int)(c / ((int64_t)nx * ny));
+  int i, j, k;
+  split_cell((uint32_t)c, D.fnx, D.fny, i, j, k);
   T r = b[c] - mg_apply(nx, ny, nz, gx, gy, gz, e, x, c, i, j, k);
   xo[c] = x[c] + w * r * dinv[c];
 }
 
 // coarse rhs = sum over children of the fine residual (b - S x)
 template <typename T>
-__global__ void k_mg_restrict_residual(int fx, int fy, int fz, const T* __restrict__ gx,
+__global__ void k_mg_restrict_residual(Dims DF, const T* __restrict__ gx,
                                        const T* __restrict__ gy,
                                        const T* __restrict__ gz,
                                        const T* __restrict__ e, const T* __restrict__ b,
-                                       const T* __restrict__ x, int cx, int cy, int cz,
+                                       const T* __restrict__ x, Dims DC,
                                        T* bc, const double* done) {
   PCG_SKIP(done);
+  const int fx = DF.nx, fy = DF.ny, fz = DF.nz;
+  const int cx = DC.nx, cy = DC.ny, cz = DC.nz;
   int64_t n = (int64_t)cx * cy * cz;
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= n) return;
-  int I = (int)(q % cx);
-  int J = (int)((q / cx) % cy);
-  int K = (int)(q / ((int64_t)cx * cy));
+  int I, J, K;
+  split_cell((uint32_t)q, DC.fnx, DC.fny, I, J, K);
   const int64_t fsy = fx, fsz = (int64_t)fx * fy;
   T s = 0.0;
   for (int k = 2 * K; k <= min(2 * K + 1, fz - 1); ++k)
@@ -342,15 +357,14 @@ __global__ void k_mg_restrict_residual(int fx, int fy, int fz, const T* __restri
 
 // x_f += P x_c (piecewise constant)
 template <typename T>
-__global__ void k_mg_prolong(int fx, int fy, int fz, T* x, int cx, int cy,
+__global__ void k_mg_prolong(Dims DF, T* x, int cx, int cy,
                              const T* __restrict__ xc, const double* done) {
   PCG_SKIP(done);
-  int64_t n = (int64_t)fx * fy * fz;
+  int64_t n = (int64_t)DF.nx * DF.ny * DF.nz;
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
-  int i = (int)(c % fx);
-  int j = (int)((c / fx) % fy);
-  int k = (int)(c / ((int64_t)fx * fy));
+  int i, j, k;
+  split_cell((uint32_t)c, DF.fnx, DF.fny, i, j, k);
   x[c] += xc[((int64_t)(k >> 1) * cy + (j >> 1)) * cx + (i >> 1)];
 }
 
@@ -405,9 +419,8 @@ __global__ void k_proj_rhs(GridDev g, const double* __restrict__ u, const double
   double acc[1] = {0.0};
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)RED_BLOCKS * blockDim.x) {
-    int i = (int)(c % nx);
-    int j = (int)((c / nx) % ny);
-    int k = (int)(c / sz);
+    int i, j, k;
+    split_cell((uint32_t)c, g.fnx, g.fny, i, j, k);
     double div;
     if (i > 0) div = (u[c] - u[c - 1]) / g.dx;
     else div = (u[c] - u_in[(int64_t)k * ny + j]) / g.dx;
@@ -426,18 +439,18 @@ __global__ void k_proj_rhs(GridDev g, const double* __restrict__ u, const double
 }
 
 // q = S p and partial of p.q
-__global__ void k_pcg_matvec(int nx, int ny, int nz, const double* __restrict__ gx,
+__global__ void k_pcg_matvec(Dims D, const double* __restrict__ gx,
                              const double* __restrict__ gy, const double* __restrict__ gz,
                              const double* __restrict__ e, const double* __restrict__ p, double* q,
                              double* partial, const double* done) {
   PCG_SKIP(done);
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
   const int64_t n = (int64_t)nx * ny * nz;
   double acc[1] = {0.0};
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)RED_BLOCKS * blockDim.x) {
-    int i = (int)(c % nx);
-    int j = (int)((c / nx) % ny);
-    int k = (int)(c / ((int64_t)nx * ny));
+    int i, j, k;
+    split_cell((uint32_t)c, D.fnx, D.fny, i, j, k);
     double y = mg_apply(nx, ny, nz, gx, gy, gz, e, p, c, i, j, k);
     q[c] = y;
     acc[0] += p[c] * y;
@@ -455,9 +468,8 @@ __global__ void k_pcg_residual(GridDev g, const double* __restrict__ gx,
   double acc[1] = {0.0};
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)RED_BLOCKS * blockDim.x) {
-    int i = (int)(c % nx);
-    int j = (int)((c / nx) % ny);
-    int k = (int)(c / ((int64_t)nx * ny));
+    int i, j, k;
+    split_cell((uint32_t)c, g.fnx, g.fny, i, j, k);
     double rr = b[c] - mg_apply(nx, ny, nz, gx, gy, gz, e, x, c, i, j, k);
     r[c] = rr;
     double ra = rr / g.dz[k];
@@ -473,14 +485,13 @@ __global__ void k_pcg_update(GridDev g, const double* __restrict__ scal, double*
   PCG_SKIP(scal + SC_DONE);
   const int64_t n = ncells_dev(g);
   const double alpha = scal[0] / scal[1];
-  const int64_t sz = (int64_t)g.nx * g.ny;
   double acc[1] = {0.0};
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)RED_BLOCKS * blockDim.x) {
     x[c] += alpha * p[c];
     double rr = r[c] - alpha * q[c];
     r[c] = rr;
-    double ra = rr / g.dz[(int)(c / sz)];
+    double ra = rr / g.dz[(int)fdiv(fdiv((uint32_t)c, g.fnx), g.fny)];
     acc[0] += ra * ra;
   }
   block_sums_store<1>(acc, partial);
@@ -557,16 +568,16 @@ __global__ void k_fcg_alpha(double* scal) {
 
 // out = b - S x (level operator, any precision)
 template <typename T>
-__global__ void k_lp_residual(int nx, int ny, int nz, const T* __restrict__ gx,
+__global__ void k_lp_residual(Dims D, const T* __restrict__ gx,
                               const T* __restrict__ gy, const T* __restrict__ gz,
                               const T* __restrict__ e, const T* __restrict__ b,
                               const T* __restrict__ x, T* out) {
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
   int64_t n = (int64_t)nx * ny * nz;
   int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
-  int i = (int)(c % nx);
-  int j = (int)((c / nx) % ny);
-  int k = (int)(c / ((int64_t)nx * ny));
+  int i, j, k;
+  split_cell((uint32_t)c, D.fnx, D.fny, i, j, k);
   out[c] = b[c] - mg_apply(nx, ny, nz, gx, gy, gz, e, x, c, i, j, k);
 }
 
@@ -625,9 +636,8 @@ __global__ void k_div_resid_max(GridDev g, const double* __restrict__ u,
   bool nan = false;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x) {
-    int i = (int)(c % nx);
-    int j = (int)((c / nx) % ny);
-    int k = (int)(c / sz);
+    int i, j, k;
+    split_cell((uint32_t)c, g.fnx, g.fny, i, j, k);
     double div;
     if (i > 0) div = (u[c] - u[c - 1]) / g.dx;
     else div = (u[c] - u_in[(int64_t)k * ny + j]) / g.dx;
@@ -668,6 +678,7 @@ void* proj_create(const GridDev& g) {
   while (true) {
     MGLevel& lv = P->lev[L];
     lv.nx = nx; lv.ny = ny; lv.nz = nz; lv.n = (int64_t)nx * ny * nz;
+    lv.dims = dims_make(nx, ny, nz);
     lv.gx = dalloc(lv.n); lv.gy = dalloc(lv.n); lv.gz = dalloc(lv.n); lv.e = dalloc(lv.n);
     lv.dinv = dalloc(lv.n); lv.x = dalloc(lv.n); lv.b = dalloc(lv.n); lv.t = dalloc(lv.n);
     lv.s = dalloc(lv.n);
@@ -764,11 +775,11 @@ static void rebuild_levels(ProjCtx* P, MGLevelT<T>* lev, T* Ainv, cudaStream_t s
     if (l > 0) {
       MGLevelT<T>& pf = lev[l - 1];
       k_mg_coarsen<T><<<blocks_for(f.n, 128), 128, 0, st>>>(pf.nx, pf.ny, pf.nz, pf.gx, pf.gy,
-                                                           pf.gz, pf.e, f.nx, f.ny, f.nz, f.gx,
+                                                           pf.gz, pf.e, f.dims, f.gx,
                                                            f.gy, f.gz, f.e, 0.5);
       fs_count_launch();
     }
-    k_mg_diag<T><<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e,
+    k_mg_diag<T><<<blocks_for(f.n, 256), 256, 0, st>>>(f.dims, f.gx, f.gy, f.gz, f.e,
                                                        f.dinv);
     fs_count_launch();
   }
@@ -810,7 +821,7 @@ int proj_set_precision(void* h, int fp32) {
     for (int l = 0; l < P->nlev; ++l) {
       MGLevelT<float>& lv = P->lev32[l];
       const MGLevel& ld = P->lev[l];
-      lv.nx = ld.nx; lv.ny = ld.ny; lv.nz = ld.nz; lv.n = ld.n;
+      lv.nx = ld.nx; lv.ny = ld.ny; lv.nz = ld.nz; lv.n = ld.n; lv.dims = ld.dims;
       float** arrs[9] = {&lv.gx, &lv.gy, &lv.gz, &lv.e, &lv.dinv, &lv.x, &lv.b, &lv.t, &lv.s};
       for (float** a : arrs)
         if (cudaMalloc(a, sizeof(float) * (size_t)(lv.n > 0 ? lv.n : 1)) != cudaSuccess)
@@ -892,9 +903,8 @@ __device__ __forceinline__ void tail_jacobi(const MGLevelT<T>& f, const T* b, co
       xo[c] = w * b[c] * f.dinv[c];
       continue;
     }
-    int i = (int)(c % f.nx);
-    int j = (int)((c / f.nx) % f.ny);
-    int k = (int)(c / ((int64_t)f.nx * f.ny));
+    int i, j, k;
+    split_cell((uint32_t)c, f.dims.fnx, f.dims.fny, i, j, k);
     T r = b[c] - tail_apply(f, x, c, i, j, k);
     xo[c] = x[c] + w * r * f.dinv[c];
   }
@@ -912,7 +922,7 @@ __global__ void __launch_bounds__(MG_TAIL_THREADS, 1)
     const MGLevelT<T>& g = a.lev[q];
     const int64_t n = g.n;
     MGLevelT<T>& f = L[q];
-    f.nx = g.nx; f.ny = g.ny; f.nz = g.nz; f.n = n;
+    f.nx = g.nx; f.ny = g.ny; f.nz = g.nz; f.n = n; f.dims = g.dims;
     f.gx = sp; f.gy = sp + n; f.gz = sp + 2 * n; f.e = sp + 3 * n; f.dinv = sp + 4 * n;
     f.b = sp + 5 * n; f.x = sp + 6 * n; f.t = sp + 7 * n; f.s = sp + 8 * n;
     sp += 9 * n;
@@ -942,9 +952,8 @@ __global__ void __launch_bounds__(MG_TAIL_THREADS, 1)
     const MGLevelT<T>& cl = L[l + 1];
     const int64_t fsy = f.nx, fsz = (int64_t)f.nx * f.ny;
     for (int64_t q = threadIdx.x; q < cl.n; q += blockDim.x) {
-      int I = (int)(q % cl.nx);
-      int J = (int)((q / cl.nx) % cl.ny);
-      int K = (int)(q / ((int64_t)cl.nx * cl.ny));
+      int I, J, K;
+      split_cell((uint32_t)q, cl.dims.fnx, cl.dims.fny, I, J, K);
       T sum = 0.0;
       for (int k = 2 * K; k <= min(2 * K + 1, f.nz - 1); ++k)
         for (int j = 2 * J; j <= min(2 * J + 1, f.ny - 1); ++j)
@@ -983,9 +992,8 @@ __global__ void __launch_bounds__(MG_TAIL_THREADS, 1)
     const MGLevelT<T>& f = L[l];
     const MGLevelT<T>& cl = L[l + 1];
     for (int64_t c = threadIdx.x; c < f.n; c += blockDim.x) {
-      int i = (int)(c % f.nx);
-      int j = (int)((c / f.nx) % f.ny);
-      int k = (int)(c / ((int64_t)f.nx * f.ny));
+      int i, j, k;
+      split_cell((uint32_t)c, f.dims.fnx, f.dims.fny, i, j, k);
       f.t[c] += cl.x[((int64_t)(k >> 1) * cl.ny + (j >> 1)) * cl.nx + (i >> 1)];
     }
     __syncthreads();
@@ -1027,14 +1035,14 @@ static int vcycle(ProjCtx* P, MGLevelT<T>* lev, const T* Ainv, int l, const T* b
       ++nk;
     } else {
       // not coarsenable and too large for the dense solve: smoothing only
-      k_mg_jacobi<T><<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz,
+      k_mg_jacobi<T><<<blocks_for(f.n, 256), 256, 0, st>>>(f.dims, f.gx, f.gy, f.gz,
                                                           f.e, f.dinv, b, nullptr, x, MG_OMEGA,
                                                           done);
       ++nk;
       for (int s = 0; s < 8; ++s) {
         const T* src = (s & 1) ? f.t : x;
         T* dst = (s & 1) ? x : f.t;
-        k_mg_jacobi<T><<<blocks_for(f.n, 256), 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz,
+        k_mg_jacobi<T><<<blocks_for(f.n, 256), 256, 0, st>>>(f.dims, f.gx, f.gy, f.gz,
                                                             f.e, f.dinv, b, src, dst, MG_OMEGA,
                                                             done);
         ++nk;
@@ -1050,22 +1058,22 @@ static int vcycle(ProjCtx* P, MGLevelT<T>* lev, const T* Ainv, int l, const T* b
   const T* src = nullptr;
   for (int i = 0; i < nu; ++i) {
     T* dst = ((nu - 1 - i) % 2 == 0) ? f.t : f.s;
-    k_mg_jacobi<T><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, src,
+    k_mg_jacobi<T><<<nb, 256, 0, st>>>(f.dims, f.gx, f.gy, f.gz, f.e, f.dinv, b, src,
                                        dst, om, done);
     src = dst;
     ++nk;
   }
   k_mg_restrict_residual<T><<<blocks_for(cl.n, 128), 128, 0, st>>>(
-      f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, b, f.t, cl.nx, cl.ny, cl.nz, cl.b, done);
+      f.dims, f.gx, f.gy, f.gz, f.e, b, f.t, cl.dims, cl.b, done);
   ++nk;
   nk += vcycle<T>(P, lev, Ainv, l + 1, cl.b, cl.x, done, st);
-  k_mg_prolong<T><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.t, cl.nx, cl.ny, cl.x, done);
+  k_mg_prolong<T><<<nb, 256, 0, st>>>(f.dims, f.t, cl.nx, cl.ny, cl.x, done);
   ++nk;
   // post-smoothing from t, ending in x:  s, t, s, ... then x
   src = f.t;
   for (int i = 0; i < nu; ++i) {
     T* dst = (i == nu - 1) ? x : ((i % 2 == 0) ? f.s : f.t);
-    k_mg_jacobi<T><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv, b, src,
+    k_mg_jacobi<T><<<nb, 256, 0, st>>>(f.dims, f.gx, f.gy, f.gz, f.e, f.dinv, b, src,
                                        dst, om, done);
     src = dst;
     ++nk;
@@ -1133,7 +1141,7 @@ static int pcg_iteration(ProjCtx* P, double* x, cudaStream_t st) {
   k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 2, done);  // rz_new
   k_pcg_dir<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, P->pc_z, P->pc_p);
   k_set_scal<<<1, 1, 0, st>>>(P->scal, 0, 2);  // rz = rz_new
-  k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.nx, l0.ny, l0.nz, l0.gx, l0.gy, l0.gz,
+  k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.dims, l0.gx, l0.gy, l0.gz,
                                                    l0.e, P->pc_p, P->pc_q, P->partial, done);
   k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 1, done);  // pq
   k_pcg_update<<<RED_BLOCKS, RED_THREADS, 0, st>>>(P->g, P->scal, x, P->pc_r, P->pc_p, P->pc_q,
@@ -1204,12 +1212,12 @@ static void lp_presmooth(ProjCtx* P, cudaStream_t st) {
   const float* src = nullptr;
   for (int i = 0; i < P->nu; ++i) {
     float* dst = ((P->nu - 1 - i) % 2 == 0) ? f.t : f.s;
-    k_mg_jacobi<float><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv,
+    k_mg_jacobi<float><<<nb, 256, 0, st>>>(f.dims, f.gx, f.gy, f.gz, f.e, f.dinv,
                                            P->r32, src, dst, P->omega, nullptr);
     src = dst;
     fs_count_launch();
   }
-  k_lp_residual<float><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, P->r32, f.t,
+  k_lp_residual<float><<<nb, 256, 0, st>>>(f.dims, f.gx, f.gy, f.gz, f.e, P->r32, f.t,
                                            f.b);
   fs_count_launch();
 }
@@ -1231,7 +1239,7 @@ static int learned_precond(ProjCtx* P, cudaStream_t st) {
   const float* src = f.s;
   for (int i = 0; i < P->nu; ++i) {
     float* dst = (i == P->nu - 1) ? P->z32 : ((i % 2 == 0) ? f.t : f.x);
-    k_mg_jacobi<float><<<nb, 256, 0, st>>>(f.nx, f.ny, f.nz, f.gx, f.gy, f.gz, f.e, f.dinv,
+    k_mg_jacobi<float><<<nb, 256, 0, st>>>(f.dims, f.gx, f.gy, f.gz, f.e, f.dinv,
                                            P->r32, src, dst, P->omega, nullptr);
     src = dst;
     fs_count_launch();
@@ -1274,7 +1282,7 @@ static int fcg_iteration(ProjCtx* P, double* x, int it, cudaStream_t st) {
     fs_count_launch(); fs_count_launch();
   }
   k_fcg_dir<<<blocks_for(n, 256), 256, 0, st>>>(n, P->scal, P->pc_z, P->pc_p);
-  k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.nx, l0.ny, l0.nz, l0.gx, l0.gy, l0.gz,
+  k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.dims, l0.gx, l0.gy, l0.gz,
                                                    l0.e, P->pc_p, P->pc_q, P->partial, done);
   k_finish_sums<<<1, 32, 0, st>>>(P->partial, 1, P->scal + 1, done);  // p.q
   k_dot<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, P->pc_p, P->pc_r, P->partial, done);
@@ -1431,7 +1439,7 @@ int launch_div_resid_max(const GridDev& g, const double* u, const double* v, con
 int proj_apply(void* h, const double* x, double* y, cudaStream_t st) {
   ProjCtx* P = (ProjCtx*)h;
   MGLevel& l0 = P->lev[0];
-  k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.nx, l0.ny, l0.nz, l0.gx, l0.gy, l0.gz, l0.e,
+  k_pcg_matvec<<<RED_BLOCKS, RED_THREADS, 0, st>>>(l0.dims, l0.gx, l0.gy, l0.gz, l0.e,
                                                    x, y, P->partial, nullptr); fs_count_launch();
   return cuda_status();
 }

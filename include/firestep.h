@@ -421,6 +421,10 @@ int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
 int fs_dom_set_octant_groups(void* handle, int groups);
 /* The path in use (0 before the first solve or intensity load). */
 int fs_dom_sweep_mode(void* handle);
+/* The division by a run-time invariant divisor that the kernels use to split
+ * a flat cell index into (i, j, k): q[t] = x[t] / d for t < n, computed on the
+ * host by the same multiply-high formula.  FS_EARG for d == 0 or n < 0. */
+int fs_index_divide(uint32_t d, int64_t n, const uint32_t* x, uint32_t* q);
 /* Path 8's launch shape, once the path is resolved: out[0] CTAs per cluster,
  * out[1] k' rows per CTA, out[2] threads per CTA, out[3] dynamic shared
  * memory per CTA in bytes, out[4] clusters (ordinate groups) per octant.

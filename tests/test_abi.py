@@ -53,3 +53,23 @@ def test_ctx_create_rejects_an_invalid_case_without_a_gpu():
     assert L.fs_ctx_create(ctypes.byref(desc), ctypes.byref(init), ctypes.byref(h)) == 1
     assert h.value is None
     assert b"invalid case description" in L.fs_last_error()
+
+
+def test_index_division_is_exact():
+    """The multiply-high division the kernels use to split flat cell indices
+    (fs_index_divide runs the same formula on the host) equals integer
+    division: every divisor up to 4096 against edge and random dividends,
+    and large divisors against the full 32-bit range."""
+    import numpy as np
+    from firewebapp_b200 import _lib
+    lib = _lib.lib()
+    rng = np.random.default_rng(7)
+    edge = np.array([0, 1, 2, 3, 2**31 - 1, 2**31, 2**32 - 2, 2**32 - 1], dtype=np.uint64)
+    for d in list(range(1, 4097)) + [65535, 65536, 65537, 2**31 - 1, 2**31, 2**32 - 1]:
+        x = np.concatenate([edge, rng.integers(0, 2**32, 64, dtype=np.uint64),
+                            np.arange(3 * d, dtype=np.uint64)[:256] if d < 4097 else edge])
+        x = x.astype(np.uint32)
+        q = np.empty_like(x)
+        assert lib.fs_index_divide(d, x.size, x.ctypes.data, q.ctypes.data) == 0
+        assert np.array_equal(q, x // np.uint32(d)), d
+    assert lib.fs_index_divide(0, 1, x.ctypes.data, q.ctypes.data) != 0
