@@ -425,8 +425,11 @@ __device__ __forceinline__ bool cl_try_wait(uint32_t addr, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase of the given parity; a thread whose wait gave up
-// records it in *err and waits no more (the sweep's results are then not to
-// be trusted, and the host reports FS_ETIMEOUT).
+// records it in *err and from then on neither waits nor signals nor stores
+// into the ring (so no barrier phase is re-armed before it completed, and no
+// bytes arrive for a phase nobody announced); its neighbours' waits then give
+// up in turn, every CTA reaches the final cluster barrier, and the host
+// reports FS_ETIMEOUT (the sweep's results are not to be trusted).
 __device__ __forceinline__ void cl_wait(uint32_t addr, uint32_t parity, bool& failed, int* err) {
   if (failed) return;
   for (int it = 0; it < CL_WAIT_LIMIT; ++it)
@@ -640,7 +643,9 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
     if (helper) {
       // the slot read on hyperplane d-1 awaits its next fill, and the
       // upstream CTA may write it
-      if (hl == 0 && rank > 0 && d >= 2) {
+      // (after a wait that gave up, no barrier is touched again: a phase that
+      // did not complete is never re-armed)
+      if (hl == 0 && rank > 0 && d >= 2 && !failed) {
         cl_arrive_expect(smem_u32(&full[(d - 2) % CL_RING]), fill_bytes);
         cl_arrive_remote(empty_up + 8u * ((d - 2) % CL_RING));
       }
@@ -727,7 +732,7 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
             }
           }
         };
-        if (push)
+        if (push && !failed)
           update(std::true_type{});
         else
           update(std::false_type{});
@@ -746,7 +751,7 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
           for (int m = 0; m < MO; ++m) sh_st(ac + (uint32_t)m * TS, I_amb);
         }
         // an idle last-row pencil still delivers its share of the fill's bytes
-        if (push) {
+        if (push && !failed) {
 #pragma unroll
           for (int m = 0; m < MO; ++m) cl_st_async(apush + (uint32_t)m * TS, I_amb, pbar);
         }
