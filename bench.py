@@ -46,7 +46,7 @@ METRIC = "3D solver cell-steps/s on 1 B200 (plain FP64 Tier-3 step)"
 UNIT = "cell-steps/s"
 WORKLOAD = "tier3_step_400x120x60_S8_fp64"
 # measured DRAM bytes per cell of one launch (see the traffic comment in main)
-TRAFFIC_PER_CELL = {"dom_sweep": (16.7488e6 + 3.00672e6) / 720000.0}
+TRAFFIC_PER_CELL = {"dom_sweep": (16.780544e6 + 4.06528e6) / 720000.0}
 
 
 def _peaks():
