@@ -175,6 +175,7 @@ SIGNATURES = {
     "fs_dom_set_sweep_mode": (I, [P, I, I]),
     "fs_dom_sweep_mode": (I, [P]),
     "fs_dom_launch_shape": (I, [P, P]),
+    "fs_dom_set_wait_test": (I, [P, I]),
     "fs_index_divide": (I, [C.c_uint32, C.c_int64, P, P]),
     "fs_dom_set_octant_groups": (I, [P, I]),
     "fs_dom_set_precision": (I, [P, I]),

@@ -99,6 +99,8 @@ static int check(int st, const char* where) {
     fs_set_error("%s: non-finite value", where);
   else if (st == FS_ENOCONV)
     fs_set_error("%s: solver did not converge", where);
+  else if (st == FS_ETIMEOUT)
+    fs_set_error("%s: a bounded device wait gave up (results of that call not valid)", where);
   else
     fs_set_error("%s: status %d", where, st);
   return st;
@@ -710,6 +712,11 @@ int fs_index_divide(uint32_t d, int64_t n, const uint32_t* x, uint32_t* q) {
   const FastDiv f = fastdiv_make(d);
   for (int64_t t = 0; t < n; ++t) q[t] = fdiv(x[t], f);
   return FS_OK;
+}
+
+int fs_dom_set_wait_test(void* handle, int plane) {
+  if (!handle) return check(FS_EARG, "fs_dom_set_wait_test");
+  return dom_set_wait_test(handle, plane);
 }
 
 int fs_dom_launch_shape(void* handle, int* out5) {

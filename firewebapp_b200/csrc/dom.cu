@@ -55,6 +55,7 @@ struct DomCtx {
   int mode_req, force_C;      // requested path (0 auto) and cluster size (0 auto)
   int groups;                 // ordinate groups per octant (clusters per octant)
   int force_groups;           // requested groups (0 automatic)
+  int withhold_plane;         // test switch: hyperplane whose ring fill is withheld (-1 none)
   int fp32;                   // single-precision sweep (path 8)
   // path 8 buffers (FP64 or FP32, by fp32): (kappa, kappa*B) per cell, octant
   // partial G (8*groups x N), octant partial ground flux (8*groups x Ny*Nx),
@@ -331,6 +332,7 @@ struct ClArgs {
   unsigned down_slots;  // 4 bits per octant: ground-flux slot, 15 = upward octant
   const int* done;  // device flag: nonzero = the source iteration has converged, do nothing
   int* err;         // device flag: set when a bounded hand-off wait gave up
+  int withhold;     // test switch: the first CTA withholds its fill of this hyperplane (-1 none)
 };
 // Inputs (kappa, kappa*B, the ground intensity and the y-inflow of a row's
 // first pencil) arrive this many hyperplanes ahead through cp.async commit
@@ -654,6 +656,8 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
     const int sl = d % CL_AHEAD;
     const int zslot = (d + CL_RING - 1) % CL_RING;
     const int pslot = d % CL_RING;
+    // (test switch: a fill that never arrives, so the next CTA's bounded wait runs out)
+    const bool hold = rank == 0 && d == a.withhold;
     const uint32_t a_prev = (d & 1) ? a_buf0 : a_buf1;
     const uint32_t a_cur = (d & 1) ? a_buf1 : a_buf0;
     T gsv[PPT], qsv[PPT];
@@ -732,7 +736,7 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
             }
           }
         };
-        if (push && !failed)
+        if (push && !failed && !hold)
           update(std::true_type{});
         else
           update(std::false_type{});
@@ -751,7 +755,7 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
           for (int m = 0; m < MO; ++m) sh_st(ac + (uint32_t)m * TS, I_amb);
         }
         // an idle last-row pencil still delivers its share of the fill's bytes
-        if (push && !failed) {
+        if (push && !failed && !hold) {
 #pragma unroll
           for (int m = 0; m < MO; ++m) cl_st_async(apush + (uint32_t)m * TS, I_amb, pbar);
         }
@@ -926,6 +930,7 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   cudaMemcpy(D->w, w, sizeof(double) * M, cudaMemcpyHostToDevice);
   D->I = nullptr; D->kb = nullptr; D->Goct = nullptr; D->Qoct = nullptr; D->wrap = nullptr;
   D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1; D->force_groups = 0;
+  D->withhold_plane = -1;
   D->fp32 = 0; D->cl_ppt = 1; D->cl_waves = 0; D->begun = 0; D->pend_I_amb = 0.0;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemset(D->G, 0, sizeof(double) * N);
@@ -1115,6 +1120,10 @@ int dom_set_mode(void* h, int mode, int cluster_ctas) {
 }
 
 int dom_mode(void* h) { return ((DomCtx*)h)->mode; }
+int dom_set_wait_test(void* h, int plane) {
+  ((DomCtx*)h)->withhold_plane = plane < 0 ? -1 : plane;
+  return FS_OK;
+}
 int dom_launch_shape(void* h, int* out5) {
   const DomCtx* D = (const DomCtx*)h;
   if (D->mode != 8) {
@@ -1437,6 +1446,7 @@ int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStre
     ca.ox = D->ox; ca.oy = D->oy; ca.oz = D->oz; ca.w = D->w; ca.Ig = D->Ig_out;
     ca.C = D->cl_C; ca.rows = D->cl_rows; ca.periodic = 1; ca.groups = D->groups;
     ca.down_slots = 0;
+    ca.withhold = D->withhold_plane;
     int nslots = 0;
     for (int o = 0; o < 8; ++o) {
       ca.down_slots |= (unsigned)(D->down_slot[o] >= 0 ? D->down_slot[o] : 15) << (4 * o);

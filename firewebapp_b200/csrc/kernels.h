@@ -135,6 +135,7 @@ int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStre
 int dom_set_groups(void* h, int groups);
 int dom_mode(void* h);
 int dom_launch_shape(void* h, int* out5);
+int dom_set_wait_test(void* h, int plane);
 int dom_set_precision(void* h, int fp32);
 int dom_load_intensity(void* h, const double* I_full, cudaStream_t st);
 int64_t dom_wrap_size(void* h);

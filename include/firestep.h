@@ -407,8 +407,9 @@ double* fs_dom_intensity(void* handle);
  * cluster shape fits the grid, else path 3), 3 one launch per hyperplane
  * over all ordinates with the full intensity field stored (any quadrature,
  * FP64 only), 8 octant clusters: one thread-block cluster per octant (or per
- * half of its ordinates), the cluster's CTAs splitting the k' rows, a cluster
- * barrier per hyperplane, one or two pencils per thread, planned so that all
+ * half of its ordinates), the cluster's CTAs splitting the k' rows and
+ * handing each hyperplane's last row to the next CTA through a ring in its
+ * shared memory, one or two pencils per thread, planned so that all
  * clusters are resident at once where the part allows it; cluster_ctas 0 =
  * automatic, else CTAs per octant (1..16).  Only before the first solve or
  * intensity load.  Path 8 computes the numerator with fused multiply-adds
@@ -425,6 +426,13 @@ int fs_dom_sweep_mode(void* handle);
  * a flat cell index into (i, j, k): q[t] = x[t] / d for t < n, computed on the
  * host by the same multiply-high formula.  FS_EARG for d == 0 or n < 0. */
 int fs_index_divide(uint32_t d, int64_t n, const uint32_t* x, uint32_t* q);
+/* Test switch for the bounded waits of path 8's row hand-off: with plane >= 0
+ * the first CTA of every octant cluster withholds its ring fill of that
+ * hyperplane, so the next CTA's wait for it runs out; the sweep then stops
+ * all hand-off traffic, every CTA finishes, and the solve returns
+ * FS_ETIMEOUT with the object still usable.  plane < 0 (the default) turns
+ * it off.  No counterpart in the reference. */
+int fs_dom_set_wait_test(void* handle, int plane);
 /* Path 8's launch shape, once the path is resolved: out[0] CTAs per cluster,
  * out[1] k' rows per CTA, out[2] threads per CTA, out[3] dynamic shared
  * memory per CTA in bytes, out[4] clusters (ordinate groups) per octant.
@@ -523,7 +531,8 @@ typedef struct FsCaseDesc {
   /* soil column (soil_3d.py:73-103): host arrays of n_soil */
   int n_soil;
   const double *soil_dz, *soil_d_above, *soil_d_below;
-  /* solver options: form 0 plain FP64, 1 mixed (FP32 DOM sweep and V-cycle);
+  /* solver options: form 0 plain FP64, 1 mixed (FP32 DOM sweep, V-cycle and
+   * chemistry/transport sub-steps);
    * the CG tolerance and iteration cap of each pressure solve; overlap_dom 1
    * runs the DOM solve on a second stream concurrently with momentum, the
    * projection and k-epsilon (results identical either way) */

@@ -85,3 +85,49 @@ def test_learned_stall_falls_back_and_converges():
             assert st["learned_iters"] >= 3 and st["vcycle_iters"] >= 1
     assert fell >= 1 and fcg_stats(s)["fallbacks_total"] == fell
     s.close()
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_dom_hand_off_wait_runs_out_with_status_4(fp32):
+    """Path 8's CTAs wait for one another's rows with bounded waits.  With the
+    test switch one CTA withholds a row (a fill that nothing else sends), the
+    next CTA's wait runs out, the solve returns FS_ETIMEOUT (4) instead of
+    hanging, and the same object then solves normally."""
+    from gpu_helpers import Grid, call, dev, host, lib, stream
+    from firewebapp_b200._lib import dbl_array, ptr
+    from firewebapp_b200.quadrature import level_symmetric
+    om, wq = level_symmetric(8)
+    nz, ny, nx = 29, 40, 48
+    rng = np.random.default_rng(3)
+    g = Grid(nz, ny, nx, 0.5, 0.5, np.full(nz, 0.1))
+    h = C.c_void_p()
+    call("fs_dom_create", g.ref, om.shape[0], dbl_array(om[:, 0]), dbl_array(om[:, 1]),
+         dbl_array(om[:, 2]), dbl_array(wq), 0.5, C.byref(h))
+    shape = (nz, ny, nx)
+    Ts = dev(300.0 + 900.0 * rng.random(shape) ** 4)
+    Tg = dev(300.0 + 1500.0 * rng.random(shape) ** 6)
+    a = dev(np.where(rng.random(shape) < 0.3, 0.002 * rng.random(shape), 0.0))
+    zero = dev(np.zeros(shape))
+    M = dev(0.05 + 0.1 * rng.random(shape))
+    rho = dev(np.ones(shape))
+    Tsoil = dev(np.full((ny, nx), 300.0))
+    qs, qg = torch.zeros_like(Ts), torch.zeros_like(Ts)
+    qsoil = torch.zeros((ny, nx), dtype=torch.float64, device="cuda")
+
+    def solve():
+        return lib().fs_dom_solve(h, ptr(Ts), ptr(Tg), ptr(a), ptr(zero), 5000.0, 300.0,
+                                  ptr(Tsoil), ptr(zero), ptr(rho), ptr(M), ptr(qs), ptr(qg),
+                                  ptr(qsoil), stream())
+    try:
+        if fp32:
+            call("fs_dom_set_precision", h, 1)
+        call("fs_dom_set_sweep_mode", h, 8, 0)
+        assert solve() == 0
+        call("fs_dom_set_wait_test", h, 5)
+        assert solve() == 4
+        assert b"gave up" in lib().fs_last_error()
+        call("fs_dom_set_wait_test", h, -1)
+        assert solve() == 0
+        assert np.all(np.isfinite(host(qs))) and np.all(np.isfinite(host(qg)))
+    finally:
+        lib().fs_dom_destroy(h)
