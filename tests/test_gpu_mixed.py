@@ -72,3 +72,17 @@ def test_mixed_form_full_run_within_two_percent(form):
     ros_ref = np.polyfit(ref["t"][okr], ref["lead_x_Ts600"][okr], 1)[0]
     assert abs(ros - ros_ref) <= 0.02 * ros_ref, (ros, ros_ref)
     assert abs(max(hrr) - ref["hrr_peak_x"].max()) <= 0.02 * ref["hrr_peak_x"].max()
+
+
+def test_compare_forms_on_workload_geometry():
+    """compare_forms on a 40-cell-long slice of the 400 x 120 x 60 workload
+    with a seeded wind and moisture: every field of the mixed form within the
+    same bound of the FP64 form after ten steps."""
+    from firewebapp_b200.cases import learned_cases
+    from firewebapp_b200.compare_forms import compare_steps
+    case = learned_cases(1, seed0=300, nx=40)[0]
+    errs = compare_steps(case, steps=(10,))
+    assert list(errs) == [10]
+    print("workload slice, mixed vs fp64 after 10 steps:",
+          {k: f"{v:.2e}" for k, v in errs[10].items()})
+    assert all(v <= TOL for v in errs[10].values()), errs[10]
