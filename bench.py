@@ -6,8 +6,8 @@ dz = 0.0625 m, DOM S8 with 80 ordinates, U10 = 6 m/s, moisture 0.06,
 rho_b = 0.35 kg/m^3, 16 bed particles per surface cell, seeded jitter), plain
 FP64 path, projection tolerance 1e-6 (the reference's production default).
 Synthetic initial state built from the case deck (no dataset exists for this
-solver).  Inputs exceed L2 (state ~0.7 GB + DOM intensities 1.84 GB), so no
-L2 flush is needed between steps.
+solver).  Inputs exceed L2 (state ~0.7 GB, the DOM's octant partial G fields
+0.18 GB), so no L2 flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
