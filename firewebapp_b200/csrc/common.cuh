@@ -55,6 +55,24 @@ struct GridDev {
   FastDiv fnx, fny;
 };
 
+// Set-up work (copies of host arrays, clearing of new buffers) runs on a
+// private non-blocking stream that is synchronised before the set-up returns:
+// it neither waits for nor disturbs other threads' streams, one of which may
+// be capturing a CUDA graph (a cudaDeviceSynchronize or a legacy default
+// stream operation would then fail or break that capture).
+struct SetupStream {
+  cudaStream_t s = nullptr;
+  SetupStream() {
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) s = nullptr;
+  }
+  ~SetupStream() {
+    if (s) cudaStreamDestroy(s);
+  }
+  SetupStream(const SetupStream&) = delete;
+  SetupStream& operator=(const SetupStream&) = delete;
+  bool sync() const { return s && cudaStreamSynchronize(s) == cudaSuccess; }
+};
+
 // (i, j, k) of flat cell index c = (k*ny + j)*nx + i
 __device__ __forceinline__ void split_cell(uint32_t c, const FastDiv& fnx, const FastDiv& fny,
                                            int& i, int& j, int& k) {

@@ -922,19 +922,20 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   D->hox.assign(ox, ox + M); D->hoy.assign(oy, oy + M); D->hoz.assign(oz, oz + M);
   D->hw.assign(w, w + M);
   int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
+  SetupStream ss;
   cudaMalloc(&D->ox, sizeof(double) * M); cudaMalloc(&D->oy, sizeof(double) * M);
   cudaMalloc(&D->oz, sizeof(double) * M); cudaMalloc(&D->w, sizeof(double) * M);
-  cudaMemcpy(D->ox, ox, sizeof(double) * M, cudaMemcpyHostToDevice);
-  cudaMemcpy(D->oy, oy, sizeof(double) * M, cudaMemcpyHostToDevice);
-  cudaMemcpy(D->oz, oz, sizeof(double) * M, cudaMemcpyHostToDevice);
-  cudaMemcpy(D->w, w, sizeof(double) * M, cudaMemcpyHostToDevice);
+  cudaMemcpyAsync(D->ox, ox, sizeof(double) * M, cudaMemcpyHostToDevice, ss.s);
+  cudaMemcpyAsync(D->oy, oy, sizeof(double) * M, cudaMemcpyHostToDevice, ss.s);
+  cudaMemcpyAsync(D->oz, oz, sizeof(double) * M, cudaMemcpyHostToDevice, ss.s);
+  cudaMemcpyAsync(D->w, w, sizeof(double) * M, cudaMemcpyHostToDevice, ss.s);
   D->I = nullptr; D->kb = nullptr; D->Goct = nullptr; D->Qoct = nullptr; D->wrap = nullptr;
   D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1; D->force_groups = 0;
   D->withhold_plane = -1;
   D->fp32 = 0; D->cl_ppt = 1; D->cl_waves = 0; D->begun = 0; D->pend_I_amb = 0.0;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
-  cudaMemset(D->G, 0, sizeof(double) * N);
-  cudaMemset(D->Gp, 0, sizeof(double) * N);
+  cudaMemsetAsync(D->G, 0, sizeof(double) * N, ss.s);
+  cudaMemsetAsync(D->Gp, 0, sizeof(double) * N, ss.s);
   cudaMalloc(&D->ks, sizeof(double) * N); cudaMalloc(&D->kg, sizeof(double) * N);
   cudaMalloc(&D->ksafe, sizeof(double) * N); cudaMalloc(&D->B, sizeof(double) * N);
   cudaMalloc(&D->Ig_out, sizeof(double) * n2); cudaMalloc(&D->Isoil, sizeof(double) * n2);
@@ -950,9 +951,8 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
     cudaEventCreate(&D->ev0[q]);
     cudaEventCreate(&D->ev1[q]);
   }
-  // the copies and the clearing above run on the legacy default stream; wait
-  // for them here, since the solves run on streams that do not order after it
-  if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+  // the copies and the clearing above are complete before any solve is queued
+  if (!ss.sync() || cudaGetLastError() != cudaSuccess) {
     dom_destroy(D);
     return nullptr;
   }

@@ -699,11 +699,13 @@ void* proj_create(const GridDev& g) {
   cudaMallocHost(&P->h_scal, sizeof(double) * 16);
   P->p_prev = dalloc(n0);
   P->ir = dalloc(n0);
-  cudaMemset(P->p_prev, 0, sizeof(double) * n0);
-  cudaMemset(P->scal, 0, sizeof(double) * 16);
-  // the clearing runs on the legacy default stream; solves may run on streams
-  // that do not order after it
-  cudaDeviceSynchronize();
+  {
+    // cleared before any solve is queued, on a private stream
+    SetupStream ss;
+    cudaMemsetAsync(P->p_prev, 0, sizeof(double) * n0, ss.s);
+    cudaMemsetAsync(P->scal, 0, sizeof(double) * 16, ss.s);
+    ss.sync();
+  }
   P->have_prev = 0;
   P->last_iters = 0;
   P->iter_exec = nullptr;

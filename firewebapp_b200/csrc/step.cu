@@ -298,9 +298,9 @@ static void ctx_free(FsCtx* C) {
   delete C;
 }
 
-static bool copy_in(void* dst, const void* src, size_t bytes) {
+static bool copy_in(cudaStream_t st, void* dst, const void* src, size_t bytes) {
   if (!src) return false;
-  return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
 }
 
 extern "C" {
@@ -343,27 +343,28 @@ int fs_ctx_create(const FsCaseDesc* desc, const FsInitState* init, FsCtx** out) 
   C->n2 = (int64_t)c.nx * c.ny;
   const int64_t n = C->n, n2 = C->n2;
   bool ok = true;
+  SetupStream ss;  // the copies and clearing below, complete before the first step
   C->dz = dev_alloc(c.nz, ok); C->da = dev_alloc(c.nz, ok); C->db = dev_alloc(c.nz, ok);
-  ok = ok && copy_in(C->dz, c.dz, 8 * c.nz) && copy_in(C->da, c.d_above, 8 * c.nz) &&
-       copy_in(C->db, c.d_below, 8 * c.nz);
+  ok = ok && copy_in(ss.s, C->dz, c.dz, 8 * c.nz) && copy_in(ss.s, C->da, c.d_above, 8 * c.nz) &&
+       copy_in(ss.s, C->db, c.d_below, 8 * c.nz);
   C->g = FsGrid{c.nx, c.ny, c.nz, c.dx, c.dy, C->dz, C->da, C->db};
   for (int q = 0; q < NSLOT; ++q) C->f[q] = dev_alloc(n, ok);
   const double* init_fields[14] = {init->rho, init->u, init->v, init->w, init->T_g,
                                    init->Y_fuel, init->Y_O2, init->Y_H2O, init->T_s,
                                    init->alpha_s, init->k_turb, init->eps_turb, init->nu_t,
                                    init->phi};
-  for (int q = 0; q < 14 && ok; ++q) ok = copy_in(C->f[q], init_fields[q], 8 * n);
-  for (int q = 14; q < NSLOT && ok; ++q) ok = cudaMemset(C->f[q], 0, 8 * n) == cudaSuccess;
+  for (int q = 0; q < 14 && ok; ++q) ok = copy_in(ss.s, C->f[q], init_fields[q], 8 * n);
+  for (int q = 14; q < NSLOT && ok; ++q) ok = cudaMemsetAsync(C->f[q], 0, 8 * n, ss.s) == cudaSuccess;
   C->u_inlet = dev_alloc((int64_t)c.nz * c.ny, ok);
   C->sigma_x = dev_alloc(c.nx, ok);
-  ok = ok && copy_in(C->u_inlet, init->u_inlet, 8 * (size_t)c.nz * c.ny) &&
-       copy_in(C->sigma_x, init->sigma_x, 8 * (size_t)c.nx);
+  ok = ok && copy_in(ss.s, C->u_inlet, init->u_inlet, 8 * (size_t)c.nz * c.ny) &&
+       copy_in(ss.s, C->sigma_x, init->sigma_x, 8 * (size_t)c.nx);
   C->k_wall = dev_alloc(n2, ok); C->eps_wall = dev_alloc(n2, ok);
   C->zero2 = dev_alloc((int64_t)c.nz * c.ny, ok);
   if (ok) {
     std::vector<double> kw(n2, K_MIN), ew(n2, EPS_MIN);
-    ok = copy_in(C->k_wall, kw.data(), 8 * n2) && copy_in(C->eps_wall, ew.data(), 8 * n2) &&
-         cudaMemset(C->zero2, 0, 8 * (size_t)c.nz * c.ny) == cudaSuccess;
+    ok = copy_in(ss.s, C->k_wall, kw.data(), 8 * n2) && copy_in(ss.s, C->eps_wall, ew.data(), 8 * n2) &&
+         cudaMemsetAsync(C->zero2, 0, 8 * (size_t)c.nz * c.ny, ss.s) == cudaSuccess;
   }
   C->hcond_scratch = dev_alloc((int64_t)std::max(c.n_z_bed, 1) * n2, ok);
   C->max_scratch = dev_alloc(64, ok);
@@ -379,11 +380,11 @@ int fs_ctx_create(const FsCaseDesc* desc, const FsInitState* init, FsCtx** out) 
   C->q_in_soil = dev_alloc(n2, ok);
   C->soil_dz = dev_alloc(c.n_soil, ok); C->soil_da = dev_alloc(c.n_soil, ok);
   C->soil_db = dev_alloc(c.n_soil, ok);
-  ok = ok && copy_in(C->T_soil, init->T_soil, 8 * (size_t)c.n_soil * n2) &&
-       cudaMemset(C->q_in_soil, 0, 8 * n2) == cudaSuccess &&
-       copy_in(C->soil_dz, c.soil_dz, 8 * c.n_soil) &&
-       copy_in(C->soil_da, c.soil_d_above, 8 * c.n_soil) &&
-       copy_in(C->soil_db, c.soil_d_below, 8 * c.n_soil);
+  ok = ok && copy_in(ss.s, C->T_soil, init->T_soil, 8 * (size_t)c.n_soil * n2) &&
+       cudaMemsetAsync(C->q_in_soil, 0, 8 * n2, ss.s) == cudaSuccess &&
+       copy_in(ss.s, C->soil_dz, c.soil_dz, 8 * c.n_soil) &&
+       copy_in(ss.s, C->soil_da, c.soil_d_above, 8 * c.n_soil) &&
+       copy_in(ss.s, C->soil_db, c.soil_d_below, 8 * c.n_soil);
   // particles and segments
   C->np = init->n_particles;
   const double* pin[10] = {init->px, init->py, init->pz, init->m_solid, init->m_water,
@@ -391,7 +392,7 @@ int fs_ctx_create(const FsCaseDesc* desc, const FsInitState* init, FsCtx** out) 
                            init->m_char_max};
   for (int q = 0; q < 10 && ok; ++q) {
     C->pd[q] = dev_alloc(C->np, ok);
-    ok = ok && (C->np == 0 || copy_in(C->pd[q], pin[q], 8 * (size_t)C->np));
+    ok = ok && (C->np == 0 || copy_in(ss.s, C->pd[q], pin[q], 8 * (size_t)C->np));
   }
   if (ok && C->np > 0 && (!init->alive || !init->px || !init->py || !init->pz)) ok = false;
   if (ok) {
@@ -408,11 +409,11 @@ int fs_ctx_create(const FsCaseDesc* desc, const FsInitState* init, FsCtx** out) 
          cudaMalloc(&C->seg_cell, sizeof(int) * std::max<size_t>(segcell.size(), 1)) ==
              cudaSuccess &&
          cudaMalloc(&C->seg_of_cell, sizeof(int) * (size_t)n) == cudaSuccess;
-    ok = ok && (C->np == 0 || copy_in(C->alive, alive.data(), (size_t)C->np)) &&
-         (perm.empty() || copy_in(C->perm, perm.data(), sizeof(int) * perm.size())) &&
-         copy_in(C->seg_start, starts.data(), sizeof(int) * starts.size()) &&
-         (segcell.empty() || copy_in(C->seg_cell, segcell.data(), sizeof(int) * segcell.size())) &&
-         copy_in(C->seg_of_cell, soc.data(), sizeof(int) * (size_t)n);
+    ok = ok && (C->np == 0 || copy_in(ss.s, C->alive, alive.data(), (size_t)C->np)) &&
+         (perm.empty() || copy_in(ss.s, C->perm, perm.data(), sizeof(int) * perm.size())) &&
+         copy_in(ss.s, C->seg_start, starts.data(), sizeof(int) * starts.size()) &&
+         (segcell.empty() || copy_in(ss.s, C->seg_cell, segcell.data(), sizeof(int) * segcell.size())) &&
+         copy_in(ss.s, C->seg_of_cell, soc.data(), sizeof(int) * (size_t)n);
   }
   C->parts = FsBedParticles{C->pd[0], C->pd[1], C->pd[2], C->alive, C->pd[3], C->pd[4],
                             C->pd[5], C->pd[6], C->pd[7], C->pd[8], C->pd[9]};
@@ -430,7 +431,7 @@ int fs_ctx_create(const FsCaseDesc* desc, const FsInitState* init, FsCtx** out) 
              cudaEventCreateWithFlags(&C->ev_inputs, cudaEventDisableTiming) != cudaSuccess ||
              cudaEventCreateWithFlags(&C->ev_done, cudaEventDisableTiming) != cudaSuccess))
     ok = false;
-  if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
+  if (!ok || !ss.sync()) {
     cudaGetLastError();
     fs_set_error("fs_ctx_create: device allocation or copy failed");
     ctx_free(C);

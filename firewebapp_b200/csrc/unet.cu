@@ -850,12 +850,14 @@ int unet_create(int nz, int ny, int nx, void** out) {
     unet_destroy(U);
     return FS_ECUDA;
   }
-  cudaMemset(U->params, 0, sizeof(float) * np);
-  cudaMemset(U->am, 0, sizeof(float) * np);
-  cudaMemset(U->av, 0, sizeof(float) * np);
-  // the clearing runs on the legacy default stream; later work may run on
-  // streams that do not order after it
-  cudaDeviceSynchronize();
+  {
+    // cleared before any later work is queued, on a private stream
+    SetupStream ss;
+    cudaMemsetAsync(U->params, 0, sizeof(float) * np, ss.s);
+    cudaMemsetAsync(U->am, 0, sizeof(float) * np, ss.s);
+    cudaMemsetAsync(U->av, 0, sizeof(float) * np, ss.s);
+    ss.sync();
+  }
   *out = U;
   return cuda_status();
 }

@@ -7,6 +7,8 @@ that finds the first call's scratch contents.
 Collected last on purpose: it must pass in a fresh process and after the
 other GPU tests.
 """
+import gc
+
 import numpy as np
 import pytest
 import torch
@@ -39,13 +41,21 @@ def _run(entry, n, t, scratch=None):
     args = [n, ptr(t["rho"]), ptr(Tg), ptr(Yf), ptr(YO), ptr(t["k"]), ptr(t["e"]), ptr(t["YH"]),
             ptr(om), 0.34, 1100.0, 2e-3, 1, 1.3, 17e6, 0]
     torch.cuda.synchronize()
-    before = (torch.cuda.memory_allocated(), torch.cuda.memory_reserved())
-    if entry == "fs_edc":
-        st = L.fs_edc(*args, ptr(scratch), s)
-    else:
-        st = L.fs_edc_noalloc(*args, s)
-    torch.cuda.synchronize()
-    after = (torch.cuda.memory_allocated(), torch.cuda.memory_reserved())
+    # tensors left unreachable by earlier tests are freed now, and no
+    # collection runs between the two readings, so any change between them is
+    # the call's own
+    gc.collect()
+    gc.disable()
+    try:
+        before = (torch.cuda.memory_allocated(), torch.cuda.memory_reserved())
+        if entry == "fs_edc":
+            st = L.fs_edc(*args, ptr(scratch), s)
+        else:
+            st = L.fs_edc_noalloc(*args, s)
+        torch.cuda.synchronize()
+        after = (torch.cuda.memory_allocated(), torch.cuda.memory_reserved())
+    finally:
+        gc.enable()
     _lib.check(st, entry)
     return (Tg, Yf, YO, om), before, after
 
