@@ -126,6 +126,13 @@ __device__ __forceinline__ void cp_async_val(void* dst, const float* src) {
 __device__ __forceinline__ void st_cs(double* p, double v) {
   asm volatile("st.global.cs.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
 }
+// two adjacent values in one 16-byte (8-byte for FP32) streaming store
+__device__ __forceinline__ void st_cs2(double* p, double lo, double hi) {
+  asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(lo), "d"(hi) : "memory");
+}
+__device__ __forceinline__ void st_cs2(float* p, float lo, float hi) {
+  asm volatile("st.global.cs.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(lo), "f"(hi) : "memory");
+}
 __device__ __forceinline__ void st_cs(float* p, float v) {
   asm volatile("st.global.cs.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }
@@ -634,6 +641,14 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
   const uint32_t full_dn = rank < C - 1 ? cl_mapa(smem_u32(full), (unsigned)(rank + 1)) : 0u;
   const uint32_t empty_up = rank > 0 ? cl_mapa(smem_u32(empty), (unsigned)(rank - 1)) : 0u;
   bool failed = false;
+  // With an even nx a pencil's octant-partial G goes out in aligned pairs of
+  // x-adjacent cells, which it visits on consecutive hyperplanes: the first
+  // value of a pair waits in a register for the second (every pair
+  // completes, the first and last cells included).
+  const bool gpair = (nx & 1) == 0;
+  T gpend[PPT];
+#pragma unroll
+  for (int pp = 0; pp < PPT; ++pp) gpend[pp] = (T)0;
   for (int d = 0; d < nplanes; ++d) {
     prefetch(d + CL_AHEAD - 1);  // an empty group past the last plane
     cp_async_wait<CL_AHEAD - 1>();  // this plane's group has landed
@@ -768,7 +783,15 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
       const int ip = d - pjp[pp] - pkp[pp];
       if ((prole[pp] & 1u) && ip >= 0 && ip < nx) {
         const int i = fx ? ip : nx - 1 - ip;
-        st_cs(Go + prb[pp] + i, gsv[pp]);
+        if (!gpair) {
+          st_cs(Go + prb[pp] + i, gsv[pp]);
+        } else if (((i & 1) == 0) == fx) {
+          gpend[pp] = gsv[pp];  // first of its pair in visiting order
+        } else if (fx) {
+          st_cs2(Go + prb[pp] + (i - 1), gpend[pp], gsv[pp]);
+        } else {
+          st_cs2(Go + prb[pp] + i, gsv[pp], gpend[pp]);
+        }
         if (prole[pp] & 16u) {
           const int j = fy ? pjp[pp] : ny - 1 - pjp[pp];
           Qoct[(int64_t)slot * n2 + (int64_t)j * nx + i] = qsv[pp];

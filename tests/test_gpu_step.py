@@ -135,15 +135,18 @@ def test_workload_geometry_matches_reference(fixture, case_name, steps):
 
 def test_host_stepper_state_equals_device_state():
     """api.HostStepper (the e2e path: upload, step, download, with the early
-    fields downloaded on a copy stream from the DOM phase on) leaves in host
-    memory exactly the state that stepping the solver directly gives."""
+    fields downloaded on a copy stream from the DOM phase on, and the fields
+    no step writes not downloaded) leaves in host memory exactly the state
+    that stepping the solver directly gives."""
     import numpy as np
     from firewebapp_b200.api import HostStepper
     from firewebapp_b200.cases import TINY
     from firewebapp_b200.solver import Tier3Solver
     hs = HostStepper(TINY)
     ref = Tier3Solver(TINY)
-    for n in range(3):
+    # twelve steps cross a level-set reinitialisation (every tenth step), the
+    # only steps on which phi is written back
+    for n in range(12):
         # the caller changes its host state between steps: every field must
         # reach the device before the step reads it (the same change is made
         # to the directly stepped solver)
