@@ -594,50 +594,68 @@ struct DiffArgs {
   int clip;
 };
 
-// One thread per cell in 32 x 8 (x, y) tiles of one z-level (y-neighbours
-// from L1); the level's reciprocal spacings are computed once per block.
+// A block owns a 32 x 8 (x, y) tile and marches up a chunk of z-levels: each
+// thread keeps its column's values at k-1, k and k+1 of every field in
+// registers (the z-neighbours cost no loads) and reads the next level one
+// step ahead; x- and y-neighbours come from L1.  The chunk's reciprocal
+// spacings are computed once per block.  The arithmetic of each cell is the
+// one-thread-per-cell form's, expression for expression.
+#define TD_MAXKZ 64
 template <int NF>
 __global__ void __launch_bounds__(SP_TX * SP_TY, 4)
 k_turb_diff(GridDev g, DiffArgs a, const double* __restrict__ nu_t, double sc_t, double dt_sub,
-            double inv_dx2, double inv_dy2) {
-  __shared__ double rk[3];  // 1/dz, 1/da, 1/db of the block's level
+            double inv_dx2, double inv_dy2, int kz) {
+  __shared__ double rk[TD_MAXKZ][3];  // 1/dz, 1/da, 1/db of the chunk's levels
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int64_t sy = nx, sz = (int64_t)nx * ny;
-  const int k = blockIdx.z;
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    rk[0] = 1.0 / g.dz[k];
-    rk[1] = 1.0 / g.da[k];
-    rk[2] = 1.0 / g.db[k];
+  const int k0 = blockIdx.z * kz;
+  const int k1 = min(nz, k0 + kz);
+  const int tid = threadIdx.y * SP_TX + threadIdx.x;
+  for (int q = tid; q < k1 - k0; q += SP_TX * SP_TY) {
+    rk[q][0] = 1.0 / g.dz[k0 + q];
+    rk[q][1] = 1.0 / g.da[k0 + q];
+    rk[q][2] = 1.0 / g.db[k0 + q];
   }
   __syncthreads();
   const int i = blockIdx.x * SP_TX + threadIdx.x;
   const int j = blockIdx.y * SP_TY + threadIdx.y;
-  if (i >= nx || j >= ny) return;
-  const int64_t crow = (int64_t)k * sz + i;
-  const int64_t c = crow + (int64_t)j * sy;
-  const int64_t cjp = crow + wrapj(j + 1, ny) * sy, cjm = crow + wrapj(j - 1, ny) * sy;
-  const double inv_dz_k = rk[0];
-  const double inv_d_above = rk[1];
-  const double inv_d_below = rk[2];
-  const double D_t = nu_t[c] / sc_t;
+  if (i >= nx || j >= ny || k0 >= nz) return;
+  const int64_t col = (int64_t)j * sy + i;
+  const int64_t cjp0 = (int64_t)wrapj(j + 1, ny) * sy + i, cjm0 = (int64_t)wrapj(j - 1, ny) * sy + i;
+  double fL[NF], fC[NF];
 #pragma unroll
   for (int s = 0; s < NF; ++s) {
-    const double* __restrict__ f = a.f[s];
-    const double fc = f[c];
-    const double fxL = (i == 0) ? fc : f[c - 1];
-    const double fxR = (i == nx - 1) ? fc : f[c + 1];
-    const double fzL = (k == 0) ? fc : f[c - sz];
-    const double fzR = (k == nz - 1) ? fc : f[c + sz];
-    double d2x = (fxR - 2.0 * fc + fxL) * inv_dx2;
-    double d2y = (f[cjp] - 2.0 * fc + f[cjm]) * inv_dy2;
-    double d2z = ((fzR - fc) * inv_d_above - (fc - fzL) * inv_d_below) * inv_dz_k;
-    double df = D_t * (d2x + d2y + d2z) * dt_sub;
-    double nv = fc + df;
-    if (a.clip) {
-      if (nv < a.lo[s]) nv = a.lo[s];
-      if (nv > a.hi[s]) nv = a.hi[s];
+    fC[s] = a.f[s][(int64_t)k0 * sz + col];
+    fL[s] = (k0 == 0) ? fC[s] : a.f[s][(int64_t)(k0 - 1) * sz + col];
+  }
+  for (int k = k0; k < k1; ++k) {
+    const int64_t ks = (int64_t)k * sz;
+    const int64_t c = ks + col;
+    const double inv_dz_k = rk[k - k0][0];
+    const double inv_d_above = rk[k - k0][1];
+    const double inv_d_below = rk[k - k0][2];
+    const double D_t = nu_t[c] / sc_t;
+#pragma unroll
+    for (int s = 0; s < NF; ++s) {
+      const double* __restrict__ f = a.f[s];
+      const double fc = fC[s];
+      const double fxL = (i == 0) ? fc : f[c - 1];
+      const double fxR = (i == nx - 1) ? fc : f[c + 1];
+      const double fzL = fL[s];
+      const double fzR = (k == nz - 1) ? fc : f[c + sz];
+      double d2x = (fxR - 2.0 * fc + fxL) * inv_dx2;
+      double d2y = (f[ks + cjp0] - 2.0 * fc + f[ks + cjm0]) * inv_dy2;
+      double d2z = ((fzR - fc) * inv_d_above - (fc - fzL) * inv_d_below) * inv_dz_k;
+      double df = D_t * (d2x + d2y + d2z) * dt_sub;
+      double nv = fc + df;
+      if (a.clip) {
+        if (nv < a.lo[s]) nv = a.lo[s];
+        if (nv > a.hi[s]) nv = a.hi[s];
+      }
+      a.fo[s][c] = nv;
+      fL[s] = fc;
+      fC[s] = fzR;
     }
-    a.fo[s][c] = nv;
   }
 }
 
@@ -653,14 +671,23 @@ int launch_turb_diff(const GridDev& g, int nfield, const double* const* f, doubl
     a.lo[s] = clip ? lo[s] : 0.0;
     a.hi[s] = clip ? hi[s] : 0.0;
   }
-  const dim3 nb((g.nx + SP_TX - 1) / SP_TX, (g.ny + SP_TY - 1) / SP_TY, g.nz);
+  // z-chunks: about six blocks per SM of the 148, at least four levels each
+  const int tiles = ((g.nx + SP_TX - 1) / SP_TX) * ((g.ny + SP_TY - 1) / SP_TY);
+  int chunks = (6 * 148 + tiles - 1) / tiles;
+  if (chunks > g.nz) chunks = g.nz;
+  if (chunks < 1) chunks = 1;
+  int kz = (g.nz + chunks - 1) / chunks;
+  if (kz < 4) kz = g.nz < 4 ? g.nz : 4;
+  if (kz > TD_MAXKZ) kz = TD_MAXKZ;
+  chunks = (g.nz + kz - 1) / kz;
+  const dim3 nb((g.nx + SP_TX - 1) / SP_TX, (g.ny + SP_TY - 1) / SP_TY, chunks);
   const dim3 tb(SP_TX, SP_TY);
   const double ix2 = 1.0 / (g.dx * g.dx), iy2 = 1.0 / (g.dy * g.dy);
   switch (nfield) {
-    case 1: k_turb_diff<1><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
-    case 2: k_turb_diff<2><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
-    case 3: k_turb_diff<3><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
-    default: k_turb_diff<4><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2); break;
+    case 1: k_turb_diff<1><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2, kz); break;
+    case 2: k_turb_diff<2><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2, kz); break;
+    case 3: k_turb_diff<3><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2, kz); break;
+    default: k_turb_diff<4><<<nb, tb, 0, st>>>(g, a, nu_t, sc_t, dt_sub, ix2, iy2, kz); break;
   }
   fs_count_launch();
   return cuda_status();
