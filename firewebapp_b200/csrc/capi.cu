@@ -11,6 +11,9 @@
 #include <atomic>
 
 static thread_local char g_err[512] = "";
+// set when a message was written since the last status check consumed one, so
+// that check() keeps a specific message instead of a generic one
+static thread_local bool g_err_fresh = false;
 static std::atomic<unsigned long long> g_launches{0};
 
 void fs_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -20,6 +23,7 @@ void fs_set_error(const char* fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(g_err, sizeof(g_err), fmt, ap);
   va_end(ap);
+  g_err_fresh = true;
 }
 
 // Host wait for a stream through a blocking-sync event: the calling thread
@@ -89,9 +93,19 @@ static SmallScratch* small_scratch() {
 }
 
 static int check(int st, const char* where) {
-  if (st == FS_OK) return st;
+  if (st == FS_OK) {
+    g_err_fresh = false;
+    return st;
+  }
   cudaError_t e = cudaGetLastError();
-  if (st == FS_ECUDA)
+  if (g_err_fresh && st != FS_ECUDA && strncmp(g_err, where, strlen(where)) != 0) {
+    // the failing function said what was wrong: keep it, naming the entry point
+    char inner[sizeof(g_err)];
+    memcpy(inner, g_err, sizeof(g_err));
+    fs_set_error("%s: %s", where, inner);
+  } else if (g_err_fresh && st != FS_ECUDA) {
+    // already names the entry point
+  } else if (st == FS_ECUDA)
     fs_set_error("%s: CUDA error: %s", where, cudaGetErrorString(e));
   else if (st == FS_EARG)
     fs_set_error("%s: bad argument", where);
@@ -103,6 +117,7 @@ static int check(int st, const char* where) {
     fs_set_error("%s: a bounded device wait gave up (results of that call not valid)", where);
   else
     fs_set_error("%s: status %d", where, st);
+  g_err_fresh = false;
   return st;
 }
 
