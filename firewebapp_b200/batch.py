@@ -20,6 +20,7 @@ import threading
 import time
 from dataclasses import dataclass, field
 
+import numpy as np
 import torch
 
 from .solver import Tier3Solver
@@ -173,3 +174,93 @@ def time_concurrent(cases, steps: int, warmup: int = 3, form: str = "plain",
     finally:
         for s in solvers:
             s.close()
+
+
+def _print_line(text):
+    print(text, flush=True)
+
+
+def main(argv=None):
+    """``python -m firewebapp_b200.batch --cases 32 --steps 2000 --concurrency 4``:
+    the batched sweep of uneven domains (``cases.batch_cases``) through the
+    work queue of ``run_batch``; one JSON line per case as it finishes, then a
+    summary line (cell-steps/s over the whole sweep by the host clock)."""
+    import argparse
+    import json
+    from .cases import batch_cases
+    ap = argparse.ArgumentParser(description="batched sweep of independent Tier-3 cases")
+    ap.add_argument("--cases", type=int, default=32)
+    ap.add_argument("--seed0", type=int, default=0)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--concurrency", type=int, default=4)
+    ap.add_argument("--form", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--engine", default="python", choices=["python", "ctx"],
+                    help="python: Tier3Solver work queue (run_batch); ctx: groups of "
+                         "--concurrency whole-step contexts stepped together from C++ "
+                         "(fs_batch_run, no interpreter lock while stepping)")
+    args = ap.parse_args(argv)
+    cases = batch_cases(args.cases, seed0=args.seed0)
+    if args.engine == "ctx":
+        return _main_ctx(cases, args)
+
+    out_lock = threading.Lock()
+
+    def done(r):
+        c = cases[r.index]
+        with out_lock:
+            _print_line(json.dumps({"case": r.index, "cells": r.cells, "nx": int(round(c["Lx"] / c["dx"])),
+                          "U10": c["wind_speed_m_s"], "steps": r.steps, "t": r.t,
+                          "finished": r.finished, "wall_s": r.wall_s,
+                          "cell_steps_per_s": r.cells * r.steps / max(r.wall_s, 1e-12)}))
+
+    t0 = time.perf_counter()
+    res = run_batch(cases, args.steps, form=args.form, concurrency=args.concurrency,
+                    on_case_done=done)
+    wall = time.perf_counter() - t0
+    work = sum(r.cells * r.steps for r in res)
+    print(json.dumps({"cases": len(res), "steps_per_case": args.steps,
+                      "concurrency": args.concurrency, "form": args.form,
+                      "cell_steps": work, "wall_s": wall, "cell_steps_per_s": work / wall,
+                      "note": "wall clock includes each case's set-up"}), flush=True)
+
+
+
+def _main_ctx(cases, args):
+    """The sweep through whole-step contexts: each group of ``concurrency``
+    cases is built (host set-up), then stepped together by ``fs_batch_run``
+    (one C++ host thread and stream pair per case)."""
+    import json
+    from .ctx import StepContext, batch_run
+    t0 = time.perf_counter()
+    work, step_wall = 0, 0.0
+    for g0 in range(0, len(cases), args.concurrency):
+        idx = list(range(g0, min(g0 + args.concurrency, len(cases))))
+        ctxs = [StepContext(cases[i], form=args.form) for i in idx]
+        try:
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            outs = batch_run(ctxs, args.steps)
+            dt = time.perf_counter() - t1
+            step_wall += dt
+            cells = [int(np.prod(c.shape)) for c in ctxs]
+            gw = sum(n * o.steps for n, o in zip(cells, outs))
+            work += gw
+            _print_line(json.dumps({"group": idx, "cells": cells,
+                                    "steps": [o.steps for o in outs],
+                                    "finished": [int(o.finished) for o in outs],
+                                    "wall_s": dt, "cell_steps_per_s": gw / dt}))
+        finally:
+            for c in ctxs:
+                c.close()
+    wall = time.perf_counter() - t0
+    _print_line(json.dumps({"cases": len(cases), "steps_per_case": args.steps,
+                            "concurrency": args.concurrency, "form": args.form,
+                            "engine": "ctx", "cell_steps": work, "wall_s": wall,
+                            "cell_steps_per_s": work / wall,
+                            "stepping_cell_steps_per_s": work / step_wall,
+                            "note": "wall_s includes each group's set-up; the stepping "
+                                    "figure times the fs_batch_run calls only"}))
+
+
+if __name__ == "__main__":
+    main()
