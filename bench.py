@@ -308,6 +308,10 @@ def main():
     ap.add_argument("--mg-fine-sweeps", type=int, default=None,
                     help="Jacobi sweeps before and after the coarse correction on the finest "
                          "multigrid level (fs_proj_set_fine_sweeps; default: the library's)")
+    ap.add_argument("--mg-sweeps", type=int, default=None,
+                    help="Jacobi sweeps before and after the coarse correction on every "
+                         "multigrid level (fs_proj_configure; with --mg-fine-sweeps the finest "
+                         "level keeps its own count; default: the library's)")
     ap.add_argument("--dom-sweep", type=int, default=0,
                     help="force a DOM sweep path (fs_dom_set_sweep_mode); 0 picks automatically")
     ap.add_argument("--batch", type=int, default=0,
@@ -342,7 +346,7 @@ def main():
         from firewebapp_b200.cases import scaled
         case = dict(scaled(CFG2, nx=args.nx), jitter_seed=rank)
     solver = Tier3Solver(case, form=args.form, dom_sweep=args.dom_sweep,
-                         mg_fine_sweeps=args.mg_fine_sweeps)
+                         mg_sweeps=args.mg_sweeps, mg_fine_sweeps=args.mg_fine_sweeps)
     cells = solver.n
     M = solver.Omega.shape[0]
     clocks = ClockSampler(local) if not args.no_clocks else None

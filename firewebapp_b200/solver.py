@@ -191,7 +191,9 @@ class Tier3Solver:
         check(self.lib.fs_proj_create(self.gp, _ctypes_byref(h)), "fs_proj_create")
         self.proj = h
         if mg_sweeps is not None:
-            check(self.lib.fs_proj_configure(self.proj, int(mg_sweeps), 0.8), "fs_proj_configure")
+            # the sweeps on every level (the finest too unless mg_fine_sweeps is
+            # given), at the library's default damping
+            check(self.lib.fs_proj_configure(self.proj, int(mg_sweeps), 0.9), "fs_proj_configure")
         if mg_fine_sweeps is not None:
             check(self.lib.fs_proj_set_fine_sweeps(self.proj, int(mg_fine_sweeps)),
                   "fs_proj_set_fine_sweeps")
