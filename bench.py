@@ -314,6 +314,9 @@ def main():
                          "level keeps its own count; default: the library's)")
     ap.add_argument("--dom-sweep", type=int, default=0,
                     help="force a DOM sweep path (fs_dom_set_sweep_mode); 0 picks automatically")
+    ap.add_argument("--dom-kernel", type=int, default=0,
+                    help="path 8's sweep kernel (fs_dom_set_sweep_kernel): 0 automatic, "
+                         "1 pencil per thread, 2 lane column")
     ap.add_argument("--batch", type=int, default=0,
                     help="instead of the headline line: N cases of the batched sweep of uneven "
                          "domains (Nx 200-600) stepped concurrently, against the same cases "
@@ -346,7 +349,8 @@ def main():
         from firewebapp_b200.cases import scaled
         case = dict(scaled(CFG2, nx=args.nx), jitter_seed=rank)
     solver = Tier3Solver(case, form=args.form, dom_sweep=args.dom_sweep,
-                         mg_sweeps=args.mg_sweeps, mg_fine_sweeps=args.mg_fine_sweeps)
+                         mg_sweeps=args.mg_sweeps, mg_fine_sweeps=args.mg_fine_sweeps,
+                         dom_kernel=args.dom_kernel)
     cells = solver.n
     M = solver.Omega.shape[0]
     clocks = ClockSampler(local) if not args.no_clocks else None
@@ -509,6 +513,8 @@ def kernel_roofline(solver, kt, steps, form, peak, peak_src):
         if lib.fs_dom_launch_shape(solver.dom, shape) == 0:
             out["dom_cluster"] = dict(zip(("ctas", "rows", "threads", "smem_bytes", "groups"),
                                           list(shape)))
+            out["dom_cluster"]["kernel"] = {1: "pencil per thread", 2: "lane column"}.get(
+                int(lib.fs_dom_sweep_kernel(solver.dom)), "none")
     if dom_k == "dom_sweep":
         out["fused_sweep_bytes_per_launch"] = fused_dom
         out["fused_sweep_achieved"] = fused_dom / (avg_ms * 1e-3) / 1e9

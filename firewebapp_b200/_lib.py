@@ -108,6 +108,8 @@ SIGNATURES = {
     "fs_edc": (I, [I64, P, P, P, P, P, P, P, P, D, D, D, I, D, D, I, P, P]),
     "fs_edc_noalloc": (I, [I64, P, P, P, P, P, P, P, P, D, D, D, I, D, D, I, P]),
     "fs_gas_energy_update": (I, [_G, P, P, P, P, P, P, P, P, P, D, D, D, I, I, I, I, P]),
+    "fs_gas_energy_solid_update": (I, [_G, P, P, P, P, P, P, P, P, P, D, D, D, I, I, I, I,
+                                       P, P, D, D, D, D, D, P]),
     "fs_eos": (I, [_G, P, P, P, P, D, P]),
     "fs_clip": (I, [I64, P, D, D, P]),
     "fs_div_target": (I, [I64, P, P, P, P, D, P, P]),
@@ -174,6 +176,8 @@ SIGNATURES = {
     "fs_dom_iterations": (I, [P]),
     "fs_dom_set_sweep_mode": (I, [P, I, I]),
     "fs_dom_sweep_mode": (I, [P]),
+    "fs_dom_set_sweep_kernel": (I, [P, I]),
+    "fs_dom_sweep_kernel": (I, [P]),
     "fs_dom_launch_shape": (I, [P, P]),
     "fs_dom_set_wait_test": (I, [P, I]),
     "fs_index_divide": (I, [C.c_uint32, C.c_int64, P, P]),

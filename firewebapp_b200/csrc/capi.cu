@@ -362,6 +362,26 @@ int fs_gas_energy_update(const FsGrid* g, double* T_g, const double* rho, const 
                "fs_gas_energy_update");
 }
 
+int fs_gas_energy_solid_update(const FsGrid* g, double* T_g, const double* rho,
+                               const double* Y_H2O, const double* T_s, const double* S_pyro,
+                               const double* S_drying, const double* Q_g_conv,
+                               const double* q_rad_gas, double* Q_comb_out, double dt_sub,
+                               double T_amb, double h_bed, int drip_on, int n_z_bed, int i_src0,
+                               int i_src1, const double* alpha_s, double* T_s_out,
+                               double k_solid, double rho_solid, double cp_solid, double Ts_lo,
+                               double Ts_hi, void* stream) {
+  GRID("fs_gas_energy_solid_update");
+  if (!T_s || !T_s_out || T_s_out == T_s || !alpha_s) {
+    fs_set_error("fs_gas_energy_solid_update: T_s_out must be a buffer other than T_s");
+    return FS_EARG;
+  }
+  return check(launch_gas_solid(gd, T_g, rho, Y_H2O, T_s, S_pyro, S_drying, Q_g_conv, q_rad_gas,
+                                Q_comb_out, dt_sub, T_amb, h_bed, drip_on, n_z_bed, i_src0,
+                                i_src1, alpha_s, T_s_out, k_solid, rho_solid, cp_solid, Ts_lo,
+                                Ts_hi, ST(stream)),
+               "fs_gas_energy_solid_update");
+}
+
 int fs_eos(const FsGrid* g, double* rho, double* rho_prev, const double* T_g, double* Y_O2,
            double T_amb, void* stream) {
   GRID("fs_eos");
@@ -719,6 +739,11 @@ int fs_dom_set_octant_groups(void* handle, int groups) {
   return check(dom_set_groups(handle, groups), "fs_dom_set_octant_groups");
 }
 int fs_dom_sweep_mode(void* handle) { return handle ? dom_mode(handle) : -1; }
+int fs_dom_set_sweep_kernel(void* handle, int kernel) {
+  if (!handle) return check(FS_EARG, "fs_dom_set_sweep_kernel");
+  return check(dom_set_sweep_kernel(handle, kernel), "fs_dom_set_sweep_kernel");
+}
+int fs_dom_sweep_kernel(void* handle) { return handle ? dom_sweep_kernel(handle) : -1; }
 int fs_index_divide(uint32_t d, int64_t n, const uint32_t* x, uint32_t* q) {
   if (d == 0 || n < 0 || (n > 0 && (!x || !q))) {
     fs_set_error("fs_index_divide: divisor %u, count %lld", d, (long long)n);

@@ -92,30 +92,102 @@ __device__ __forceinline__ int wrapj(int j, int ny) {
   return r < 0 ? r + ny : r;
 }
 
-// minmod limiter (muscl_3d.py:37-44), as selects (no divergent branches):
-// 0 when a*b <= 0, else the argument of smaller magnitude
+// minmod limiter (muscl_3d.py:37-44): 0 when a*b <= 0, else the argument of
+// smaller magnitude.  When a*b > 0 both arguments are finite, non-zero and of
+// one sign, so that argument is exactly copysign(min(|a|, |b|), a): one
+// hardware minimum in place of compare-and-select chains.  Symmetric in a, b
+// (the product and the chosen value do not depend on the order).
 __device__ __forceinline__ double minmod(double a, double b) {
-  const double lo = a < b ? a : b, hi = a > b ? a : b;
-  const double m = a > 0.0 ? lo : hi;
+  const double m = copysign(fmin(fabs(a), fabs(b)), a);
   return (a * b <= 0.0) ? 0.0 : m;
 }
 
 // upwind-biased MUSCL face value at i+1/2 from cells i-1..i+2 (muscl_3d.py:47-64):
 // uf >= 0: pi + 0.5 minmod(pi - pim1, pip1 - pi); else pip1 - 0.5 minmod(pip1 - pi,
-// pip2 - pip1).  Both sides are formed by selects; x + (-0.5 s) equals x - 0.5 s
-// exactly, so the values are the branchy form's bit for bit.
+// pip2 - pip1).  The difference pip1 - pi is common to both sides, so by the
+// limiter's symmetry only its other argument is selected; x + (-0.5 s) equals
+// x - 0.5 s exactly, so the values are the branchy form's bit for bit.
 __device__ __forceinline__ double muscl_face(double pim1, double pi, double pip1,
                                              double pip2, double uf) {
   const bool up = uf >= 0.0;
-  const double a = up ? pi - pim1 : pip1 - pi;
-  const double b = up ? pip1 - pi : pip2 - pip1;
+  const double m = minmod(pip1 - pi, up ? pi - pim1 : pip2 - pip1);
   const double base = up ? pi : pip1;
   const double half = up ? 0.5 : -0.5;
-  return base + half * minmod(a, b);
+  return base + half * m;
 }
 
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
+// Vertical solid conduction of one cell (solid_conduction_3d.py:56-127): the
+// harmonic-mean face conductances to the bed cells above and below and the
+// explicit update; cap = 1 clips the result to [lo, hi] (the T_s cap that
+// follows the conduction, spread_3d.py:3193-3196).  T0 = Ts[c].
+__device__ __forceinline__ double solid_cond_cell(const GridDev& g, const double* __restrict__ Ts,
+                                                  const double* __restrict__ as, int k, int64_t c,
+                                                  double T0, double k_solid, double inv_rho_cp,
+                                                  double dt, int cap, double lo, double hi) {
+  const int64_t sz = (int64_t)g.nx * g.ny;
+  const double asc = as[c];
+  if (asc <= 0.0) {
+    double x = T0;
+    if (cap) {
+      if (x > hi) x = hi;
+      if (x < lo) x = lo;
+    }
+    return x;
+  }
+  double fu = 0.0, fd = 0.0;
+  if (k < g.nz - 1) {
+    double aa = as[c + sz];
+    if (aa > 0.0) {
+      double ae = 2.0 * asc * aa / (asc + aa);
+      fu = k_solid * ae * (Ts[c + sz] - T0) / g.da[k];
+    }
+  }
+  if (k > 0) {
+    double ab = as[c - sz];
+    if (ab > 0.0) {
+      double ae = 2.0 * asc * ab / (asc + ab);
+      fd = k_solid * ae * (Ts[c - sz] - T0) / g.db[k];
+    }
+  }
+  double src = (fu + fd) / g.dz[k];
+  double dT = dt * src * inv_rho_cp / asc;
+  double x = T0 + dT;
+  if (cap) {
+    if (x > hi) x = hi;
+    if (x < lo) x = lo;
+  }
+  return x;
+}
+
+// EDC flag scan tiling: a block of EDC_TPB threads owns EDC_TILE consecutive
+// cells, EDC_CPT per thread (thread t: cells EDC_CPT*t .. EDC_CPT*t + 3 of the
+// tile), so a thread's loads are two 16-byte vectors per FP64 field and the
+// tile's flat order is thread order, then the order within the thread.
+#define EDC_TPB 256
+#define EDC_CPT 4
+#define EDC_TILE (EDC_TPB * EDC_CPT)
+
+// Exclusive max-scan over the block's threads of `last` (every thread's
+// largest code, -1 for none): the largest code of the threads before this
+// one.  `sh` holds EDC_TPB / 32 ints; one barrier.
+__device__ __forceinline__ int edc_block_exclusive_max(int last, int* sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int v = last;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v = max(v, y);
+  }
+  if (lane == 31) sh[wid] = v;
+  int ex = __shfl_up_sync(0xffffffffu, v, 1);
+  if (lane == 0) ex = -1;
+  __syncthreads();
+  for (int w = 0; w < wid; ++w) ex = max(ex, sh[w]);
+  return ex;
+}
 
 // Launch geometry helpers: one thread per cell, x fastest.
 struct Launch3 {

@@ -63,6 +63,8 @@ struct DomCtx {
   void *kb, *Goct, *Qoct, *wrap;
   int Mo, cl_C, cl_rows, cl_threads, cl_ppt, cl_waves;
   size_t cl_smem;
+  int sweep_kernel;           // requested path-8 kernel: 0/1 pencil per thread, 2 lane column
+  int cl_lane;                // resolved: 1 = the lane-column kernel
   int begun;                  // dom_begin done, dom_end due
   double pend_I_amb;          // ambient intensity of the begun solve
   int down_slot[8];
@@ -810,6 +812,284 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
   cluster_wait_acquire();
 }
 
+// ---- path 8, lane-column form ------------------------------------------------
+// The same sweep (cluster per octant, CTAs splitting the k' rows, the ring
+// hand-off between CTAs, the same inputs, outputs and arithmetic, so the same
+// results bit for bit) with another mapping of pencils to threads: lane jp of
+// the CTA owns the pencils (jp, kp) of all of the CTA's rows and keeps their
+// latest intensities (rows x ordinates) in registers.  Within a hyperplane all
+// cells are independent; a cell's x-inflow is its own pencil's latest value,
+// its z-inflow the latest value of the pencil below (same lane; the first row
+// takes the ring or the ground), its y-inflow the latest value of the pencil
+// to the left: the lane below by a warp shuffle, for a warp's first lane the
+// previous warp's last lane through a two-slot exchange buffer, for the first
+// column the row's y-inflow.  A hyperplane costs one barrier over ny/32
+// compute warps and the helper, and each lane has rows x ordinates
+// independent updates per hyperplane, where the pencil-per-thread form moves
+// every intensity through shared memory and waits at a barrier over 24 warps
+// that each have ten.  Measured on the 400 x 120 x 60 S8 workload it is the
+// slower of the two (3.85 against 1.95 ms per FP64 sweep): with one warp per
+// scheduler a lane's updates do not overlap enough to cover the latency of
+// the reciprocal and its corrections, which the other form hides with six
+// warps per scheduler.  It is built for comparison and chosen only on request.
+#define LC_MAX_WARPS 4  // compute warps (ny <= 128)
+struct LcLayout {
+  size_t bars, kab, ig, yin, xb, ring, kz, cxy, cwq, total;
+};
+__host__ __device__ inline LcLayout lc_layout(int tsize, int Mo, int rows, int nw, int ny, int nz) {
+  LcLayout L;
+  const size_t NWL = (size_t)nw * 32;
+  const size_t Mp = (size_t)cl_mpad(Mo);
+  size_t o = 0;
+  L.bars = o; o = up16(o + 2 * CL_RING * sizeof(unsigned long long));
+  L.kab = o; o = up16(o + (size_t)CL_AHEAD * rows * NWL * 2 * tsize);
+  L.ig = o; o = up16(o + (size_t)CL_AHEAD * NWL * sizeof(double));
+  L.yin = o; o = up16(o + (size_t)CL_AHEAD * rows * Mo * tsize);
+  L.xb = o; o = up16(o + (size_t)2 * nw * rows * Mo * tsize);
+  L.ring = o; o = up16(o + (size_t)CL_RING * Mp * ny * tsize);
+  L.kz = o; o = up16(o + (size_t)nz * Mo * 2 * tsize);
+  L.cxy = o; o = up16(o + (size_t)Mo * 2 * tsize);
+  L.cwq = o; o = up16(o + (size_t)Mo * 2 * tsize);
+  L.total = o;
+  return L;
+}
+
+template <typename T, int MO, int ROWS>
+__global__ void __launch_bounds__(32 * (LC_MAX_WARPS + 1), 1)
+    k_dom_octant_lc(GridDev g, ClArgs a) {
+  using T2 = typename Vec2Of<T>::type;
+  constexpr int MP = cl_mpad(MO);
+  extern __shared__ __align__(16) unsigned char shraw[];
+  if (a.done && *(volatile const int*)a.done) return;
+  cg::cluster_group cl = cg::this_cluster();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int C = a.C;
+  const int rank = (int)cl.block_rank();
+  const int part = blockIdx.x / C;
+  const int oct = part / a.groups;
+  const int grp = part - oct * a.groups;
+  const int n0 = part * MO;
+  const int nw = (int)(blockDim.x >> 5) - 1;  // compute warps; the last warp is the helper
+  const int NWL = nw * 32;
+  const LcLayout L = lc_layout((int)sizeof(T), MO, ROWS, nw, ny, nz);
+  unsigned long long* full = (unsigned long long*)(shraw + L.bars);
+  unsigned long long* empty = full + CL_RING;
+  T2* kab_ring = (T2*)(shraw + L.kab);
+  double* ig_ring = (double*)(shraw + L.ig);
+  T* yin = (T*)(shraw + L.yin);
+  T* xb = (T*)(shraw + L.xb);
+  T* ring = (T*)(shraw + L.ring);
+  T2* kz = (T2*)(shraw + L.kz);
+  T2* cxy = (T2*)(shraw + L.cxy);
+  T2* cwq = (T2*)(shraw + L.cwq);
+  const T2* kb = (const T2*)a.kb;
+  T* Goct = (T*)a.Goct;
+  T* Qoct = (T*)a.Qoct;
+  T* wrap = (T*)a.wrap;
+  const T I_amb = (T)a.I_amb;
+  const int nplanes = nx + ny + nz - 2;
+  const int lane = (int)threadIdx.x & 31, wid = (int)threadIdx.x >> 5;
+  const bool helper = wid == nw;
+  const int jp = (int)threadIdx.x;  // the lane's column (compute warps)
+  const bool has = !helper && jp < ny;
+  for (int t = threadIdx.x; t < MO * nz; t += blockDim.x) {
+    const int k = t / MO, m = t - k * MO;
+    const double ax = fabs(a.ox[n0 + m]) / g.dx, ay = fabs(a.oy[n0 + m]) / g.dy;
+    const double az = fabs(a.oz[n0 + m]) / g.dz[k];
+    T2 v;
+    v.x = (T)az;
+    v.y = (T)(ax + ay + az);
+    kz[t] = v;
+  }
+  for (int m = threadIdx.x; m < MO; m += blockDim.x) {
+    T2 xy, wq;
+    xy.x = (T)(fabs(a.ox[n0 + m]) / g.dx);
+    xy.y = (T)(fabs(a.oy[n0 + m]) / g.dy);
+    wq.x = (T)a.w[n0 + m];
+    wq.y = (T)(a.w[n0 + m] * fabs(a.oz[n0 + m]));
+    cxy[m] = xy;
+    cwq[m] = wq;
+  }
+  for (int t = threadIdx.x; t < 2 * nw * ROWS * MO; t += blockDim.x) xb[t] = I_amb;
+  for (int t = threadIdx.x; t < CL_RING * MP * ny; t += blockDim.x) ring[t] = I_amb;
+  const uint32_t fill_bytes = (uint32_t)(ny * MO * sizeof(T));
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < CL_RING; ++s) {
+      cl_mbar_init(&full[s], 1u);
+      cl_mbar_init(&empty[s], 1u);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  const bool fx = a.ox[n0] >= 0.0, fy = a.oy[n0] >= 0.0, fz = a.oz[n0] >= 0.0;
+  const int r0 = rank * ROWS;
+  const int64_t N = ncells_dev(g);
+  const int64_t n2 = (int64_t)nx * ny;
+  const int slot_bits = (int)((a.down_slots >> (4 * oct)) & 15u);
+  const int slot = slot_bits == 15 ? -1 : slot_bits * a.groups + grp;
+  T* Go = Goct + (int64_t)part * N;
+  const int64_t wstride = (int64_t)nz * nx;
+  T* wrap0 = wrap + (int64_t)n0 * wstride;
+  const bool periodic = a.periodic != 0;
+  const uint64_t keep = l2_policy_evict_last();
+  const int j = fy ? jp : ny - 1 - jp;  // the column's y index (compute lanes with has)
+  // the inputs of hyperplane d for the lane's cells: (kappa, kappa*B), the
+  // ground intensity under the first row of the first CTA, the y-inflow of
+  // the first column
+  auto prefetch = [&](int d) {
+    if (has) {
+      const int sl = d % CL_AHEAD;
+#pragma unroll
+      for (int kl = 0; kl < ROWS; ++kl) {
+        const int kp = r0 + kl;
+        const int ip = d - jp - kp;
+        if (kp < nz && ip >= 0 && ip < nx) {
+          const int i = fx ? ip : nx - 1 - ip;
+          const int k = fz ? kp : nz - 1 - kp;
+          cp_async_kb(&kab_ring[(size_t)(sl * ROWS + kl) * NWL + jp],
+                      &kb[((int64_t)k * ny + j) * nx + i], keep);
+          if (fz && kp == 0) cp_async8(&ig_ring[(size_t)sl * NWL + jp], &a.Ig[(int64_t)j * nx + i]);
+          if (jp == 0) {
+            T* dst = yin + (size_t)(sl * ROWS + kl) * MO;
+            const T* src = wrap0 + (int64_t)k * nx + i;
+#pragma unroll
+            for (int m = 0; m < MO; ++m) {
+              if (periodic)
+                cp_async_val(&dst[m], src + m * wstride);
+              else
+                dst[m] = I_amb;
+            }
+          }
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  for (int d = 0; d < CL_AHEAD - 1; ++d) prefetch(d);
+  __syncthreads();
+  if (helper && lane == 0 && rank > 0)
+    for (int s = 0; s < CL_RING; ++s) cl_arrive_expect(smem_u32(&full[s]), fill_bytes);
+  cluster_arrive_release();
+  cluster_wait_acquire();
+  constexpr uint32_t TS = (uint32_t)sizeof(T);
+  constexpr uint32_t PS = (uint32_t)MP * TS;
+  const uint32_t a_ring = smem_u32(ring);
+  const uint32_t a_dring = rank < C - 1 ? cl_mapa(a_ring, (unsigned)(rank + 1)) : 0u;
+  const uint32_t full_dn = rank < C - 1 ? cl_mapa(smem_u32(full), (unsigned)(rank + 1)) : 0u;
+  const uint32_t empty_up = rank > 0 ? cl_mapa(smem_u32(empty), (unsigned)(rank - 1)) : 0u;
+  const bool pusher = has && rank < C - 1;  // the last row feeds the next CTA
+  // the column of ring slots this lane reads and writes (idle lanes: column 0)
+  const int jr = has ? jp : 0;
+  bool failed = false;
+  T st[ROWS][MO];
+#pragma unroll
+  for (int kl = 0; kl < ROWS; ++kl)
+#pragma unroll
+    for (int m = 0; m < MO; ++m) st[kl][m] = I_amb;
+  for (int d = 0; d < nplanes; ++d) {
+    prefetch(d + CL_AHEAD - 1);  // an empty group past the last plane
+    cp_async_wait<CL_AHEAD - 1>();
+    if (helper && lane == 0 && rank > 0 && d > 0)
+      cl_wait(smem_u32(&full[(d - 1) % CL_RING]), (uint32_t)(((d - 1) / CL_RING) & 1), failed,
+              a.err);
+    __syncthreads();  // hyperplane d-1 complete in this CTA
+    if (helper) {
+      if (lane == 0 && rank > 0 && d >= 2 && !failed) {
+        cl_arrive_expect(smem_u32(&full[(d - 2) % CL_RING]), fill_bytes);
+        cl_arrive_remote(empty_up + 8u * ((d - 2) % CL_RING));
+      }
+      continue;
+    }
+    const int sl = d % CL_AHEAD;
+    const int zslot = (d + CL_RING - 1) % CL_RING;
+    const int pslot = d % CL_RING;
+    const int par = d & 1;
+    const bool hold = rank == 0 && d == a.withhold;
+    // this thread's own acquire of the ring slot the first row reads
+    if (rank > 0 && d > 0)
+      cl_wait(smem_u32(&full[zslot]), (uint32_t)(((d - 1) / CL_RING) & 1), failed, a.err);
+    // the downstream CTA has finished with the slot this hyperplane fills
+    if (pusher && d >= CL_RING)
+      cl_wait(smem_u32(&empty[pslot]), (uint32_t)((d / CL_RING - 1) & 1), failed, a.err);
+    const bool push = pusher && !failed && !hold;
+    const uint32_t apush = a_dring + (uint32_t)(pslot * ny + jr) * PS;
+    const uint32_t pbar = full_dn + 8u * pslot;
+    // rows from the top down: row kl's z-inflow is row kl-1's value of d-1
+#pragma unroll
+    for (int kl = ROWS - 1; kl >= 0; --kl) {
+      const int kp = r0 + kl;
+      const int ip = d - jp - kp;
+      const bool act = has && kp < nz && ip >= 0 && ip < nx;
+      const int k = kp < nz ? (fz ? kp : nz - 1 - kp) : 0;
+      T Iy[MO], Iz[MO], v[MO];
+#pragma unroll
+      for (int m = 0; m < MO; ++m) Iy[m] = __shfl_up_sync(0xffffffffu, st[kl][m], 1);
+      if (lane == 0) {
+        const T* src = jp == 0 ? yin + (size_t)(sl * ROWS + kl) * MO
+                               : xb + (size_t)(((par ^ 1) * nw + (wid - 1)) * ROWS + kl) * MO;
+#pragma unroll
+        for (int m = 0; m < MO; ++m) Iy[m] = src[m];
+      }
+      if (kl > 0) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) Iz[m] = st[kl > 0 ? kl - 1 : 0][m];
+      } else if (rank == 0) {
+        const T z = fz ? (T)ig_ring[(size_t)sl * NWL + jp] : I_amb;
+#pragma unroll
+        for (int m = 0; m < MO; ++m) Iz[m] = z;
+      } else {
+        const T* zr = ring + (size_t)(zslot * ny + jr) * MP;
+#pragma unroll
+        for (int m = 0; m < MO; ++m) Iz[m] = zr[m];
+      }
+      const T2 kab = kab_ring[(size_t)(sl * ROWS + kl) * NWL + jp];
+      const T2* kzr = kz + k * MO;
+#pragma unroll
+      for (int m = 0; m < MO; ++m) {
+        const T2 zc = kzr[m];
+        const T2 xy = cxy[m];
+        const T num = fmat(zc.x, Iz[m], fmat(xy.y, Iy[m], fmat(xy.x, st[kl][m], kab.y)));
+        v[m] = sweep_quot(num, kab.x + zc.y);
+      }
+      T gs = (T)0;
+#pragma unroll
+      for (int m = 0; m < MO; ++m) gs = fmat(cwq[m].x, v[m], gs);
+#pragma unroll
+      for (int m = 0; m < MO; ++m) st[kl][m] = act ? v[m] : st[kl][m];
+      if (kl == ROWS - 1 && push) {
+#pragma unroll
+        for (int m = 0; m < MO; ++m) cl_st_async(apush + (uint32_t)m * TS, act ? v[m] : I_amb, pbar);
+      }
+      if (lane == 31 && wid < nw - 1) {
+        T* xo = xb + (size_t)((par * nw + wid) * ROWS + kl) * MO;
+#pragma unroll
+        for (int m = 0; m < MO; ++m) xo[m] = st[kl][m];
+      }
+      if (act) {
+        const int i = fx ? ip : nx - 1 - ip;
+        st_cs(Go + ((int64_t)k * ny + j) * nx + i, gs);
+        if (!fz && k == 0 && slot >= 0) {
+          T qs = (T)0;
+#pragma unroll
+          for (int m = 0; m < MO; ++m) qs = fmat(cwq[m].y, v[m], qs);
+          Qoct[(int64_t)slot * n2 + (int64_t)j * nx + i] = qs;
+        }
+        if (jp == ny - 1 && periodic) {
+          // the y-outflow, read by the next sweep at the row's other end
+          T* wo = wrap0 + (int64_t)k * nx + i;
+#pragma unroll
+          for (int m = 0; m < MO; ++m) wo[m * wstride] = v[m];
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  if (helper && lane == 0 && rank > 0)
+    cl_wait(smem_u32(&full[(nplanes - 1) % CL_RING]), (uint32_t)(((nplanes - 1) / CL_RING) & 1),
+            failed, a.err);
+  cluster_arrive_release();
+  cluster_wait_acquire();
+}
+
 static const void* octant_cl_ptr(bool fp32, int Mo, int ppt) {
 #define CLP(T, M, P) (const void*)k_dom_octant_cl<T, M, P>
   if (ppt == 1) {
@@ -828,6 +1108,22 @@ static const void* octant_cl_ptr(bool fp32, int Mo, int ppt) {
     }
   }
 #undef CLP
+  return nullptr;
+}
+
+// The lane-column kernels built: ten ordinates per cluster (the S8 octant),
+// 4 to 8 k' rows per CTA.
+static const void* octant_lc_ptr(bool fp32, int Mo, int rows) {
+#define LCP(T, R) (const void*)k_dom_octant_lc<T, 10, R>
+  if (Mo != 10) return nullptr;
+  switch (rows) {
+    case 4: return fp32 ? LCP(float, 4) : LCP(double, 4);
+    case 5: return fp32 ? LCP(float, 5) : LCP(double, 5);
+    case 6: return fp32 ? LCP(float, 6) : LCP(double, 6);
+    case 7: return fp32 ? LCP(float, 7) : LCP(double, 7);
+    case 8: return fp32 ? LCP(float, 8) : LCP(double, 8);
+  }
+#undef LCP
   return nullptr;
 }
 
@@ -956,6 +1252,7 @@ void* dom_create(const GridDev& g, int M, const double* ox, const double* oy, co
   D->mode = 0; D->mode_req = 0; D->force_C = 0; D->groups = 1; D->force_groups = 0;
   D->withhold_plane = -1;
   D->fp32 = 0; D->cl_ppt = 1; D->cl_waves = 0; D->begun = 0; D->pend_I_amb = 0.0;
+  D->sweep_kernel = 0; D->cl_lane = 0;
   cudaMalloc(&D->G, sizeof(double) * N); cudaMalloc(&D->Gp, sizeof(double) * N);
   cudaMemsetAsync(D->G, 0, sizeof(double) * N, ss.s);
   cudaMemsetAsync(D->Gp, 0, sizeof(double) * N, ss.s);
@@ -1092,12 +1389,56 @@ static bool plan_cl(DomCtx* D, int force_C) {
 // so the clearing is ordered before that stream's first sweep (a plain
 // cudaMemset runs on the legacy default stream, which does not order work on
 // streams created non-blocking, such as torch's side streams).
+// The lane-column kernel for the planned shape (same clusters, rows and
+// ordinate groups), when it is requested, built for the shape, and all
+// clusters stay resident at once as with the pencil-per-thread kernel.
+static bool plan_lc(DomCtx* D) {
+  const GridDev& g = D->g;
+  const int Mo = D->M / 8 / D->groups;
+  const int nw = (g.ny + 31) / 32;
+  const void* fn = octant_lc_ptr(D->fp32 != 0, Mo, D->cl_rows);
+  if (!fn || nw > LC_MAX_WARPS || D->cl_rows * D->cl_C < g.nz) return false;
+  int dev = 0, optin = 0, smem_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  const int tsize = D->fp32 ? (int)sizeof(float) : (int)sizeof(double);
+  const size_t need = lc_layout(tsize, Mo, D->cl_rows, nw, g.ny, g.nz).total;
+  const size_t pad = (size_t)smem_sm / 2 + 1024;  // no two CTAs on one SM
+  const size_t smem = need > pad ? need : pad;
+  if (smem > (size_t)optin) return false;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  const int threads = 32 * (nw + 1);
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = D->cl_C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(8 * D->groups * D->cl_C); cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem; cfg.attrs = at; cfg.numAttrs = 1;
+  int active = 0;
+  if (cudaOccupancyMaxActiveClusters(&active, fn, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (active < 1 || (8 * D->groups + active - 1) / active > D->cl_waves) return false;
+  D->cl_lane = 1;
+  D->cl_threads = threads;
+  D->cl_smem = smem;
+  return true;
+}
+
 static int dom_prepare(DomCtx* D, cudaStream_t st) {
   if (D->mode != 0) return FS_OK;
   const GridDev& g = D->g;
   const int64_t N = ncells(g), n2 = (int64_t)g.nx * g.ny;
   const int want = D->mode_req;
   const bool oct = (want == 0 || want == 8) && octant_grouping(D) && plan_cl(D, D->force_C);
+  if (oct && D->sweep_kernel == 2 && !plan_lc(D)) {
+    fs_set_error("the lane-column sweep kernel is not built for this shape (ten ordinates per "
+                 "cluster, 4 to 8 k' rows per CTA, ny <= %d)", 32 * LC_MAX_WARPS);
+    return FS_EARG;
+  }
   if (oct) {
     D->mode = 8;
     D->Mo = D->M / 8;
@@ -1140,6 +1481,24 @@ int dom_set_mode(void* h, int mode, int cluster_ctas) {
   D->mode_req = mode;
   D->force_C = cluster_ctas;
   return FS_OK;
+}
+
+int dom_set_sweep_kernel(void* h, int kernel) {
+  DomCtx* D = (DomCtx*)h;
+  if (kernel < 0 || kernel > 2) {
+    fs_set_error("sweep kernel %d: 0 (automatic), 1 (pencil per thread), 2 (lane column)", kernel);
+    return FS_EARG;
+  }
+  if (D->mode != 0) {
+    fs_set_error("the sweep kernel must be set before the first solve or intensity load");
+    return FS_EARG;
+  }
+  D->sweep_kernel = kernel;
+  return FS_OK;
+}
+int dom_sweep_kernel(void* h) {
+  const DomCtx* D = (const DomCtx*)h;
+  return D->mode != 8 ? 0 : (D->cl_lane ? 2 : 1);
 }
 
 int dom_mode(void* h) { return ((DomCtx*)h)->mode; }
@@ -1282,6 +1641,19 @@ static int launch_cl_sweep(DomCtx* D, const ClArgs& a, cudaStream_t st) {
   cfg.numAttrs = 1;
   cudaError_t e = cudaErrorInvalidValue;
   const bool f = D->fp32 != 0;
+  if (D->cl_lane) {
+#define LCL(T, R) e = cudaLaunchKernelEx(&cfg, k_dom_octant_lc<T, 10, R>, D->g, a)
+    switch (D->cl_rows) {
+      case 4: if (f) LCL(float, 4); else LCL(double, 4); break;
+      case 5: if (f) LCL(float, 5); else LCL(double, 5); break;
+      case 6: if (f) LCL(float, 6); else LCL(double, 6); break;
+      case 7: if (f) LCL(float, 7); else LCL(double, 7); break;
+      case 8: if (f) LCL(float, 8); else LCL(double, 8); break;
+    }
+#undef LCL
+    fs_count_launch();
+    return e == cudaSuccess ? FS_OK : FS_ECUDA;
+  }
 #define CLL(T, M, P) e = cudaLaunchKernelEx(&cfg, k_dom_octant_cl<T, M, P>, D->g, a)
   switch ((D->Mo / D->groups) * 4 + D->cl_ppt) {
     case 3 * 4 + 1: if (f) CLL(float, 3, 1); else CLL(double, 3, 1); break;

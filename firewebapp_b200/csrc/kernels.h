@@ -70,6 +70,12 @@ int launch_gas_update(const GridDev& g, double* Tg, const double* rho, const dou
                       const double* qrg, double* Qcomb_out, unsigned long long* qc_max,
                       double dt_sub, double T_amb, double h_bed, int drip_on, int n_z_bed,
                       int i_src0, int i_src1, cudaStream_t st);
+int launch_gas_solid(const GridDev& g, double* Tg, const double* rho, const double* YH,
+                     const double* Ts, const double* Sp, const double* Sd, const double* Qgc,
+                     const double* qrg, double* Qcomb_out, double dt_sub, double T_amb,
+                     double h_bed, int drip_on, int n_z_bed, int i_src0, int i_src1,
+                     const double* as, double* Ts_out, double k_solid, double rho_s, double cp_s,
+                     double lo, double hi, cudaStream_t st);
 int launch_eos(const GridDev& g, double* rho, double* rho_prev, const double* Tg, double* YO,
                double P0, double R_air, double T_amb, cudaStream_t st);
 int launch_clip(int64_t n, double* f, double lo, double hi, cudaStream_t st);
@@ -134,6 +140,8 @@ int dom_begin(void* h, const double* Ts, const double* Tg, const double* as, con
 int dom_end(void* h, double* q_solid, double* q_gas, double* q_in_soil, cudaStream_t st);
 int dom_set_groups(void* h, int groups);
 int dom_mode(void* h);
+int dom_set_sweep_kernel(void* h, int kernel);
+int dom_sweep_kernel(void* h);
 int dom_launch_shape(void* h, int* out5);
 int dom_set_wait_test(void* h, int plane);
 int dom_set_precision(void* h, int fp32);

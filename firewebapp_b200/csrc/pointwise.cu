@@ -11,12 +11,16 @@
 // skip that branch reuse the value left by the previously visited cell, which
 // with one thread is the previous cell in flat k-j-i order (initially False).
 // The flag gates the wet-bulb relaxation of T_g.  To reproduce that order on
-// the GPU the flag is resolved by a flat-order "last assigned value" scan:
-//   pass 1: per 1024-cell block, the last assigned flag (or none);
-//   pass 2: one thread carries the flag across blocks;
-//   pass 3: in-block inclusive scan + carry, then the EDC update itself.
+// the GPU the flag is resolved by a flat-order "last assigned value" scan over
+// tiles of EDC_TILE cells:
+//   pass 1: per tile, the last assigned flag (or none);
+//   pass 2: one block carries the flag across tiles;
+//   pass 3: in-tile scan + carry, then the EDC update itself.
+// Passes 1 and 3 give each thread EDC_CPT consecutive cells and issue all of
+// a thread's loads before the scan's barrier, so the block's memory requests
+// are in flight together instead of after it.
 // ---------------------------------------------------------------------------
-#define EDC_BLK 1024
+#define EDC_BLK EDC_TILE
 
 __device__ __forceinline__ int edc_flag_code(double Yf, double YO2, double YH, int t) {
   // -1: flag not assigned in this cell; else (t << 1) | flag
@@ -30,27 +34,57 @@ __device__ __forceinline__ int edc_flag_code(double Yf, double YO2, double YH, i
   return (t << 1) | f;
 }
 
-__device__ __forceinline__ int block_max_int(int v, int* sh) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+// EDC_CPT consecutive values from p + c0: two 16-byte loads when `vec` (the
+// four cells are all inside the array and p is 16-byte aligned), else
+// element by element with 0 past n.
+__device__ __forceinline__ void edc_ld4(const double* p, int64_t c0, int64_t n, bool vec,
+                                        double* v) {
+  if (vec) {
+    const double2 x = *reinterpret_cast<const double2*>(p + c0);
+    const double2 y = *reinterpret_cast<const double2*>(p + c0 + 2);
+    v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+  } else {
+#pragma unroll
+    for (int q = 0; q < EDC_CPT; ++q) v[q] = (c0 + q < n) ? p[c0 + q] : 0.0;
+  }
+}
+
+__device__ __forceinline__ void edc_st4(double* p, int64_t c0, int64_t n, bool vec,
+                                        const double* v) {
+  if (vec) {
+    *reinterpret_cast<double2*>(p + c0) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2*>(p + c0 + 2) = make_double2(v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < EDC_CPT; ++q)
+      if (c0 + q < n) p[c0 + q] = v[q];
+  }
+}
+
+__global__ void __launch_bounds__(EDC_TPB)
+k_edc_agg(int64_t n, const double* Yf, const double* YO, const double* YH, int vec_ok,
+          signed char* agg) {
+  __shared__ int sh[EDC_TPB / 32];
+  const int t = threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * EDC_TILE + EDC_CPT * t;
+  const bool vec = vec_ok && c0 + EDC_CPT <= n;
+  double yf[EDC_CPT], yo[EDC_CPT], yh[EDC_CPT];
+  edc_ld4(Yf, c0, n, vec, yf);
+  edc_ld4(YO, c0, n, vec, yo);
+  edc_ld4(YH, c0, n, vec, yh);
+  int v = -1;
+#pragma unroll
+  for (int q = 0; q < EDC_CPT; ++q)
+    if (c0 + q < n) v = max(v, edc_flag_code(yf[q], yo[q], yh[q], EDC_CPT * t + q));
+  const int lane = t & 31, wid = t >> 5;
+#pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
   if (lane == 0) sh[wid] = v;
   __syncthreads();
-  int nw = (blockDim.x + 31) >> 5;
-  v = (threadIdx.x < nw) ? sh[threadIdx.x] : -1;
-  if (wid == 0) {
-    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (t == 0) {
+    for (int w = 1; w < EDC_TPB / 32; ++w) v = max(v, sh[w]);
+    agg[blockIdx.x] = (signed char)(v < 0 ? -1 : (v & 1));
   }
-  return v;  // valid in thread 0
-}
-
-__global__ void k_edc_agg(int64_t n, const double* __restrict__ Yf, const double* __restrict__ YO,
-                          const double* __restrict__ YH, signed char* agg) {
-  __shared__ int sh[32];
-  int64_t c = (int64_t)blockIdx.x * EDC_BLK + threadIdx.x;
-  int v = -1;
-  if (c < n) v = edc_flag_code(Yf[c], YO[c], YH[c], threadIdx.x);
-  v = block_max_int(v, sh);
-  if (threadIdx.x == 0) agg[blockIdx.x] = (signed char)(v < 0 ? -1 : (v & 1));
 }
 
 // Carry of the last assigned flag into every block: each thread folds a
@@ -113,42 +147,16 @@ struct EdcArgs {
   // by them, by rho and by tau* are multiplications
   double inv_s, inv_dt;
   int extinction, nsub;
+  int vec_ok;  // every array 16-byte aligned
 };
 
-__global__ void k_edc_main(int64_t n, EdcArgs a) {
-  __shared__ int sh[32];
-  const int t = threadIdx.x;
-  const int64_t c = (int64_t)blockIdx.x * EDC_BLK + t;
-  const bool live = c < n;
-  double Yf = 0, YO2 = 0, YH = 0;
-  if (live) { Yf = a.Yf[c]; YO2 = a.YO[c]; YH = a.YH[c]; }
-  int v = live ? edc_flag_code(Yf, YO2, YH, t) : -1;
-  // inclusive max-scan over the block (flat order == thread order)
-  const int lane = t & 31, wid = t >> 5;
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v = max(v, y);
-  }
-  if (lane == 31) sh[wid] = v;
-  __syncthreads();
-  if (wid == 0) {
-    int w = (lane < (blockDim.x >> 5)) ? sh[lane] : -1;
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w = max(w, y);
-    }
-    sh[lane] = w;
-  }
-  __syncthreads();
-  if (wid > 0) v = max(v, sh[wid - 1]);
-  if (!live) return;
-  bool flag = (v >= 0) ? (v & 1) : (a.carry[blockIdx.x] > 0);
-
-  double Tg = a.Tg[c];
-  const double rho_i = a.rho[c];
-  double k_t = a.kt[c];
+// One cell's EDC update (edc.py:180-330 for one cell, `flag` the quench flag
+// it sees on entry); Yf, YO2, Tg updated in place, the mean reaction rate
+// returned.
+__device__ __forceinline__ double edc_cell(const EdcArgs& a, bool flag, double& Yf, double& YO2,
+                                           double YH, double& Tg, double rho_i, double k_t,
+                                           double e_t) {
   if (k_t < 1.0e-4) k_t = 1.0e-4;
-  double e_t = a.et[c];
   if (e_t < 1.0e-6) e_t = 1.0e-6;
   double ratio = 1.5e-5 * e_t / (k_t * k_t);
   if (ratio < 1e-30) ratio = 1e-30;
@@ -214,16 +222,54 @@ __global__ void k_edc_main(int64_t n, EdcArgs a) {
     if (Tg > 2400.0) Tg = 2400.0;
     acc += omega * h;
   }
-  a.Yf[c] = Yf;
-  a.YO[c] = YO2;
-  a.Tg[c] = Tg;
-  a.omega[c] = a.dt > 0.0 ? acc * a.inv_dt : 0.0;
+  return a.dt > 0.0 ? acc * a.inv_dt : 0.0;
+}
+
+__global__ void __launch_bounds__(EDC_TPB)
+k_edc_main(int64_t n, EdcArgs a) {
+  __shared__ int sh[EDC_TPB / 32];
+  const int t = threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * EDC_TILE + EDC_CPT * t;
+  const bool vec = a.vec_ok && c0 + EDC_CPT <= n;
+  // every input of the thread's cells is requested before the scan's barrier
+  double yf[EDC_CPT], yo[EDC_CPT], yh[EDC_CPT], tg[EDC_CPT], rh[EDC_CPT], kt[EDC_CPT],
+      et[EDC_CPT];
+  edc_ld4(a.Yf, c0, n, vec, yf);
+  edc_ld4(a.YO, c0, n, vec, yo);
+  edc_ld4(a.YH, c0, n, vec, yh);
+  edc_ld4(a.Tg, c0, n, vec, tg);
+  edc_ld4(a.rho, c0, n, vec, rh);
+  edc_ld4(a.kt, c0, n, vec, kt);
+  edc_ld4(a.et, c0, n, vec, et);
+  const bool carry_in = a.carry[blockIdx.x] > 0;
+  int code[EDC_CPT];
+  int last = -1;
+#pragma unroll
+  for (int q = 0; q < EDC_CPT; ++q) {
+    code[q] = (c0 + q < n) ? edc_flag_code(yf[q], yo[q], yh[q], EDC_CPT * t + q) : -1;
+    last = max(last, code[q]);
+  }
+  int run = edc_block_exclusive_max(last, sh);
+  if (c0 >= n) return;
+  double om[EDC_CPT];
+#pragma unroll
+  for (int q = 0; q < EDC_CPT; ++q) {
+    run = max(run, code[q]);
+    const bool flag = (run >= 0) ? (run & 1) : carry_in;
+    om[q] = edc_cell(a, flag, yf[q], yo[q], yh[q], tg[q], rh[q], kt[q], et[q]);
+  }
+  edc_st4(a.Yf, c0, n, vec, yf);
+  edc_st4(a.YO, c0, n, vec, yo);
+  edc_st4(a.Tg, c0, n, vec, tg);
+  edc_st4(a.omega, c0, n, vec, om);
 }
 
 int edc_scratch_bytes(int64_t n) {
   int64_t nb = (n + EDC_BLK - 1) / EDC_BLK;
   return (int)(2 * nb + 16);
 }
+
+static bool al16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
 int launch_edc(int64_t n, const double* rho, double* Tg, double* Yf, double* YO, const double* kt,
                const double* et, const double* YH, double* omega, double chi_rad, double cp_g,
@@ -232,7 +278,9 @@ int launch_edc(int64_t n, const double* rho, double* Tg, double* Yf, double* YO,
   int64_t nb = (n + EDC_BLK - 1) / EDC_BLK;
   signed char* agg = (signed char*)scratch;
   signed char* carry = agg + nb;
-  k_edc_agg<<<(unsigned)nb, EDC_BLK, 0, st>>>(n, Yf, YO, YH, agg); fs_count_launch();
+  const int vec_ok = al16(rho) && al16(Tg) && al16(Yf) && al16(YO) && al16(kt) && al16(et) &&
+                     al16(YH) && al16(omega);
+  k_edc_agg<<<(unsigned)nb, EDC_TPB, 0, st>>>(n, Yf, YO, YH, vec_ok, agg); fs_count_launch();
   k_edc_carry<<<1, EDC_CARRY_THREADS, 0, st>>>((int)nb, agg, carry, nullptr); fs_count_launch();
   EdcArgs a{};
   a.rho = rho; a.Tg = Tg; a.Yf = Yf; a.YO = YO; a.kt = kt; a.et = et; a.YH = YH;
@@ -244,7 +292,8 @@ int launch_edc(int64_t n, const double* rho, double* Tg, double* Yf, double* YO,
   a.nsub = n_substeps > 1 ? n_substeps : 1;
   a.relax = 1.0 - exp(-(dt / (double)a.nsub) / 0.5);
   a.extinction = extinction;
-  k_edc_main<<<(unsigned)nb, EDC_BLK, 0, st>>>(n, a); fs_count_launch();
+  a.vec_ok = vec_ok;
+  k_edc_main<<<(unsigned)nb, EDC_TPB, 0, st>>>(n, a); fs_count_launch();
   return cuda_status();
 }
 
@@ -274,19 +323,17 @@ struct GasArgs {
   int drip_on, n_z_bed, i_src0, i_src1;
 };
 
-__global__ void k_gas_update(GridDev g, GasArgs a) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int k = blockIdx.z;
-  if (i >= g.nx || j >= g.ny) return;
-  int64_t c = cidx(g, k, j, i);
+// One cell of the update; T_s = Ts[c].  Returns the new T_g and the cell's
+// Q_comb in *qc (the caller stores both, after every load of the cell).
+__device__ __forceinline__ double gas_update_cell(const GridDev& g, const GasArgs& a, int k, int i,
+                                                  int64_t c, double T_s, double* qc_out) {
   double qc = 0.0;
   if (a.drip_on && k < a.n_z_bed && i >= a.i_src0 && i < a.i_src1) qc = qc + a.q_drip_gas;
   qc = qc + a.qrg[c] / g.dz[k];
   double T = a.Tg[c];
   double YH = a.YH[c];
   double cp = (1.0 - YH) * 1100.0 + YH * 2000.0;
-  double d1 = T - a.Ts[c];
+  double d1 = T - T_s;
   if (!(d1 >= 0.0)) d1 = (d1 != d1) ? d1 : 0.0;
   double d2 = T - 373.15;
   if (!(d2 >= 0.0)) d2 = (d2 != d2) ? d2 : 0.0;
@@ -296,9 +343,66 @@ __global__ void k_gas_update(GridDev g, GasArgs a) {
   double ginv = a.dt_sub / (rm * cp);
   double Tn = T + (qc - a.Qgc[c] - debit) * ginv;
   if (Tn < a.T_amb) Tn = a.T_amb;
+  *qc_out = qc;
+  return Tn;
+}
+
+__global__ void k_gas_update(GridDev g, GasArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  int64_t c = cidx(g, k, j, i);
+  double qc;
+  const double Tn = gas_update_cell(g, a, k, i, c, a.Ts[c], &qc);
   a.Tg[c] = Tn;
   if (a.Qcomb_out) a.Qcomb_out[c] = qc;
   if (a.qc_max) atomicMax(a.qc_max, dkey(qc));
+}
+
+// The gas-energy update and the capped solid conduction of the same
+// sub-step in one pass (both read the old T_s; neither reads what the other
+// writes): T_s is read once per cell, one launch replaces two, and every
+// load of a cell is issued before its stores.
+struct SolidArgs {
+  const double* as;
+  double* To;
+  double k_solid, inv_rho_cp, lo, hi;
+};
+
+__global__ void k_gas_solid(GridDev g, GasArgs a, SolidArgs b) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  int64_t c = cidx(g, k, j, i);
+  const double T_s = a.Ts[c];
+  double qc;
+  const double Tn = gas_update_cell(g, a, k, i, c, T_s, &qc);
+  const double To = solid_cond_cell(g, a.Ts, b.as, k, c, T_s, b.k_solid, b.inv_rho_cp, a.dt_sub,
+                                    1, b.lo, b.hi);
+  a.Tg[c] = Tn;
+  if (a.Qcomb_out) a.Qcomb_out[c] = qc;
+  b.To[c] = To;
+}
+
+int launch_gas_solid(const GridDev& g, double* Tg, const double* rho, const double* YH,
+                     const double* Ts, const double* Sp, const double* Sd, const double* Qgc,
+                     const double* qrg, double* Qcomb_out, double dt_sub, double T_amb,
+                     double h_bed, int drip_on, int n_z_bed, int i_src0, int i_src1,
+                     const double* as, double* Ts_out, double k_solid, double rho_s, double cp_s,
+                     double lo, double hi, cudaStream_t st) {
+  GasArgs a{};
+  a.Tg = Tg; a.rho = rho; a.YH = YH; a.Ts = Ts; a.Sp = Sp; a.Sd = Sd; a.Qgc = Qgc; a.qrg = qrg;
+  a.Qcomb_out = Qcomb_out; a.qc_max = nullptr;
+  a.dt_sub = dt_sub; a.T_amb = T_amb;
+  double q_drip = 30000.0 / (h_bed > 1e-3 ? h_bed : 1e-3);
+  a.q_drip_gas = (1.0 - 0.80) * q_drip;
+  a.drip_on = drip_on; a.n_z_bed = n_z_bed; a.i_src0 = i_src0; a.i_src1 = i_src1;
+  SolidArgs b{as, Ts_out, k_solid, 1.0 / (rho_s * cp_s), lo, hi};
+  Launch3 L = launch_cells(g);
+  k_gas_solid<<<L.grid, L.block, 0, st>>>(g, a, b); fs_count_launch();
+  return cuda_status();
 }
 
 int launch_gas_update(const GridDev& g, double* Tg, const double* rho, const double* YH,

@@ -723,13 +723,12 @@ static int substep_energy(FsCtx* C, double dt_sub, int drip, const SubCounts& sc
   const FsCaseDesc& c = C->c;
   cudaStream_t s = C->s_main;
   double** f = C->f;
-  CK(fs_gas_energy_update(&C->g, f[S_TG], f[S_RHO], f[S_YH], f[S_TS], f[B_SP], f[B_SD],
-                          f[B_QGC], f[W_QRADG], f[W_QCOMB], dt_sub, c.T_amb, c.h_bed, drip,
-                          c.n_z_bed, c.i_src_start, c.i_src_end, s),
-     "gas_update");
-  CK(fs_solid_conduction_capped(&C->g, f[S_TS], f[S_AS], f[W_T4], 0.20, 500.0, 1300.0, dt_sub,
-                                c.T_amb, T_CAP, s),
-     "solid_cond");
+  // the gas-energy update and the capped solid conduction in one pass
+  CK(fs_gas_energy_solid_update(&C->g, f[S_TG], f[S_RHO], f[S_YH], f[S_TS], f[B_SP], f[B_SD],
+                                f[B_QGC], f[W_QRADG], f[W_QCOMB], dt_sub, c.T_amb, c.h_bed, drip,
+                                c.n_z_bed, c.i_src_start, c.i_src_end, f[S_AS], f[W_T4], 0.20,
+                                500.0, 1300.0, c.T_amb, T_CAP, s),
+     "gas_update + solid_cond");
   std::swap(f[S_TS], f[W_T4]);
   if (sc.n_pr > 0) {
     const double lo[1] = {c.T_amb}, hi[1] = {T_CAP};

@@ -55,7 +55,9 @@ int launch_convert(int64_t n, int nf, const void* const* src, void* const* dst, 
 }
 
 // ---- EDC -----------------------------------------------------------------------
-#define E32_BLK 1024
+// The FP64 kernels' tiling: EDC_TPB threads own EDC_TILE consecutive cells,
+// EDC_CPT (four) per thread, one 16-byte load per field and thread.
+#define E32_BLK EDC_TILE
 
 __device__ __forceinline__ int edc_flag_code32(float Yf, float YO2, float YH, int t) {
   if (Yf <= 1e-9f || YO2 <= 1e-9f) return -1;
@@ -68,20 +70,49 @@ __device__ __forceinline__ int edc_flag_code32(float Yf, float YO2, float YH, in
   return (t << 1) | f;
 }
 
-__global__ void k_edc_agg32(int64_t n, const float* __restrict__ Yf, const float* __restrict__ YO,
-                            const float* __restrict__ YH, signed char* agg) {
-  __shared__ int sh[32];
-  const int64_t c = (int64_t)blockIdx.x * E32_BLK + threadIdx.x;
+__device__ __forceinline__ void e32_ld4(const float* p, int64_t c0, int64_t n, bool vec, float* v) {
+  if (vec) {
+    const float4 x = *reinterpret_cast<const float4*>(p + c0);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < EDC_CPT; ++q) v[q] = (c0 + q < n) ? p[c0 + q] : 0.0f;
+  }
+}
+
+__device__ __forceinline__ void e32_st4(float* p, int64_t c0, int64_t n, bool vec, const float* v) {
+  if (vec) {
+    *reinterpret_cast<float4*>(p + c0) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < EDC_CPT; ++q)
+      if (c0 + q < n) p[c0 + q] = v[q];
+  }
+}
+
+__global__ void __launch_bounds__(EDC_TPB)
+k_edc_agg32(int64_t n, const float* Yf, const float* YO, const float* YH, int vec_ok,
+            signed char* agg) {
+  __shared__ int sh[EDC_TPB / 32];
+  const int t = threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * E32_BLK + EDC_CPT * t;
+  const bool vec = vec_ok && c0 + EDC_CPT <= n;
+  float yf[EDC_CPT], yo[EDC_CPT], yh[EDC_CPT];
+  e32_ld4(Yf, c0, n, vec, yf);
+  e32_ld4(YO, c0, n, vec, yo);
+  e32_ld4(YH, c0, n, vec, yh);
   int v = -1;
-  if (c < n) v = edc_flag_code32(Yf[c], YO[c], YH[c], threadIdx.x);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < EDC_CPT; ++q)
+    if (c0 + q < n) v = max(v, edc_flag_code32(yf[q], yo[q], yh[q], EDC_CPT * t + q));
+  const int lane = t & 31, wid = t >> 5;
+#pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
   if (lane == 0) sh[wid] = v;
   __syncthreads();
-  if (wid == 0) {
-    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : -1;
-    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if (lane == 0) agg[blockIdx.x] = (signed char)(v < 0 ? -1 : (v & 1));
+  if (t == 0) {
+    for (int w = 1; w < EDC_TPB / 32; ++w) v = max(v, sh[w]);
+    agg[blockIdx.x] = (signed char)(v < 0 ? -1 : (v & 1));
   }
 }
 
@@ -93,40 +124,15 @@ struct Edc32Args {
   const signed char* carry;
   float cp_g, dt, s_stoich, HoC_eff, relax, inv_s, inv_dt;
   int extinction, nsub;
+  int vec_ok;  // every array 16-byte aligned
 };
 
-__global__ void k_edc_main32(int64_t n, Edc32Args a) {
-  __shared__ int sh[32];
-  const int t = threadIdx.x;
-  const int64_t c = (int64_t)blockIdx.x * E32_BLK + t;
-  const bool live = c < n;
-  float Yf = 0.f, YO2 = 0.f, YH = 0.f;
-  if (live) { Yf = a.Yf[c]; YO2 = a.YO[c]; YH = a.YH[c]; }
-  int v = live ? edc_flag_code32(Yf, YO2, YH, t) : -1;
-  const int lane = t & 31, wid = t >> 5;
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v = max(v, y);
-  }
-  if (lane == 31) sh[wid] = v;
-  __syncthreads();
-  if (wid == 0) {
-    int w = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : -1;
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w = max(w, y);
-    }
-    sh[lane] = w;
-  }
-  __syncthreads();
-  if (wid > 0) v = max(v, sh[wid - 1]);
-  if (!live) return;
-  const bool flag = (v >= 0) ? (v & 1) : (a.carry[blockIdx.x] > 0);
-  float Tg = a.Tg[c];
-  const float rho_i = a.rho[c];
-  float k_t = a.kt[c];
+// One cell's EDC update in float arithmetic (edc_cell's steps); Yf, YO2, Tg
+// in place, the mean reaction rate returned.
+__device__ __forceinline__ float edc_cell32(const Edc32Args& a, bool flag, float& Yf, float& YO2,
+                                            float YH, float& Tg, float rho_i, float k_t,
+                                            float e_t) {
   if (k_t < 1.0e-4f) k_t = 1.0e-4f;
-  float e_t = a.et[c];
   if (e_t < 1.0e-6f) e_t = 1.0e-6f;
   float ratio = 1.5e-5f * e_t / (k_t * k_t);
   if (ratio < 1e-30f) ratio = 1e-30f;
@@ -179,13 +185,50 @@ __global__ void k_edc_main32(int64_t n, Edc32Args a) {
     if (Tg > 2400.0f) Tg = 2400.0f;
     acc += omega * h;
   }
-  a.Yf[c] = Yf;
-  a.YO[c] = YO2;
-  a.Tg[c] = Tg;
-  a.omega[c] = a.dt > 0.0f ? acc * a.inv_dt : 0.0f;
+  return a.dt > 0.0f ? acc * a.inv_dt : 0.0f;
+}
+
+__global__ void __launch_bounds__(EDC_TPB)
+k_edc_main32(int64_t n, Edc32Args a) {
+  __shared__ int sh[EDC_TPB / 32];
+  const int t = threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * E32_BLK + EDC_CPT * t;
+  const bool vec = a.vec_ok && c0 + EDC_CPT <= n;
+  float yf[EDC_CPT], yo[EDC_CPT], yh[EDC_CPT], tg[EDC_CPT], rh[EDC_CPT], kt[EDC_CPT],
+      et[EDC_CPT];
+  e32_ld4(a.Yf, c0, n, vec, yf);
+  e32_ld4(a.YO, c0, n, vec, yo);
+  e32_ld4(a.YH, c0, n, vec, yh);
+  e32_ld4(a.Tg, c0, n, vec, tg);
+  e32_ld4(a.rho, c0, n, vec, rh);
+  e32_ld4(a.kt, c0, n, vec, kt);
+  e32_ld4(a.et, c0, n, vec, et);
+  const bool carry_in = a.carry[blockIdx.x] > 0;
+  int code[EDC_CPT];
+  int last = -1;
+#pragma unroll
+  for (int q = 0; q < EDC_CPT; ++q) {
+    code[q] = (c0 + q < n) ? edc_flag_code32(yf[q], yo[q], yh[q], EDC_CPT * t + q) : -1;
+    last = max(last, code[q]);
+  }
+  int run = edc_block_exclusive_max(last, sh);
+  if (c0 >= n) return;
+  float om[EDC_CPT];
+#pragma unroll
+  for (int q = 0; q < EDC_CPT; ++q) {
+    run = max(run, code[q]);
+    const bool flag = (run >= 0) ? (run & 1) : carry_in;
+    om[q] = edc_cell32(a, flag, yf[q], yo[q], yh[q], tg[q], rh[q], kt[q], et[q]);
+  }
+  e32_st4(a.Yf, c0, n, vec, yf);
+  e32_st4(a.YO, c0, n, vec, yo);
+  e32_st4(a.Tg, c0, n, vec, tg);
+  e32_st4(a.omega, c0, n, vec, om);
 }
 
 int64_t edc32_scratch_bytes(int64_t n) { return 2 * ((n + E32_BLK - 1) / E32_BLK) + 16; }
+
+static bool al16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
 int launch_edc32(int64_t n, const float* rho, float* Tg, float* Yf, float* YO, const float* kt,
                  const float* et, const float* YH, float* omega, double chi_rad, double cp_g,
@@ -195,7 +238,9 @@ int launch_edc32(int64_t n, const float* rho, float* Tg, float* Yf, float* YO, c
   const int64_t nb = (n + E32_BLK - 1) / E32_BLK;
   signed char* agg = (signed char*)scratch;
   signed char* carry = agg + nb;
-  k_edc_agg32<<<(unsigned)nb, E32_BLK, 0, st>>>(n, Yf, YO, YH, agg);
+  const int vec_ok = al16(rho) && al16(Tg) && al16(Yf) && al16(YO) && al16(kt) && al16(et) &&
+                     al16(YH) && al16(omega);
+  k_edc_agg32<<<(unsigned)nb, EDC_TPB, 0, st>>>(n, Yf, YO, YH, vec_ok, agg);
   fs_count_launch();
   int rc = launch_edc_carry((int)nb, agg, carry, st);
   if (rc != FS_OK) return rc;
@@ -209,26 +254,26 @@ int launch_edc32(int64_t n, const float* rho, float* Tg, float* Yf, float* YO, c
   a.nsub = n_substeps > 1 ? n_substeps : 1;
   a.relax = (float)(1.0 - exp(-(dt / (double)a.nsub) / 0.5));
   a.extinction = extinction;
-  k_edc_main32<<<(unsigned)nb, E32_BLK, 0, st>>>(n, a);
+  a.vec_ok = vec_ok;
+  k_edc_main32<<<(unsigned)nb, EDC_TPB, 0, st>>>(n, a);
   fs_count_launch();
   return cuda_status();
 }
 
 // ---- species step ------------------------------------------------------------
+// minmod and the MUSCL face value in float (the FP64 helpers' forms)
 __device__ __forceinline__ float minmod32(float a, float b) {
-  const float lo = a < b ? a : b, hi = a > b ? a : b;
-  const float m = a > 0.0f ? lo : hi;
+  const float m = copysignf(fminf(fabsf(a), fabsf(b)), a);
   return (a * b <= 0.0f) ? 0.0f : m;
 }
 
 __device__ __forceinline__ float muscl_face32(float pim1, float pi, float pip1, float pip2,
                                               float uf) {
   const bool up = uf >= 0.0f;
-  const float a = up ? pi - pim1 : pip1 - pi;
-  const float b = up ? pip1 - pi : pip2 - pip1;
+  const float m = minmod32(pip1 - pi, up ? pi - pim1 : pip2 - pip1);
   const float base = up ? pi : pip1;
   const float half = up ? 0.5f : -0.5f;
-  return base + half * minmod32(a, b);
+  return base + half * m;
 }
 
 #define S32_TX 32
@@ -341,44 +386,72 @@ struct Diff32Args {
   int clip;
 };
 
+// A block owns a 32 x 8 tile and marches up a chunk of z-levels (the FP64
+// kernel's scheme): the column's k-1, k, k+1 values stay in registers and
+// level k+2 is requested while level k computes.
+#define TD32_MAXKZ 64
 template <int NF>
 __global__ void __launch_bounds__(S32_TX * S32_TY, 4)
     k_turb_diff32(GridDev g, Diff32Args a, const float* __restrict__ nu_t, float inv_sc,
-                  float dt_sub, float inv_dx2, float inv_dy2) {
-  __shared__ float rk[3];
+                  float dt_sub, float inv_dx2, float inv_dy2, int kz) {
+  __shared__ float rk[TD32_MAXKZ][3];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int64_t sy = nx, sz = (int64_t)nx * ny;
-  const int k = blockIdx.z;
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    rk[0] = (float)(1.0 / g.dz[k]);
-    rk[1] = (float)(1.0 / g.da[k]);
-    rk[2] = (float)(1.0 / g.db[k]);
+  const int k0 = blockIdx.z * kz;
+  const int k1 = min(nz, k0 + kz);
+  const int tid = threadIdx.y * S32_TX + threadIdx.x;
+  for (int q = tid; q < k1 - k0; q += S32_TX * S32_TY) {
+    rk[q][0] = (float)(1.0 / g.dz[k0 + q]);
+    rk[q][1] = (float)(1.0 / g.da[k0 + q]);
+    rk[q][2] = (float)(1.0 / g.db[k0 + q]);
   }
   __syncthreads();
   const int i = blockIdx.x * S32_TX + threadIdx.x;
   const int j = blockIdx.y * S32_TY + threadIdx.y;
-  if (i >= nx || j >= ny) return;
-  const int64_t crow = (int64_t)k * sz + i;
-  const int64_t c = crow + (int64_t)j * sy;
-  const int64_t cjp = crow + wrapj(j + 1, ny) * sy, cjm = crow + wrapj(j - 1, ny) * sy;
-  const float D_t = nu_t[c] * inv_sc;
+  if (i >= nx || j >= ny || k0 >= nz) return;
+  const int64_t col = (int64_t)j * sy + i;
+  const int64_t cjp0 = (int64_t)wrapj(j + 1, ny) * sy + i, cjm0 = (int64_t)wrapj(j - 1, ny) * sy + i;
+  float fL[NF], fC[NF], fN[NF];
 #pragma unroll
   for (int s = 0; s < NF; ++s) {
-    const float* __restrict__ f = a.f[s];
-    const float fc = f[c];
-    const float fxL = (i == 0) ? fc : f[c - 1];
-    const float fxR = (i == nx - 1) ? fc : f[c + 1];
-    const float fzL = (k == 0) ? fc : f[c - sz];
-    const float fzR = (k == nz - 1) ? fc : f[c + sz];
-    const float d2x = (fxR - 2.0f * fc + fxL) * inv_dx2;
-    const float d2y = (f[cjp] - 2.0f * fc + f[cjm]) * inv_dy2;
-    const float d2z = ((fzR - fc) * rk[1] - (fc - fzL) * rk[2]) * rk[0];
-    float nv = fc + D_t * (d2x + d2y + d2z) * dt_sub;
-    if (a.clip) {
-      if (nv < a.lo[s]) nv = a.lo[s];
-      if (nv > a.hi[s]) nv = a.hi[s];
+    fC[s] = a.f[s][(int64_t)k0 * sz + col];
+    fL[s] = (k0 == 0) ? fC[s] : a.f[s][(int64_t)(k0 - 1) * sz + col];
+    fN[s] = (k0 == nz - 1) ? fC[s] : a.f[s][(int64_t)(k0 + 1) * sz + col];
+  }
+  float nu_c = nu_t[(int64_t)k0 * sz + col];
+  for (int k = k0; k < k1; ++k) {
+    const int64_t ks = (int64_t)k * sz;
+    const int64_t c = ks + col;
+    const bool more = k + 1 < k1;
+    float nu_n = 0.0f, fNN[NF];
+    if (more) nu_n = nu_t[c + sz];
+#pragma unroll
+    for (int s = 0; s < NF; ++s)
+      fNN[s] = (more && k + 2 < nz) ? a.f[s][c + 2 * sz] : fN[s];
+    const float D_t = nu_c * inv_sc;
+    const float r0 = rk[k - k0][0], r1 = rk[k - k0][1], r2 = rk[k - k0][2];
+#pragma unroll
+    for (int s = 0; s < NF; ++s) {
+      const float* __restrict__ f = a.f[s];
+      const float fc = fC[s];
+      const float fxL = (i == 0) ? fc : f[c - 1];
+      const float fxR = (i == nx - 1) ? fc : f[c + 1];
+      const float fzL = fL[s];
+      const float fzR = fN[s];
+      const float d2x = (fxR - 2.0f * fc + fxL) * inv_dx2;
+      const float d2y = (f[ks + cjp0] - 2.0f * fc + f[ks + cjm0]) * inv_dy2;
+      const float d2z = ((fzR - fc) * r1 - (fc - fzL) * r2) * r0;
+      float nv = fc + D_t * (d2x + d2y + d2z) * dt_sub;
+      if (a.clip) {
+        if (nv < a.lo[s]) nv = a.lo[s];
+        if (nv > a.hi[s]) nv = a.hi[s];
+      }
+      a.fo[s][c] = nv;
+      fL[s] = fc;
+      fC[s] = fzR;
+      fN[s] = fNN[s];
     }
-    a.fo[s][c] = nv;
+    nu_c = nu_n;
   }
 }
 
@@ -394,13 +467,24 @@ int launch_turb_diff32(const GridDev& g, int nfield, const float* const* f, floa
     a.lo[s] = clip ? (float)lo[s] : 0.0f;
     a.hi[s] = clip ? (float)hi[s] : 0.0f;
   }
-  const dim3 nb((g.nx + S32_TX - 1) / S32_TX, (g.ny + S32_TY - 1) / S32_TY, g.nz);
+  // z-chunks: about six blocks per SM of the 148, at least four levels each
+  const int tiles = ((g.nx + S32_TX - 1) / S32_TX) * ((g.ny + S32_TY - 1) / S32_TY);
+  int chunks = (6 * 148 + tiles - 1) / tiles;
+  if (chunks > g.nz) chunks = g.nz;
+  if (chunks < 1) chunks = 1;
+  int kz = (g.nz + chunks - 1) / chunks;
+  if (kz < 4) kz = g.nz < 4 ? g.nz : 4;
+  if (kz > TD32_MAXKZ) kz = TD32_MAXKZ;
+  chunks = (g.nz + kz - 1) / kz;
+  const dim3 nb((g.nx + S32_TX - 1) / S32_TX, (g.ny + S32_TY - 1) / S32_TY, chunks);
   const dim3 tb(S32_TX, S32_TY);
   const float ix2 = (float)(1.0 / (g.dx * g.dx)), iy2 = (float)(1.0 / (g.dy * g.dy));
   if (nfield == 1)
-    k_turb_diff32<1><<<nb, tb, 0, st>>>(g, a, nu_t, (float)(1.0 / sc_t), (float)dt_sub, ix2, iy2);
+    k_turb_diff32<1><<<nb, tb, 0, st>>>(g, a, nu_t, (float)(1.0 / sc_t), (float)dt_sub, ix2, iy2,
+                                        kz);
   else
-    k_turb_diff32<3><<<nb, tb, 0, st>>>(g, a, nu_t, (float)(1.0 / sc_t), (float)dt_sub, ix2, iy2);
+    k_turb_diff32<3><<<nb, tb, 0, st>>>(g, a, nu_t, (float)(1.0 / sc_t), (float)dt_sub, ix2, iy2,
+                                        kz);
   fs_count_launch();
   return cuda_status();
 }

@@ -596,10 +596,11 @@ struct DiffArgs {
 
 // A block owns a 32 x 8 (x, y) tile and marches up a chunk of z-levels: each
 // thread keeps its column's values at k-1, k and k+1 of every field in
-// registers (the z-neighbours cost no loads) and reads the next level one
-// step ahead; x- and y-neighbours come from L1.  The chunk's reciprocal
-// spacings are computed once per block.  The arithmetic of each cell is the
-// one-thread-per-cell form's, expression for expression.
+// registers (the z-neighbours cost no loads) and requests level k+2 (and the
+// next level's nu_t) while level k computes, so a column always has a level
+// of loads in flight; x- and y-neighbours come from L1.  The chunk's
+// reciprocal spacings are computed once per block.  The arithmetic of each
+// cell is the one-thread-per-cell form's, expression for expression.
 #define TD_MAXKZ 64
 template <int NF>
 __global__ void __launch_bounds__(SP_TX * SP_TY, 4)
@@ -622,19 +623,29 @@ k_turb_diff(GridDev g, DiffArgs a, const double* __restrict__ nu_t, double sc_t,
   if (i >= nx || j >= ny || k0 >= nz) return;
   const int64_t col = (int64_t)j * sy + i;
   const int64_t cjp0 = (int64_t)wrapj(j + 1, ny) * sy + i, cjm0 = (int64_t)wrapj(j - 1, ny) * sy + i;
-  double fL[NF], fC[NF];
+  // fL, fC, fN: the column at k-1, k and k+1 (k+1 clamped to k at the top)
+  double fL[NF], fC[NF], fN[NF];
 #pragma unroll
   for (int s = 0; s < NF; ++s) {
     fC[s] = a.f[s][(int64_t)k0 * sz + col];
     fL[s] = (k0 == 0) ? fC[s] : a.f[s][(int64_t)(k0 - 1) * sz + col];
+    fN[s] = (k0 == nz - 1) ? fC[s] : a.f[s][(int64_t)(k0 + 1) * sz + col];
   }
+  double nu_c = nu_t[(int64_t)k0 * sz + col];
   for (int k = k0; k < k1; ++k) {
     const int64_t ks = (int64_t)k * sz;
     const int64_t c = ks + col;
+    // the next level's loads: nu_t at k+1 and the fields at k+2
+    const bool more = k + 1 < k1;
+    double nu_n = 0.0, fNN[NF];
+    if (more) nu_n = nu_t[c + sz];
+#pragma unroll
+    for (int s = 0; s < NF; ++s)
+      fNN[s] = (more && k + 2 < nz) ? a.f[s][c + 2 * sz] : fN[s];
     const double inv_dz_k = rk[k - k0][0];
     const double inv_d_above = rk[k - k0][1];
     const double inv_d_below = rk[k - k0][2];
-    const double D_t = nu_t[c] / sc_t;
+    const double D_t = nu_c / sc_t;
 #pragma unroll
     for (int s = 0; s < NF; ++s) {
       const double* __restrict__ f = a.f[s];
@@ -642,7 +653,7 @@ k_turb_diff(GridDev g, DiffArgs a, const double* __restrict__ nu_t, double sc_t,
       const double fxL = (i == 0) ? fc : f[c - 1];
       const double fxR = (i == nx - 1) ? fc : f[c + 1];
       const double fzL = fL[s];
-      const double fzR = (k == nz - 1) ? fc : f[c + sz];
+      const double fzR = fN[s];
       double d2x = (fxR - 2.0 * fc + fxL) * inv_dx2;
       double d2y = (f[ks + cjp0] - 2.0 * fc + f[ks + cjm0]) * inv_dy2;
       double d2z = ((fzR - fc) * inv_d_above - (fc - fzL) * inv_d_below) * inv_dz_k;
@@ -655,7 +666,9 @@ k_turb_diff(GridDev g, DiffArgs a, const double* __restrict__ nu_t, double sc_t,
       a.fo[s][c] = nv;
       fL[s] = fc;
       fC[s] = fzR;
+      fN[s] = fNN[s];
     }
+    nu_c = nu_n;
   }
 }
 
@@ -1132,42 +1145,8 @@ __global__ void k_solid_cond(GridDev g, const double* __restrict__ Ts,
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   int k = blockIdx.z;
   if (i >= g.nx || j >= g.ny) return;
-  const int64_t sz = (int64_t)g.nx * g.ny;
   const int64_t c = cidx(g, k, j, i);
-  const double asc = as[c];
-  const double T0 = Ts[c];
-  if (asc <= 0.0) {
-    double x = T0;
-    if (cap) {
-      if (x > hi) x = hi;
-      if (x < lo) x = lo;
-    }
-    To[c] = x;
-    return;
-  }
-  double fu = 0.0, fd = 0.0;
-  if (k < g.nz - 1) {
-    double aa = as[c + sz];
-    if (aa > 0.0) {
-      double ae = 2.0 * asc * aa / (asc + aa);
-      fu = k_solid * ae * (Ts[c + sz] - T0) / g.da[k];
-    }
-  }
-  if (k > 0) {
-    double ab = as[c - sz];
-    if (ab > 0.0) {
-      double ae = 2.0 * asc * ab / (asc + ab);
-      fd = k_solid * ae * (Ts[c - sz] - T0) / g.db[k];
-    }
-  }
-  double src = (fu + fd) / g.dz[k];
-  double dT = dt * src * inv_rho_cp / asc;
-  double x = T0 + dT;
-  if (cap) {
-    if (x > hi) x = hi;
-    if (x < lo) x = lo;
-  }
-  To[c] = x;
+  To[c] = solid_cond_cell(g, Ts, as, k, c, Ts[c], k_solid, inv_rho_cp, dt, cap, lo, hi);
 }
 
 int launch_solid_cond(const GridDev& g, const double* Ts, const double* as, double* To,

@@ -93,9 +93,11 @@ class Tier3Solver:
     pressure solve in flexible CG preconditioned by the U-Net of
     ``learned.py`` (weights from ``learned_weights``, default the packaged
     file), falling back to the V-cycle when it stalls.  ``dom_sweep`` forces a
-    DOM sweep path (``fs_dom_set_sweep_mode``; 0 picks automatically) and
+    DOM sweep path (``fs_dom_set_sweep_mode``; 0 picks automatically),
     ``dom_cluster_ctas`` its CTAs per octant (0: automatic; a nonzero value
-    alone selects path 8)."""
+    alone selects path 8) and ``dom_kernel`` path 8's kernel
+    (``fs_dom_set_sweep_kernel``: 0 automatic, 1 pencil per thread, 2 lane
+    column)."""
 
     FIELDS = ("rho", "u", "v", "w", "T_g", "Y_fuel", "Y_O2", "Y_H2O", "T_s", "alpha_s",
               "k_turb", "eps_turb", "nu_t", "phi")
@@ -104,7 +106,7 @@ class Tier3Solver:
                  proj_maxiter: int = 200, mg_sweeps: int | None = None, form: str = "plain",
                  overlap_dom: bool = True, dom_sweep: int = 0, learned_weights=None,
                  learned_max: int = 30, learned_stall: float = 0.9, dom_cluster_ctas: int = 0,
-                 mg_fine_sweeps: int | None = None):
+                 mg_fine_sweeps: int | None = None, dom_kernel: int = 0):
         self.lib = _lib.lib()
         self.dev = torch.device(device)
         if self.dev.type == "cuda" and self.dev.index is None:
@@ -235,6 +237,9 @@ class Tier3Solver:
             check(self.lib.fs_dom_set_sweep_mode(self.dom, int(dom_sweep or 8),
                                                  int(dom_cluster_ctas)),
                   "fs_dom_set_sweep_mode")
+        if dom_kernel:
+            check(self.lib.fs_dom_set_sweep_kernel(self.dom, int(dom_kernel)),
+                  "fs_dom_set_sweep_kernel")
         # clock
         self.t = 0.0
         self.dt = float(self.p["dt0"])
@@ -775,18 +780,17 @@ class Tier3Solver:
         L, f, w, p, gp, g = self.lib, self.f, self.w, self.p, self.gp, self.grid
         s = self._s()
         self._phase("gas_update")
-        check(L.fs_gas_energy_update(gp, ptr(f["T_g"]), ptr(f["rho"]), ptr(f["Y_H2O"]),
-                                     ptr(f["T_s"]), ptr(Sp), ptr(Sd),
-                                     ptr(self.bed_out["Q_g_conv"]), ptr(w["q_rad_gas"]),
-                                     ptr(w["Q_comb"]), dt_sub, p["T_amb"], p["h_bed"],
-                                     drip, g.n_z_bed, p["i_src_start"], p["i_src_end"], s),
-              "gas_update")
-        self._phase("solid_cond")
-        # the conduction with the T_s cap of the sub-step's end fused in: nothing
-        # between them reads or writes T_s (spread_3d.py:3168-3196)
-        check(L.fs_solid_conduction_capped(gp, ptr(f["T_s"]), ptr(f["alpha_s"]), ptr(w["tmp4"]),
-                                           0.20, 500.0, 1300.0, dt_sub, p["T_amb"], T_CAP, s),
-              "solid_cond")
+        # the gas-energy update and the vertical solid conduction with the T_s
+        # cap of the sub-step's end in one pass: both read the old T_s and
+        # nothing between them reads or writes it (spread_3d.py:3104-3196)
+        check(L.fs_gas_energy_solid_update(gp, ptr(f["T_g"]), ptr(f["rho"]), ptr(f["Y_H2O"]),
+                                           ptr(f["T_s"]), ptr(Sp), ptr(Sd),
+                                           ptr(self.bed_out["Q_g_conv"]), ptr(w["q_rad_gas"]),
+                                           ptr(w["Q_comb"]), dt_sub, p["T_amb"], p["h_bed"],
+                                           drip, g.n_z_bed, p["i_src_start"], p["i_src_end"],
+                                           ptr(f["alpha_s"]), ptr(w["tmp4"]), 0.20, 500.0,
+                                           1300.0, p["T_amb"], T_CAP, s),
+              "gas_update + solid_cond")
         self._swap("T_s", "tmp4")
         self._phase("turb_diff_T")
         if n_pr > 0:

@@ -182,6 +182,20 @@ int fs_gas_energy_update(const FsGrid* g, double* T_g, const double* rho, const 
                          double dt_sub, double T_amb, double h_bed, int drip_on, int n_z_bed,
                          int i_src0, int i_src1, void* stream);
 
+/* The sub-step's gas-energy update and its capped solid conduction in one
+ * pass: the results of fs_gas_energy_update(g, T_g, ..., i_src1) followed by
+ * fs_solid_conduction_capped(g, T_s, alpha_s, T_s_out, k_solid, rho_solid,
+ * cp_solid, dt_sub, Ts_lo, Ts_hi), bit for bit (both read the old T_s; neither
+ * reads what the other writes).  T_s_out must not be T_s. */
+int fs_gas_energy_solid_update(const FsGrid* g, double* T_g, const double* rho,
+                               const double* Y_H2O, const double* T_s, const double* S_pyro,
+                               const double* S_drying, const double* Q_g_conv,
+                               const double* q_rad_gas, double* Q_comb_out, double dt_sub,
+                               double T_amb, double h_bed, int drip_on, int n_z_bed, int i_src0,
+                               int i_src1, const double* alpha_s, double* T_s_out,
+                               double k_solid, double rho_solid, double cp_solid, double Ts_lo,
+                               double Ts_hi, void* stream);
+
 /* spread_3d.py:2300-2317 (with S_pyro = S_pyro_bed + S_drying_bed,
  * :2147-2148): div_target = (S_pyro - (rho - rho_prev)/dt) / max(rho, 0.1),
  * the right-hand side of the pressure iterations; overwrites div_target. */
@@ -422,6 +436,18 @@ int fs_dom_set_sweep_mode(void* handle, int mode, int cluster_ctas);
 int fs_dom_set_octant_groups(void* handle, int groups);
 /* The path in use (0 before the first solve or intensity load). */
 int fs_dom_sweep_mode(void* handle);
+/* Path 8's kernel: 1 one pencil per thread (a hyperplane's intensities pass
+ * through shared memory, one barrier over all pencil warps; the default, also
+ * for 0), 2 lane column (a lane owns one y column of all of the CTA's k' rows
+ * and keeps their intensities in registers, y-neighbours by warp shuffles;
+ * built for ten ordinates per cluster, 4 to 8 rows per CTA and ny <= 128;
+ * FS_EARG at the first solve for other shapes).  Both give the same results
+ * bit for bit; the lane-column kernel is the slower one on the S8 workload
+ * (3.85 against 1.95 ms per FP64 sweep at 400 x 120 x 60).  Only before the
+ * first solve or intensity load.  fs_dom_sweep_kernel: the kernel in use (0
+ * before the path is resolved or on path 3). */
+int fs_dom_set_sweep_kernel(void* handle, int kernel);
+int fs_dom_sweep_kernel(void* handle);
 /* The division by a run-time invariant divisor that the kernels use to split
  * a flat cell index into (i, j, k): q[t] = x[t] / d for t < n, computed on the
  * host by the same multiply-high formula.  FS_EARG for d == 0 or n < 0. */

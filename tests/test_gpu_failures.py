@@ -87,17 +87,20 @@ def test_learned_stall_falls_back_and_converges():
     s.close()
 
 
+@pytest.mark.parametrize("kernel", [1, 2])
 @pytest.mark.parametrize("fp32", [0, 1])
-def test_dom_hand_off_wait_runs_out_with_status_4(fp32):
+def test_dom_hand_off_wait_runs_out_with_status_4(fp32, kernel):
     """Path 8's CTAs wait for one another's rows with bounded waits.  With the
     test switch one CTA withholds a row (a fill that nothing else sends), the
     next CTA's wait runs out, the solve returns FS_ETIMEOUT (4) instead of
-    hanging, and the same object then solves normally."""
+    hanging, and the same object then solves normally; with either sweep
+    kernel (pencil per thread on 29 levels in CTAs of 3 rows, lane column on
+    40 levels in CTAs of 4)."""
     from gpu_helpers import Grid, call, dev, host, lib, stream
     from firewebapp_b200._lib import dbl_array, ptr
     from firewebapp_b200.quadrature import level_symmetric
     om, wq = level_symmetric(8)
-    nz, ny, nx = 29, 40, 48
+    nz, ny, nx = (29, 40, 48) if kernel == 1 else (40, 40, 48)
     rng = np.random.default_rng(3)
     g = Grid(nz, ny, nx, 0.5, 0.5, np.full(nz, 0.1))
     h = C.c_void_p()
@@ -122,7 +125,9 @@ def test_dom_hand_off_wait_runs_out_with_status_4(fp32):
         if fp32:
             call("fs_dom_set_precision", h, 1)
         call("fs_dom_set_sweep_mode", h, 8, 0)
+        call("fs_dom_set_sweep_kernel", h, kernel)
         assert solve() == 0
+        assert lib().fs_dom_sweep_kernel(h) == kernel
         call("fs_dom_set_wait_test", h, 5)
         assert solve() == 4
         assert b"gave up" in lib().fs_last_error()

@@ -161,6 +161,38 @@ def test_solid_conduction_capped_equals_conduction_then_clip():
     assert np.array_equal(host(out), r)
 
 
+def test_gas_energy_solid_update_equals_the_two_calls():
+    """The fused sub-step update: T_g, Q_comb and the new T_s equal
+    fs_gas_energy_update then fs_solid_conduction_capped, bit for bit (drip on,
+    a bed of 4 levels, odd sizes so the tail blocks are partial)."""
+    rng = np.random.default_rng(31)
+    nz, ny, nx = 9, 7, 13
+    g = Grid(nz, ny, nx, 0.1, 0.1, np.linspace(0.02, 0.05, nz))
+    shape = (nz, ny, nx)
+    Tg = 300.0 + 1500.0 * rng.random(shape)
+    Ts = dev(250.0 + 2000.0 * rng.random(shape))
+    a_s = dev(np.where(rng.random(shape) < 0.6, 0.05 * rng.random(shape), 0.0))
+    rho = dev(0.2 + rng.random(shape))
+    YH = dev(0.2 * rng.random(shape))
+    Sp, Sd, Qgc = (dev(v * rng.random(shape)) for v in (0.05, 0.02, 3.0e4))
+    qrg = dev(2.0e3 * (rng.random(shape) - 0.3))
+    args = (0.01, 300.0, 0.3, 1, 4, 3, 8)
+    Tg_a, Tg_b = dev(Tg), dev(Tg)
+    qc_a, qc_b = torch.zeros_like(Tg_a), torch.zeros_like(Tg_b)
+    To_a, To_b = torch.empty_like(Ts), torch.empty_like(Ts)
+    call("fs_gas_energy_update", g.ref, ptr(Tg_a), ptr(rho), ptr(YH), ptr(Ts), ptr(Sp), ptr(Sd),
+         ptr(Qgc), ptr(qrg), ptr(qc_a), *args, stream())
+    call("fs_solid_conduction_capped", g.ref, ptr(Ts), ptr(a_s), ptr(To_a), 0.2, 500.0, 1300.0,
+         0.01, 300.0, 1800.0, stream())
+    call("fs_gas_energy_solid_update", g.ref, ptr(Tg_b), ptr(rho), ptr(YH), ptr(Ts), ptr(Sp),
+         ptr(Sd), ptr(Qgc), ptr(qrg), ptr(qc_b), *args, ptr(a_s), ptr(To_b), 0.2, 500.0, 1300.0,
+         300.0, 1800.0, stream())
+    assert np.array_equal(host(Tg_a), host(Tg_b))
+    assert np.array_equal(host(qc_a), host(qc_b))
+    assert np.array_equal(host(To_a), host(To_b))
+    assert not np.array_equal(host(Tg_a), Tg)  # the update did something
+
+
 def test_momentum(vectors):
     for name in vectors.cases("momentum"):
         c = vectors.case("momentum", name)
@@ -264,6 +296,43 @@ def test_edc_flag_scan_many_blocks():
          ptr(om), 0.34, 1100.0, 2e-3, 1, 1.3, 17e6, 0, ptr(scratch), stream())
     for got, exp in zip((Tg, Yf, YO, om), want):
         assert rel_l2(host(got), exp) <= LIBM
+
+
+@pytest.mark.parametrize("f32", [False, True])
+def test_edc_unaligned_arrays_and_ragged_tail(f32):
+    """Arrays that start 8 (4) bytes past a 16-byte boundary take the
+    element-wise loads, and n = 4 * 1024 * 37 + 3 leaves a partial last tile
+    and a thread with fewer than four cells: the results equal those of the
+    same inputs in aligned arrays, bit for bit."""
+    rng = np.random.default_rng(19)
+    n = 4 * 1024 * 37 + 3
+    dt_np = np.float32 if f32 else np.float64
+    ins = {"rho": rng.uniform(0.3, 1.2, n), "k": rng.uniform(1e-3, 1.0, n),
+           "e": rng.uniform(1e-3, 1.0, n), "Tg": rng.uniform(300.0, 1800.0, n),
+           "Yf": np.where(rng.random(n) < 3e-3, rng.uniform(0.0, 0.2, n), 0.0),
+           "YO": rng.uniform(0.0, 0.232, n), "YH": rng.uniform(0.0, 0.2, n)}
+    fn = "fs_edc_f32" if f32 else "fs_edc"
+    nscr = int(getattr(lib(), fn + "_scratch_bytes")(n)) + 16
+
+    def run(offset):
+        bufs = {}
+        for key, v in ins.items():
+            t = torch.zeros(n + 1, dtype=torch.float32 if f32 else torch.float64, device="cuda")
+            t[offset:offset + n] = torch.from_numpy(v.astype(dt_np)).cuda()
+            bufs[key] = t
+        om = torch.zeros(n + 1, dtype=bufs["Tg"].dtype, device="cuda")
+        scratch = torch.zeros(nscr, dtype=torch.uint8, device="cuda")
+        p = {key: t.data_ptr() + offset * t.element_size() for key, t in bufs.items()}
+        pom = om.data_ptr() + offset * om.element_size()
+        call(fn, n, p["rho"], p["Tg"], p["Yf"], p["YO"], p["k"], p["e"], p["YH"], pom, 0.34,
+             1100.0, 2e-3, 1, 1.3, 17e6, 1, ptr(scratch), stream())
+        torch.cuda.synchronize()
+        return [host(t[offset:offset + n]) for t in (bufs["Tg"], bufs["Yf"], bufs["YO"], om)]
+
+    aligned, shifted = run(0), run(1)
+    for a, b in zip(aligned, shifted):
+        assert np.array_equal(a, b)
+    assert not np.array_equal(aligned[0], ins["Tg"].astype(dt_np))
 
 
 def test_edc_flag_leak_crosses_blocks():
@@ -439,9 +508,12 @@ def test_dom_s8_matches_reference(fp32):
             lib().fs_dom_destroy(h)
 
 
-def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0, groups=0):
+def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0, groups=0,
+                kernel=0, want_kernel=None):
     """q_rad_solid, q_rad_gas, q_in_soil after each of ``calls`` solves of an
-    S_order DOM on seeded random fields (the y-inflow rows persist between calls)."""
+    S_order DOM on seeded random fields (the y-inflow rows persist between calls);
+    ``kernel`` picks path 8's sweep kernel (0 automatic, 1 pencil per thread,
+    2 lane column) and ``want_kernel`` is the one that must have run."""
     from firewebapp_b200.quadrature import level_symmetric
     om, wq = level_symmetric(order)
     rng = np.random.default_rng(seed)
@@ -457,6 +529,8 @@ def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0, 
         call("fs_dom_set_sweep_mode", h, mode, cluster_ctas)
         if groups:
             call("fs_dom_set_octant_groups", h, groups)
+        if kernel:
+            call("fs_dom_set_sweep_kernel", h, kernel)
         shape = (nz, ny, nx)
         for it in range(calls):
             Ts = dev(300.0 + 900.0 * rng.random(shape) ** 4)
@@ -473,9 +547,31 @@ def _dom_solves(mode, fp32, nz, ny, nx, seed, calls=2, order=8, cluster_ctas=0, 
                  ptr(Tsoil), ptr(YH), ptr(rho), ptr(M), ptr(qs), ptr(qg), ptr(qsoil), stream())
             out.append((host(qs), host(qg), host(qsoil), lib().fs_dom_iterations(h)))
         assert lib().fs_dom_sweep_mode(h) == mode
+        if want_kernel is not None:
+            assert lib().fs_dom_sweep_kernel(h) == want_kernel
     finally:
         lib().fs_dom_destroy(h)
     return out
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+@pytest.mark.parametrize("shape", [(60, 120, 24), (37, 70, 33), (40, 40, 48), (80, 64, 20)])
+def test_dom_lane_column_kernel_equals_pencil_kernel(fp32, shape):
+    """Path 8's two kernels give the same results bit for bit, with the same
+    source iterations over three solves (the y-inflow rows carried between
+    them): the workload's 60 x 120 cross-section (10 CTAs of 6 rows, 4 warps),
+    a partial last CTA (37 levels in CTAs of 4 rows) with a partial last warp
+    (70 columns) and odd nx, two warps of 40 columns, and CTAs of 8 rows over
+    two full warps.  The automatic choice is the pencil-per-thread kernel (the
+    faster one on the workload)."""
+    nz, ny, nx = shape
+    a = _dom_solves(8, fp32, nz, ny, nx, seed=21, calls=3, kernel=1, want_kernel=1)
+    b = _dom_solves(8, fp32, nz, ny, nx, seed=21, calls=3, kernel=2, want_kernel=2)
+    c = _dom_solves(8, fp32, nz, ny, nx, seed=21, calls=1, want_kernel=1)
+    for (qa, ga, sa, ia), (qb, gb, sb, ib) in zip(a, b):
+        assert ia == ib
+        assert np.array_equal(qa, qb) and np.array_equal(ga, gb) and np.array_equal(sa, sb)
+    assert np.array_equal(c[0][0], a[0][0])
 
 
 @pytest.mark.parametrize("fp32", [0, 1])
