@@ -349,7 +349,9 @@ struct ClArgs {
 #define CL_AHEAD 4
 // Slots of the ring through which a CTA hands the last row of each
 // hyperplane to the next CTA of the cluster: the upstream CTA runs up to
-// CL_RING - 2 hyperplanes ahead of the downstream one.
+// CL_RING - 1 hyperplanes ahead of the downstream one (CL_RING - 2 in the
+// lane-column kernel, which sends a row before the barrier that ends its
+// hyperplane instead of after it).
 #define CL_RING 3
 // Threads per CTA (the helper warp included): one pencil per thread up to
 // CL_MAX_THREADS_1 (80 registers a thread), else two pencils per thread up to
@@ -578,7 +580,7 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
   int pq[PPT], pjp[PPT], pkp[PPT], pk[PPT];
   int64_t prb[PPT];
   // 1 has, 2 first row, 4 first column (y-inflow), 8 last column (y-outflow),
-  // 16 ground flux, 32 ground inflow, 64 last row with a CTA below it
+  // 16 ground flux, 32 ground inflow
   unsigned prole[PPT];
 #pragma unroll
   for (int pp = 0; pp < PPT; ++pp) {
@@ -593,8 +595,7 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
     prb[pp] = ((int64_t)k * ny + j) * nx;
     prole[pp] = (has ? 1u : 0u) | (has && kl == 0 ? 2u : 0u) | (has && jp == 0 ? 4u : 0u) |
                 (has && jp == ny - 1 && periodic ? 8u : 0u) |
-                (has && !fz && k == 0 && slot >= 0 ? 16u : 0u) | (has && fz && kp == 0 ? 32u : 0u) |
-                (has && kl == rows - 1 && rank < C - 1 ? 64u : 0u);
+                (has && !fz && k == 0 && slot >= 0 ? 16u : 0u) | (has && fz && kp == 0 ? 32u : 0u);
   }
   auto prefetch = [&](int d) {
 #pragma unroll
@@ -651,6 +652,27 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
   T gpend[PPT];
 #pragma unroll
   for (int pp = 0; pp < PPT; ++pp) gpend[pp] = (T)0;
+  // The last row of hyperplane r (in the buffer at abuf) into the downstream
+  // CTA's ring slot r % CL_RING, once the downstream CTA is done with what the
+  // slot held: ny x MO values spread over all pencil threads, two or fewer
+  // each, right after the barrier that completed hyperplane r, so that no warp
+  // carries the hand-off alone.  The test switch withholds the first CTA's
+  // fill of hyperplane a.withhold, so the next CTA's bounded wait runs out.
+  auto push_row = [&](int r, uint32_t abuf) {
+    if (rank >= C - 1 || (int)threadIdx.x >= ny * MO || (rank == 0 && r == a.withhold)) return;
+    const int ps = r % CL_RING;
+    if (r >= CL_RING)
+      cl_wait(smem_u32(&empty[ps]), (uint32_t)((r / CL_RING - 1) & 1), failed, a.err);
+    if (failed) return;
+    const uint32_t src = abuf + (uint32_t)((rows - 1) * ny) * PS;
+    const uint32_t dst = a_dring + (uint32_t)(ps * ny) * PS;
+    const uint32_t bar = full_dn + 8u * ps;
+    for (int idx = threadIdx.x; idx < ny * MO; idx += TT) {
+      const int jq = idx / MO, m = idx - jq * MO;
+      const uint32_t off = (uint32_t)jq * PS + (uint32_t)m * TS;
+      cl_st_async(dst + off, sh_ld<T>(src + off), bar);
+    }
+  };
   for (int d = 0; d < nplanes; ++d) {
     prefetch(d + CL_AHEAD - 1);  // an empty group past the last plane
     cp_async_wait<CL_AHEAD - 1>();  // this plane's group has landed
@@ -672,11 +694,9 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
     }
     const int sl = d % CL_AHEAD;
     const int zslot = (d + CL_RING - 1) % CL_RING;
-    const int pslot = d % CL_RING;
-    // (test switch: a fill that never arrives, so the next CTA's bounded wait runs out)
-    const bool hold = rank == 0 && d == a.withhold;
     const uint32_t a_prev = (d & 1) ? a_buf0 : a_buf1;
     const uint32_t a_cur = (d & 1) ? a_buf1 : a_buf0;
+    if (d > 0) push_row(d - 1, a_prev);
     T gsv[PPT], qsv[PPT];
 #pragma unroll
     for (int pp = 0; pp < PPT; ++pp) {
@@ -684,12 +704,6 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
       const uint32_t qo = (uint32_t)pq[pp] * PS;
       const int ip = d - jp - kp;
       const bool act = (prole[pp] & 1u) && ip >= 0 && ip < nx;
-      const bool push = (prole[pp] & 64u) != 0;
-      // the downstream CTA has finished with what this slot held
-      if (push && d >= CL_RING)
-        cl_wait(smem_u32(&empty[pslot]), (uint32_t)((d / CL_RING - 1) & 1), failed, a.err);
-      const uint32_t apush = a_dring + (uint32_t)(pslot * ny + jp) * PS;
-      const uint32_t pbar = full_dn + 8u * pslot;
       T gs = (T)0, qs = (T)0;
       if (act) {
         const uint32_t ap = a_prev + qo;  // Ix at ap + m*TS
@@ -716,11 +730,11 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
         // The cell update of the group's ordinates, in batches of CB: every
         // shared-memory load of a batch is issued before its stores, so the
         // batch's updates overlap instead of waiting on one another's stores.
-        // Every per-ordinate offset is an immediate; a last-row pencil also
-        // stores its values into the downstream CTA's ring (one instance of
-        // the loop each way, so neither has a branch inside).
-        auto update = [&](auto push_tag) {
-          constexpr bool PUSH = decltype(push_tag)::value;
+        // Every per-ordinate offset is an immediate; only a pencil over the
+        // ground sums the ground flux (one instance of the loop per role, so
+        // neither has a branch inside).
+        auto update = [&](auto ground_tag) {
+          constexpr bool GROUND = decltype(ground_tag)::value;  // the ground-flux sum too
 #pragma unroll
           for (int m0 = 0; m0 < MO; m0 += CB) {
             T Ix[CB], Iy[CB], Iz[CB], v[CB];
@@ -743,17 +757,16 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
             for (int b = 0; b < CB; ++b) {
               const T2 wq = sh_ld2<T2>(a_cwq + (uint32_t)(m0 + b) * (2 * TS));
               gs = fmat(wq.x, v[b], gs);
-              qs = fmat(wq.y, v[b], qs);
+              if (GROUND) qs = fmat(wq.y, v[b], qs);
             }
 #pragma unroll
             for (int b = 0; b < CB; ++b) {
               const uint32_t mo = (uint32_t)(m0 + b) * TS;
               sh_st(ac + mo, v[b]);
-              if (PUSH) cl_st_async(apush + mo, v[b], pbar);
             }
           }
         };
-        if (push && !failed && !hold)
+        if (prole[pp] & 16u)
           update(std::true_type{});
         else
           update(std::false_type{});
@@ -770,11 +783,6 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
           const uint32_t ac = a_cur + qo;
 #pragma unroll
           for (int m = 0; m < MO; ++m) sh_st(ac + (uint32_t)m * TS, I_amb);
-        }
-        // an idle last-row pencil still delivers its share of the fill's bytes
-        if (push && !failed && !hold) {
-#pragma unroll
-          for (int m = 0; m < MO; ++m) cl_st_async(apush + (uint32_t)m * TS, I_amb, pbar);
         }
       }
       gsv[pp] = gs;
@@ -801,6 +809,8 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
       }
     }
   }
+  __syncthreads();  // the last hyperplane complete in this CTA
+  if (!helper) push_row(nplanes - 1, ((nplanes - 1) & 1) ? a_buf1 : a_buf0);
   cp_async_wait<0>();
   // the last hyperplane's fill (read by no one) has landed too: no store of
   // the upstream CTA is in flight to this CTA when it leaves
