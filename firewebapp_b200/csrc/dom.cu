@@ -838,7 +838,7 @@ __global__ void __launch_bounds__(PPT == 1 ? CL_MAX_THREADS_1 : CL_MAX_THREADS_2
 // independent updates per hyperplane, where the pencil-per-thread form moves
 // every intensity through shared memory and waits at a barrier over 24 warps
 // that each have ten.  Measured on the 400 x 120 x 60 S8 workload it is the
-// slower of the two (3.85 against 1.95 ms per FP64 sweep): with one warp per
+// slower of the two (3.85 ms per FP64 sweep, twice the other): with one warp per
 // scheduler a lane's updates do not overlap enough to cover the latency of
 // the reciprocal and its corrections, which the other form hides with six
 // warps per scheduler.  It is built for comparison and chosen only on request.

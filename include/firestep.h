@@ -443,7 +443,7 @@ int fs_dom_sweep_mode(void* handle);
  * built for ten ordinates per cluster, 4 to 8 rows per CTA and ny <= 128;
  * FS_EARG at the first solve for other shapes).  Both give the same results
  * bit for bit; the lane-column kernel is the slower one on the S8 workload
- * (3.85 against 1.95 ms per FP64 sweep at 400 x 120 x 60).  Only before the
+ * (3.85 ms per FP64 sweep at 400 x 120 x 60, about twice the other).  Only before the
  * first solve or intensity load.  fs_dom_sweep_kernel: the kernel in use (0
  * before the path is resolved or on path 3). */
 int fs_dom_set_sweep_kernel(void* handle, int kernel);
