@@ -177,3 +177,27 @@ def test_unprovided_physics_branches_raise():
     del case["turbulence_model"]  # the reference's default is laminar
     with pytest.raises(NotImplementedError, match="turbulence_model"):
         build_setup(case)
+
+
+def test_compare_forms_field_errors():
+    """The mixed-against-plain error measure: relative L2 per field, the
+    velocity components against the norm of the whole velocity vector (a
+    crosswind component can be orders of magnitude smaller than the others),
+    and the absolute norm for a field that is zero in the plain run."""
+    from firewebapp_b200.compare_forms import FIELDS, field_errors
+    rng = np.random.default_rng(4)
+    plain = {k: rng.random((3, 4, 5)) + 1.0 for k in FIELDS}
+    plain["v"] = 1e-6 * rng.standard_normal((3, 4, 5))
+    plain["q_rad"] = np.zeros((3, 4, 5))
+    mixed = {k: v.copy() for k, v in plain.items()}
+    assert all(e == 0.0 for e in field_errors(plain, mixed).values())
+    mixed["v"] = plain["v"] + 1e-7
+    mixed["T_g"] = plain["T_g"] * (1.0 + 1e-6)
+    mixed["q_rad"] = np.full((3, 4, 5), 2e-3)
+    err = field_errors(plain, mixed)
+    vnorm = np.sqrt(sum(np.linalg.norm(plain[k]) ** 2 for k in ("u", "v", "w")))
+    assert err["v"] == pytest.approx(np.linalg.norm(np.full(60, 1e-7)) / vnorm, rel=1e-12)
+    assert err["v"] < 1e-6 < np.linalg.norm(mixed["v"] - plain["v"]) / np.linalg.norm(plain["v"])
+    assert err["T_g"] == pytest.approx(1e-6, rel=1e-9)
+    assert err["q_rad"] == pytest.approx(np.sqrt(60) * 2e-3, rel=1e-12)
+    assert err["u"] == 0.0 and set(err) == set(FIELDS)
