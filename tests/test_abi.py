@@ -34,6 +34,26 @@ def test_library_exports_every_declared_symbol():
     assert not unbound, f"declared but not bound in _lib.SIGNATURES: {unbound}"
 
 
+@pytest.mark.parametrize("lang", ["c99", "c++17"])
+def test_header_compiles_for_c_and_cpp_hosts(tmp_path, lang):
+    """A non-Python host includes include/firestep.h directly: it must build as
+    strict C99 (no C++ types, no default arguments) and as C++17 without
+    warnings."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc" if lang == "c99" else "g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    src = tmp_path / ("host.c" if lang == "c99" else "host.cpp")
+    src.write_text('#include "firestep.h"\nint main(void) { return fs_version() == 0; }\n')
+    cmd = [cc, f"-std={lang}", "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+           f"-I{ROOT / 'include'}", str(src)]
+    if lang == "c99":
+        cmd.insert(2, "-pedantic")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_bindings_resolve():
     from firewebapp_b200 import _lib
     L = _lib.lib()
